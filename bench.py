@@ -1,0 +1,336 @@
+#!/usr/bin/env python
+"""Benchmark: adaptive Dormand-Prince steps of the 512x512x8 multilayer
+(exchange + interfacial DMI + uniaxial anisotropy + Zeeman + PBC demag) on
+B200, reported as cell-updates/s (cells x accepted steps / s).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Under torchrun (N > 1) every rank advances its own replica of the workload on
+its own GPU (independent solves: no collective on the data path); the timed
+region is bracketed by barriers and the reported time is the max over ranks.
+`--impl reference` times the CPU FP64 restatement of the reference algorithm
+(oracle/, all host cores) on bounded samples of the same workload; under
+torchrun only rank 0 runs it.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+sys.path.insert(0, os.path.join(ROOT, "oracle"))
+
+import numpy as np  # noqa: E402
+
+GAMMA_EVALS_REFERENCE_DP = 7  # the reference's Dormand-Prince evaluates the torque 7 times per step (no FSAL)
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=30)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", choices=["multilayer", "film", "precision"], default="multilayer")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--e2e-steps", type=int, default=8)
+    return ap.parse_args()
+
+
+def workload(name):
+    import mumaxplus_b200.workloads as W
+
+    return {"multilayer": W.multilayer, "film": W.film, "precision": W.precision}[name]()
+
+
+def measured_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def profile_traffic(wname):
+    """dram bytes per k_yz launch from the committed ncu summary, or None."""
+    path = os.path.join(ROOT, "profiles", f"k_yz_{wname}.md")
+    try:
+        for line in open(path):
+            if line.startswith("traffic_bytes_per_launch:"):
+                return float(line.split(":")[1])
+    except OSError:
+        pass
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled every 200 ms."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.tmp = None
+
+    def start(self):
+        try:
+            self.tmp = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=self.tmp, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.tmp.flush()
+        rows = []
+        with open(self.tmp.name) as f:
+            for line in f:
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) >= 9:
+                    rows.append(parts)
+        os.unlink(self.tmp.name)
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        smax = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4) if "Active" in r[5 + k] and "Not" not in r[5 + k]})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def cpu_baseline(w, n_evals=1):
+    """FP64 oracle on the host cores: one effective-field evaluation of the
+    full workload (a bounded sample), scaled to a reference Dormand-Prince step."""
+    import oracle as O
+    from mumaxplus_b200 import workloads as Wl
+
+    keep = []
+    ow = O.OracleWorld()
+    ow.set_world_bias(w.get("world_bias", (0, 0, 0)))
+    q = ow.add_magnet(Wl.desc(w, keep))
+    ow.set_m(q, w["m0"]())
+    t0 = time.time()
+    ow.eval(q, O.abi.Q_DEMAG_FIELD)  # builds the FP64 kernel spectrum (setup, untimed below)
+    t_setup = time.time() - t0
+    times = []
+    for _ in range(n_evals):
+        t0 = time.time()
+        ow.eval(q, O.abi.Q_EFFECTIVE_FIELD)
+        times.append(time.time() - t0)
+    t_eval = statistics.median(times)
+    N = Wl.ncells(w)
+    return {
+        "value": N / (GAMMA_EVALS_REFERENCE_DP * t_eval),
+        "unit": "cell-updates/s",
+        "cores": os.cpu_count(),
+        "kind": "port",
+        "sample": (f"{n_evals} FP64 effective-field evaluation(s) of the full {w['name']} grid "
+                   f"({t_eval:.2f} s each, kernel build {t_setup:.1f} s untimed), scaled by the "
+                   f"{GAMMA_EVALS_REFERENCE_DP} evaluations of one reference Dormand-Prince step"),
+    }
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    w = workload(args.workload)
+    from mumaxplus_b200 import workloads as Wl
+    import oracle as O
+
+    keep = []
+    ow = O.OracleWorld()
+    ow.set_world_bias(w.get("world_bias", (0, 0, 0)))
+    q = ow.add_magnet(Wl.desc(w, keep))
+    ow.set_m(q, w["m0"]())
+    ow.eval(q, O.abi.Q_DEMAG_FIELD)  # kernel build, untimed
+    for _ in range(args.warmup):
+        ow.eval(q, O.abi.Q_EFFECTIVE_FIELD)
+    t0 = time.time()
+    for _ in range(args.steps):
+        ow.eval(q, O.abi.Q_EFFECTIVE_FIELD)
+    t = (time.time() - t0) / args.steps
+    N = Wl.ncells(w)
+    value = N / (GAMMA_EVALS_REFERENCE_DP * t)
+    line = {
+        "impl": "reference", "metric": "cell-updates/s", "value": value, "unit": "cell-updates/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": GAMMA_EVALS_REFERENCE_DP * t * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": w["name"], "method": "DormandPrince", "parallelism": "host cores (OpenMP)"},
+        "cpu_baseline": {"value": value, "unit": "cell-updates/s", "cores": os.cpu_count(), "kind": "port",
+                         "sample": f"each step = one FP64 effective-field evaluation of the full grid, scaled by "
+                                   f"{GAMMA_EVALS_REFERENCE_DP} evaluations per reference Dormand-Prince step"},
+        "e2e": {"value": value, "unit": "cell-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args):
+    import torch
+
+    import mumaxplus_b200 as mpx
+    from mumaxplus_b200 import workloads as Wl
+
+    world_size = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world_size > 1:
+        import datetime
+
+        import torch.distributed as dist_mod
+
+        dist = dist_mod
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+
+    w = workload(args.workload)
+    N = Wl.ncells(w)
+    world, magnet = Wl.build(mpx, w, device=local)
+    stream = torch.cuda.Stream(device=dev)
+    world._engine.set_stream(stream.cuda_stream)
+    ts = world.timesolver
+    ts.set_method("DormandPrince")
+    eng = world._engine
+
+    # warm-up (also builds the CUDA graph of one attempt)
+    ts.steps(max(args.warmup, 1))
+    eng.synchronize()
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize(dev)
+
+    sampler = ClockSampler(local)
+    sampler.start()
+    time.sleep(0.3)
+    info0 = eng.group_info(world._group)
+    l0 = eng.launch_count()
+    barrier()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    ts.steps(args.steps)
+    e1.record(stream)
+    barrier()
+    ms = e0.elapsed_time(e1)
+    launches = eng.launch_count() - l0
+    info1 = eng.group_info(world._group)
+    clocks = sampler.stop()
+    ms_max = ms
+    if dist is not None:
+        t = torch.tensor([ms], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_max = float(t.item())
+    value = world_size * N * args.steps / (ms_max / 1e3)
+
+    # end to end through the public API: host m in (pinned), one step, host m out
+    host_in = torch.empty((3, *magnet.grid.shape), dtype=torch.float32).pin_memory().numpy()
+    host_in[...] = magnet.magnetization.get()
+    host_out = torch.empty_like(torch.from_numpy(host_in)).pin_memory().numpy()
+    k_e2e = max(1, min(args.e2e_steps, args.steps))
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(k_e2e):
+        eng.set_m(magnet._id, host_in)
+        ts.step()
+        host_out[...] = eng.get_m(magnet._id, host_in.shape)
+        host_in[...] = host_out
+    barrier()
+    e2e_s = time.perf_counter() - t0
+    e2e_value = world_size * N * k_e2e / e2e_s
+    if dist is not None:
+        t = torch.tensor([e2e_s], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_value = world_size * N * k_e2e / float(t.item())
+
+    # dominant kernel, timed live with CUDA events on the engine's stream
+    kms = eng.profile_eval(magnet._id, reps=10)
+    names = ["k_xfwd", "k_yz", "k_xinv", "k_local"]
+    dom = int(np.argmax(kms))
+    d = magnet._engine  # noqa: F841
+    nx, ny, nz = w["size"]
+    P = [1 if n == 1 else 1 << int(np.ceil(np.log2(2 * n - 1))) for n in (nx, ny, nz)]
+    Fh = P[0] // 2 + 1
+    spec_bytes = Fh * 3 * ny * nz * 8
+    kspec_bytes = Fh * (P[1] // 2 + 1) * (P[2] // 2 + 1) * (6 if P[2] > 1 else 4) * 4
+    alg_bytes = {
+        "k_xfwd": 12 * N + spec_bytes,              # read m, write the x spectrum
+        "k_yz": 2 * spec_bytes + kspec_bytes,       # read + write the spectrum, read the kernel spectrum
+        "k_xinv": spec_bytes + 12 * N + 12 * N,     # read spectrum and m, write the result
+        "k_local": 24 * N,
+    }[names[dom]]
+    peak, peak_kind = measured_peaks()
+    achieved = alg_bytes / (kms[dom] / 1e3) / 1e9
+    traffic = profile_traffic(w["name"]) if names[dom] == "k_yz" else None
+
+    cpu = None
+    if rank == 0 and world_size == 1 and not args.no_cpu_baseline:
+        try:
+            cpu = cpu_baseline(w)
+        except Exception as exc:  # the baseline is reported, never required
+            cpu = {"value": None, "unit": "cell-updates/s", "cores": os.cpu_count(), "kind": "port",
+                   "sample": f"failed: {exc}"}
+
+    if rank == 0:
+        steps = info1.steps - info0.steps
+        line = {
+            "metric": "cell-updates/s", "value": value, "unit": "cell-updates/s", "n_gpus": world_size,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic",
+            "config": {"workload": w["name"], "method": "DormandPrince (adaptive, max_error 1e-5)",
+                       "cells_per_gpu": N, "accepted_steps": int(steps),
+                       "rejected_attempts": int(info1.rejected - info0.rejected),
+                       "l2": "inputs larger than L2 (state + spectra + kernel ~ 340 MB per replica)",
+                       "parallelism": f"replicas x{world_size}" if world_size > 1 else "single GPU",
+                       "fft_padding": f"{P[0]}x{P[1]}x{P[2]}"},
+            "roofline": {"bound": "hbm", "kernel": names[dom], "achieved": achieved, "peak": peak,
+                         "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_kind,
+                         "traffic": traffic, "algorithmic_bytes_per_launch": alg_bytes,
+                         "kernel_ms": {n: round(t, 4) for n, t in zip(names, kms)}},
+            "cpu_baseline": cpu,
+            "e2e": {"value": e2e_value, "unit": "cell-updates/s", "h2d_bytes_per_step": 12 * N,
+                    "d2h_bytes_per_step": 12 * N, "steps": k_e2e},
+            "gpu_launches": int(launches),
+            "clocks": clocks,
+        }
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,255 @@
+/*
+ * mpx.h -- C ABI of the B200 effective-field + Runge-Kutta engine (libmpx.so).
+ *
+ * The engine holds ferromagnets on one GPU and evaluates their effective field
+ * (exchange, interfacial/general DMI, uniaxial anisotropy, Zeeman, FFT demag),
+ * the LLG torque, and advances them with the explicit adaptive Runge-Kutta
+ * methods of mumax+.  Everything crossing this boundary is plain C: integers,
+ * doubles, and pointers with sizes.  No call throws or exits; every entry point
+ * returns an mpx_status and mpx_last_error() gives the message of the last
+ * failing call on the calling thread.
+ *
+ * Field arrays are structure-of-arrays float32, component-major, x fastest:
+ * value(c, x, y, z) = a[c*N + x + nx*(y + ny*z)], N = nx*ny*nz.  This is the
+ * layout of the reference's Field (core/field.hpp:15-130, one device array per
+ * component) and of its numpy view (ncomp, nz, ny, nx) (bindings/fieldToArray.hpp:11-49).
+ *
+ * Reference interfaces each group of entry points replaces (paths relative to
+ * the mumax-plus source tree):
+ *   mpx_engine_*          World / MumaxWorld object (core/world.hpp:10-77,
+ *                         physics/mumaxworld.hpp:26-202)
+ *   mpx_magnet_*          MumaxWorld::addFerromagnet (physics/mumaxworld.cpp:57-80)
+ *                         and the Ferromagnet parameter bag (physics/ferromagnet.hpp:26-99)
+ *   mpx_eval / mpx_average / mpx_energy
+ *                         FieldQuantity::eval() and average()
+ *                         (core/fieldquantity.hpp:29-30, core/fieldquantity.cpp)
+ *                         as wrapped by FM_FieldQuantity (physics/quantityevaluator.hpp:18-64)
+ *   mpx_solver_*          TimeSolver (core/timesolver.hpp:14-89) and its Stepper::step()
+ *                         (core/stepper.hpp:5-13, core/rungekutta.cpp:25-84)
+ *   mpx_group_* / mpx_advance / mpx_poll
+ *                         no reference counterpart: many independent solves
+ *                         advanced together (batched and served forms).
+ */
+#ifndef MPX_H
+#define MPX_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define MPX_ABI_VERSION 1
+
+/* Status codes.  The reference raises C++ exceptions that pybind11 maps to
+ * Python errors (std::invalid_argument -> ValueError, std::out_of_range ->
+ * IndexError, std::runtime_error -> RuntimeError) and exits the process on CUDA
+ * errors (cudautil/cudaerror.hpp:6-18).  Here each becomes a return code. */
+typedef enum {
+  MPX_OK = 0,
+  MPX_ERR_INVALID = 1,     /* bad argument               (std::invalid_argument) */
+  MPX_ERR_RANGE = 2,       /* index / grid out of range  (std::out_of_range)     */
+  MPX_ERR_RUNTIME = 3,     /* invalid state              (std::runtime_error)    */
+  MPX_ERR_NOMEM = 4,       /* device memory exhausted or over the engine budget  */
+  MPX_ERR_CUDA = 5,        /* CUDA runtime error                                 */
+  MPX_ERR_UNSUPPORTED = 6, /* configuration outside what the kernels implement   */
+  MPX_ERR_TIMEOUT = 7,     /* bounded wait expired                               */
+  MPX_ERR_NODEVICE = 8     /* no CUDA device                                     */
+} mpx_status;
+
+/* Quantities for mpx_eval / mpx_average / mpx_energy.  Names follow the
+ * reference's Ferromagnet properties (mumaxplus/ferromagnet.py:678-901). */
+typedef enum {
+  MPX_Q_MAGNETIZATION = 0,
+  MPX_Q_EFFECTIVE_FIELD = 1,    /* physics/effectivefield.cpp:15-28 */
+  MPX_Q_EXCHANGE_FIELD = 2,     /* physics/exchange.cu:204-239      */
+  MPX_Q_DMI_FIELD = 3,          /* physics/dmi.cu:242-269           */
+  MPX_Q_ANISOTROPY_FIELD = 4,   /* physics/anisotropy.cu:109-140    */
+  MPX_Q_EXTERNAL_FIELD = 5,     /* physics/zeeman.cu:53-91          */
+  MPX_Q_DEMAG_FIELD = 6,        /* physics/demag.cpp:13-19          */
+  MPX_Q_TORQUE = 7,             /* physics/torque.cu:14-19          */
+  MPX_Q_LLG_TORQUE = 8,         /* physics/torque.cu:47-56          */
+  MPX_Q_DAMPING_TORQUE = 9,     /* physics/torque.cu:58-87          */
+  /* scalar (1-component) energy densities, J/m^3 (physics/energy.cu:18-50) */
+  MPX_Q_EXCHANGE_ENERGY_DENSITY = 10,
+  MPX_Q_DMI_ENERGY_DENSITY = 11,
+  MPX_Q_ANISOTROPY_ENERGY_DENSITY = 12,
+  MPX_Q_ZEEMAN_ENERGY_DENSITY = 13,
+  MPX_Q_DEMAG_ENERGY_DENSITY = 14,
+  MPX_Q_TOTAL_ENERGY_DENSITY = 15,
+  MPX_Q_COUNT = 16
+} mpx_quantity;
+
+/* Runge-Kutta methods (core/butchertableau.cpp). */
+typedef enum {
+  MPX_RK_HEUN = 0,
+  MPX_RK_BOGACKI_SHAMPINE = 1,
+  MPX_RK_CASH_KARP = 2,
+  MPX_RK_FEHLBERG = 3,       /* reference default (core/timesolver.cpp:17-19) */
+  MPX_RK_DORMAND_PRINCE = 4
+} mpx_rk_method;
+
+typedef struct mpx_engine mpx_engine;
+
+/* A material parameter: a uniform value, or per-cell values (host pointer,
+ * ncells floats; NULL means uniform).  core/parameter.hpp:16-110. */
+typedef struct {
+  double uniform;
+  const float* cells;
+} mpx_scalar;
+
+/* A vector parameter: uniform value or per-cell SoA values (3*ncells floats).
+ * core/parameter.hpp:115-240. */
+typedef struct {
+  double uniform[3];
+  const float* cells;
+} mpx_vector;
+
+/* Order of the DMI tensor components in mpx_magnet_desc.dmi
+ * (physics/dmitensor.hpp; interfacial DMI sets xxz = yyz = D). */
+enum {
+  MPX_DMI_XXY = 0, MPX_DMI_XXZ, MPX_DMI_XYZ,
+  MPX_DMI_YXY, MPX_DMI_YXZ, MPX_DMI_YYZ,
+  MPX_DMI_ZXY, MPX_DMI_ZXZ, MPX_DMI_ZYZ
+};
+
+/* One ferromagnet.  Geometry/regions/mastergrid/PBC follow core/system.hpp:10-119,
+ * core/grid.hpp:7-89 and core/world.hpp.  All pointers are host pointers, read
+ * during the call only. */
+typedef struct {
+  int size[3];                  /* nx, ny, nz                                   */
+  int origin[3];                /* grid origin in cells                         */
+  double cellsize[3];           /* m                                            */
+  int mastergrid_size[3];       /* periodic box; 0 = not periodic on that axis  */
+  int mastergrid_origin[3];
+  int pbc_repetitions[3];       /* image range of the demag kernel              */
+  const unsigned char* geometry;  /* ncells bytes (1 = in geometry) or NULL     */
+  const unsigned int* regions;    /* ncells region indices or NULL (all 0)      */
+  mpx_scalar msat;              /* A/m   (reference default 1)                  */
+  mpx_scalar aex;               /* J/m   (default 0)                            */
+  mpx_scalar alpha;             /* (default 0)                                  */
+  mpx_scalar ku1, ku2;          /* J/m^3 (default 0)                            */
+  mpx_scalar frozen_spins;      /* nonzero = frozen (default 0)                 */
+  mpx_vector anis_u;            /* uniaxial axis, normalised per cell           */
+  mpx_vector bias_magnetic_field; /* per-magnet bias, T                         */
+  mpx_scalar dmi[9];            /* J/m^2, order MPX_DMI_*                       */
+  int lut_regions;              /* region count covered by the two LUTs below   */
+  double inter_exchange;        /* uniform inter-region exchange (default 0)    */
+  const float* inter_exchange_lut;  /* lut_regions*(lut_regions-1)/2 or NULL    */
+  double scale_exchange;        /* uniform inter-region scale (default 1)       */
+  const float* scale_exchange_lut;
+  int enable_demag;             /* default 1                                    */
+  int enable_openbc;            /* default 0                                    */
+} mpx_magnet_desc;
+
+/* Time-solver settings (core/timesolver.hpp:74-82 defaults in brackets). */
+typedef struct {
+  int method;                       /* mpx_rk_method [FEHLBERG]        */
+  int adaptive;                     /* [1]                             */
+  double max_error;                 /* [1e-5]                          */
+  double headroom;                  /* [0.8]                           */
+  double lower_bound;               /* [0.5]                           */
+  double upper_bound;               /* [2.0]                           */
+  double sensible_factor;           /* [0.01]                          */
+  double sensible_timestep_default; /* [1e-14]                         */
+} mpx_solver_params;
+
+/* Per-group counters and state. */
+typedef struct {
+  double time, timestep;
+  int64_t steps, rejected, evaluations;
+  int status;            /* 0 idle, 1 running, 2 finished, 3 failed (NaN) */
+  double last_error;     /* last max-norm error estimate                  */
+  double max_torque;     /* max |torque| at the last check (rad/s), or -1 */
+} mpx_group_info;
+
+/* ---- library ---------------------------------------------------------- */
+const char* mpx_version(void);
+/* Message of the last failing call on this thread ("" if none). */
+const char* mpx_last_error(void);
+/* Number of CUDA devices visible (0 if none). */
+int mpx_device_count(void);
+
+/* ---- engine (one GPU, one stream) -------------------------------------- */
+mpx_status mpx_engine_create(int device, mpx_engine** out);
+mpx_status mpx_engine_destroy(mpx_engine* e);
+/* Launch subsequent work on this cudaStream_t (NULL = the engine's own stream). */
+mpx_status mpx_engine_set_stream(mpx_engine* e, void* stream);
+mpx_status mpx_engine_synchronize(mpx_engine* e);
+/* Uniform field over the whole world, T (physics/mumaxworld.hpp biasMagneticField). */
+mpx_status mpx_engine_set_world_bias(mpx_engine* e, const double b[3]);
+/* Device bytes currently held by the engine (buffers, spectra, kernels). */
+mpx_status mpx_engine_memory(mpx_engine* e, int64_t* bytes);
+/* Number of kernels this engine has launched since creation. */
+mpx_status mpx_engine_launch_count(mpx_engine* e, int64_t* count);
+
+/* ---- solve groups: magnets that share one time and time step ----------- */
+mpx_status mpx_group_create(mpx_engine* e, int* group);
+mpx_status mpx_group_destroy(mpx_engine* e, int group);   /* removes its magnets */
+mpx_status mpx_group_info_get(mpx_engine* e, int group, mpx_group_info* out);
+
+/* ---- magnets ------------------------------------------------------------ */
+/* Adds a ferromagnet to `group`; builds its FP64 Newell kernel spectrum when
+ * demag is enabled.  Initial magnetization is +x until set. */
+mpx_status mpx_magnet_add(mpx_engine* e, int group, const mpx_magnet_desc* d, int* magnet);
+/* Re-reads all parameters; rebuilds the demag kernel only when the cell size,
+ * geometry-independent grid data, mastergrid or PBC changed. */
+mpx_status mpx_magnet_update(mpx_engine* e, int magnet, const mpx_magnet_desc* d);
+mpx_status mpx_magnet_remove(mpx_engine* e, int magnet);
+/* Sets m (3*N floats) and normalises it per cell (core/variable.cpp:76-87). */
+mpx_status mpx_magnet_set_m(mpx_engine* e, int magnet, const float* m, int on_device);
+mpx_status mpx_magnet_get_m(mpx_engine* e, int magnet, float* m, int on_device);
+/* Evaluates a quantity into out (3*N floats, or N for energy densities).
+ * on_device: 0 = out is a host pointer, 1 = out is a device pointer,
+ * 2 = evaluate into the engine's scratch buffer only (out may be NULL). */
+mpx_status mpx_eval(mpx_engine* e, int magnet, int quantity, float* out, int on_device);
+/* Per-component mean over the cells in the geometry, FP64 accumulation
+ * (core/reduce.cu:101-151). */
+mpx_status mpx_average(mpx_engine* e, int magnet, int quantity, double out[3]);
+/* Max |v| over the geometry (core/reduce.cu:53-99), FP64 accumulation. */
+mpx_status mpx_max_norm(mpx_engine* e, int magnet, int quantity, double* out);
+/* Energy of a term = ncells * <energy density> * cell volume (physics/energy.cu:52-92). */
+mpx_status mpx_energy(mpx_engine* e, int magnet, int quantity, double* out);
+/* Measurement: times each kernel of one effective-field evaluation of `magnet`
+ * with CUDA events on the engine's stream, `reps` times after one warm-up, and
+ * writes the mean milliseconds per launch of [x-forward FFT, y/z FFT + kernel
+ * multiply, x-inverse FFT + epilogue, local-terms-only] (0 for kernels the
+ * magnet does not use).  No reference counterpart (FieldQuantity::_bench times
+ * the whole evaluation, mumaxplus/fieldquantity.py:111-118). */
+mpx_status mpx_profile_eval(mpx_engine* e, int magnet, int reps, double ms[4]);
+/* Real-space demag kernel, 6*K floats on the reference's kernel grid
+ * (physics/strayfieldkernel.cu:80-99; bindings/wrap_magnet.cpp:56-59).
+ * dims receives the kernel grid size (Kx, Ky, Kz). Pass out=NULL to query dims. */
+mpx_status mpx_demag_kernel(mpx_engine* e, int magnet, float* out, int dims[3]);
+
+/* ---- time solver of a group (core/timesolver.cpp) ----------------------- */
+mpx_status mpx_solver_set_params(mpx_engine* e, int group, const mpx_solver_params* p);
+mpx_status mpx_solver_get_params(mpx_engine* e, int group, mpx_solver_params* p);
+mpx_status mpx_solver_set_time(mpx_engine* e, int group, double t);
+mpx_status mpx_solver_get_time(mpx_engine* e, int group, double* t);
+mpx_status mpx_solver_set_timestep(mpx_engine* e, int group, double dt);
+mpx_status mpx_solver_get_timestep(mpx_engine* e, int group, double* dt);
+/* sensibleFactor / max|torque| (core/timesolver.cpp:37-47). */
+mpx_status mpx_solver_sensible_timestep(mpx_engine* e, int group, double* dt);
+/* TimeSolver::step / steps / run (core/timesolver.cpp:77-111).  Blocking. */
+mpx_status mpx_solver_step(mpx_engine* e, int group);
+mpx_status mpx_solver_steps(mpx_engine* e, int group, int nsteps);
+mpx_status mpx_solver_run(mpx_engine* e, int group, double duration);
+
+/* ---- many groups at once (batched / served forms) ----------------------- */
+/* Arms `group` to run for `duration` seconds, or until max|torque|/gamma_LL
+ * drops below torque_stop tesla (torque_stop <= 0 disables that test).  The
+ * group then advances with every mpx_advance call until it finishes. */
+mpx_status mpx_group_start(mpx_engine* e, int group, double duration, double torque_stop);
+/* Enqueues `attempts` Runge-Kutta attempts for every armed group (asynchronous,
+ * CUDA-graph replay; finished groups skip their work on the device). */
+mpx_status mpx_advance(mpx_engine* e, int attempts);
+/* Waits for enqueued work; writes up to `cap` ids of groups that finished
+ * since the last poll into done[] and their count into *n_done, and the number
+ * of groups still running into *n_running. */
+mpx_status mpx_poll(mpx_engine* e, int* done, int cap, int* n_done, int* n_running);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* MPX_H */

@@ -1,0 +1,1569 @@
+// engine.cu -- host engine and C ABI (include/mpx.h) of libmpx.so.
+//
+// An engine owns one CUDA stream on one device, the ferromagnets added to it
+// (their parameters, field buffers, demag spectra) and the solve groups that
+// step them.  All per-step decisions (accept/reject, new time step, run/steps
+// bookkeeping) are taken on the device by k_controller, so a run is a stream of
+// kernel launches with a status read every few attempts; no per-kernel host
+// synchronisation as in the reference (cudautil/cudalaunch.hpp:10-19).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "../../include/mpx.h"
+#include "kernels.cuh"
+#include "newell.cuh"
+
+using namespace mpx;
+
+namespace {
+
+thread_local std::string g_last_error;
+
+mpx_status fail(mpx_status st, const std::string& msg) {
+  g_last_error = msg;
+  return st;
+}
+
+#define CUDA_TRY(expr)                                                                    \
+  do {                                                                                    \
+    cudaError_t _e = (expr);                                                              \
+    if (_e != cudaSuccess) return fail(MPX_ERR_CUDA, std::string(#expr) + ": " + cudaGetErrorString(_e)); \
+  } while (0)
+
+#define MPX_TRY(expr)               \
+  do {                              \
+    mpx_status _s = (expr);         \
+    if (_s != MPX_OK) return _s;    \
+  } while (0)
+
+int ilog2(int v) {
+  int l = 0;
+  while ((1 << l) < v) ++l;
+  return l;
+}
+
+// padded FFT length: smallest power of two >= 2n-1 (1 when n == 1)
+int padded(int n) { return n == 1 ? 1 : 1 << ilog2(2 * n - 1); }
+
+constexpr int MAX_FFT = 4096;
+constexpr int SMEM_MAX = 227 * 1024;
+// dynamic shared memory left next to the static descriptor copies of a block
+constexpr int SMEM_DYN_MAX = SMEM_MAX - 2048;
+
+// ------------------------------------------------------------ tableaus
+// core/butchertableau.cpp: Heun, Bogacki-Shampine, Cash-Karp, Fehlberg, Dormand-Prince
+TableauDev make_tableau(int method) {
+  TableauDev t;
+  std::memset(&t, 0, sizeof(t));
+  switch (method) {
+    case MPX_RK_HEUN:
+      t.S = 2; t.order1 = 2; t.order2 = 1;
+      t.c[1] = 1; t.a[1][0] = 1;
+      t.b1[0] = 1. / 2.; t.b1[1] = 1. / 2.; t.b2[0] = 1.; t.b2[1] = 0.;
+      break;
+    case MPX_RK_BOGACKI_SHAMPINE:
+      t.S = 4; t.order1 = 3; t.order2 = 2;
+      t.c[1] = 1. / 2.; t.c[2] = 3. / 4.; t.c[3] = 1.;
+      t.a[1][0] = 1. / 2.; t.a[2][0] = 0.; t.a[2][1] = 3. / 4.;
+      t.a[3][0] = 2. / 9.; t.a[3][1] = 1. / 3.; t.a[3][2] = 4. / 9.;
+      t.b1[0] = 2. / 9.; t.b1[1] = 1. / 3.; t.b1[2] = 4. / 9.; t.b1[3] = 0.;
+      t.b2[0] = 7. / 24.; t.b2[1] = 1. / 4.; t.b2[2] = 1. / 3.; t.b2[3] = 1. / 8.;
+      break;
+    case MPX_RK_CASH_KARP:
+      t.S = 6; t.order1 = 5; t.order2 = 4;
+      t.c[1] = 1. / 5.; t.c[2] = 3. / 10.; t.c[3] = 3. / 5.; t.c[4] = 1.; t.c[5] = 7. / 8.;
+      t.a[1][0] = 1. / 5.;
+      t.a[2][0] = 3. / 40.; t.a[2][1] = 9. / 40.;
+      t.a[3][0] = 3. / 10.; t.a[3][1] = -9. / 10.; t.a[3][2] = 6. / 5.;
+      t.a[4][0] = -11. / 54.; t.a[4][1] = 5. / 2.; t.a[4][2] = -70. / 27.; t.a[4][3] = 35. / 27.;
+      t.a[5][0] = 1631. / 55296.; t.a[5][1] = 175. / 512.; t.a[5][2] = 575. / 13824.;
+      t.a[5][3] = 44275. / 110592.; t.a[5][4] = 253. / 4096.;
+      t.b1[0] = 37. / 378.; t.b1[2] = 250. / 621.; t.b1[3] = 125. / 594.; t.b1[5] = 512. / 1771.;
+      t.b2[0] = 2825. / 27648.; t.b2[2] = 18575. / 48384.; t.b2[3] = 13525. / 55296.;
+      t.b2[4] = 277. / 14336.; t.b2[5] = 1. / 4.;
+      break;
+    case MPX_RK_FEHLBERG:
+      t.S = 6; t.order1 = 5; t.order2 = 4;
+      t.c[1] = 1. / 4.; t.c[2] = 3. / 8.; t.c[3] = 12. / 13.; t.c[4] = 1.; t.c[5] = 1. / 2.;
+      t.a[1][0] = 1. / 4.;
+      t.a[2][0] = 3. / 32.; t.a[2][1] = 9. / 32.;
+      t.a[3][0] = 1932. / 2197.; t.a[3][1] = -7200. / 2197.; t.a[3][2] = 7296. / 2197.;
+      t.a[4][0] = 439. / 216.; t.a[4][1] = -8.; t.a[4][2] = 3680. / 513.; t.a[4][3] = -845. / 4104.;
+      t.a[5][0] = -8. / 27.; t.a[5][1] = 2.; t.a[5][2] = -3544. / 2565.; t.a[5][3] = 1859. / 4104.;
+      t.a[5][4] = -11. / 40.;
+      t.b1[0] = 16. / 135.; t.b1[2] = 6656. / 12825.; t.b1[3] = 28561. / 56430.; t.b1[4] = -9. / 50.;
+      t.b1[5] = 2. / 55.;
+      t.b2[0] = 25. / 216.; t.b2[2] = 1408. / 2565.; t.b2[3] = 2197. / 4104.; t.b2[4] = -1. / 5.;
+      break;
+    default:  // MPX_RK_DORMAND_PRINCE
+      t.S = 7; t.order1 = 5; t.order2 = 4;
+      t.c[1] = 1. / 5.; t.c[2] = 3. / 10.; t.c[3] = 4. / 5.; t.c[4] = 8. / 9.; t.c[5] = 1.; t.c[6] = 1.;
+      t.a[1][0] = 1. / 5.;
+      t.a[2][0] = 3. / 40.; t.a[2][1] = 9. / 40.;
+      t.a[3][0] = 44. / 45.; t.a[3][1] = -56. / 15.; t.a[3][2] = 32. / 9.;
+      t.a[4][0] = 19372. / 6561.; t.a[4][1] = -25360. / 2187.; t.a[4][2] = 64448. / 6561.;
+      t.a[4][3] = -212. / 729.;
+      t.a[5][0] = 9017. / 3168.; t.a[5][1] = -355. / 33.; t.a[5][2] = 46732. / 5247.;
+      t.a[5][3] = 49. / 176.; t.a[5][4] = -5103. / 18656.;
+      t.a[6][0] = 35. / 384.; t.a[6][2] = 500. / 1113.; t.a[6][3] = 125. / 192.;
+      t.a[6][4] = -2187. / 6784.; t.a[6][5] = 11. / 84.;
+      t.b1[0] = 35. / 384.; t.b1[2] = 500. / 1113.; t.b1[3] = 125. / 192.; t.b1[4] = -2187. / 6784.;
+      t.b1[5] = 11. / 84.;
+      t.b2[0] = 5179. / 57600.; t.b2[2] = 7571. / 16695.; t.b2[3] = 393. / 640.;
+      t.b2[4] = -92097. / 339200.; t.b2[5] = 187. / 2100.; t.b2[6] = 1. / 40.;
+      t.fsal = 1;  // last row of a equals b1: x_new is the last stage state, k_new0 = k_last
+      break;
+  }
+  return t;
+}
+
+// ---------------------------------------------------------------- objects
+struct Magnet {
+  int slot = -1, group = -1;
+  MagnetDev dev;
+  std::vector<void*> allocs;  // per-magnet device allocations (params, masks, buffers...)
+  int64_t bytes = 0;
+  bool demag = false;
+  int ty = 4;
+  int P[3] = {1, 1, 1};
+  // kernel-defining geometry (rebuild the spectrum when it changes)
+  int kkey_n[3], kkey_mg[3], kkey_pbc[3];
+  double kkey_cs[3];
+  bool kspec_ready = false;
+  float* kspec = nullptr;
+  float2* spec = nullptr;
+  float* fields = nullptr;   // 9 buffers of 3N floats
+  int64_t fields_bytes = 0, spec_bytes = 0, kspec_bytes = 0;
+  unsigned char* geom = nullptr;
+  int ngeo = 0;
+  std::vector<Work> tiles;   // row tiles (mag, z, y0, ty)
+  std::vector<Work> kxw;     // (mag, kx)
+  Work* d_tiles = nullptr;   // eval tables of this magnet only
+  Work* d_kxw = nullptr;
+};
+
+struct Group {
+  int slot = -1;
+  mpx_solver_params sp{MPX_RK_FEHLBERG, 1, 1e-5, 0.8, 0.5, 2.0, 0.01, 1e-14};
+  std::vector<int> magnets;
+};
+
+}  // namespace
+
+struct mpx_engine {
+  int device = 0;
+  cudaStream_t own = nullptr, stream = nullptr;
+  std::vector<std::unique_ptr<Magnet>> mags;
+  std::vector<std::unique_ptr<Group>> groups;
+  MagnetDev* d_mags = nullptr;
+  int d_mags_cap = 0;
+  GroupDev* d_groups = nullptr;
+  int d_groups_cap = 0;
+  float2* d_tw = nullptr;
+  double* d_red = nullptr;   // reduction partials
+  double* d_redout = nullptr;
+  float* d_scratch = nullptr;
+  size_t scratch_bytes = 0;
+  // run tables over all magnets
+  bool tables_dirty = true;
+  Work *d_t_demag = nullptr, *d_t_local = nullptr;
+  int n_t_demag = 0, n_t_local = 0;
+  // k_yz work per z-length class (Pz = 1, 2, 4, 8, 16 -> class log2 Pz)
+  Work* d_kx_demag[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
+  int n_kx_demag[5] = {0, 0, 0, 0, 0};
+  int smem_yz[5] = {0, 0, 0, 0, 0};
+  int smem_x = 0, nt_x = 256;
+  bool any_nodemag = false;
+  int64_t bytes = 0;
+  int64_t launches = 0;
+  double wb[3] = {0, 0, 0};
+  int tab_method = -1;
+  // CUDA graph of one attempt
+  cudaGraphExec_t graph = nullptr;
+  int graph_method = -1;
+  bool graph_dirty = true;
+};
+
+namespace {
+
+struct DeviceGuard {
+  int prev = -1;
+  explicit DeviceGuard(int dev) {
+    cudaGetDevice(&prev);
+    if (prev != dev) cudaSetDevice(dev);
+  }
+  ~DeviceGuard() {
+    int cur = -1;
+    cudaGetDevice(&cur);
+    if (prev >= 0 && cur != prev) cudaSetDevice(prev);
+  }
+};
+
+mpx_status dalloc(mpx_engine* e, Magnet* m, void** p, size_t bytes) {
+  *p = nullptr;
+  if (bytes == 0) return MPX_OK;
+  cudaError_t st = cudaMalloc(p, bytes);
+  if (st != cudaSuccess) {
+    cudaGetLastError();
+    return fail(MPX_ERR_NOMEM, "device allocation of " + std::to_string(bytes) + " bytes failed: " +
+                                   cudaGetErrorString(st));
+  }
+  if (m) {
+    m->allocs.push_back(*p);
+    m->bytes += (int64_t)bytes;
+  }
+  e->bytes += (int64_t)bytes;
+  return MPX_OK;
+}
+
+void free_magnet(mpx_engine* e, Magnet* m) {
+  for (void* p : m->allocs) cudaFree(p);
+  e->bytes -= m->bytes;
+  m->allocs.clear();
+  m->bytes = 0;
+}
+
+// Frees every device allocation of a magnet.
+void release_all(mpx_engine* e, Magnet* m) {
+  free_magnet(e, m);
+  if (m->fields) cudaFree(m->fields);
+  if (m->spec) cudaFree(m->spec);
+  if (m->kspec) cudaFree(m->kspec);
+  e->bytes -= m->fields_bytes + m->spec_bytes + m->kspec_bytes;
+  m->fields = nullptr;
+  m->spec = nullptr;
+  m->kspec = nullptr;
+  m->fields_bytes = m->spec_bytes = m->kspec_bytes = 0;
+  if (m->d_tiles) cudaFree(m->d_tiles);
+  if (m->d_kxw) cudaFree(m->d_kxw);
+  m->d_tiles = nullptr;
+  m->d_kxw = nullptr;
+}
+
+Magnet* get_mag(mpx_engine* e, int id) {
+  if (!e || id < 0 || id >= (int)e->mags.size()) return nullptr;
+  return e->mags[id].get();
+}
+Group* get_group(mpx_engine* e, int id) {
+  if (!e || id < 0 || id >= (int)e->groups.size()) return nullptr;
+  return e->groups[id].get();
+}
+
+mpx_status read_group(mpx_engine* e, int g, GroupDev* out) {
+  CUDA_TRY(cudaMemcpyAsync(out, e->d_groups + g, sizeof(GroupDev), cudaMemcpyDeviceToHost, e->stream));
+  CUDA_TRY(cudaStreamSynchronize(e->stream));
+  return MPX_OK;
+}
+mpx_status write_group(mpx_engine* e, int g, const GroupDev* in) {
+  CUDA_TRY(cudaMemcpyAsync(e->d_groups + g, in, sizeof(GroupDev), cudaMemcpyHostToDevice, e->stream));
+  CUDA_TRY(cudaStreamSynchronize(e->stream));
+  return MPX_OK;
+}
+
+mpx_status upload_magnet_desc(mpx_engine* e, Magnet* m) {
+  if (m->slot >= e->d_mags_cap) {
+    int cap = std::max(16, e->d_mags_cap * 2);
+    while (cap <= m->slot) cap *= 2;
+    MagnetDev* nd = nullptr;
+    CUDA_TRY(cudaMalloc(&nd, sizeof(MagnetDev) * cap));
+    if (e->d_mags) {
+      CUDA_TRY(cudaMemcpyAsync(nd, e->d_mags, sizeof(MagnetDev) * e->d_mags_cap, cudaMemcpyDeviceToDevice, e->stream));
+      CUDA_TRY(cudaStreamSynchronize(e->stream));
+      cudaFree(e->d_mags);
+    }
+    e->d_mags = nd;
+    e->d_mags_cap = cap;
+    e->graph_dirty = true;
+  }
+  CUDA_TRY(cudaMemcpyAsync(e->d_mags + m->slot, &m->dev, sizeof(MagnetDev), cudaMemcpyHostToDevice, e->stream));
+  CUDA_TRY(cudaStreamSynchronize(e->stream));
+  return MPX_OK;
+}
+
+mpx_status ensure_group_capacity(mpx_engine* e, int slot) {
+  if (slot < e->d_groups_cap) return MPX_OK;
+  int cap = std::max(16, e->d_groups_cap * 2);
+  while (cap <= slot) cap *= 2;
+  GroupDev* nd = nullptr;
+  CUDA_TRY(cudaMalloc(&nd, sizeof(GroupDev) * cap));
+  CUDA_TRY(cudaMemsetAsync(nd, 0, sizeof(GroupDev) * cap, e->stream));
+  if (e->d_groups)
+    CUDA_TRY(cudaMemcpyAsync(nd, e->d_groups, sizeof(GroupDev) * e->d_groups_cap, cudaMemcpyDeviceToDevice, e->stream));
+  CUDA_TRY(cudaStreamSynchronize(e->stream));
+  if (e->d_groups) cudaFree(e->d_groups);
+  e->d_groups = nd;
+  e->d_groups_cap = cap;
+  e->graph_dirty = true;
+  return MPX_OK;
+}
+
+mpx_status ensure_scratch(mpx_engine* e, size_t bytes) {
+  if (bytes <= e->scratch_bytes) return MPX_OK;
+  if (e->d_scratch) cudaFree(e->d_scratch);
+  e->d_scratch = nullptr;
+  e->scratch_bytes = 0;
+  CUDA_TRY(cudaMalloc(&e->d_scratch, bytes));
+  e->scratch_bytes = bytes;
+  return MPX_OK;
+}
+
+template <typename T>
+mpx_status upload_vec(mpx_engine* e, Work** d, const std::vector<T>& v) {
+  if (*d) cudaFree(*d);
+  *d = nullptr;
+  if (v.empty()) return MPX_OK;
+  CUDA_TRY(cudaMalloc(d, sizeof(T) * v.size()));
+  CUDA_TRY(cudaMemcpyAsync(*d, v.data(), sizeof(T) * v.size(), cudaMemcpyHostToDevice, e->stream));
+  CUDA_TRY(cudaStreamSynchronize(e->stream));
+  return MPX_OK;
+}
+
+// dynamic shared memory: padded rows / columns plus the twiddle table of the length
+int x_smem(const Magnet* m) {
+  return ((m->ty + (m->ty + 1) / 2) * plen(m->P[0]) + m->P[0]) * (int)sizeof(float2);
+}
+int yz_smem(const Magnet* m) { return (3 * m->dev.n[2] * plen(m->P[1]) + m->P[1]) * (int)sizeof(float2); }
+int yz_class(const Magnet* m) { return ilog2(m->P[2]); }
+constexpr int YZ_THREADS = 384;
+
+// k_yz<PZ> launch for one z-length class
+mpx_status launch_yz(mpx_engine* e, int cls, const Work* work, int n, int smem, int stage, int gate) {
+  if (n <= 0) return MPX_OK;
+  switch (cls) {
+    case 0: k_yz<1><<<n, YZ_THREADS, smem, e->stream>>>(e->d_mags, e->d_groups, work, stage, gate, e->d_tw); break;
+    case 1: k_yz<2><<<n, YZ_THREADS, smem, e->stream>>>(e->d_mags, e->d_groups, work, stage, gate, e->d_tw); break;
+    case 2: k_yz<4><<<n, YZ_THREADS, smem, e->stream>>>(e->d_mags, e->d_groups, work, stage, gate, e->d_tw); break;
+    case 3: k_yz<8><<<n, YZ_THREADS, smem, e->stream>>>(e->d_mags, e->d_groups, work, stage, gate, e->d_tw); break;
+    default: k_yz<16><<<n, YZ_THREADS, smem, e->stream>>>(e->d_mags, e->d_groups, work, stage, gate, e->d_tw); break;
+  }
+  e->launches++;
+  return MPX_OK;
+}
+int x_threads(const Magnet* m) {
+  int rows = m->ty + (m->ty + 1) / 2;
+  int t = (rows * m->P[0] + 7) / 8;  // 8 values per thread in the x FFTs
+  t = ((t + 31) / 32) * 32;
+  return std::min(512, std::max(256, t));
+}
+
+mpx_status rebuild_tables(mpx_engine* e) {
+  std::vector<Work> td, tl, kd[5];
+  e->smem_x = 0;
+  e->nt_x = 256;
+  for (int c = 0; c < 5; ++c) e->smem_yz[c] = 0;
+  for (auto& mp : e->mags) {
+    if (!mp) continue;
+    Magnet* m = mp.get();
+    if (m->demag) {
+      const int cls = yz_class(m);
+      td.insert(td.end(), m->tiles.begin(), m->tiles.end());
+      kd[cls].insert(kd[cls].end(), m->kxw.begin(), m->kxw.end());
+      e->smem_x = std::max(e->smem_x, x_smem(m));
+      e->smem_yz[cls] = std::max(e->smem_yz[cls], yz_smem(m));
+      e->nt_x = std::max(e->nt_x, x_threads(m));
+    } else {
+      tl.insert(tl.end(), m->tiles.begin(), m->tiles.end());
+    }
+  }
+  MPX_TRY(upload_vec(e, &e->d_t_demag, td));
+  MPX_TRY(upload_vec(e, &e->d_t_local, tl));
+  for (int c = 0; c < 5; ++c) {
+    MPX_TRY(upload_vec(e, &e->d_kx_demag[c], kd[c]));
+    e->n_kx_demag[c] = (int)kd[c].size();
+  }
+  e->n_t_demag = (int)td.size();
+  e->n_t_local = (int)tl.size();
+  e->tables_dirty = false;
+  e->graph_dirty = true;
+  return MPX_OK;
+}
+
+// ------------------------------------------------ demag kernel construction
+mpx_status build_kernel_spectrum(mpx_engine* e, Magnet* m) {
+  MagnetDev& d = m->dev;
+  KernelGeom g;
+  for (int a = 0; a < 3; ++a) {
+    g.n[a] = d.n[a];
+    g.mg[a] = m->kkey_mg[a];
+    g.pbc[a] = m->kkey_pbc[a];
+    g.cs[a] = m->kkey_cs[a];
+  }
+  const long long noct = (long long)d.n[0] * d.n[1] * d.n[2];
+  const long long PP = (long long)m->P[0] * m->P[1] * m->P[2];
+  double* oct = nullptr;
+  double2 *f0 = nullptr, *f1 = nullptr;
+  CUDA_TRY(cudaMalloc(&oct, sizeof(double) * 6 * noct));
+  cudaError_t st = cudaMalloc(&f0, sizeof(double2) * PP);
+  if (st == cudaSuccess) st = cudaMalloc(&f1, sizeof(double2) * PP);
+  if (st != cudaSuccess) {
+    cudaGetLastError();
+    cudaFree(oct);
+    if (f0) cudaFree(f0);
+    return fail(MPX_ERR_NOMEM, "demag kernel construction: out of device memory");
+  }
+  const int grid = 148 * 8;
+  k_newell_octant<<<grid, 128, 0, e->stream>>>(oct, g);
+  e->launches++;
+  const int kcomp = d.kcomp;
+  const int comps6[6] = {0, 1, 2, 3, 4, 5};
+  const double pref = -MU0_D / (double)PP;
+  for (int kc = 0; kc < kcomp; ++kc) {
+    const int c = comps6[kc];
+    k_kernel_expand<<<grid, 256, 0, e->stream>>>(f0, oct, c, g, m->P[0], m->P[1], m->P[2]);
+    e->launches++;
+    double2 *in = f0, *out = f1;
+    for (int axis = 0; axis < 3; ++axis) {
+      for (int Ns = 1; Ns < m->P[axis]; Ns <<= 1) {
+        k_fft64_pass<<<grid, 256, 0, e->stream>>>(in, out, m->P[0], m->P[1], m->P[2], axis, Ns);
+        e->launches++;
+        std::swap(in, out);
+      }
+    }
+    k_kernel_extract<<<grid, 256, 0, e->stream>>>(m->kspec, in, kc, kcomp, m->P[0], m->P[1], m->P[2], pref);
+    e->launches++;
+  }
+  st = cudaGetLastError();
+  cudaError_t st2 = cudaStreamSynchronize(e->stream);
+  cudaFree(oct);
+  cudaFree(f0);
+  cudaFree(f1);
+  if (st != cudaSuccess) return fail(MPX_ERR_CUDA, std::string("kernel build launch: ") + cudaGetErrorString(st));
+  if (st2 != cudaSuccess) return fail(MPX_ERR_CUDA, std::string("kernel build: ") + cudaGetErrorString(st2));
+  m->kspec_ready = true;
+  return MPX_OK;
+}
+
+// ------------------------------------------------------- parameter upload
+mpx_status load_scalar(mpx_engine* e, Magnet* m, DScalar* out, const mpx_scalar& s, int N) {
+  out->u = (float)s.uniform;
+  out->p = nullptr;
+  if (s.cells) {
+    void* p;
+    MPX_TRY(dalloc(e, m, &p, sizeof(float) * (size_t)N));
+    CUDA_TRY(cudaMemcpyAsync(p, s.cells, sizeof(float) * (size_t)N, cudaMemcpyHostToDevice, e->stream));
+    out->p = (const float*)p;
+  }
+  return MPX_OK;
+}
+mpx_status load_vector(mpx_engine* e, Magnet* m, DVector* out, const mpx_vector& s, int N) {
+  for (int c = 0; c < 3; ++c) out->u[c] = (float)s.uniform[c];
+  out->p = nullptr;
+  if (s.cells) {
+    void* p;
+    MPX_TRY(dalloc(e, m, &p, sizeof(float) * 3 * (size_t)N));
+    CUDA_TRY(cudaMemcpyAsync(p, s.cells, sizeof(float) * 3 * (size_t)N, cudaMemcpyHostToDevice, e->stream));
+    out->p = (const float*)p;
+  }
+  return MPX_OK;
+}
+
+bool scalar_zero(const mpx_scalar& s) { return !s.cells && s.uniform == 0.0; }
+bool vector_zero(const mpx_vector& s) {
+  return !s.cells && s.uniform[0] == 0.0 && s.uniform[1] == 0.0 && s.uniform[2] == 0.0;
+}
+
+mpx_status validate_desc(const mpx_magnet_desc* d) {
+  if (!d) return fail(MPX_ERR_INVALID, "null magnet description");
+  for (int a = 0; a < 3; ++a) {
+    if (d->size[a] <= 0) return fail(MPX_ERR_INVALID, "grid size must be positive");
+    if (d->cellsize[a] <= 0) return fail(MPX_ERR_INVALID, "The cell size should be larger than 0");
+    if (d->pbc_repetitions[a] < 0) return fail(MPX_ERR_INVALID, "Number of pbcRepetitions should not be negative.");
+    if ((d->mastergrid_size[a] == 0) != (d->pbc_repetitions[a] == 0))
+      return fail(MPX_ERR_INVALID, "0 in size of mastergrid should match 0 in pbcRepetitions.");
+    if (d->mastergrid_size[a] > 0) {  // core/world.cpp inMastergrid
+      const int d1 = d->origin[a] - d->mastergrid_origin[a];
+      const int d2 = d1 + d->size[a] - d->mastergrid_size[a];
+      if (d1 < 0 || d2 > 0)
+        return fail(MPX_ERR_RANGE, "Can not add magnet because the grid does not fit in the mastergrid ");
+    }
+  }
+  const long long N = (long long)d->size[0] * d->size[1] * d->size[2];
+  if (N >= (1LL << 31) / 3) return fail(MPX_ERR_UNSUPPORTED, "grid too large for 32-bit cell indices");
+  return MPX_OK;
+}
+
+// Fill the parameter part of the device description from d (allocating per-cell arrays).
+mpx_status load_params(mpx_engine* e, Magnet* m, const mpx_magnet_desc* d) {
+  MagnetDev& D = m->dev;
+  const int N = D.N;
+  MPX_TRY(load_scalar(e, m, &D.msat, d->msat, N));
+  MPX_TRY(load_scalar(e, m, &D.aex, d->aex, N));
+  MPX_TRY(load_scalar(e, m, &D.alpha, d->alpha, N));
+  MPX_TRY(load_scalar(e, m, &D.ku1, d->ku1, N));
+  MPX_TRY(load_scalar(e, m, &D.ku2, d->ku2, N));
+  MPX_TRY(load_scalar(e, m, &D.frozen, d->frozen_spins, N));
+  MPX_TRY(load_vector(e, m, &D.anisU, d->anis_u, N));
+  MPX_TRY(load_vector(e, m, &D.bias, d->bias_magnetic_field, N));
+  for (int c = 0; c < 9; ++c) MPX_TRY(load_scalar(e, m, &D.dmi[c], d->dmi[c], N));
+  D.inter_u = (float)d->inter_exchange;
+  D.scale_u = (float)d->scale_exchange;
+  D.inter_lut = nullptr;
+  D.scale_lut = nullptr;
+  const int L = d->lut_regions * (d->lut_regions - 1) / 2;
+  if (d->inter_exchange_lut && L > 0) {
+    void* p;
+    MPX_TRY(dalloc(e, m, &p, sizeof(float) * L));
+    CUDA_TRY(cudaMemcpyAsync(p, d->inter_exchange_lut, sizeof(float) * L, cudaMemcpyHostToDevice, e->stream));
+    D.inter_lut = (const float*)p;
+  }
+  if (d->scale_exchange_lut && L > 0) {
+    void* p;
+    MPX_TRY(dalloc(e, m, &p, sizeof(float) * L));
+    CUDA_TRY(cudaMemcpyAsync(p, d->scale_exchange_lut, sizeof(float) * L, cudaMemcpyHostToDevice, e->stream));
+    D.scale_lut = (const float*)p;
+  }
+  D.geom = nullptr;
+  m->ngeo = N;
+  if (d->geometry) {
+    void* p;
+    MPX_TRY(dalloc(e, m, &p, (size_t)N));
+    CUDA_TRY(cudaMemcpyAsync(p, d->geometry, (size_t)N, cudaMemcpyHostToDevice, e->stream));
+    D.geom = (const unsigned char*)p;
+    m->geom = (unsigned char*)p;
+    int ng = 0;
+    for (int i = 0; i < N; ++i) ng += d->geometry[i] ? 1 : 0;
+    m->ngeo = ng;
+  } else {
+    m->geom = nullptr;
+  }
+  D.reg = nullptr;
+  if (d->regions) {
+    void* p;
+    MPX_TRY(dalloc(e, m, &p, sizeof(unsigned) * (size_t)N));
+    CUDA_TRY(cudaMemcpyAsync(p, d->regions, sizeof(unsigned) * (size_t)N, cudaMemcpyHostToDevice, e->stream));
+    D.reg = (const unsigned*)p;
+  }
+  // terms that are assured zero are skipped (physics/*AssuredZero)
+  const bool msat0 = scalar_zero(d->msat);
+  unsigned terms = 0;
+  const bool inter0 = !d->inter_exchange_lut && d->inter_exchange == 0.0;
+  const bool scale0 = !d->scale_exchange_lut && d->scale_exchange == 0.0;
+  if (!((scalar_zero(d->aex) && inter0) || scale0 || msat0)) terms |= TERM_EXCH;
+  bool dmi0 = true;
+  for (int c = 0; c < 9; ++c) dmi0 = dmi0 && scalar_zero(d->dmi[c]);
+  if (!(dmi0 || msat0)) terms |= TERM_DMI;
+  if (!((scalar_zero(d->ku1) && scalar_zero(d->ku2)) || vector_zero(d->anis_u) || msat0)) terms |= TERM_ANIS;
+  const bool wb0 = e->wb[0] == 0 && e->wb[1] == 0 && e->wb[2] == 0;
+  if (!(wb0 && vector_zero(d->bias_magnetic_field))) terms |= TERM_EXT;
+  if (!vector_zero(d->bias_magnetic_field)) terms |= FLAG_MAGNET_BIAS;
+  if (d->enable_demag && !msat0) terms |= TERM_DEMAG;
+  if (d->enable_openbc) terms |= FLAG_OPENBC;
+  D.terms = terms;
+  for (int c = 0; c < 3; ++c) D.wb[c] = (float)e->wb[c];
+  return MPX_OK;
+}
+
+mpx_status setup_magnet(mpx_engine* e, Magnet* m, const mpx_magnet_desc* d, bool keep_fields) {
+  // keep the state buffers and the spectrum when only parameters change
+  MagnetDev& D = m->dev;
+  float* old_fields = m->fields;
+  float2* old_spec = m->spec;
+  float* old_kspec = m->kspec;
+  const bool same_grid = keep_fields && D.n[0] == d->size[0] && D.n[1] == d->size[1] && D.n[2] == d->size[2];
+  bool kernel_same = same_grid && m->kspec_ready;
+  for (int a = 0; a < 3; ++a) {
+    kernel_same = kernel_same && m->kkey_mg[a] == d->mastergrid_size[a] && m->kkey_pbc[a] == d->pbc_repetitions[a] &&
+                  m->kkey_cs[a] == d->cellsize[a];
+  }
+  // release parameter allocations (everything except fields/spec/kspec which are tracked separately)
+  for (void* p : m->allocs) cudaFree(p);
+  e->bytes -= m->bytes;
+  m->allocs.clear();
+  m->bytes = 0;
+  if (!same_grid) {
+    if (old_fields) cudaFree(old_fields);
+    if (old_spec) cudaFree(old_spec);
+    if (old_kspec) cudaFree(old_kspec);
+    e->bytes -= m->fields_bytes + m->spec_bytes + m->kspec_bytes;
+    m->fields_bytes = m->spec_bytes = m->kspec_bytes = 0;
+    m->fields = nullptr;
+    m->spec = nullptr;
+    m->kspec = nullptr;
+    m->kspec_ready = false;
+    old_fields = nullptr;
+    old_spec = nullptr;
+    old_kspec = nullptr;
+    kernel_same = false;
+  }
+  for (int a = 0; a < 3; ++a) {
+    D.n[a] = d->size[a];
+    D.o[a] = d->origin[a];
+    D.mg[a] = d->mastergrid_size[a];
+    D.mgo[a] = d->mastergrid_origin[a];
+    D.cs[a] = (float)d->cellsize[a];
+    const float c = (float)d->cellsize[a];
+    D.w[a] = 1.0f / (c * c);
+  }
+  D.N = D.n[0] * D.n[1] * D.n[2];
+  D.group = m->group;
+  MPX_TRY(load_params(e, m, d));
+  const int N = D.N;
+  // demag plan
+  m->demag = (D.terms & TERM_DEMAG) != 0;
+  for (int a = 0; a < 3; ++a) {
+    m->P[a] = padded(D.n[a]);
+    D.P[a] = m->P[a];
+    D.logP[a] = ilog2(m->P[a]);
+  }
+  D.Fh = m->P[0] / 2 + 1;
+  D.kcomp = (m->P[2] == 1) ? 4 : 6;
+  m->ty = std::min(4, D.n[1]);
+  if (m->demag) {
+    if (m->P[0] > MAX_FFT || m->P[1] > MAX_FFT)
+      return fail(MPX_ERR_UNSUPPORTED, "demag: padded FFT length above 4096 (grid side > 2048)");
+    if (m->P[2] > 16) return fail(MPX_ERR_UNSUPPORTED, "demag: nz > 8 is not implemented by the fused y/z pass");
+    if (yz_smem(m) > SMEM_DYN_MAX)
+      return fail(MPX_ERR_UNSUPPORTED, "demag: 3*nz*Py complex values exceed shared memory (nz*Py > 9472)");
+    if (x_smem(m) > SMEM_DYN_MAX) return fail(MPX_ERR_UNSUPPORTED, "demag: x-pass tile exceeds shared memory");
+  }
+  // field buffers (9 x 3N floats) and spectrum
+  size_t fbytes = sizeof(float) * 9 * 3 * (size_t)N;
+  if (!old_fields) {
+    MPX_TRY(dalloc(e, nullptr, (void**)&old_fields, fbytes));
+    CUDA_TRY(cudaMemsetAsync(old_fields, 0, fbytes, e->stream));
+    m->fields_bytes = (int64_t)fbytes;
+  }
+  m->fields = old_fields;
+  for (int b = 0; b < 9; ++b) D.buf[b] = old_fields + (size_t)b * 3 * N;
+  const size_t sbytes = sizeof(float2) * (size_t)D.Fh * 3 * D.n[1] * D.n[2];  // S[kx][c][z][y]
+  if (m->demag && !old_spec) {
+    MPX_TRY(dalloc(e, nullptr, (void**)&old_spec, sbytes));
+    m->spec_bytes = (int64_t)sbytes;
+  }
+  m->spec = old_spec;
+  D.spec = old_spec;
+  const size_t kbytes = sizeof(float) * (size_t)D.Fh * (m->P[1] / 2 + 1) * (m->P[2] / 2 + 1) * D.kcomp;
+  if (m->demag && !old_kspec) {
+    MPX_TRY(dalloc(e, nullptr, (void**)&old_kspec, kbytes));
+    m->kspec_bytes = (int64_t)kbytes;
+    kernel_same = false;
+  }
+  m->kspec = old_kspec;
+  D.kspec = old_kspec;
+  if (m->demag && !kernel_same) {
+    for (int a = 0; a < 3; ++a) {
+      m->kkey_n[a] = D.n[a];
+      m->kkey_mg[a] = d->mastergrid_size[a];
+      m->kkey_pbc[a] = d->pbc_repetitions[a];
+      m->kkey_cs[a] = d->cellsize[a];
+    }
+    m->kspec_ready = false;
+    MPX_TRY(build_kernel_spectrum(e, m));
+  }
+  // tiles
+  m->tiles.clear();
+  m->kxw.clear();
+  for (int z = 0; z < D.n[2]; ++z)
+    for (int y0 = 0; y0 < D.n[1]; y0 += m->ty) m->tiles.push_back(Work{m->slot, z, y0, std::min(m->ty, D.n[1] - y0)});
+  if (m->demag)
+    for (int kx = 0; kx < D.Fh; ++kx) m->kxw.push_back(Work{m->slot, kx, 0, 0});
+  {
+    cudaFree(m->d_tiles);
+    cudaFree(m->d_kxw);
+    m->d_tiles = nullptr;
+    m->d_kxw = nullptr;
+    MPX_TRY(upload_vec(e, &m->d_tiles, m->tiles));
+    MPX_TRY(upload_vec(e, &m->d_kxw, m->kxw));
+  }
+  MPX_TRY(upload_magnet_desc(e, m));
+  e->tables_dirty = true;
+  return MPX_OK;
+}
+
+// The tableau lives in one __constant__ symbol per device, shared by all
+// engines on that device; it is re-uploaded on the engine's stream before
+// every run so that engines with different methods never see a stale one.
+mpx_status upload_tableau(mpx_engine* e, int method) {
+  TableauDev t = make_tableau(method);
+  CUDA_TRY(cudaMemcpyToSymbolAsync(c_tab, &t, sizeof(t), 0, cudaMemcpyHostToDevice, e->stream));
+  e->tab_method = method;
+  return MPX_OK;
+}
+
+mpx_status check_launch(mpx_engine* e, const char* what) {
+  cudaError_t st = cudaGetLastError();
+  if (st != cudaSuccess) return fail(MPX_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(st));
+  (void)e;
+  return MPX_OK;
+}
+
+// --------------------------------------------------- field evaluation
+// Evaluate quantity q of magnet m into the device buffer out.
+mpx_status eval_into(mpx_engine* e, Magnet* m, int q, float* out) {
+  if (e->tables_dirty) MPX_TRY(rebuild_tables(e));
+  const int N = m->dev.N;
+  if (q == MPX_Q_MAGNETIZATION) {
+    GroupDev G;
+    MPX_TRY(read_group(e, m->group, &G));
+    CUDA_TRY(cudaMemcpyAsync(out, m->dev.buf[G.map[0]], sizeof(float) * 3 * (size_t)N, cudaMemcpyDeviceToDevice,
+                             e->stream));
+    return MPX_OK;
+  }
+  EpiArgs ea;
+  ea.mode = EPI_EVAL;
+  ea.stage = 0;
+  ea.quantity = q;
+  ea.fsal_err = 0;
+  ea.gate = 0;
+  ea.out = out;
+  ea.msrc = nullptr;
+  const bool needs_demag = (q == MPX_Q_EFFECTIVE_FIELD || q == MPX_Q_DEMAG_FIELD || q == MPX_Q_TORQUE ||
+                            q == MPX_Q_LLG_TORQUE || q == MPX_Q_DAMPING_TORQUE || q == MPX_Q_DEMAG_ENERGY_DENSITY ||
+                            q == MPX_Q_TOTAL_ENERGY_DENSITY);
+  const int ntile = (int)m->tiles.size();
+  if (m->demag && needs_demag) {
+    const int sx = x_smem(m), syz = yz_smem(m), nt = x_threads(m);
+    k_xfwd<false><<<ntile, nt, sx, e->stream>>>(e->d_mags, e->d_groups, m->d_tiles, 0, 0, nullptr, e->d_tw);
+    MPX_TRY(launch_yz(e, yz_class(m), m->d_kxw, (int)m->kxw.size(), syz, 0, 0));
+    k_xinv<<<ntile, nt, sx, e->stream>>>(e->d_mags, e->d_groups, m->d_tiles, ea, e->d_tw);
+    e->launches += 2;
+  } else {
+    k_local<<<ntile, 256, 0, e->stream>>>(e->d_mags, e->d_groups, m->d_tiles, ea);
+    e->launches += 1;
+  }
+  return check_launch(e, "eval");
+}
+
+// One Runge-Kutta attempt for every running group (core/rungekutta.cpp:39-83).
+mpx_status launch_attempt(mpx_engine* e, const TableauDev& T) {
+  const int S = T.S;
+  for (int s = 0; s < S; ++s) {
+    EpiArgs ea;
+    ea.mode = EPI_STAGE;
+    ea.stage = s;
+    ea.quantity = 0;
+    ea.fsal_err = (T.fsal && s == S - 1) ? 1 : 0;
+    ea.gate = 1;
+    ea.out = nullptr;
+    ea.msrc = nullptr;
+    if (e->n_t_demag > 0) {
+      if (s == 0)
+        k_xfwd<false><<<e->n_t_demag, e->nt_x, e->smem_x, e->stream>>>(e->d_mags, e->d_groups, e->d_t_demag, 0, 1,
+                                                                       nullptr, e->d_tw);
+      else
+        k_xfwd<true><<<e->n_t_demag, e->nt_x, e->smem_x, e->stream>>>(e->d_mags, e->d_groups, e->d_t_demag, s, 1,
+                                                                      nullptr, e->d_tw);
+      for (int c = 0; c < 5; ++c) MPX_TRY(launch_yz(e, c, e->d_kx_demag[c], e->n_kx_demag[c], e->smem_yz[c], s, 1));
+      k_xinv<<<e->n_t_demag, e->nt_x, e->smem_x, e->stream>>>(e->d_mags, e->d_groups, e->d_t_demag, ea, e->d_tw);
+      e->launches += 2;
+    }
+    if (e->n_t_local > 0) {
+      if (s > 0) {
+        k_combine<<<e->n_t_local, 256, 0, e->stream>>>(e->d_mags, e->d_groups, e->d_t_local, s, 0);
+        e->launches++;
+      }
+      k_local<<<e->n_t_local, 256, 0, e->stream>>>(e->d_mags, e->d_groups, e->d_t_local, ea);
+      e->launches++;
+    }
+  }
+  if (!T.fsal) {
+    if (e->n_t_demag > 0) {
+      k_combine<<<e->n_t_demag, 256, 0, e->stream>>>(e->d_mags, e->d_groups, e->d_t_demag, S, 1);
+      e->launches++;
+    }
+    if (e->n_t_local > 0) {
+      k_combine<<<e->n_t_local, 256, 0, e->stream>>>(e->d_mags, e->d_groups, e->d_t_local, S, 1);
+      e->launches++;
+    }
+  }
+  const int ng = (int)e->groups.size();
+  k_controller<<<(ng + 127) / 128, 128, 0, e->stream>>>(e->d_groups, ng);
+  e->launches++;
+  return check_launch(e, "attempt");
+}
+
+mpx_status prepare_run(mpx_engine* e, int method) {
+  if (e->tables_dirty) MPX_TRY(rebuild_tables(e));
+  MPX_TRY(upload_tableau(e, method));
+  return MPX_OK;
+}
+
+// Replays `n` attempts (through a CUDA graph of one attempt).
+mpx_status run_attempts(mpx_engine* e, int method, int n) {
+  MPX_TRY(prepare_run(e, method));
+  const TableauDev T = make_tableau(method);
+  if (e->graph_dirty || e->graph_method != method || !e->graph) {
+    if (e->graph) {
+      cudaGraphExecDestroy(e->graph);
+      e->graph = nullptr;
+    }
+    cudaGraph_t g = nullptr;
+    CUDA_TRY(cudaStreamBeginCapture(e->stream, cudaStreamCaptureModeThreadLocal));
+    const int64_t before = e->launches;
+    mpx_status st = launch_attempt(e, T);
+    cudaError_t ce = cudaStreamEndCapture(e->stream, &g);
+    e->launches = before;
+    if (st != MPX_OK) {
+      if (g) cudaGraphDestroy(g);
+      return st;
+    }
+    if (ce != cudaSuccess) return fail(MPX_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(ce));
+    ce = cudaGraphInstantiate(&e->graph, g, 0);
+    cudaGraphDestroy(g);
+    if (ce != cudaSuccess) return fail(MPX_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(ce));
+    e->graph_method = method;
+    e->graph_dirty = false;
+  }
+  // launches per attempt (for the launch counter)
+  int per = 1;
+  {
+    const int S = T.S;
+    int nyz = 0;
+    for (int c = 0; c < 5; ++c) nyz += e->n_kx_demag[c] > 0 ? 1 : 0;
+    if (e->n_t_demag > 0) per += (2 + nyz) * S + (T.fsal ? 0 : 1);
+    if (e->n_t_local > 0) per += S + (S - 1) + (T.fsal ? 0 : 1);
+  }
+  for (int i = 0; i < n; ++i) {
+    CUDA_TRY(cudaGraphLaunch(e->graph, e->stream));
+    e->launches += per;
+  }
+  return MPX_OK;
+}
+
+mpx_status sensible_timestep(mpx_engine* e, Group* g, double* out) {
+  // core/timesolver.cpp:37-47: sensibleFactor / max|torque| over the group's magnets
+  if (g->magnets.empty()) {
+    *out = 0.0;
+    return MPX_OK;
+  }
+  double gmax = 0;
+  for (int id : g->magnets) {
+    Magnet* m = get_mag(e, id);
+    const int N = m->dev.N;
+    MPX_TRY(ensure_scratch(e, sizeof(float) * 3 * (size_t)N));
+    MPX_TRY(eval_into(e, m, MPX_Q_TORQUE, e->d_scratch));
+    const int nb = 256;
+    k_reduce_partial<<<nb, 256, 0, e->stream>>>(e->d_scratch, N, 3, m->geom, 1, e->d_red);
+    k_reduce_final<<<1, 32, 0, e->stream>>>(e->d_red, nb, 1, e->d_redout);
+    e->launches += 2;
+    double r[3];
+    CUDA_TRY(cudaMemcpyAsync(r, e->d_redout, sizeof(r), cudaMemcpyDeviceToHost, e->stream));
+    CUDA_TRY(cudaStreamSynchronize(e->stream));
+    gmax = std::max(gmax, r[0]);
+  }
+  *out = (gmax == 0) ? g->sp.sensible_timestep_default : g->sp.sensible_factor / gmax;
+  return MPX_OK;
+}
+
+void fill_group_params(GroupDev& G, const mpx_solver_params& sp) {
+  G.max_error = sp.max_error;
+  G.headroom = sp.headroom;
+  G.lower = sp.lower_bound;
+  G.upper = sp.upper_bound;
+  G.adaptive = sp.adaptive;
+}
+
+// Blocks until the group leaves the running state.
+mpx_status drive_group(mpx_engine* e, Group* g) {
+  int chunk = 1;
+  for (;;) {
+    MPX_TRY(run_attempts(e, g->sp.method, chunk));
+    GroupDev G;
+    MPX_TRY(read_group(e, g->slot, &G));
+    if (G.status == GS_FAILED) {
+      G.status = GS_IDLE;
+      G.finished_flag = 0;
+      MPX_TRY(write_group(e, g->slot, &G));
+      return fail(MPX_ERR_RUNTIME, "time integration failed: the error estimate is NaN");
+    }
+    if (G.status != GS_RUNNING) {
+      G.status = GS_IDLE;
+      G.finished_flag = 0;
+      MPX_TRY(write_group(e, g->slot, &G));
+      return MPX_OK;
+    }
+    chunk = std::min(chunk * 2, 16);
+  }
+}
+
+// Random unit vectors for a new magnet (the reference seeds its generator with
+// the clock, ferromagnet.cpp:62-76; here the seed is the magnet slot).
+void initial_random(std::vector<float>& m, int N, int seed) {
+  uint64_t s = 0x9E3779B97F4A7C15ull * (uint64_t)(seed + 1) + 12345;
+  auto next = [&]() {
+    s ^= s << 13;
+    s ^= s >> 7;
+    s ^= s << 17;
+    return (double)(s >> 11) * (1.0 / 9007199254740992.0);
+  };
+  m.resize(3 * (size_t)N);
+  for (size_t i = 0; i < m.size(); ++i) {  // Box-Muller
+    double u1 = next(), u2 = next();
+    if (u1 < 1e-300) u1 = 1e-300;
+    m[i] = (float)(std::sqrt(-2.0 * std::log(u1)) * std::cos(2 * M_PI * u2));
+  }
+}
+
+mpx_status set_m_device(mpx_engine* e, Magnet* m, const float* src_dev) {
+  GroupDev G;
+  MPX_TRY(read_group(e, m->group, &G));
+  const int N = m->dev.N;
+  k_normalize_into<<<(N + 255) / 256, 256, 0, e->stream>>>(m->dev.buf[G.map[0]], src_dev, N, m->geom);
+  e->launches++;
+  MPX_TRY(check_launch(e, "set m"));
+  G.k0_valid = 0;
+  MPX_TRY(write_group(e, m->group, &G));
+  return MPX_OK;
+}
+
+}  // namespace
+
+// =================================================================== C ABI
+extern "C" {
+
+const char* mpx_version(void) { return "mpx 0.1 (sm_100a)"; }
+const char* mpx_last_error(void) { return g_last_error.c_str(); }
+
+int mpx_device_count(void) {
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
+  return n;
+}
+
+mpx_status mpx_engine_create(int device, mpx_engine** out) {
+  if (!out) return fail(MPX_ERR_INVALID, "null output pointer");
+  *out = nullptr;
+  int n = mpx_device_count();
+  if (n <= 0) return fail(MPX_ERR_NODEVICE, "no CUDA device available");
+  if (device < 0 || device >= n) return fail(MPX_ERR_RANGE, "device index out of range");
+  DeviceGuard guard(device);
+  auto e = std::make_unique<mpx_engine>();
+  e->device = device;
+  CUDA_TRY(cudaStreamCreateWithFlags(&e->own, cudaStreamNonBlocking));
+  e->stream = e->own;
+  // twiddle table exp(-2 pi i k / 4096), computed in FP64
+  std::vector<float2> tw(TW_N);
+  for (int k = 0; k < TW_N; ++k) {
+    const double a = -2.0 * M_PI * k / TW_N;
+    tw[k] = make_float2((float)std::cos(a), (float)std::sin(a));
+  }
+  CUDA_TRY(cudaMalloc(&e->d_tw, sizeof(float2) * TW_N));
+  CUDA_TRY(cudaMemcpy(e->d_tw, tw.data(), sizeof(float2) * TW_N, cudaMemcpyHostToDevice));
+  CUDA_TRY(cudaMalloc(&e->d_red, sizeof(double) * 3 * 1024));
+  CUDA_TRY(cudaMalloc(&e->d_redout, sizeof(double) * 3));
+  // large dynamic shared memory and the max-shared carveout for the FFT kernels
+  const void* fft_kernels[] = {(const void*)k_xfwd<false>, (const void*)k_xfwd<true>, (const void*)k_xinv,
+                               (const void*)k_yz<1>, (const void*)k_yz<2>, (const void*)k_yz<4>,
+                               (const void*)k_yz<8>, (const void*)k_yz<16>};
+  for (const void* k : fft_kernels) {
+    cudaFuncAttributes fa;
+    CUDA_TRY(cudaFuncGetAttributes(&fa, k));
+    CUDA_TRY(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  SMEM_MAX - (int)fa.sharedSizeBytes));
+    CUDA_TRY(cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared));
+  }
+  *out = e.release();
+  return MPX_OK;
+}
+
+mpx_status mpx_engine_destroy(mpx_engine* e) {
+  if (!e) return MPX_OK;
+  DeviceGuard guard(e->device);
+  cudaStreamSynchronize(e->stream);
+  if (e->graph) cudaGraphExecDestroy(e->graph);
+  for (auto& m : e->mags)
+    if (m) release_all(e, m.get());
+  cudaFree(e->d_mags);
+  cudaFree(e->d_groups);
+  cudaFree(e->d_tw);
+  cudaFree(e->d_red);
+  cudaFree(e->d_redout);
+  cudaFree(e->d_scratch);
+  cudaFree(e->d_t_demag);
+  for (int c = 0; c < 5; ++c) cudaFree(e->d_kx_demag[c]);
+  cudaFree(e->d_t_local);
+  if (e->own) cudaStreamDestroy(e->own);
+  delete e;
+  return MPX_OK;
+}
+
+mpx_status mpx_engine_set_stream(mpx_engine* e, void* stream) {
+  if (!e) return fail(MPX_ERR_INVALID, "null engine");
+  e->stream = stream ? (cudaStream_t)stream : e->own;
+  return MPX_OK;
+}
+
+mpx_status mpx_engine_synchronize(mpx_engine* e) {
+  if (!e) return fail(MPX_ERR_INVALID, "null engine");
+  DeviceGuard guard(e->device);
+  CUDA_TRY(cudaStreamSynchronize(e->stream));
+  return MPX_OK;
+}
+
+mpx_status mpx_engine_set_world_bias(mpx_engine* e, const double b[3]) {
+  if (!e || !b) return fail(MPX_ERR_INVALID, "null argument");
+  DeviceGuard guard(e->device);
+  for (int c = 0; c < 3; ++c) e->wb[c] = b[c];
+  const bool wb0 = b[0] == 0 && b[1] == 0 && b[2] == 0;
+  for (auto& mp : e->mags) {
+    if (!mp) continue;
+    Magnet* m = mp.get();
+    for (int c = 0; c < 3; ++c) m->dev.wb[c] = (float)b[c];
+    const bool mb = (m->dev.terms & FLAG_MAGNET_BIAS) != 0;
+    if (wb0 && !mb) m->dev.terms &= ~TERM_EXT;
+    else m->dev.terms |= TERM_EXT;
+    MPX_TRY(upload_magnet_desc(e, m));
+  }
+  for (auto& g : e->groups)
+    if (g) {
+      GroupDev G;
+      MPX_TRY(read_group(e, g->slot, &G));
+      G.k0_valid = 0;
+      MPX_TRY(write_group(e, g->slot, &G));
+    }
+  return MPX_OK;
+}
+
+mpx_status mpx_engine_memory(mpx_engine* e, int64_t* bytes) {
+  if (!e || !bytes) return fail(MPX_ERR_INVALID, "null argument");
+  *bytes = e->bytes;
+  return MPX_OK;
+}
+
+mpx_status mpx_engine_launch_count(mpx_engine* e, int64_t* count) {
+  if (!e || !count) return fail(MPX_ERR_INVALID, "null argument");
+  *count = e->launches;
+  return MPX_OK;
+}
+
+mpx_status mpx_group_create(mpx_engine* e, int* group) {
+  if (!e || !group) return fail(MPX_ERR_INVALID, "null argument");
+  DeviceGuard guard(e->device);
+  int slot = -1;
+  for (int i = 0; i < (int)e->groups.size(); ++i)
+    if (!e->groups[i]) { slot = i; break; }
+  if (slot < 0) {
+    slot = (int)e->groups.size();
+    e->groups.emplace_back();
+  }
+  MPX_TRY(ensure_group_capacity(e, slot));
+  auto g = std::make_unique<Group>();
+  g->slot = slot;
+  GroupDev G;
+  std::memset(&G, 0, sizeof(G));
+  fill_group_params(G, g->sp);
+  for (int b = 0; b < 9; ++b) G.map[b] = b;
+  G.status = GS_IDLE;
+  MPX_TRY(write_group(e, slot, &G));
+  e->groups[slot] = std::move(g);
+  e->graph_dirty = true;  // controller grid covers all group slots
+  *group = slot;
+  return MPX_OK;
+}
+
+mpx_status mpx_group_destroy(mpx_engine* e, int group) {
+  Group* g = get_group(e, group);
+  if (!g) return fail(MPX_ERR_RANGE, "no such group");
+  DeviceGuard guard(e->device);
+  std::vector<int> ms = g->magnets;
+  for (int id : ms) MPX_TRY(mpx_magnet_remove(e, id));
+  GroupDev G;
+  std::memset(&G, 0, sizeof(G));
+  G.status = GS_IDLE;
+  MPX_TRY(write_group(e, group, &G));
+  e->groups[group].reset();
+  return MPX_OK;
+}
+
+mpx_status mpx_group_info_get(mpx_engine* e, int group, mpx_group_info* out) {
+  Group* g = get_group(e, group);
+  if (!g || !out) return fail(MPX_ERR_RANGE, "no such group");
+  DeviceGuard guard(e->device);
+  GroupDev G;
+  MPX_TRY(read_group(e, group, &G));
+  out->time = G.t;
+  out->timestep = G.dt;
+  out->steps = G.steps;
+  out->rejected = G.rejected;
+  out->evaluations = G.attempts;
+  out->status = G.status;
+  out->last_error = 0;
+  out->max_torque = -1;
+  return MPX_OK;
+}
+
+mpx_status mpx_magnet_add(mpx_engine* e, int group, const mpx_magnet_desc* d, int* magnet) {
+  if (!e || !magnet) return fail(MPX_ERR_INVALID, "null argument");
+  Group* g = get_group(e, group);
+  if (!g) return fail(MPX_ERR_RANGE, "no such group");
+  MPX_TRY(validate_desc(d));
+  DeviceGuard guard(e->device);
+  int slot = -1;
+  for (int i = 0; i < (int)e->mags.size(); ++i)
+    if (!e->mags[i]) { slot = i; break; }
+  if (slot < 0) {
+    slot = (int)e->mags.size();
+    e->mags.emplace_back();
+  }
+  auto m = std::make_unique<Magnet>();
+  std::memset(&m->dev, 0, sizeof(MagnetDev));
+  m->slot = slot;
+  m->group = group;
+  mpx_status st = setup_magnet(e, m.get(), d, false);
+  if (st != MPX_OK) {
+    std::string msg = g_last_error;
+    release_all(e, m.get());
+    e->mags[slot].reset();
+    g_last_error = msg;
+    return st;
+  }
+  // initial magnetisation: normalised random vectors
+  std::vector<float> m0;
+  initial_random(m0, m->dev.N, slot);
+  const size_t bytes = sizeof(float) * m0.size();
+  MPX_TRY(ensure_scratch(e, bytes));
+  CUDA_TRY(cudaMemcpyAsync(e->d_scratch, m0.data(), bytes, cudaMemcpyHostToDevice, e->stream));
+  Magnet* mp = m.get();
+  e->mags[slot] = std::move(m);
+  g->magnets.push_back(slot);
+  e->tables_dirty = true;
+  MPX_TRY(set_m_device(e, mp, e->d_scratch));
+  // core/timesolver.cpp:49-52: new equations -> sensible time step (adaptive solvers)
+  if (g->sp.adaptive) {
+    double dt;
+    MPX_TRY(sensible_timestep(e, g, &dt));
+    GroupDev G;
+    MPX_TRY(read_group(e, group, &G));
+    G.dt = dt;
+    MPX_TRY(write_group(e, group, &G));
+  }
+  *magnet = slot;
+  return MPX_OK;
+}
+
+mpx_status mpx_magnet_update(mpx_engine* e, int magnet, const mpx_magnet_desc* d) {
+  Magnet* m = get_mag(e, magnet);
+  if (!m) return fail(MPX_ERR_RANGE, "no such magnet");
+  MPX_TRY(validate_desc(d));
+  DeviceGuard guard(e->device);
+  MPX_TRY(setup_magnet(e, m, d, true));
+  GroupDev G;
+  MPX_TRY(read_group(e, m->group, &G));
+  G.k0_valid = 0;
+  MPX_TRY(write_group(e, m->group, &G));
+  return MPX_OK;
+}
+
+mpx_status mpx_magnet_remove(mpx_engine* e, int magnet) {
+  Magnet* m = get_mag(e, magnet);
+  if (!m) return fail(MPX_ERR_RANGE, "no such magnet");
+  DeviceGuard guard(e->device);
+  cudaStreamSynchronize(e->stream);
+  Group* g = get_group(e, m->group);
+  if (g) g->magnets.erase(std::remove(g->magnets.begin(), g->magnets.end(), magnet), g->magnets.end());
+  release_all(e, m);
+  e->mags[magnet].reset();
+  e->tables_dirty = true;
+  return MPX_OK;
+}
+
+mpx_status mpx_magnet_set_m(mpx_engine* e, int magnet, const float* src, int on_device) {
+  Magnet* m = get_mag(e, magnet);
+  if (!m || !src) return fail(MPX_ERR_INVALID, "no such magnet / null data");
+  DeviceGuard guard(e->device);
+  const size_t bytes = sizeof(float) * 3 * (size_t)m->dev.N;
+  const float* dsrc = src;
+  if (!on_device) {
+    MPX_TRY(ensure_scratch(e, bytes));
+    CUDA_TRY(cudaMemcpyAsync(e->d_scratch, src, bytes, cudaMemcpyHostToDevice, e->stream));
+    dsrc = e->d_scratch;
+  }
+  return set_m_device(e, m, dsrc);
+}
+
+mpx_status mpx_magnet_get_m(mpx_engine* e, int magnet, float* out, int on_device) {
+  Magnet* m = get_mag(e, magnet);
+  if (!m || !out) return fail(MPX_ERR_INVALID, "no such magnet / null data");
+  DeviceGuard guard(e->device);
+  GroupDev G;
+  MPX_TRY(read_group(e, m->group, &G));
+  const size_t bytes = sizeof(float) * 3 * (size_t)m->dev.N;
+  CUDA_TRY(cudaMemcpyAsync(out, m->dev.buf[G.map[0]], bytes,
+                           on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, e->stream));
+  CUDA_TRY(cudaStreamSynchronize(e->stream));
+  return MPX_OK;
+}
+
+mpx_status mpx_eval(mpx_engine* e, int magnet, int quantity, float* out, int on_device) {
+  Magnet* m = get_mag(e, magnet);
+  if (!m || (!out && on_device != 2)) return fail(MPX_ERR_INVALID, "no such magnet / null output");
+  if (quantity < 0 || quantity >= MPX_Q_COUNT) return fail(MPX_ERR_INVALID, "unknown quantity");
+  DeviceGuard guard(e->device);
+  const int nc = quantity >= MPX_Q_EXCHANGE_ENERGY_DENSITY ? 1 : 3;
+  const size_t bytes = sizeof(float) * nc * (size_t)m->dev.N;
+  float* dst = out;
+  if (on_device == 2) {
+    MPX_TRY(ensure_scratch(e, sizeof(float) * 3 * (size_t)m->dev.N));
+    MPX_TRY(eval_into(e, m, quantity, e->d_scratch));
+    CUDA_TRY(cudaStreamSynchronize(e->stream));
+    return MPX_OK;
+  }
+  if (!on_device) {
+    MPX_TRY(ensure_scratch(e, sizeof(float) * 3 * (size_t)m->dev.N));
+    dst = e->d_scratch;
+  }
+  MPX_TRY(eval_into(e, m, quantity, dst));
+  if (!on_device) CUDA_TRY(cudaMemcpyAsync(out, dst, bytes, cudaMemcpyDeviceToHost, e->stream));
+  CUDA_TRY(cudaStreamSynchronize(e->stream));
+  return MPX_OK;
+}
+
+static mpx_status reduce_quantity(mpx_engine* e, Magnet* m, int quantity, int op, double out[3]) {
+  const int nc = quantity >= MPX_Q_EXCHANGE_ENERGY_DENSITY ? 1 : 3;
+  const int N = m->dev.N;
+  MPX_TRY(ensure_scratch(e, sizeof(float) * 3 * (size_t)N));
+  MPX_TRY(eval_into(e, m, quantity, e->d_scratch));
+  const int nb = 256;
+  k_reduce_partial<<<nb, 256, 0, e->stream>>>(e->d_scratch, N, nc, m->geom, op, e->d_red);
+  k_reduce_final<<<1, 32, 0, e->stream>>>(e->d_red, nb, op, e->d_redout);
+  e->launches += 2;
+  MPX_TRY(check_launch(e, "reduce"));
+  CUDA_TRY(cudaMemcpyAsync(out, e->d_redout, sizeof(double) * 3, cudaMemcpyDeviceToHost, e->stream));
+  CUDA_TRY(cudaStreamSynchronize(e->stream));
+  return MPX_OK;
+}
+
+mpx_status mpx_average(mpx_engine* e, int magnet, int quantity, double out[3]) {
+  Magnet* m = get_mag(e, magnet);
+  if (!m || !out) return fail(MPX_ERR_INVALID, "no such magnet / null output");
+  if (quantity < 0 || quantity >= MPX_Q_COUNT) return fail(MPX_ERR_INVALID, "unknown quantity");
+  DeviceGuard guard(e->device);
+  double r[3];
+  MPX_TRY(reduce_quantity(e, m, quantity, 0, r));
+  const int nc = quantity >= MPX_Q_EXCHANGE_ENERGY_DENSITY ? 1 : 3;
+  for (int c = 0; c < 3; ++c) out[c] = (c < nc && m->ngeo > 0) ? r[c] / m->ngeo : 0.0;
+  return MPX_OK;
+}
+
+mpx_status mpx_max_norm(mpx_engine* e, int magnet, int quantity, double* out) {
+  Magnet* m = get_mag(e, magnet);
+  if (!m || !out) return fail(MPX_ERR_INVALID, "no such magnet / null output");
+  if (quantity < 0 || quantity >= MPX_Q_COUNT) return fail(MPX_ERR_INVALID, "unknown quantity");
+  DeviceGuard guard(e->device);
+  double r[3];
+  MPX_TRY(reduce_quantity(e, m, quantity, 1, r));
+  *out = r[0];
+  return MPX_OK;
+}
+
+mpx_status mpx_energy(mpx_engine* e, int magnet, int quantity, double* out) {
+  Magnet* m = get_mag(e, magnet);
+  if (!m || !out) return fail(MPX_ERR_INVALID, "no such magnet / null output");
+  if (quantity < MPX_Q_EXCHANGE_ENERGY_DENSITY || quantity >= MPX_Q_COUNT)
+    return fail(MPX_ERR_INVALID, "energy needs an energy-density quantity");
+  double avg[3];
+  MPX_TRY(mpx_average(e, magnet, quantity, avg));
+  *out = (double)m->dev.N * avg[0] * ((double)m->dev.cs[0] * m->dev.cs[1] * m->dev.cs[2]);
+  return MPX_OK;
+}
+
+mpx_status mpx_profile_eval(mpx_engine* e, int magnet, int reps, double ms[4]) {
+  Magnet* m = get_mag(e, magnet);
+  if (!m || !ms || reps <= 0) return fail(MPX_ERR_INVALID, "no such magnet / bad arguments");
+  DeviceGuard guard(e->device);
+  if (e->tables_dirty) MPX_TRY(rebuild_tables(e));
+  MPX_TRY(ensure_scratch(e, sizeof(float) * 3 * (size_t)m->dev.N));
+  EpiArgs ea;
+  ea.mode = EPI_EVAL;
+  ea.stage = 0;
+  ea.quantity = MPX_Q_EFFECTIVE_FIELD;
+  ea.fsal_err = 0;
+  ea.gate = 0;
+  ea.out = e->d_scratch;
+  ea.msrc = nullptr;
+  const int ntile = (int)m->tiles.size();
+  const int sx = x_smem(m), syz = yz_smem(m), nt = x_threads(m);
+  cudaEvent_t ev[5];
+  for (auto& x : ev) CUDA_TRY(cudaEventCreate(&x));
+  double acc[4] = {0, 0, 0, 0};
+  for (int r = 0; r <= reps; ++r) {  // r == 0 is the warm-up
+    float t[4] = {0, 0, 0, 0};
+    if (m->demag) {
+      CUDA_TRY(cudaEventRecord(ev[0], e->stream));
+      k_xfwd<false><<<ntile, nt, sx, e->stream>>>(e->d_mags, e->d_groups, m->d_tiles, 0, 0, nullptr, e->d_tw);
+      CUDA_TRY(cudaEventRecord(ev[1], e->stream));
+      MPX_TRY(launch_yz(e, yz_class(m), m->d_kxw, (int)m->kxw.size(), syz, 0, 0));
+      CUDA_TRY(cudaEventRecord(ev[2], e->stream));
+      k_xinv<<<ntile, nt, sx, e->stream>>>(e->d_mags, e->d_groups, m->d_tiles, ea, e->d_tw);
+      CUDA_TRY(cudaEventRecord(ev[3], e->stream));
+      e->launches += 2;
+      CUDA_TRY(cudaEventSynchronize(ev[3]));
+      for (int k = 0; k < 3; ++k) CUDA_TRY(cudaEventElapsedTime(&t[k], ev[k], ev[k + 1]));
+    } else {
+      CUDA_TRY(cudaEventRecord(ev[3], e->stream));
+      k_local<<<ntile, 256, 0, e->stream>>>(e->d_mags, e->d_groups, m->d_tiles, ea);
+      CUDA_TRY(cudaEventRecord(ev[4], e->stream));
+      e->launches += 1;
+      CUDA_TRY(cudaEventSynchronize(ev[4]));
+      CUDA_TRY(cudaEventElapsedTime(&t[3], ev[3], ev[4]));
+    }
+    MPX_TRY(check_launch(e, "profile"));
+    if (r > 0)
+      for (int k = 0; k < 4; ++k) acc[k] += t[k];
+  }
+  for (auto& x : ev) cudaEventDestroy(x);
+  for (int k = 0; k < 4; ++k) ms[k] = acc[k] / reps;
+  return MPX_OK;
+}
+
+mpx_status mpx_demag_kernel(mpx_engine* e, int magnet, float* out, int dims[3]) {
+  Magnet* m = get_mag(e, magnet);
+  if (!m || !dims) return fail(MPX_ERR_INVALID, "no such magnet / null dims");
+  DeviceGuard guard(e->device);
+  int K[3], O[3];
+  for (int a = 0; a < 3; ++a) {
+    K[a] = 2 * m->dev.n[a] - 1;
+    const int pad = (K[a] > 5 && K[a] % 2 == 1) ? 1 : 0;
+    K[a] += pad;
+    O[a] = -(m->dev.n[a] - 1) - pad;
+    dims[a] = K[a];
+  }
+  if (!out) return MPX_OK;
+  KernelGeom g;
+  for (int a = 0; a < 3; ++a) {
+    g.n[a] = m->dev.n[a];
+    g.mg[a] = m->dev.mg[a];
+    g.pbc[a] = m->kkey_pbc[a];
+    g.cs[a] = m->kkey_cs[a];
+  }
+  if (!m->kspec_ready) {  // kernel geometry of a magnet without demag
+    for (int a = 0; a < 3; ++a) {
+      g.pbc[a] = 0;
+      g.cs[a] = m->dev.cs[a];
+    }
+  }
+  const size_t KK = (size_t)K[0] * K[1] * K[2];
+  float* d = nullptr;
+  CUDA_TRY(cudaMalloc(&d, sizeof(float) * 6 * KK));
+  k_newell_reflayout<<<148 * 8, 128, 0, e->stream>>>(d, g, K[0], K[1], K[2], O[0], O[1], O[2]);
+  e->launches++;
+  cudaError_t st = cudaMemcpyAsync(out, d, sizeof(float) * 6 * KK, cudaMemcpyDeviceToHost, e->stream);
+  if (st == cudaSuccess) st = cudaStreamSynchronize(e->stream);
+  cudaFree(d);
+  if (st != cudaSuccess) return fail(MPX_ERR_CUDA, cudaGetErrorString(st));
+  return MPX_OK;
+}
+
+mpx_status mpx_solver_set_params(mpx_engine* e, int group, const mpx_solver_params* p) {
+  Group* g = get_group(e, group);
+  if (!g || !p) return fail(MPX_ERR_INVALID, "no such group / null params");
+  if (p->method < 0 || p->method > MPX_RK_DORMAND_PRINCE) return fail(MPX_ERR_INVALID, "invalid Runge Kutta method");
+  if (p->lower_bound >= p->upper_bound)
+    return fail(MPX_ERR_RUNTIME, "The lower bound should be lower than the upper bound.");
+  if (p->sensible_timestep_default < 0)
+    return fail(MPX_ERR_RUNTIME, "The sensible timestep should be larger than zero.");
+  DeviceGuard guard(e->device);
+  const bool method_changed = p->method != g->sp.method;
+  g->sp = *p;
+  GroupDev G;
+  MPX_TRY(read_group(e, group, &G));
+  fill_group_params(G, g->sp);
+  if (method_changed) G.k0_valid = 0;
+  MPX_TRY(write_group(e, group, &G));
+  if (method_changed && g->sp.adaptive) {  // core/timesolver.cpp:23-27
+    double dt;
+    MPX_TRY(sensible_timestep(e, g, &dt));
+    MPX_TRY(read_group(e, group, &G));
+    G.dt = dt;
+    MPX_TRY(write_group(e, group, &G));
+  }
+  return MPX_OK;
+}
+
+mpx_status mpx_solver_get_params(mpx_engine* e, int group, mpx_solver_params* p) {
+  Group* g = get_group(e, group);
+  if (!g || !p) return fail(MPX_ERR_INVALID, "no such group / null params");
+  *p = g->sp;
+  return MPX_OK;
+}
+
+mpx_status mpx_solver_set_time(mpx_engine* e, int group, double t) {
+  Group* g = get_group(e, group);
+  if (!g) return fail(MPX_ERR_RANGE, "no such group");
+  DeviceGuard guard(e->device);
+  GroupDev G;
+  MPX_TRY(read_group(e, group, &G));
+  G.t = t;
+  MPX_TRY(write_group(e, group, &G));
+  return MPX_OK;
+}
+
+mpx_status mpx_solver_get_time(mpx_engine* e, int group, double* t) {
+  Group* g = get_group(e, group);
+  if (!g || !t) return fail(MPX_ERR_RANGE, "no such group");
+  DeviceGuard guard(e->device);
+  GroupDev G;
+  MPX_TRY(read_group(e, group, &G));
+  *t = G.t;
+  return MPX_OK;
+}
+
+mpx_status mpx_solver_set_timestep(mpx_engine* e, int group, double dt) {
+  Group* g = get_group(e, group);
+  if (!g) return fail(MPX_ERR_RANGE, "no such group");
+  DeviceGuard guard(e->device);
+  GroupDev G;
+  MPX_TRY(read_group(e, group, &G));
+  G.dt = dt;
+  MPX_TRY(write_group(e, group, &G));
+  return MPX_OK;
+}
+
+mpx_status mpx_solver_get_timestep(mpx_engine* e, int group, double* dt) {
+  Group* g = get_group(e, group);
+  if (!g || !dt) return fail(MPX_ERR_RANGE, "no such group");
+  DeviceGuard guard(e->device);
+  GroupDev G;
+  MPX_TRY(read_group(e, group, &G));
+  *dt = G.dt;
+  return MPX_OK;
+}
+
+mpx_status mpx_solver_sensible_timestep(mpx_engine* e, int group, double* dt) {
+  Group* g = get_group(e, group);
+  if (!g || !dt) return fail(MPX_ERR_RANGE, "no such group");
+  DeviceGuard guard(e->device);
+  return sensible_timestep(e, g, dt);
+}
+
+static mpx_status start_group(mpx_engine* e, Group* g, int mode, long long nsteps, double duration,
+                              double torque_stop, bool* nothing_to_do) {
+  *nothing_to_do = false;
+  GroupDev G;
+  MPX_TRY(read_group(e, g->slot, &G));
+  if (g->magnets.empty()) {  // core/rungekutta.cpp:26-30: no equations, only time advances
+    if (mode == 1) {
+      if (!(G.dt > 0)) return fail(MPX_ERR_RUNTIME, "Timesolver can not make a step because the timestep is smaller than or equal to zero.");
+      G.t += G.dt * (double)nsteps;
+    } else if (duration > 0) {
+      const double stop = G.t + duration;
+      while (G.t < stop - G.dt) G.t += G.dt;
+      G.t = stop;
+    }
+    MPX_TRY(write_group(e, g->slot, &G));
+    *nothing_to_do = true;
+    return MPX_OK;
+  }
+  if (!(G.dt > 0))
+    return fail(MPX_ERR_RUNTIME,
+                "Timesolver can not make a step because the timestep is smaller than or equal to zero.");
+  fill_group_params(G, g->sp);
+  G.mode = mode;
+  G.phase = 0;
+  G.steps_left = nsteps;
+  G.torque_stop = torque_stop;
+  G.err_bits = 0;
+  G.tmax_bits = 0;
+  G.finished_flag = 0;
+  if (mode == 0) {
+    G.t_stop = G.t + duration;
+    if (!(G.t < G.t_stop - G.dt)) {  // core/timesolver.cpp:100-109
+      G.phase = 1;
+      G.dt_saved = G.dt;
+      G.dt = G.t_stop - G.t;
+    }
+  }
+  G.status = GS_RUNNING;
+  MPX_TRY(write_group(e, g->slot, &G));
+  return MPX_OK;
+}
+
+mpx_status mpx_solver_steps(mpx_engine* e, int group, int nsteps) {
+  Group* g = get_group(e, group);
+  if (!g) return fail(MPX_ERR_RANGE, "no such group");
+  if (nsteps <= 0) return MPX_OK;
+  DeviceGuard guard(e->device);
+  bool none;
+  MPX_TRY(start_group(e, g, 1, nsteps, 0.0, 0.0, &none));
+  if (none) return MPX_OK;
+  return drive_group(e, g);
+}
+
+mpx_status mpx_solver_step(mpx_engine* e, int group) { return mpx_solver_steps(e, group, 1); }
+
+mpx_status mpx_solver_run(mpx_engine* e, int group, double duration) {
+  Group* g = get_group(e, group);
+  if (!g) return fail(MPX_ERR_RANGE, "no such group");
+  if (duration <= 0) return MPX_OK;
+  DeviceGuard guard(e->device);
+  bool none;
+  MPX_TRY(start_group(e, g, 0, 0, duration, 0.0, &none));
+  if (none) return MPX_OK;
+  return drive_group(e, g);
+}
+
+mpx_status mpx_group_start(mpx_engine* e, int group, double duration, double torque_stop) {
+  Group* g = get_group(e, group);
+  if (!g) return fail(MPX_ERR_RANGE, "no such group");
+  if (duration <= 0) return fail(MPX_ERR_INVALID, "duration must be positive");
+  if (torque_stop > 0 && g->sp.method != MPX_RK_DORMAND_PRINCE)
+    return fail(MPX_ERR_UNSUPPORTED, "the torque stop criterion needs the DormandPrince method");
+  // all running groups of an engine advance with one method
+  for (auto& og : e->groups)
+    if (og && og.get() != g && og->sp.method != g->sp.method) {
+      GroupDev G;
+      MPX_TRY(read_group(e, og->slot, &G));
+      if (G.status == GS_RUNNING) return fail(MPX_ERR_INVALID, "running groups must share one Runge Kutta method");
+    }
+  DeviceGuard guard(e->device);
+  bool none;
+  MPX_TRY(start_group(e, g, 0, 0, duration, torque_stop, &none));
+  if (none) {
+    GroupDev G;
+    MPX_TRY(read_group(e, group, &G));
+    G.finished_flag = 1;
+    G.status = GS_FINISHED;
+    MPX_TRY(write_group(e, group, &G));
+  }
+  return MPX_OK;
+}
+
+mpx_status mpx_advance(mpx_engine* e, int attempts) {
+  if (!e) return fail(MPX_ERR_INVALID, "null engine");
+  if (attempts <= 0) return MPX_OK;
+  DeviceGuard guard(e->device);
+  int method = -1;
+  for (auto& g : e->groups)
+    if (g && !g->magnets.empty()) { method = g->sp.method; break; }
+  if (method < 0) return MPX_OK;
+  return run_attempts(e, method, attempts);
+}
+
+mpx_status mpx_poll(mpx_engine* e, int* done, int cap, int* n_done, int* n_running) {
+  if (!e) return fail(MPX_ERR_INVALID, "null engine");
+  DeviceGuard guard(e->device);
+  const int ng = (int)e->groups.size();
+  std::vector<GroupDev> G(ng);
+  if (ng > 0) {
+    CUDA_TRY(cudaMemcpyAsync(G.data(), e->d_groups, sizeof(GroupDev) * ng, cudaMemcpyDeviceToHost, e->stream));
+    CUDA_TRY(cudaStreamSynchronize(e->stream));
+  }
+  int nd = 0, nr = 0;
+  for (int i = 0; i < ng; ++i) {
+    if (!e->groups[i]) continue;
+    if (G[i].status == GS_RUNNING) nr++;
+    if (G[i].finished_flag && nd < cap) {
+      if (done) done[nd] = i;
+      nd++;
+      G[i].finished_flag = 0;
+      if (G[i].status == GS_FINISHED) G[i].status = GS_IDLE;
+      CUDA_TRY(cudaMemcpyAsync(e->d_groups + i, &G[i], sizeof(GroupDev), cudaMemcpyHostToDevice, e->stream));
+    }
+  }
+  CUDA_TRY(cudaStreamSynchronize(e->stream));
+  if (n_done) *n_done = nd;
+  if (n_running) *n_running = nr;
+  return MPX_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,199 @@
+// fft.cuh -- shared-memory FFTs for the demag convolution (sm_100a, FP32).
+//
+// Power-of-two complex FFTs run in place in shared memory as Stockham
+// autosort passes of radix 2/4/8/16 (natural-order output, no bit reversal):
+// pass with sub-transform size Ns and radix R takes butterfly j of a column,
+// loads x[j + r*L/R], twiddles by W_{Ns R}^{r (j mod Ns)}, does an R-point DFT
+// in registers and stores to ((j - j mod Ns) R + j mod Ns) + r Ns.
+// Every thread holds 16 complex values per pass, so one call transforms at
+// most 16*blockDim.x elements; callers loop over groups of columns.
+//
+// Shared-memory layout: element i of a column sits at pidx(i) = i + i/16 (one
+// float2 of padding per 16), which makes the strided stores of the first
+// passes (stride R) bank-conflict free.  All index arithmetic is shifts and
+// masks (lengths are powers of two).
+//
+// Twiddles come from a 4096-entry table exp(-2 pi i k / 4096) computed in FP64
+// on the host (accurate to FP32 rounding); each block copies the L entries of
+// its transform length into shared memory once.
+#pragma once
+#include <cuda_runtime.h>
+
+namespace mpx {
+
+constexpr int TW_LOG = 12;  // twiddle table covers transforms up to 4096 points
+constexpr int TW_N = 1 << TW_LOG;
+
+__device__ __forceinline__ float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ float2 csub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
+__device__ __forceinline__ float2 cmul(float2 a, float2 b) {
+  return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+__device__ __forceinline__ float2 cconj(float2 a) { return make_float2(a.x, -a.y); }
+
+// padded shared-memory index and padded column length
+__device__ __forceinline__ int pidx(int i) { return i + (i >> 4); }
+__host__ __device__ constexpr int plen(int L) { return L + (L >> 4); }
+
+// exp(DIR * 2 pi i e / L) from a shared-memory table of the L forward
+// twiddles exp(-2 pi i e / L) (DIR = -1 forward, +1 inverse)
+template <int DIR>
+__device__ __forceinline__ float2 twiddle_raw(const float2* tw, int e) {
+  const float2 w = tw[e];
+  return DIR < 0 ? w : make_float2(w.x, -w.y);
+}
+
+// Fill a shared-memory table of the L = 2^logL twiddles from the global
+// 4096-entry table (the caller synchronises before use).
+__device__ __forceinline__ void load_twiddles(float2* dst, const float2* __restrict__ tw4096, int logL) {
+  const int L = 1 << logL;
+  for (int e = threadIdx.x; e < L; e += blockDim.x) dst[e] = __ldg(&tw4096[e << (TW_LOG - logL)]);
+}
+
+// cos(2 pi m / 16), m = 0..4 (decimal expansions of the constants)
+__host__ __device__ constexpr float c16(int m) {
+  return m == 0 ? 1.0f : m == 1 ? 0.923879532511286756f : m == 2 ? 0.707106781186547524f
+         : m == 3 ? 0.382683432365089772f : 0.0f;
+}
+
+// Multiply by exp(DIR * 2 pi i M / 16), M a compile-time constant in [0, 16).
+template <int DIR, int M>
+__device__ __forceinline__ float2 rot16(float2 v) {
+  constexpr int q = M / 4, r = M % 4;  // quarter turns and remainder
+  float2 a = v;
+  if (q == 1) a = DIR < 0 ? make_float2(v.y, -v.x) : make_float2(-v.y, v.x);
+  if (q == 2) a = make_float2(-v.x, -v.y);
+  if (q == 3) a = DIR < 0 ? make_float2(-v.y, v.x) : make_float2(v.y, -v.x);
+  if (r == 0) return a;
+  constexpr float c = c16(r), s = DIR * c16(4 - r);
+  return make_float2(a.x * c - a.y * s, a.x * s + a.y * c);
+}
+
+// Recursive radix-2 DFT of N values held in registers (N = 1, 2, 4, 8, 16),
+// unnormalised, natural order in and out.  The even / odd split and the
+// twiddles exp(DIR 2 pi i k / N) are all compile-time, so the values stay in
+// registers.
+template <int DIR, int N, int K>
+__device__ __forceinline__ float2 rotN(float2 v) {
+  static_assert(16 % N == 0 || N == 1, "radix");
+  return rot16<DIR, (K * (16 / N)) % 16>(v);
+}
+
+template <int N, int DIR>
+struct Dft {
+  template <int K>
+  __device__ __forceinline__ static void combine(float2 (&v)[N], const float2 (&e)[N / 2], const float2 (&o)[N / 2]) {
+    if constexpr (K < N / 2) {
+      const float2 t = rotN<DIR, N, K>(o[K]);
+      v[K] = cadd(e[K], t);
+      v[K + N / 2] = csub(e[K], t);
+      combine<K + 1>(v, e, o);
+    }
+  }
+  template <int I>
+  __device__ __forceinline__ static void split(const float2 (&v)[N], float2 (&e)[N / 2], float2 (&o)[N / 2]) {
+    if constexpr (I < N / 2) {
+      e[I] = v[2 * I];
+      o[I] = v[2 * I + 1];
+      split<I + 1>(v, e, o);
+    }
+  }
+  __device__ __forceinline__ static void run(float2 (&v)[N]) {
+    float2 e[N / 2], o[N / 2];
+    split<0>(v, e, o);
+    Dft<N / 2, DIR>::run(e);
+    Dft<N / 2, DIR>::run(o);
+    combine<0>(v, e, o);
+  }
+};
+template <int DIR>
+struct Dft<1, DIR> {
+  __device__ __forceinline__ static void run(float2 (&)[1]) {}
+};
+
+// In-register R-point DFT (R = 1, 2, 4, 8, 16), unnormalised.
+template <int R, int DIR>
+__device__ __forceinline__ void dft_reg(float2 (&v)[R]) {
+  Dft<R, DIR>::run(v);
+}
+
+// One Stockham pass of radix 2^LR over `ncols` padded columns of length 2^logL
+// (column c at buf + c*cs), each thread holding VPT values.
+// Requires ncols*L <= VPT*blockDim.x.
+template <int LR, int DIR, int VPT>
+__device__ __forceinline__ void stockham_pass(float2* buf, int logL, int logNs, int ncols, int cs,
+                                              const float2* __restrict__ tw) {
+  constexpr int R = 1 << LR, BPT = VPT / R;
+  const int lognb = logL - LR;
+  const int nb = 1 << lognb;
+  const int total = ncols << lognb;
+  const int Ns = 1 << logNs;
+  const int twshift = logL - logNs - LR;  // tw holds the 2^logL twiddles of this length
+  float2 v[BPT][R];
+#pragma unroll
+  for (int q = 0; q < BPT; ++q) {
+    const int b = threadIdx.x + q * blockDim.x;
+    if (b < total) {
+      const float2* base = buf + (b >> lognb) * cs;
+      const int j = b & (nb - 1);
+#pragma unroll
+      for (int r = 0; r < R; ++r) v[q][r] = base[pidx(j + (r << lognb))];
+    }
+  }
+  __syncthreads();
+#pragma unroll
+  for (int q = 0; q < BPT; ++q) {
+    const int b = threadIdx.x + q * blockDim.x;
+    if (b < total) {
+      float2* base = buf + (b >> lognb) * cs;
+      const int j = b & (nb - 1);
+      const int k = j & (Ns - 1);
+      if (logNs > 0) {
+#pragma unroll
+        for (int r = 1; r < R; ++r) v[q][r] = cmul(v[q][r], twiddle_raw<DIR>(tw, (r * k) << twshift));
+      }
+      dft_reg<R, DIR>(v[q]);
+      const int o = ((j - k) << LR) + k;
+#pragma unroll
+      for (int r = 0; r < R; ++r) base[pidx(o + (r << logNs))] = v[q][r];
+    }
+  }
+  __syncthreads();
+}
+
+// log2 radix of pass i (of ceil(logL/MAXLR) passes) for a 2^logL transform
+__device__ __forceinline__ int fft_npass(int logL, int maxlr) { return (logL + maxlr - 1) / maxlr; }
+__device__ __forceinline__ int fft_pass_lr(int logL, int maxlr, int i) {
+  const int p = fft_npass(logL, maxlr);
+  const int base = logL / p, extra = logL - base * p;
+  return base + (i < extra ? 1 : 0);
+}
+
+// In-place FFT of `ncols` padded columns of length 2^logL with radices up to
+// 2^MAXLR and 2^MAXLR values per thread (ncols*L <= 2^MAXLR*blockDim.x).
+// All threads of the block must call it.
+template <int DIR, int MAXLR>
+__device__ void fft_cols(float2* buf, int logL, int ncols, int cs, const float2* __restrict__ tw) {
+  constexpr int VPT = 1 << MAXLR;
+  if (logL == 0) return;
+  const int p = fft_npass(logL, MAXLR);
+  int logNs = 0;
+  for (int i = 0; i < p; ++i) {
+    const int lr = fft_pass_lr(logL, MAXLR, i);
+    if (lr == 1) stockham_pass<1, DIR, VPT>(buf, logL, logNs, ncols, cs, tw);
+    else if (lr == 2) stockham_pass<2, DIR, VPT>(buf, logL, logNs, ncols, cs, tw);
+    else if (lr == 3 || MAXLR == 3) stockham_pass<(MAXLR >= 3 ? 3 : 2), DIR, VPT>(buf, logL, logNs, ncols, cs, tw);
+    else stockham_pass<(MAXLR >= 4 ? 4 : 2), DIR, VPT>(buf, logL, logNs, ncols, cs, tw);
+    logNs += lr;
+  }
+}
+
+// FFT of many padded columns, in groups that fit 2^MAXLR values per thread.
+template <int DIR, int MAXLR>
+__device__ void fft_many(float2* buf, int logL, int ncols, int cs, const float2* __restrict__ tw) {
+  if (logL == 0) return;
+  const int per = max(1, ((1 << MAXLR) * (int)blockDim.x) >> logL);
+  for (int c0 = 0; c0 < ncols; c0 += per) fft_cols<DIR, MAXLR>(buf + c0 * cs, logL, min(per, ncols - c0), cs, tw);
+}
+
+}  // namespace mpx

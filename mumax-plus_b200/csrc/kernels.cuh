@@ -1,0 +1,743 @@
+// kernels.cuh -- the demag / effective-field / Runge-Kutta kernels.
+//
+// Demag convolution (replaces physics/strayfieldfft.cu:191-246, whose k_pad,
+// 3 cuFFT R2C, k_apply_kernel_3d/2d, 3 cuFFT C2R and k_unpad are 9 launches over
+// the padded grid) as three passes over a spectrum that only holds the rows
+// that are not zero padding:
+//   k_xfwd   per tile of TY rows (fixed z): [RK stage combination] -> Ms*m ->
+//            real-to-complex FFT along x (two real rows per complex FFT) ->
+//            S[kx][c][z][y]
+//   k_yz     per kx: FFT along y of the 3*nz columns, then per ky an in-register
+//            FFT along z split over two lanes (even / odd kz), the 3x3 multiply
+//            by the real Newell spectrum (its -mu0/P prefactor folded in) and
+//            the inverse z FFT, then the inverse FFT along y; writes back S
+//   k_xinv   per tile: complex-to-real FFT along x -> B_demag in shared memory ->
+//            epilogue: local terms + LLG torque (-> k_s) or a requested quantity,
+//            and for the last stage of an FSAL method the max-norm error and the
+//            max torque of the step.
+// The padded sizes are powers of two P >= 2n-1 and the kernel is stored
+// circularly (r = 0 at index 0), so the result is the reference's linear
+// convolution of the zero-padded magnetisation (strayfieldkernel.cu:80-99).
+// Each block first copies its magnet and group descriptors to shared memory.
+#pragma once
+#include "fft.cuh"
+#include "physics.cuh"
+
+namespace mpx {
+
+// Butcher tableau of the current method (core/butchertableau.cpp), in constant memory.
+struct TableauDev {
+  int S, order1, order2, fsal;
+  double c[7];
+  double a[7][7];
+  double b1[7], b2[7];
+};
+__constant__ TableauDev c_tab;
+
+// Work item of the row-tile kernels: magnet slot, z, first row y0, rows in tile (<= 4).
+// Work item of k_yz: magnet slot, kx (in z).
+struct Work {
+  int mag, z, y0, ty;
+};
+
+enum { EPI_STAGE = 0, EPI_EVAL = 1 };
+
+struct EpiArgs {
+  int mode;      // EPI_STAGE: write k_s ; EPI_EVAL: write `quantity` into out
+  int stage;
+  int quantity;  // mpx_quantity
+  int fsal_err;  // fuse error + max torque (last stage of an FSAL method)
+  int gate;      // skip groups that are not running
+  float* out;    // EPI_EVAL output (device, 3N or N floats)
+  const float* msrc;  // EPI_EVAL: magnetisation source (NULL: group state x0)
+};
+
+template <typename T>
+__device__ __forceinline__ void copy_to_smem(T* dst, const T* __restrict__ src) {
+  static_assert(sizeof(T) % 4 == 0, "descriptor size");
+  const int* s = reinterpret_cast<const int*>(src);
+  int* d = reinterpret_cast<int*>(dst);
+  for (int i = threadIdx.x; i < (int)(sizeof(T) / 4); i += blockDim.x) d[i] = s[i];
+}
+
+// Loads the magnet and group descriptors of this block; returns false when the
+// block has nothing to do (group not running, or k0 already valid for stage 0).
+__device__ __forceinline__ bool load_descs(MagnetDev& sM, GroupDev& sG, const MagnetDev* __restrict__ mags,
+                                           const GroupDev* __restrict__ groups, int mag, int gate, int stage) {
+  copy_to_smem(&sM, mags + mag);
+  __syncthreads();
+  copy_to_smem(&sG, groups + sM.group);
+  __syncthreads();
+  if (!gate) return true;
+  if (sG.status != GS_RUNNING) return false;
+  if (stage == 0 && sG.k0_valid) return false;
+  return true;
+}
+
+// Current magnetisation used by stage `stage`: x0 for stage 0, the stage state otherwise.
+__device__ __forceinline__ const float* stage_m(const MagnetDev& M, const GroupDev& G, int stage) {
+  return stage == 0 ? M.buf[G.map[0]] : M.buf[G.map[1]];
+}
+
+// Stage combination x_s = normalize(x0 + sum_j dt a_sj k_j) of one cell
+// (core/rungekutta.cpp:108-134, core/fieldops.cu:232-258).
+__device__ __forceinline__ float3 combine_cell(const MagnetDev& M, const GroupDev& G, int stage, int i,
+                                               bool final_b1) {
+  const int N = M.N;
+  float3 v = ldg3(M.buf[G.map[0]], N, i);
+  const int nj = final_b1 ? c_tab.S : stage;
+  for (int j = 0; j < nj; ++j) {
+    const double co = final_b1 ? c_tab.b1[j] : c_tab.a[stage][j];
+    const float cf = (float)(G.dt * co);
+    const float3 k = ldg3(M.buf[G.map[2 + j]], N, i);
+    v = f3(v.x + cf * k.x, v.y + cf * k.y, v.z + cf * k.z);
+  }
+  const float inv = rsqrtf(v.x * v.x + v.y * v.y + v.z * v.z);
+  return f3(v.x * inv, v.y * inv, v.z * inv);
+}
+
+// row index within a tile of at most 4 rows of length n, without division
+__device__ __forceinline__ int tile_row(int e, int n) { return (e >= n) + (e >= 2 * n) + (e >= 3 * n); }
+
+// ------------------------------------------------------------------ k_xfwd
+// smem: padded rows [ty] for (Mx + i My) of each row, then [(ty+1)/2] for
+// (Mz(y) + i Mz(y+1)).
+template <bool COMBINE>
+__global__ void __launch_bounds__(512, 2) k_xfwd(const MagnetDev* __restrict__ mags, const GroupDev* __restrict__ groups,
+                                              const Work* __restrict__ work, int stage, int gate,
+                                              const float* __restrict__ msrc_override,
+                                              const float2* __restrict__ tw) {
+  extern __shared__ float2 sm[];
+  __shared__ MagnetDev M;
+  __shared__ GroupDev G;
+  const Work wk = work[blockIdx.x];
+  if (!load_descs(M, G, mags, groups, wk.mag, gate, stage)) return;
+  const int z = wk.z, y0 = wk.y0, ty = wk.ty;
+  const int nx = M.n[0], ny = M.n[1], nz = M.n[2], N = M.N;
+  const int logL = M.logP[0], L = 1 << logL, cs = plen(L);
+  const int nzrows = (ty + 1) >> 1;
+  const float* src = msrc_override ? msrc_override : stage_m(M, G, stage);
+  float* xs = M.buf[G.map[1]];
+  const float* x0 = M.buf[G.map[0]];
+  const int rowbase = nx * (y0 + ny * z);
+  float2* tws = sm + (ty + nzrows) * cs;  // twiddles of length L
+  load_twiddles(tws, tw, logL);
+
+#pragma unroll 2
+  for (int e = threadIdx.x; e < (ty << logL); e += blockDim.x) {
+    const int yl = e >> logL, x = e & (L - 1);
+    float3 Mv = f3(0, 0, 0);
+    if (x < nx) {
+      const int i = rowbase + yl * nx + x;
+      if (in_geom(M, i)) {
+        float3 m;
+        if (COMBINE) {
+          m = combine_cell(M, G, stage, i, false);
+          store3(xs, N, i, m);
+        } else {
+          m = ldg3(src, N, i);
+        }
+        Mv = M.msat.at(i) * m;
+      } else if (COMBINE) {
+        store3(xs, N, i, load3(x0, N, i));
+      }
+    }
+    sm[yl * cs + pidx(x)] = make_float2(Mv.x, Mv.y);
+    float* zr = reinterpret_cast<float*>(sm + (ty + (yl >> 1)) * cs + pidx(x));
+    zr[yl & 1] = Mv.z;
+    if ((ty & 1) && yl == ty - 1) zr[1] = 0.0f;
+  }
+  __syncthreads();
+  fft_many<-1, 3>(sm, logL, ty + nzrows, cs, tws);
+
+  // unpack the two real transforms of each complex row and store the half spectrum
+  const int Fh = M.Fh;
+  float2* S = M.spec;
+  for (int e = threadIdx.x; e < Fh * 12; e += blockDim.x) {
+    const int yl = e & 3;
+    if (yl >= ty) continue;
+    const int rest = e >> 2;
+    const int c = rest % 3, kx = rest / 3;
+    const float2* Z = (c < 2) ? (sm + yl * cs) : (sm + (ty + (yl >> 1)) * cs);
+    const float2 zk = Z[pidx(kx)];
+    const float2 zc = cconj(Z[pidx((L - kx) & (L - 1))]);
+    float2 val;
+    const bool second = (c == 1) || (c == 2 && (yl & 1));
+    if (!second) {
+      val = make_float2(0.5f * (zk.x + zc.x), 0.5f * (zk.y + zc.y));
+    } else {  // -i/2 (zk - zc)
+      val = make_float2(0.5f * (zk.y - zc.y), -0.5f * (zk.x - zc.x));
+    }
+    S[((size_t)(kx * 3 + c) * nz + z) * ny + y0 + yl] = val;
+  }
+}
+
+// --------------------------------------------------------------------- k_yz
+// Kernel spectrum entry (comp cc of the xx,yy,zz,xy,xz,yz order) at (kx, ky, kz)
+// from the symmetry-reduced storage [kx][kz'][kcomp][ky'].
+template <int PZ>
+__device__ __forceinline__ void kernel_at(const float* __restrict__ Kx, int kc, int hy, int kyp, float sy, int kz,
+                                          float& kxx, float& kyy, float& kzz, float& kxy, float& kxz, float& kyz) {
+  const int kzp = min(kz, PZ - kz);
+  const float sz = (kz > PZ / 2) ? -1.f : 1.f;
+  const float* Kk = Kx + (size_t)kzp * kc * hy + kyp;
+  kxx = __ldg(Kk);
+  kyy = __ldg(Kk + hy);
+  kzz = __ldg(Kk + 2 * hy);
+  kxy = sy * __ldg(Kk + 3 * hy);
+  if (kc == 6) {
+    kxz = sz * __ldg(Kk + 4 * hy);
+    kyz = sy * sz * __ldg(Kk + 5 * hy);
+  } else {
+    kxz = kyz = 0.f;
+  }
+}
+
+__device__ __forceinline__ void apply3(float2* v0, float2* v1, float2* v2, float kxx, float kyy, float kzz, float kxy,
+                                       float kxz, float kyz) {
+  const float2 mx = *v0, my = *v1, mz = *v2;
+  *v0 = make_float2(kxx * mx.x + kxy * my.x + kxz * mz.x, kxx * mx.y + kxy * my.y + kxz * mz.y);
+  *v1 = make_float2(kxy * mx.x + kyy * my.x + kyz * mz.x, kxy * mx.y + kyy * my.y + kyz * mz.y);
+  *v2 = make_float2(kxz * mx.x + kyz * my.x + kzz * mz.x, kxz * mx.y + kyz * my.y + kzz * mz.y);
+}
+
+// z stage of one ky, half = 0 / 1 computing the even / odd kz of the PZ-point
+// transform of nz <= PZ/2 inputs as a PZ/2-point transform (of x, or of
+// x[n] W_PZ^n); the partner lane holds the other half and the two inverse
+// halves are summed with one shuffle.
+template <int PZ>
+__device__ __forceinline__ void zstage_pair(float2* D, int cs, const MagnetDev& M, int kx, int ky, int half, int nz,
+                                            int Py) {
+  constexpr int H = PZ / 2;
+  float2 v[3][H];
+  const int pky = pidx(ky);
+  // kernel spectrum of this lane's kz values, issued before the transforms
+  const int hy = Py / 2 + 1;
+  const int kyp = min(ky, Py - ky);
+  const float sy = (ky > Py / 2) ? -1.f : 1.f;
+  const int kc = M.kcomp;
+  const float* __restrict__ Kx = M.kspec + (size_t)kx * (PZ / 2 + 1) * kc * hy;
+  float kk[H][6];
+#pragma unroll
+  for (int q = 0; q < H; ++q)
+    kernel_at<PZ>(Kx, kc, hy, kyp, sy, 2 * q + half, kk[q][0], kk[q][1], kk[q][2], kk[q][3], kk[q][4], kk[q][5]);
+#pragma unroll
+  for (int c = 0; c < 3; ++c)
+#pragma unroll
+    for (int n = 0; n < H; ++n) v[c][n] = (n < nz) ? D[(c * nz + n) * cs + pky] : make_float2(0.f, 0.f);
+  if (half) {
+#pragma unroll
+    for (int n = 1; n < H; ++n)
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        switch ((16 / PZ) * n) {  // times exp(-2 pi i n / PZ)
+          case 1: v[c][n] = rot16<-1, 1>(v[c][n]); break;
+          case 2: v[c][n] = rot16<-1, 2>(v[c][n]); break;
+          case 3: v[c][n] = rot16<-1, 3>(v[c][n]); break;
+          case 4: v[c][n] = rot16<-1, 4>(v[c][n]); break;
+          case 5: v[c][n] = rot16<-1, 5>(v[c][n]); break;
+          case 6: v[c][n] = rot16<-1, 6>(v[c][n]); break;
+          case 7: v[c][n] = rot16<-1, 7>(v[c][n]); break;
+          default: break;
+        }
+      }
+  }
+#pragma unroll
+  for (int c = 0; c < 3; ++c) dft_reg<H, -1>(v[c]);
+#pragma unroll
+  for (int q = 0; q < H; ++q)
+    apply3(&v[0][q], &v[1][q], &v[2][q], kk[q][0], kk[q][1], kk[q][2], kk[q][3], kk[q][4], kk[q][5]);
+#pragma unroll
+  for (int c = 0; c < 3; ++c) dft_reg<H, 1>(v[c]);
+  if (half) {
+#pragma unroll
+    for (int n = 1; n < H; ++n)
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        switch ((16 / PZ) * n) {  // times exp(+2 pi i n / PZ)
+          case 1: v[c][n] = rot16<1, 1>(v[c][n]); break;
+          case 2: v[c][n] = rot16<1, 2>(v[c][n]); break;
+          case 3: v[c][n] = rot16<1, 3>(v[c][n]); break;
+          case 4: v[c][n] = rot16<1, 4>(v[c][n]); break;
+          case 5: v[c][n] = rot16<1, 5>(v[c][n]); break;
+          case 6: v[c][n] = rot16<1, 6>(v[c][n]); break;
+          case 7: v[c][n] = rot16<1, 7>(v[c][n]); break;
+          default: break;
+        }
+      }
+  }
+  const unsigned mask = __activemask();
+#pragma unroll
+  for (int c = 0; c < 3; ++c)
+#pragma unroll
+    for (int n = 0; n < H; ++n) {
+      const float ox = __shfl_xor_sync(mask, v[c][n].x, 1);
+      const float oy = __shfl_xor_sync(mask, v[c][n].y, 1);
+      v[c][n] = make_float2(v[c][n].x + ox, v[c][n].y + oy);
+    }
+  // both lanes hold the sum; lane `half` writes the outputs n with n % 2 == half
+#pragma unroll
+  for (int c = 0; c < 3; ++c)
+#pragma unroll
+    for (int n = 0; n < H; ++n)
+      if (n < nz && (n & 1) == half) D[(c * nz + n) * cs + pky] = v[c][n];
+}
+
+__device__ __forceinline__ void zstage_single(float2* D, int cs, const MagnetDev& M, int kx, int ky, int Py) {
+  const int pky = pidx(ky);
+  float2 v0 = D[pky], v1 = D[cs + pky], v2 = D[2 * cs + pky];
+  const int hy = Py / 2 + 1;
+  const int kyp = min(ky, Py - ky);
+  const float sy = (ky > Py / 2) ? -1.f : 1.f;
+  const int kc = M.kcomp;
+  const float* __restrict__ Kx = M.kspec + (size_t)kx * kc * hy;
+  float kxx, kyy, kzz, kxy, kxz, kyz;
+  kernel_at<1>(Kx, kc, hy, kyp, sy, 0, kxx, kyy, kzz, kxy, kxz, kyz);
+  apply3(&v0, &v1, &v2, kxx, kyy, kzz, kxy, kxz, kyz);
+  D[pky] = v0;
+  D[cs + pky] = v1;
+  D[2 * cs + pky] = v2;
+}
+
+template <int PZ>
+__global__ void __launch_bounds__(384) k_yz(const MagnetDev* __restrict__ mags, const GroupDev* __restrict__ groups,
+                                            const Work* __restrict__ work, int stage, int gate,
+                                            const float2* __restrict__ tw) {
+  extern __shared__ float2 sm[];
+  __shared__ MagnetDev M;
+  __shared__ GroupDev G;
+  const Work wk = work[blockIdx.x];
+  if (!load_descs(M, G, mags, groups, wk.mag, gate, stage)) return;
+  const int kx = wk.z;
+  const int ny = M.n[1], nz = M.n[2];
+  const int logPy = M.logP[1], Py = 1 << logPy, cs = plen(Py);
+  float2* S = M.spec + (size_t)kx * 3 * nz * ny;
+  float2* D = sm;  // [3*nz] padded columns of length Py
+  const int ncol = 3 * nz;
+  float2* tws = sm + ncol * cs;  // twiddles of length Py
+  load_twiddles(tws, tw, logPy);
+  // slab load: 8 independent read-only loads in flight per thread
+  const int total = ncol << logPy;
+  for (int e0 = threadIdx.x; e0 < total; e0 += 8 * blockDim.x) {
+    float2 r[8];
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+      const int e = e0 + u * blockDim.x;
+      const int col = e >> logPy, y = e & (Py - 1);
+      r[u] = (e < total && y < ny) ? __ldg(S + col * ny + y) : make_float2(0.f, 0.f);
+    }
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+      const int e = e0 + u * blockDim.x;
+      if (e < total) D[(e >> logPy) * cs + pidx(e & (Py - 1))] = r[u];
+    }
+  }
+  __syncthreads();
+  fft_many<-1, 4>(D, logPy, ncol, cs, tws);
+  if constexpr (PZ == 1) {
+    for (int ky = threadIdx.x; ky < Py; ky += blockDim.x) zstage_single(D, cs, M, kx, ky, Py);
+  } else {
+    for (int t = threadIdx.x; t < 2 * Py; t += blockDim.x) zstage_pair<PZ>(D, cs, M, kx, t >> 1, t & 1, nz, Py);
+  }
+  __syncthreads();
+  fft_many<1, 4>(D, logPy, ncol, cs, tws);
+  for (int e = threadIdx.x; e < (ncol << logPy); e += blockDim.x) {
+    const int col = e >> logPy, y = e & (Py - 1);
+    if (y < ny) S[col * ny + y] = D[col * cs + pidx(y)];
+  }
+}
+
+// ------------------------------------------------------------- epilogue
+__device__ __forceinline__ void block_max2(double a, double b, unsigned long long* pa, unsigned long long* pb) {
+  // warp max then one atomic per warp (values are >= 0 or NaN; NaN bits order above +inf)
+  unsigned long long ua = __double_as_longlong(a), ub = __double_as_longlong(b);
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    ua = max(ua, (unsigned long long)__shfl_xor_sync(0xffffffffu, (long long)ua, o));
+    ub = max(ub, (unsigned long long)__shfl_xor_sync(0xffffffffu, (long long)ub, o));
+  }
+  if ((threadIdx.x & 31) == 0) {
+    if (ua) atomicMax(pa, ua);
+    if (ub) atomicMax(pb, ub);
+  }
+}
+
+// Per-cell epilogue: effective field (+ B_demag) -> torque or requested quantity.
+// err_n / tq_n receive the cell's error and torque norms for the FSAL error fusion.
+__device__ __forceinline__ void epilogue_cell(const MagnetDev& M, const GroupDev& G, const EpiArgs& ea,
+                                              const float* __restrict__ m, int x, int y, int z, int i, float3 bdemag,
+                                              double& err_n, double& tq_n) {
+  const int N = M.N;
+  const bool ing = in_geom(M, i);
+  const float3 mc = load3(m, N, i);
+  if (ea.mode == EPI_STAGE) {
+    float3 k = f3(0, 0, 0);
+    if (ing && M.frozen.at(i) == 0.0f) {
+      float3 h = f3(0, 0, 0);
+      if (M.msat.at(i) != 0.0f) {
+        const LocalOut lo = local_terms(M, m, x, y, z, i, mc, TERM_EXCH | TERM_DMI | TERM_ANIS | TERM_EXT);
+        h = lo.exch;
+        h = h + lo.anis;
+        h = h + lo.ext;
+        h = h + lo.dmi;
+      } else if (M.terms & TERM_EXT) {
+        h = local_terms(M, m, x, y, z, i, mc, TERM_EXT).ext;
+      }
+      h = h + bdemag;
+      k = llg_torque(mc, h, M.alpha.at(i));
+    }
+    store3(M.buf[G.map[2 + ea.stage]], N, i, k);
+    if (ea.fsal_err && ing) {
+      float3 e = f3(0, 0, 0);
+      for (int j = 0; j < c_tab.S; ++j) {
+        const float cf = (float)(G.dt * (c_tab.b1[j] - c_tab.b2[j]));
+        const float3 kj = (j == ea.stage) ? k : load3(M.buf[G.map[2 + j]], N, i);
+        e = f3(e.x + cf * kj.x, e.y + cf * kj.y, e.z + cf * kj.z);
+      }
+      err_n = sqrt((double)e.x * e.x + (double)e.y * e.y + (double)e.z * e.z);
+      tq_n = sqrt((double)k.x * k.x + (double)k.y * k.y + (double)k.z * k.z);
+    }
+    return;
+  }
+  // ---- EPI_EVAL
+  const int q = ea.quantity;
+  float* out = ea.out;
+  const bool scalar = q >= 10;
+  if (!ing) {
+    if (scalar) {
+      out[i] = 0.f;
+    } else if (q == 5 && (M.terms & TERM_EXT)) {  // external field outside the geometry: world bias
+      store3(out, N, i, f3(M.wb[0], M.wb[1], M.wb[2]));
+    } else if (q == 0) {
+      store3(out, N, i, mc);
+    } else {
+      store3(out, N, i, f3(0, 0, 0));
+    }
+    return;
+  }
+  const float ms = M.msat.at(i);
+  LocalOut lo;
+  lo.exch = lo.anis = lo.ext = lo.dmi = f3(0, 0, 0);
+  if (ms != 0.0f) {
+    lo = local_terms(M, m, x, y, z, i, mc, TERM_EXCH | TERM_DMI | TERM_ANIS | TERM_EXT);
+  } else if (M.terms & TERM_EXT) {
+    lo.ext = local_terms(M, m, x, y, z, i, mc, TERM_EXT).ext;
+  }
+  float3 h = lo.exch;
+  h = h + lo.anis;
+  h = h + lo.ext;
+  h = h + lo.dmi;
+  h = h + bdemag;
+  float3 r = f3(0, 0, 0);
+  float s = 0.f;
+  switch (q) {
+    case 0: r = mc; break;
+    case 1: r = h; break;
+    case 2: r = lo.exch; break;
+    case 3: r = lo.dmi; break;
+    case 4: r = lo.anis; break;
+    case 5: r = lo.ext; break;
+    case 6: r = bdemag; break;
+    case 7:
+    case 8:
+      if (M.frozen.at(i) == 0.0f) r = llg_torque(mc, h, M.alpha.at(i));
+      break;
+    case 9:
+      if (M.frozen.at(i) == 0.0f) r = (-GAMMA_LL) * cross3(mc, cross3(mc, h));
+      break;
+    case 10: s = (M.terms & TERM_EXCH) ? -0.5f * ms * dot3(mc, lo.exch) : 0.f; break;
+    case 11: s = (M.terms & TERM_DMI) ? -0.5f * ms * dot3(mc, lo.dmi) : 0.f; break;
+    case 12:
+    case 15: {
+      float ea_ = 0.f;
+      if ((M.terms & TERM_ANIS) && ms != 0.0f) {  // physics/anisotropy.cu:142-173
+        float3 u = M.anisU.at(i, N);
+        const float nu = sqrtf(dot3(u, u));
+        u = ((nu == 0.0f) ? 0.0f : 1.0f / nu) * u;
+        const float mu = dot3(mc, u);
+        ea_ -= M.ku1.at(i) * mu * mu;
+        ea_ -= M.ku2.at(i) * mu * mu * mu * mu;
+      }
+      if (q == 12) {
+        s = ea_;
+      } else {  // total energy density (physics/energy.cu:37-56)
+        float t = 0.f;
+        if (M.terms & TERM_EXCH) t += -0.5f * ms * dot3(mc, lo.exch);
+        if (M.terms & TERM_ANIS) t += ea_;
+        if (M.terms & TERM_EXT) t += -1.0f * ms * dot3(mc, lo.ext);
+        if (M.terms & TERM_DMI) t += -0.5f * ms * dot3(mc, lo.dmi);
+        if (M.terms & TERM_DEMAG) t += -0.5f * ms * dot3(mc, bdemag);
+        s = t;
+      }
+      break;
+    }
+    case 13: s = (M.terms & TERM_EXT) ? -1.0f * ms * dot3(mc, lo.ext) : 0.f; break;
+    case 14: s = (M.terms & TERM_DEMAG) ? -0.5f * ms * dot3(mc, bdemag) : 0.f; break;
+    default: break;
+  }
+  if (scalar) out[i] = s;
+  else store3(out, N, i, r);
+}
+
+// ------------------------------------------------------------------ k_xinv
+__global__ void __launch_bounds__(512, 2) k_xinv(const MagnetDev* __restrict__ mags, GroupDev* __restrict__ groups,
+                                              const Work* __restrict__ work, EpiArgs ea,
+                                              const float2* __restrict__ tw) {
+  extern __shared__ float2 sm[];
+  __shared__ MagnetDev M;
+  __shared__ GroupDev G;
+  const Work wk = work[blockIdx.x];
+  if (!load_descs(M, G, mags, groups, wk.mag, ea.gate, ea.stage)) return;
+  const int z = wk.z, y0 = wk.y0, ty = wk.ty;
+  const int nx = M.n[0], ny = M.n[1], nz = M.n[2];
+  const int logL = M.logP[0], L = 1 << logL, cs = plen(L);
+  const int nzrows = (ty + 1) >> 1;
+  const int Fh = M.Fh;
+  float2* rows_z = sm + ty * cs;
+  float2* tws = sm + (ty + nzrows) * cs;  // twiddles of length L
+  load_twiddles(tws, tw, logL);
+  const float2* __restrict__ S = M.spec;
+  const size_t cstride = (size_t)nz * ny;
+  // rebuild full-length Hermitian rows: Z = A + iB
+#pragma unroll 2
+  for (int e = threadIdx.x; e < Fh * 4; e += blockDim.x) {
+    const int yl = e & 3, kx = e >> 2;
+    if (yl >= ty) continue;
+    const size_t base = (size_t)kx * 3 * cstride + (size_t)z * ny + y0 + yl;
+    float2 A = __ldg(S + base), B = __ldg(S + base + cstride);
+    const bool edge = (kx == 0) || (2 * kx == L);
+    if (edge) {
+      A.y = 0.f;
+      B.y = 0.f;
+    }
+    sm[yl * cs + pidx(kx)] = make_float2(A.x - B.y, A.y + B.x);
+    if (kx > 0 && 2 * kx < L) sm[yl * cs + pidx(L - kx)] = make_float2(A.x + B.y, -A.y + B.x);
+    if ((yl & 1) == 0) {
+      float2 C = __ldg(S + base + 2 * cstride);
+      float2 Dv = (yl + 1 < ty) ? __ldg(S + base + 2 * cstride + 1) : make_float2(0.f, 0.f);
+      if (edge) {
+        C.y = 0.f;
+        Dv.y = 0.f;
+      }
+      rows_z[(yl >> 1) * cs + pidx(kx)] = make_float2(C.x - Dv.y, C.y + Dv.x);
+      if (kx > 0 && 2 * kx < L) rows_z[(yl >> 1) * cs + pidx(L - kx)] = make_float2(C.x + Dv.y, -C.y + Dv.x);
+    }
+  }
+  __syncthreads();
+  fft_many<1, 3>(sm, logL, ty + nzrows, cs, tws);
+
+  const float* m = ea.msrc ? ea.msrc : stage_m(M, G, ea.stage);
+  double en = 0.0, tn = 0.0;
+  const int rowbase = nx * (y0 + ny * z);
+  for (int e = threadIdx.x; e < ty * nx; e += blockDim.x) {
+    const int yl = tile_row(e, nx), x = e - yl * nx;
+    const int i = rowbase + e;
+    float3 bd = f3(0, 0, 0);
+    if (in_geom(M, i)) {
+      const float2 hxy = sm[yl * cs + pidx(x)];
+      const float2 hz2 = rows_z[(yl >> 1) * cs + pidx(x)];
+      bd = f3(hxy.x, hxy.y, (yl & 1) ? hz2.y : hz2.x);
+    }
+    double a = 0.0, b = 0.0;
+    epilogue_cell(M, G, ea, m, x, y0 + yl, z, i, bd, a, b);
+    en = (a > en || a != a) ? a : en;
+    tn = fmax(tn, b);
+  }
+  if (ea.fsal_err) block_max2(en, tn, &groups[M.group].err_bits, &groups[M.group].tmax_bits);
+}
+
+// Local terms only (no demag): same tiles, no dynamic shared memory.
+__global__ void __launch_bounds__(256) k_local(const MagnetDev* __restrict__ mags, GroupDev* __restrict__ groups,
+                                               const Work* __restrict__ work, EpiArgs ea) {
+  __shared__ MagnetDev M;
+  __shared__ GroupDev G;
+  const Work wk = work[blockIdx.x];
+  if (!load_descs(M, G, mags, groups, wk.mag, ea.gate, ea.stage)) return;
+  const int nx = M.n[0], ny = M.n[1];
+  const float* m = ea.msrc ? ea.msrc : stage_m(M, G, ea.stage);
+  double en = 0.0, tn = 0.0;
+  const int rowbase = nx * (wk.y0 + ny * wk.z);
+  for (int e = threadIdx.x; e < wk.ty * nx; e += blockDim.x) {
+    const int yl = tile_row(e, nx), x = e - yl * nx;
+    double a = 0.0, b = 0.0;
+    epilogue_cell(M, G, ea, m, x, wk.y0 + yl, wk.z, rowbase + e, f3(0, 0, 0), a, b);
+    en = (a > en || a != a) ? a : en;
+    tn = fmax(tn, b);
+  }
+  if (ea.fsal_err) block_max2(en, tn, &groups[M.group].err_bits, &groups[M.group].tmax_bits);
+}
+
+// Stage combination without a demag pass (writes the stage state xs), or the
+// final combination of a non-FSAL method with its error estimate
+// (core/rungekutta.cpp:123-151).
+__global__ void __launch_bounds__(256) k_combine(const MagnetDev* __restrict__ mags, GroupDev* __restrict__ groups,
+                                                 const Work* __restrict__ work, int stage, int final_b1) {
+  __shared__ MagnetDev M;
+  __shared__ GroupDev G;
+  const Work wk = work[blockIdx.x];
+  if (!load_descs(M, G, mags, groups, wk.mag, 1, 1)) return;
+  const int nx = M.n[0], ny = M.n[1], N = M.N;
+  float* xs = M.buf[G.map[1]];
+  const float* x0 = M.buf[G.map[0]];
+  double en = 0.0;
+  const int rowbase = nx * (wk.y0 + ny * wk.z);
+  for (int e = threadIdx.x; e < wk.ty * nx; e += blockDim.x) {
+    const int i = rowbase + e;
+    if (!in_geom(M, i)) {
+      store3(xs, N, i, load3(x0, N, i));
+      continue;
+    }
+    store3(xs, N, i, combine_cell(M, G, stage, i, final_b1 != 0));
+    if (final_b1 && G.adaptive) {
+      float3 ev = f3(0, 0, 0);
+      for (int j = 0; j < c_tab.S; ++j) {
+        const float cf = (float)(G.dt * (c_tab.b1[j] - c_tab.b2[j]));
+        const float3 kj = load3(M.buf[G.map[2 + j]], N, i);
+        ev = f3(ev.x + cf * kj.x, ev.y + cf * kj.y, ev.z + cf * kj.z);
+      }
+      const double a = sqrt((double)ev.x * ev.x + (double)ev.y * ev.y + (double)ev.z * ev.z);
+      en = (a > en || a != a) ? a : en;
+    }
+  }
+  if (final_b1) block_max2(en, 0.0, &groups[M.group].err_bits, &groups[M.group].tmax_bits);
+}
+
+// --------------------------------------------------------------- controller
+// core/rungekutta.cpp:60-82 and core/timesolver.cpp:60-111, one thread per group,
+// in FP64.  Also runs the run()/steps() state machine on the device.
+__global__ void k_controller(GroupDev* __restrict__ groups, int ngroups) {
+  const int g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= ngroups) return;
+  GroupDev& G = groups[g];
+  if (G.status != GS_RUNNING) return;
+  const double err = __longlong_as_double((long long)G.err_bits);
+  const double tmax = __longlong_as_double((long long)G.tmax_bits);
+  G.err_bits = 0ull;
+  G.tmax_bits = 0ull;
+  G.attempts++;
+  const double dt = G.dt;
+  bool success = true;
+  if (G.adaptive) {
+    success = err < G.max_error;
+    double corr = success ? pow(G.max_error / err, 1.0 / (c_tab.order2 + 1))
+                          : pow(G.max_error / err, 1.0 / (c_tab.order1 + 1));
+    if (isnan(corr)) corr = 1.0;
+    corr *= G.headroom;
+    corr = corr > G.upper ? G.upper : corr;
+    corr = corr < G.lower ? G.lower : corr;
+    G.dt = dt * corr;
+    if (isnan(err)) {  // the reference would retry forever; fail the solve instead
+      G.status = GS_FAILED;
+      G.finished_flag = 1;
+      return;
+    }
+  }
+  if (!success) {
+    G.rejected++;
+    G.k0_valid = 1;
+    return;
+  }
+  // accept: t = t0 + dt; x0 <- x_new; FSAL: k0 <- k_{S-1}
+  G.t += dt;
+  G.steps++;
+  const int t0 = G.map[0];
+  G.map[0] = G.map[1];
+  G.map[1] = t0;
+  if (c_tab.fsal) {
+    const int k0 = G.map[2];
+    G.map[2] = G.map[2 + c_tab.S - 1];
+    G.map[2 + c_tab.S - 1] = k0;
+    G.k0_valid = 1;
+  } else {
+    G.k0_valid = 0;
+  }
+  bool done = false;
+  if (G.phase == 1) {
+    done = true;
+    if (!G.adaptive) G.dt = G.dt_saved;
+  } else if (G.mode == 1) {
+    if (--G.steps_left <= 0) done = true;
+  } else {
+    if (G.torque_stop > 0.0 && c_tab.fsal && tmax / (double)GAMMA_LL < G.torque_stop) {
+      done = true;
+    } else if (!(G.t < G.t_stop - G.dt)) {
+      G.phase = 1;
+      G.dt_saved = G.dt;
+      G.dt = G.t_stop - G.t;
+    }
+  }
+  if (done) {
+    G.status = GS_FINISHED;
+    G.finished_flag = 1;
+    G.phase = 0;
+  }
+}
+
+// ---------------------------------------------------------------- reductions
+// Deterministic two-level reductions over the geometry: block partials in a
+// fixed order, then one block.  op 0: per-component sum, op 1: max |v|.
+__global__ void k_reduce_partial(const float* __restrict__ a, int N, int ncomp,
+                                 const unsigned char* __restrict__ geom, int op, double* partial) {
+  __shared__ double sh[3][256];
+  double acc[3] = {0, 0, 0};
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x) {
+    if (geom && !geom[i]) continue;
+    if (op == 0) {
+      for (int c = 0; c < ncomp; ++c) acc[c] += (double)a[(size_t)c * N + i];
+    } else {
+      double s = 0;
+      for (int c = 0; c < ncomp; ++c) {
+        const double v = a[(size_t)c * N + i];
+        s += v * v;
+      }
+      s = sqrt(s);
+      acc[0] = (s > acc[0] || s != s) ? s : acc[0];
+    }
+  }
+  for (int c = 0; c < 3; ++c) sh[c][threadIdx.x] = acc[c];
+  __syncthreads();
+  for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+    if (threadIdx.x < s)
+      for (int c = 0; c < 3; ++c) {
+        if (op == 0) sh[c][threadIdx.x] += sh[c][threadIdx.x + s];
+        else {
+          const double o = sh[c][threadIdx.x + s];
+          if (o > sh[c][threadIdx.x] || o != o) sh[c][threadIdx.x] = o;
+        }
+      }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0)
+    for (int c = 0; c < 3; ++c) partial[blockIdx.x * 3 + c] = sh[c][0];
+}
+
+__global__ void k_reduce_final(const double* __restrict__ partial, int nblocks, int op, double* out) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  double r[3] = {0, 0, 0};
+  for (int b = 0; b < nblocks; ++b)
+    for (int c = 0; c < 3; ++c) {
+      const double v = partial[b * 3 + c];
+      if (op == 0) r[c] += v;
+      else if (v > r[c] || v != v) r[c] = v;
+    }
+  for (int c = 0; c < 3; ++c) out[c] = r[c];
+}
+
+// Set m: normalise per cell inside the geometry (core/variable.cpp:76-87).
+__global__ void k_normalize_into(float* dst, const float* __restrict__ src, int N,
+                                 const unsigned char* __restrict__ geom) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= N) return;
+  float x = src[i], y = src[N + i], z = src[2 * N + i];
+  if (!geom || geom[i]) {
+    const float inv = rsqrtf(x * x + y * y + z * z);
+    x *= inv;
+    y *= inv;
+    z *= inv;
+  }
+  dst[i] = x;
+  dst[N + i] = y;
+  dst[2 * N + i] = z;
+}
+
+}  // namespace mpx

@@ -1,0 +1,274 @@
+// physics.cuh -- device-side magnet description and the local effective-field
+// terms (exchange, DMI, uniaxial anisotropy, Zeeman) plus the LLG torque.
+//
+// Each term follows the reference kernel cell by cell (paths relative to the
+// mumax-plus source tree):
+//   exchange   physics/exchange.cu:20-104  (harmonic-mean A, inter-region LUT,
+//              Neumann ghost m + Gamma/(2A) delta, open boundaries)
+//   DMI        physics/dmi.cu:19-110, getGamma physics/dmi.hpp:53-69
+//   anisotropy physics/anisotropy.cu:25-55 (uniaxial)
+//   Zeeman     physics/zeeman.cu:53-91 (world bias + magnet bias)
+//   torque     physics/torque.cu:21-45 (LLG), :58-77 (damping only)
+// Grid indexing and wrapping: core/grid.hpp:55-89, core/system.hpp:91-119.
+// The terms are evaluated from SoA float32 m with FP32 arithmetic, like the
+// reference SINGLE build, and summed in the order of
+// physics/effectivefield.cpp:15-28 (exchange, anisotropy, external, DMI, demag).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace mpx {
+
+constexpr float GAMMA_LL = 1.7595e11f;     // rad/(T s), physics/constants.hpp
+constexpr double MU0_D = 1.25663706212e-6; // H/m
+
+// Term bits of a magnet (a term whose parameters are assured zero is skipped,
+// as the reference's *AssuredZero checks do).
+enum : unsigned {
+  TERM_EXCH = 1u, TERM_DMI = 2u, TERM_ANIS = 4u, TERM_EXT = 8u, TERM_DEMAG = 16u,
+  FLAG_OPENBC = 256u, FLAG_MAGNET_BIAS = 512u
+};
+
+struct DScalar {  // uniform value or per-cell array
+  float u;
+  const float* __restrict__ p;
+  __device__ __forceinline__ float at(int i) const { return p ? __ldg(p + i) : u; }
+};
+struct DVector {  // uniform value or per-cell SoA array (3*N)
+  float u[3];
+  const float* __restrict__ p;
+  __device__ __forceinline__ float3 at(int i, int N) const {
+    if (!p) return make_float3(u[0], u[1], u[2]);
+    return make_float3(__ldg(p + i), __ldg(p + N + i), __ldg(p + 2 * N + i));
+  }
+};
+
+// Device description of one magnet (lives in a device array, indexed by slot).
+struct MagnetDev {
+  int n[3], N;
+  int o[3];          // grid origin
+  int mg[3], mgo[3]; // mastergrid size / origin (size 0: no wrap)
+  float cs[3];       // cell size
+  float w[3];        // 1/cellsize^2
+  const unsigned char* __restrict__ geom;  // NULL: all cells in geometry
+  const unsigned* __restrict__ reg;        // NULL: region 0
+  DScalar msat, aex, alpha, ku1, ku2, frozen;
+  DVector anisU, bias;
+  DScalar dmi[9];  // xxy, xxz, xyz, yxy, yxz, yyz, zxy, zxz, zyz
+  float inter_u, scale_u;
+  const float* __restrict__ inter_lut;
+  const float* __restrict__ scale_lut;
+  float wb[3];       // world bias field
+  unsigned terms;    // TERM_* and FLAG_* bits
+  int group;         // solve group slot
+  // demag FFT plan: padded sizes P = 2^logP, Fh = Px/2+1
+  int logP[3], P[3], Fh;
+  int kcomp;         // 6 (3-D kernel) or 4 (Pz == 1)
+  float2* spec;      // spectrum S[kx][c][z][y]
+  const float* __restrict__ kspec;  // kernel spectrum [kx][kz'][kcomp][ky']
+  float* buf[9];     // field buffers (3N floats each); roles given by the group map
+};
+
+// Solve-group state (time integration); lives in a device array.
+struct GroupDev {
+  double t, dt, t_stop, dt_saved, max_error, headroom, lower, upper, torque_stop;
+  unsigned long long err_bits;   // max error of the current attempt (double bits)
+  unsigned long long tmax_bits;  // max |torque| of the accepted state (double bits)
+  long long steps, rejected, attempts, steps_left;
+  int status;     // 0 idle, 1 running, 2 finished, 3 failed
+  int mode;       // 0 run(duration), 1 steps(n)
+  int phase;      // 0 regular steps, 1 final step of run()
+  int adaptive;
+  int k0_valid;
+  int finished_flag;  // set when the group finished, cleared by the host poll
+  int map[9];     // buffer roles: [0] x0 (state), [1] xs (stage / new state), [2+s] k_s
+};
+
+enum { GS_IDLE = 0, GS_RUNNING = 1, GS_FINISHED = 2, GS_FAILED = 3 };
+
+__device__ __forceinline__ float harmonic_mean(float a, float b) {  // core/datatypes.hpp
+  if (a + b == 0.0f) return 0.0f;
+  if (a == b) return a;
+  return 2 * a * b / (a + b);
+}
+
+__device__ __forceinline__ float3 f3(float x, float y, float z) { return make_float3(x, y, z); }
+__device__ __forceinline__ float3 operator+(float3 a, float3 b) { return f3(a.x + b.x, a.y + b.y, a.z + b.z); }
+__device__ __forceinline__ float3 operator-(float3 a, float3 b) { return f3(a.x - b.x, a.y - b.y, a.z - b.z); }
+__device__ __forceinline__ float3 operator*(float s, float3 a) { return f3(s * a.x, s * a.y, s * a.z); }
+__device__ __forceinline__ float3 operator/(float3 a, float s) { return f3(a.x / s, a.y / s, a.z / s); }
+__device__ __forceinline__ float dot3(float3 a, float3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+__device__ __forceinline__ float3 cross3(float3 a, float3 b) {
+  return f3(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x);
+}
+
+__device__ __forceinline__ bool in_geom(const MagnetDev& M, int i) { return !M.geom || M.geom[i]; }
+
+__device__ __forceinline__ float3 load3(const float* __restrict__ a, int N, int i) {
+  return f3(a[i], a[N + i], a[2 * N + i]);
+}
+// read-only path: for buffers a kernel never writes
+__device__ __forceinline__ float3 ldg3(const float* __restrict__ a, int N, int i) {
+  return f3(__ldg(a + i), __ldg(a + N + i), __ldg(a + 2 * N + i));
+}
+__device__ __forceinline__ void store3(float* a, int N, int i, float3 v) {
+  a[i] = v.x;
+  a[N + i] = v.y;
+  a[2 * N + i] = v.z;
+}
+
+// Neighbour coordinate along one axis after the mastergrid wrap
+// (core/grid.hpp:73-81); -1 when it leaves the grid.  The grid lies inside the
+// mastergrid, so one conditional wrap suffices.
+__device__ __forceinline__ int nb_coord(int c, int d, int n, int go, int mg, int mgo) {
+  int g = c + d + go;
+  if (mg > 0) {
+    int r = g - mgo;
+    r = r < 0 ? r + mg : (r >= mg ? r - mg : r);
+    g = mgo + r;
+  }
+  const int l = g - go;
+  return (l >= 0 && l < n) ? l : -1;
+}
+
+// physics/dmi.hpp:53-69 getGamma with normal (nx, ny, nz)
+__device__ __forceinline__ float3 get_gamma(const MagnetDev& M, int i, int nx, int ny, int nz, float3 m) {
+  const float Dxxy = M.dmi[0].at(i), Dxxz = M.dmi[1].at(i), Dxyz = M.dmi[2].at(i);
+  const float Dyxy = M.dmi[3].at(i), Dyxz = M.dmi[4].at(i), Dyyz = M.dmi[5].at(i);
+  const float Dzxy = M.dmi[6].at(i), Dzxz = M.dmi[7].at(i), Dzyz = M.dmi[8].at(i);
+  return f3(-Dxxy * nx * m.y - Dxxz * nx * m.z - Dyxz * ny * m.z - Dzxy * nz * m.y - Dyxy * ny * m.y -
+                Dzxz * nz * m.z,
+            Dxxy * nx * m.x - Dzyz * nz * m.z + Dyxy * ny * m.x - Dxyz * nx * m.z + Dzxy * nz * m.x -
+                Dyyz * ny * m.z,
+            Dxxz * nx * m.x + Dyyz * ny * m.y + Dxyz * nx * m.y + Dyxz * ny * m.x + Dzxz * nz * m.x +
+                Dzyz * nz * m.y);
+}
+
+__device__ __forceinline__ float lut_value(const float* __restrict__ lut, float u, unsigned i, unsigned j) {
+  if (!lut) return u;
+  const int k = (i > j) ? (int)(i * (i - 1) / 2 + j) : (int)(j * (j - 1) / 2 + i);
+  return __ldg(lut + k);
+}
+
+// The local terms of the effective field of cell (x, y, z) = i, which is in the
+// geometry with msat != 0.  `mask` selects terms (TERM_*).  Each term is
+// computed on its own, then added in the reference's order.
+struct LocalOut {
+  float3 exch, anis, ext, dmi;
+};
+
+__device__ __forceinline__ LocalOut local_terms(const MagnetDev& M, const float* __restrict__ m, int x, int y,
+                                                int z, int i, float3 mc, unsigned mask) {
+  LocalOut o;
+  o.exch = o.anis = o.ext = o.dmi = f3(0, 0, 0);
+  const int N = M.N;
+  const float ms = M.msat.at(i);
+  const bool openbc = (M.terms & FLAG_OPENBC) != 0;
+  const bool do_exch = (mask & TERM_EXCH) && (M.terms & TERM_EXCH);
+  const bool do_dmi = (mask & TERM_DMI) && (M.terms & TERM_DMI);
+  if (do_exch || do_dmi) {
+    const float a = M.aex.at(i);
+    const bool dmi_open = (a == 0.0f) ? true : openbc;
+    float3 he = f3(0, 0, 0), hd = f3(0, 0, 0);
+#pragma unroll
+    for (int r = 0; r < 6; ++r) {
+      const int axis = r >> 1;
+      const int d = (r & 1) ? 1 : -1;
+      int xx = x, yy = y, zz = z;
+      int nc;
+      if (axis == 0) { nc = nb_coord(x, d, M.n[0], M.o[0], M.mg[0], M.mgo[0]); xx = nc; }
+      else if (axis == 1) { nc = nb_coord(y, d, M.n[1], M.o[1], M.mg[1], M.mgo[1]); yy = nc; }
+      else { nc = nb_coord(z, d, M.n[2], M.o[2], M.mg[2], M.mgo[2]); zz = nc; }
+      const int j = (nc >= 0) ? xx + M.n[0] * (yy + M.n[1] * zz) : -1;
+      const bool nin = (nc >= 0) && in_geom(M, j);
+      const float delta = d * M.cs[axis];
+      const int nx_ = axis == 0, ny_ = axis == 1, nz_ = axis == 2;
+      // ---- exchange (physics/exchange.cu:58-102)
+      if (do_exch) {
+        bool skip = (!nin && openbc) || (openbc && M.msat.at(j) == 0.0f);
+        if (!skip) {
+          float inter = 0.0f, scale = 1.0f, a_;
+          float3 m_;
+          bool neumann_skip = false;
+          if (nin) {
+            m_ = ldg3(m, N, j);
+            a_ = M.aex.at(j);
+            const unsigned ri = M.reg ? M.reg[i] : 0u, rj = M.reg ? M.reg[j] : 0u;
+            if (ri != rj) {
+              scale = lut_value(M.scale_lut, M.scale_u, ri, rj);
+              inter = lut_value(M.inter_lut, M.inter_u, ri, rj);
+            }
+          } else {
+            if (a == 0.0f) {
+              neumann_skip = true;
+              m_ = mc;
+              a_ = a;
+            } else {
+              const float3 G = get_gamma(M, i, nx_, ny_, nz_, mc);
+              m_ = mc + delta * (G / (2 * a));
+              a_ = a;
+            }
+          }
+          if (!neumann_skip) {
+            float A = (inter != 0.0f) ? inter : harmonic_mean(a, a_);
+            A *= scale;
+            he = he + (2 * A * M.w[axis]) * (m_ - mc);
+          }
+        }
+      }
+      // ---- DMI (physics/dmi.cu:46-106)
+      if (do_dmi) {
+        const int jj = nin ? j : i;
+        const bool skip = dmi_open && (!nin || M.msat.at(jj) == 0.0f);
+        if (!skip) {
+          const int c0 = 3 * axis;  // x: xxy,xxz,xyz ; y: yxy,yxz,yyz ; z: zxy,zxz,zyz
+          float Dxy, Dxz, Dyz;
+          if (jj == i) {
+            Dxy = M.dmi[c0].at(i); Dxz = M.dmi[c0 + 1].at(i); Dyz = M.dmi[c0 + 2].at(i);
+          } else {
+            Dxy = harmonic_mean(M.dmi[c0].at(i), M.dmi[c0].at(jj));
+            Dxz = harmonic_mean(M.dmi[c0 + 1].at(i), M.dmi[c0 + 1].at(jj));
+            Dyz = harmonic_mean(M.dmi[c0 + 2].at(i), M.dmi[c0 + 2].at(jj));
+          }
+          const float Dzx = -Dxz, Dyx = -Dxy, Dzy = -Dyz;
+          float3 m_;
+          if (!nin && !dmi_open) {
+            const float3 G = get_gamma(M, i, nx_, ny_, nz_, mc);
+            m_ = mc + delta * (G / (2 * a));
+          } else {
+            m_ = ldg3(m, N, jj);
+          }
+          hd.x += (Dxy * m_.y + Dxz * m_.z) / delta;
+          hd.y += (Dyx * m_.x + Dyz * m_.z) / delta;
+          hd.z += (Dzx * m_.x + Dzy * m_.y) / delta;
+        }
+      }
+    }
+    if (do_exch) o.exch = he / ms;
+    if (do_dmi) o.dmi = hd / ms;
+  }
+  if ((mask & TERM_ANIS) && (M.terms & TERM_ANIS)) {  // physics/anisotropy.cu:45-54
+    float3 u = M.anisU.at(i, N);
+    const float nu = sqrtf(dot3(u, u));
+    const float s = (nu == 0.0f) ? 0.0f : 1.0f / nu;
+    u = s * u;
+    const float k1 = M.ku1.at(i), k2 = M.ku2.at(i);
+    const float mu = dot3(mc, u);
+    o.anis = ((2 * k1 * mu + 4 * k2 * mu * mu * mu) * u) / ms;
+  }
+  if ((mask & TERM_EXT) && (M.terms & TERM_EXT)) {  // physics/zeeman.cu:64-68
+    float3 b = f3(M.wb[0], M.wb[1], M.wb[2]);
+    if (M.terms & FLAG_MAGNET_BIAS) b = b + M.bias.at(i, N);
+    o.ext = b;
+  }
+  return o;
+}
+
+// physics/torque.cu:36-42
+__device__ __forceinline__ float3 llg_torque(float3 m, float3 h, float a) {
+  const float3 mxh = cross3(m, h);
+  const float3 mxmxh = cross3(m, mxh);
+  return (-GAMMA_LL / (1 + a * a)) * (mxh + a * mxmxh);
+}
+
+}  // namespace mpx

@@ -1,0 +1,182 @@
+"""World (mirror of mumaxplus/world.py; core/world.cpp, physics/mumaxworld.cpp).
+
+A World owns one engine (one CUDA stream on one GPU) and one solve group: all
+its magnets share the time and time step of the world's TimeSolver.
+"""
+import warnings
+
+from ._engine import Engine
+from .grid import Grid
+from .timesolver import TimeSolver
+
+
+class World:
+    """A world with a given cell size, optional periodic box (mastergrid) and
+    demag image repetitions (pbc_repetitions)."""
+
+    def __init__(self, cellsize, pbc_repetitions=(0, 0, 0), mastergrid=Grid((0, 0, 0)), device=None):
+        if len(cellsize) != 3:
+            raise ValueError("'cellsize' should have three dimensions.")
+        if len(pbc_repetitions) != 3:
+            raise ValueError("'pbc_repetitions' should have three dimensions.")
+        if not all(isinstance(item, int) for item in pbc_repetitions):
+            raise ValueError("All elements of `pbc_repetitions` must be integers.")
+        if any(c <= 0 for c in cellsize):
+            raise ValueError("The cell size should be larger than 0")
+        self._cellsize = tuple(float(c) for c in cellsize)
+        self._check_pbc(mastergrid, pbc_repetitions)
+        self._pbc = tuple(int(p) for p in pbc_repetitions)
+        self._mastergrid = Grid(mastergrid.size, mastergrid.origin)
+        self._engine = Engine(device)
+        self._group = self._engine.group_create()
+        self._magnets = {}
+        self._bias = (0.0, 0.0, 0.0)
+        self._unnamed = 1
+        self._timesolver = TimeSolver(self)
+
+    def __repr__(self):
+        return f"World(cellsize={self.cellsize})"
+
+    # ------------------------------------------------------------- internals
+    @staticmethod
+    def _check_pbc(mastergrid, pbc):
+        """core/world.cpp checkPbcRepetitions / checkPbcCompatibility"""
+        if any(p < 0 for p in pbc):
+            raise ValueError("Number of pbcRepetitions should not be negative.")
+        for a in range(3):
+            if (mastergrid.size[a] == 0) != (pbc[a] == 0):
+                raise ValueError("0 in size of mastergrid should match 0 in pbcRepetitions.")
+
+    def _in_mastergrid(self, grid):
+        mg = self._mastergrid
+        for a in range(3):
+            if mg.size[a] > 0:
+                d1 = grid.origin[a] - mg.origin[a]
+                d2 = d1 + grid.size[a] - mg.size[a]
+                if d1 < 0 or d2 > 0:
+                    return False
+        return True
+
+    def _check_addibility(self, grid, name):
+        """physics/mumaxworld.cpp:35-55"""
+        if not self._in_mastergrid(grid):
+            raise IndexError("Can not add magnet because the grid does not fit in the mastergrid ")
+        for m in self._magnets.values():
+            if grid.overlaps(m.grid):
+                raise IndexError("Can not add magnet because it overlaps with another magnet.")
+        if name and name in self._magnets:
+            raise RuntimeError(f"A magnet with the name '{name}' already exists")
+
+    def _next_name(self):
+        name = f"ferromagnet_{self._unnamed}"
+        self._unnamed += 1
+        return name
+
+    def _register(self, magnet):
+        if self._magnets:
+            warnings.warn("stray fields between different magnets of one world are not included "
+                          "(each magnet only feels its own demag field)", UserWarning, stacklevel=3)
+        self._magnets[magnet.name] = magnet
+
+    def _update_all(self):
+        for m in self._magnets.values():
+            m._update()
+
+    # ------------------------------------------------------------- API
+    @property
+    def timesolver(self):
+        return self._timesolver
+
+    @property
+    def cellsize(self):
+        return self._cellsize
+
+    @property
+    def bias_magnetic_field(self):
+        return self._bias
+
+    @bias_magnetic_field.setter
+    def bias_magnetic_field(self, value):
+        v = tuple(float(x) for x in value)
+        if len(v) != 3:
+            raise ValueError("the bias field needs three components")
+        self._bias = v
+        self._engine.set_world_bias(v)
+
+    @property
+    def ferromagnets(self):
+        return dict(self._magnets)
+
+    def get_ferromagnet(self, name):
+        if name not in self._magnets:
+            raise KeyError(f"No magnet named {name}")
+        return self._magnets[name]
+
+    @property
+    def mastergrid(self):
+        return self._mastergrid
+
+    @mastergrid.setter
+    def mastergrid(self, mastergrid):
+        self._check_pbc(mastergrid, self._pbc)
+        self._mastergrid = Grid(mastergrid.size, mastergrid.origin)
+        self._check_all_in_mastergrid()
+        self._update_all()
+
+    @property
+    def pbc_repetitions(self):
+        return self._pbc
+
+    @pbc_repetitions.setter
+    def pbc_repetitions(self, value):
+        if len(value) != 3:
+            raise ValueError("'pbc_repetitions' should have three dimensions.")
+        if not all(isinstance(item, int) for item in value):
+            raise ValueError("All elements of `pbc_repetitions` must be integers.")
+        self._check_pbc(self._mastergrid, value)
+        self._pbc = tuple(value)
+        self._update_all()
+
+    def _check_all_in_mastergrid(self):
+        for m in self._magnets.values():
+            if not self._in_mastergrid(m.grid):
+                raise IndexError("Not all magnets of the world fit inside the mastergrid.")
+
+    @property
+    def bounding_grid(self):
+        """Smallest grid containing all magnets (physics/mumaxworld.cpp boundingGrid)."""
+        if not self._magnets:
+            raise IndexError("Cannot find minimum bounding box if there are no magnets in the world.")
+        grids = [m.grid for m in self._magnets.values()]
+        lo = [min(g.origin[a] for g in grids) for a in range(3)]
+        hi = [max(g.origin[a] + g.size[a] for g in grids) for a in range(3)]
+        return Grid([hi[a] - lo[a] for a in range(3)], lo)
+
+    def set_pbc(self, pbc_repetitions, mastergrid=None):
+        """Set the periodic boundary conditions (physics/mumaxworld.cpp setPBC)."""
+        if len(pbc_repetitions) != 3:
+            raise ValueError("'pbc_repetitions' should have three dimensions.")
+        if not all(isinstance(item, int) for item in pbc_repetitions):
+            raise ValueError("All elements of `pbc_repetitions` must be integers.")
+        if any(p < 0 for p in pbc_repetitions):
+            raise ValueError("Number of pbcRepetitions should not be negative.")
+        if mastergrid is None:
+            bg = self.bounding_grid
+            size = [bg.size[a] if pbc_repetitions[a] != 0 else 0 for a in range(3)]
+            mastergrid = Grid(size, bg.origin)
+        self._check_pbc(mastergrid, pbc_repetitions)
+        self._pbc = tuple(int(p) for p in pbc_repetitions)
+        self._mastergrid = Grid(mastergrid.size, mastergrid.origin)
+        self._check_all_in_mastergrid()
+        self._update_all()
+
+    def unset_pbc(self):
+        self._pbc = (0, 0, 0)
+        self._mastergrid = Grid((0, 0, 0))
+        self._update_all()
+
+    def relax(self, tol=1e-9):
+        raise NotImplementedError("relax() is not implemented on the accelerated path yet")
+
+    def minimize(self, tol=1e-6, nsamples=10):
+        raise NotImplementedError("minimize() is not implemented on the accelerated path yet")

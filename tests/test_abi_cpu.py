@@ -1,0 +1,179 @@
+"""CPU checks of the C ABI and the host-side logic (no GPU, no compute calls)."""
+import ctypes as C
+import os
+import subprocess
+import tempfile
+
+import numpy as np
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+LIB = os.path.join(ROOT, "mumax-plus_b200", "libmpx.so")
+
+
+@pytest.fixture(scope="module")
+def built_lib():
+    import importlib.util
+
+    spec = importlib.util.spec_from_file_location("_mpx_build", os.path.join(ROOT, "mumax-plus_b200", "build.py"))
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod.build()
+
+
+def test_library_exports_every_header_symbol(built_lib):
+    import mumaxplus_b200 as mpx
+
+    names = mpx._abi.header_symbols()
+    assert len(names) >= 30
+    lib = C.CDLL(built_lib)
+    missing = [n for n in names if not hasattr(lib, n)]
+    assert not missing, missing
+    # the ctypes signature table covers the whole header
+    assert sorted(mpx._abi.SIGNATURES) == names
+
+
+def test_device_count_without_gpu_is_safe(built_lib):
+    lib = C.CDLL(built_lib)
+    n = lib.mpx_device_count()
+    assert n >= 0
+    lib.mpx_version.restype = C.c_char_p
+    assert b"sm_100a" in lib.mpx_version()
+
+
+def test_engine_create_fails_loudly_without_device(built_lib):
+    lib = C.CDLL(built_lib)
+    if lib.mpx_device_count() > 0:
+        pytest.skip("a device is present")
+    h = C.c_void_p()
+    st = lib.mpx_engine_create(0, C.byref(h))
+    assert st == 8  # MPX_ERR_NODEVICE
+    import mumaxplus_b200 as mpx
+
+    with pytest.raises(RuntimeError, match="no CUDA device"):
+        mpx.World((1e-9, 1e-9, 1e-9))
+
+
+LAYOUT_C = r"""
+#include <stdio.h>
+#include <stddef.h>
+#include "mpx.h"
+#define P(T, f) printf(#T "." #f " %zu\n", offsetof(T, f));
+int main(void) {
+  printf("mpx_magnet_desc %zu\n", sizeof(mpx_magnet_desc));
+  printf("mpx_solver_params %zu\n", sizeof(mpx_solver_params));
+  printf("mpx_group_info %zu\n", sizeof(mpx_group_info));
+  P(mpx_magnet_desc, geometry) P(mpx_magnet_desc, regions) P(mpx_magnet_desc, msat)
+  P(mpx_magnet_desc, anis_u) P(mpx_magnet_desc, bias_magnetic_field) P(mpx_magnet_desc, dmi)
+  P(mpx_magnet_desc, lut_regions) P(mpx_magnet_desc, scale_exchange_lut) P(mpx_magnet_desc, enable_openbc)
+  P(mpx_solver_params, max_error) P(mpx_solver_params, sensible_timestep_default)
+  P(mpx_group_info, status) P(mpx_group_info, max_torque)
+  return 0;
+}
+"""
+
+
+def test_ctypes_struct_layout_matches_header():
+    import mumaxplus_b200 as mpx
+
+    abi = mpx._abi
+    with tempfile.TemporaryDirectory() as d:
+        src = os.path.join(d, "layout.c")
+        exe = os.path.join(d, "layout")
+        open(src, "w").write(LAYOUT_C)
+        subprocess.run(["gcc", "-I", os.path.join(ROOT, "include"), src, "-o", exe], check=True)
+        out = subprocess.run([exe], capture_output=True, text=True, check=True).stdout
+    got = dict(line.rsplit(" ", 1) for line in out.strip().splitlines())
+    got = {k: int(v) for k, v in got.items()}
+    assert got["mpx_magnet_desc"] == C.sizeof(abi.MagnetDesc)
+    assert got["mpx_solver_params"] == C.sizeof(abi.SolverParams)
+    assert got["mpx_group_info"] == C.sizeof(abi.GroupInfo)
+    types = {"mpx_magnet_desc": abi.MagnetDesc, "mpx_solver_params": abi.SolverParams,
+             "mpx_group_info": abi.GroupInfo}
+    for key, off in got.items():
+        if "." in key:
+            t, f = key.split(".")
+            assert getattr(types[t], f).offset == off, key
+
+
+class _FakeMagnet:
+    """Stand-in owner for host-side Parameter tests."""
+
+    def __init__(self, size=(4, 3, 2)):
+        import mumaxplus_b200 as mpx
+
+        self.grid = mpx.Grid(size)
+        self.name = "fake"
+        self._regions = None
+        self.changes = 0
+        nx, ny, nz = size
+        idx = np.flip(np.mgrid[0:nz, 0:ny, 0:nx], axis=0)
+        self.meshgrid = np.array([idx[c] * 1e-9 for c in range(3)])
+
+    def _geometry_mask(self):
+        return None
+
+    def touch(self):
+        self.changes += 1
+
+
+def test_parameter_set_semantics():
+    import mumaxplus_b200 as mpx
+
+    fm = _FakeMagnet()
+    p = mpx.Parameter(fm, "msat", "A/m", 1, 1.0, fm.touch)
+    assert p.is_uniform and p.uniform_value == 1.0
+    p.set(8e5)
+    assert p.eval().shape == (1, 2, 3, 4) and np.all(p.eval() == 8e5)
+    arr = np.arange(24, dtype=np.float32).reshape(2, 3, 4)
+    p.set(arr)
+    assert not p.is_uniform and np.array_equal(p.eval()[0], arr)
+    p.set(lambda x, y, z: x * 1e9)  # function of position
+    assert p.eval()[0, 0, 0, 3] == pytest.approx(3.0)
+    with pytest.raises(NotImplementedError):
+        p.set(lambda t: 1.0)  # time-dependent term
+    with pytest.raises(ValueError):
+        p.set(np.zeros((3, 3, 3), np.float32))
+    v = mpx.Parameter(fm, "anisU", "", 3, (0, 0, 0), fm.touch)
+    v.set((0, 0, 1))
+    assert v.eval()[2].min() == 1.0
+    assert fm.changes == 4
+
+
+def test_interparameter_lut_index():
+    import mumaxplus_b200 as mpx
+
+    fm = _FakeMagnet()
+    fm._regions = np.array([0, 1, 2, 3], dtype=np.uint32)
+    ip = mpx.InterParameter(fm, "inter_exchange", "J/m", 0.0, fm.touch)
+    ip.set_between(3, 1, 7.0)
+    ip.set_between(0, 2, 5.0)
+    lut = ip._lut()
+    # core/inter_parameter.hpp getLutIndex: i(i-1)/2 + j for i > j
+    assert lut[3 * 2 // 2 + 1] == 7.0
+    assert lut[2 * 1 // 2 + 0] == 5.0
+    assert ip.get_between(1, 3) == 7.0 and ip.get_between(1, 2) == 0.0
+
+
+def test_dmi_tensor_helpers():
+    import mumaxplus_b200 as mpx
+
+    fm = _FakeMagnet()
+    t = mpx.DmiTensor(fm, fm.touch)
+    t.set_interfacial_dmi(3e-3)
+    assert t.xxz.uniform_value == 3e-3 and t.yyz.uniform_value == 3e-3 and t.xyz.uniform_value == 0
+    t.set_bulk_dmi(2e-3)
+    assert t.xyz.uniform_value == 2e-3 and t.yxz.uniform_value == -2e-3 and t.zxy.uniform_value == 2e-3
+    assert t.xxz.uniform_value == 0
+
+
+def test_grid_semantics():
+    import mumaxplus_b200 as mpx
+
+    g = mpx.Grid((4, 5, 6), (1, 2, 3))
+    assert g.shape == (6, 5, 4) and g.ncells == 120
+    assert g == mpx.Grid((4, 5, 6), (1, 2, 3)) and g != mpx.Grid((4, 5, 6))
+    assert g.overlaps(mpx.Grid((2, 2, 2), (4, 6, 8)))
+    assert not g.overlaps(mpx.Grid((2, 2, 2), (5, 2, 3)))
+    with pytest.raises(ValueError):
+        mpx.Grid((1, 2))

@@ -1,0 +1,311 @@
+"""GPU parity: the sm_100a engine (through the mumaxplus-style Python API and the
+C ABI) against the CPU FP64 oracle on identical seeded float32 inputs.
+
+Tolerances: fields |dB|max / |B|max <= 1e-5 (the FP32 bound stated for B_eff);
+<m>(t) trajectories <= 1e-4 absolute; the analytic macrospin test keeps the
+reference's own 1e-4 (test/test_timesolver.py:120-122).
+"""
+import numpy as np
+import pytest
+
+import oracle as O
+from spec import MagnetSpec, max_rel, random_m
+
+abi = O.abi
+pytestmark = pytest.mark.gpu
+GAMMALL = 1.7595e11
+
+FIELD_TOL = 1e-5
+
+LOCAL_QUANTITIES = [abi.Q_EXCHANGE_FIELD, abi.Q_DMI_FIELD, abi.Q_ANISOTROPY_FIELD, abi.Q_EXTERNAL_FIELD]
+
+
+def compare(spec, mpx, quantities, seed=1, smooth=2, tol=FIELD_TOL):
+    m0 = random_m(spec.shape, seed=seed, smooth=smooth)
+    ow, q = spec.oracle_world(m0)
+    world, magnet = spec.product(mpx, m0)
+    eng = magnet._engine
+    worst = {}
+    for quantity in quantities:
+        nc = 1 if quantity >= abi.Q_EXCHANGE_ENERGY_DENSITY else 3
+        got = eng.eval(magnet._id, quantity, (nc, *spec.shape))
+        want = ow.eval(q, quantity)
+        if np.max(np.abs(want)) == 0:
+            assert np.max(np.abs(got)) == 0, f"quantity {quantity} should be zero"
+            continue
+        err = max_rel(got, want)
+        worst[quantity] = err
+        assert err < tol, f"quantity {quantity}: rel err {err:.3e}"
+    return worst
+
+
+def test_library_loads_and_sees_device(mpx):
+    lib = mpx._abi.load()
+    assert lib.mpx_device_count() >= 1
+
+
+def test_exchange_neumann(mpx):
+    compare(MagnetSpec(size=(16, 16, 4), cellsize=(1e-9, 2e-9, 3e-9), aex=1.3e-11, msat=8e5, enable_demag=False),
+            mpx, [abi.Q_EXCHANGE_FIELD])
+
+
+def test_exchange_openbc_and_pbc_wrap(mpx):
+    s = MagnetSpec(size=(24, 12, 3), cellsize=(2e-9, 2e-9, 1e-9), aex=1.5e-11, msat=5.8e5,
+                   mastergrid_size=(24, 12, 0), pbc=(1, 1, 0), enable_demag=False)
+    compare(s, mpx, [abi.Q_EXCHANGE_FIELD])
+    s.enable_openbc = True
+    compare(s, mpx, [abi.Q_EXCHANGE_FIELD])
+
+
+def test_exchange_mastergrid_larger_than_grid(mpx):
+    # wrapped neighbours that land outside the magnet take the Neumann ghost
+    s = MagnetSpec(size=(10, 8, 2), origin=(3, 2, 0), cellsize=(1e-9, 1e-9, 1e-9), aex=1e-11, msat=6e5,
+                   mastergrid_size=(14, 8, 0), mastergrid_origin=(1, 2, 0), pbc=(1, 1, 0),
+                   dmi={"xxz": 2e-3, "yyz": 2e-3}, enable_demag=False)
+    compare(s, mpx, [abi.Q_EXCHANGE_FIELD, abi.Q_DMI_FIELD])
+
+
+@pytest.mark.parametrize("openbc", [False, True])
+def test_interfacial_dmi(mpx, openbc):
+    s = MagnetSpec(size=(20, 12, 3), cellsize=(1.1e-9, 2e-9, 3.2e-9), msat=6e5, aex=1e-11,
+                   dmi={"xxz": 3e-3, "yyz": 3e-3}, enable_openbc=openbc, enable_demag=False)
+    compare(s, mpx, [abi.Q_DMI_FIELD, abi.Q_EXCHANGE_FIELD])
+
+
+def test_general_dmi_tensor_per_cell(mpx):
+    shape = (3, 9, 13)
+    rng = np.random.default_rng(4)
+    dmi = {k: (rng.uniform(0.5e-3, 3e-3, shape).astype(np.float32) if i % 2 == 0 else float(rng.uniform(-2e-3, 2e-3)))
+           for i, k in enumerate(abi.DMI_ORDER)}
+    s = MagnetSpec(size=(13, 9, 3), cellsize=(1e-9, 1.5e-9, 2e-9), msat=7e5, aex=1.2e-11, dmi=dmi,
+                   enable_demag=False)
+    compare(s, mpx, [abi.Q_DMI_FIELD, abi.Q_EXCHANGE_FIELD])
+
+
+def test_anisotropy_zeeman_per_cell(mpx):
+    shape = (2, 6, 10)
+    rng = np.random.default_rng(5)
+    u = rng.standard_normal((3, *shape)).astype(np.float32)
+    bias = (rng.standard_normal((3, *shape)) * 0.05).astype(np.float32)
+    s = MagnetSpec(size=(10, 6, 2), msat=rng.uniform(3e5, 9e5, shape).astype(np.float32),
+                   ku1=rng.uniform(1e5, 8e5, shape).astype(np.float32), ku2=2e4, anisU=u, bias=bias,
+                   world_bias=(0.01, -0.02, 0.03), enable_demag=False)
+    compare(s, mpx, [abi.Q_ANISOTROPY_FIELD, abi.Q_EXTERNAL_FIELD, abi.Q_ANISOTROPY_ENERGY_DENSITY,
+                     abi.Q_ZEEMAN_ENERGY_DENSITY])
+
+
+def test_geometry_regions_lut_frozen(mpx):
+    shape = (2, 10, 12)
+    geom = np.ones(shape, dtype=bool)
+    geom[:, 4:7, 5:9] = False
+    geom[1, 0, :] = False
+    regions = np.zeros(shape, dtype=np.uint32)
+    regions[:, :, 6:] = 1
+    regions[1] = 2
+    frozen = np.zeros(shape, np.float32)
+    frozen[0, 2, 3] = 1
+    msat = np.full(shape, 8e5, np.float32)
+    msat[0, 8, 8] = 0.0
+    s = MagnetSpec(size=(12, 10, 2), cellsize=(2e-9, 2e-9, 1e-9), geometry=geom, regions=regions, msat=msat,
+                   aex=1.3e-11, alpha=0.1, dmi={"xxz": 1e-3, "yyz": 1e-3}, frozen=frozen,
+                   inter_pairs={(1, 0): 5e-12}, scale_pairs={(2, 1): 0.5}, world_bias=(0, 0, 0.1))
+    compare(s, mpx, [abi.Q_EXCHANGE_FIELD, abi.Q_DMI_FIELD, abi.Q_EXTERNAL_FIELD, abi.Q_DEMAG_FIELD,
+                     abi.Q_EFFECTIVE_FIELD, abi.Q_TORQUE])
+
+
+@pytest.mark.parametrize("size", [(16, 4, 3), (17, 4, 1), (8, 10, 2), (33, 20, 5), (1, 1, 1), (64, 1, 1),
+                                  (5, 3, 8), (40, 7, 4)])
+def test_demag_shapes(mpx, size):
+    compare(MagnetSpec(size=size, cellsize=(1e-9, 2e-9, 3.1e-9), msat=8e5), mpx, [abi.Q_DEMAG_FIELD])
+
+
+@pytest.mark.parametrize("pbc", [(1, 2, 0), (2, 2, 0), (1, 0, 1)])
+def test_demag_pbc(mpx, pbc):
+    size = (16, 12, 2)
+    s = MagnetSpec(size=size, cellsize=(2e-9, 2e-9, 1e-9), msat=5.8e5,
+                   mastergrid_size=tuple(size[a] if pbc[a] else 0 for a in range(3)), pbc=pbc)
+    compare(s, mpx, [abi.Q_DEMAG_FIELD])
+
+
+def test_demag_kernel_reference_layout(mpx):
+    s = MagnetSpec(size=(16, 4, 3), cellsize=(1e-9, 1e-9, 1e-9))
+    ow, q = s.oracle_world()
+    world, magnet = s.product(mpx)
+    got = magnet._engine.demag_kernel(magnet._id)
+    want = ow.demag_kernel(q)
+    assert got.shape == want.shape
+    assert np.max(np.abs(got - want)) <= 1e-6 * np.max(np.abs(want))
+
+
+def test_small_film_effective_field_torque_energies(mpx):
+    # 256x64x1-like film (exchange + demag + Zeeman), scaled down
+    s = MagnetSpec(size=(64, 16, 1), cellsize=(3e-9, 3e-9, 3e-9), msat=8.6e5, aex=1.3e-11, alpha=0.02,
+                   world_bias=(-0.030, 0.005, 0.0))
+    compare(s, mpx, [abi.Q_EFFECTIVE_FIELD, abi.Q_DEMAG_FIELD, abi.Q_TORQUE, abi.Q_DAMPING_TORQUE,
+                     abi.Q_EXCHANGE_ENERGY_DENSITY, abi.Q_DEMAG_ENERGY_DENSITY, abi.Q_ZEEMAN_ENERGY_DENSITY,
+                     abi.Q_TOTAL_ENERGY_DENSITY], seed=1, smooth=3)
+
+
+def test_multilayer_effective_field(mpx):
+    # 512x512x8 multilayer parameters, scaled down: PBC in x,y, iDMI, Ku1 along z
+    s = MagnetSpec(size=(32, 32, 8), cellsize=(2e-9, 2e-9, 1e-9), msat=5.8e5, aex=1.5e-11,
+                   dmi={"xxz": 3e-3, "yyz": 3e-3}, ku1=8e5, anisU=(0, 0, 1), alpha=0.1,
+                   world_bias=(0, 0, 0.2), mastergrid_size=(32, 32, 0), pbc=(2, 2, 0))
+    compare(s, mpx, [abi.Q_EFFECTIVE_FIELD, abi.Q_TORQUE, abi.Q_DEMAG_FIELD], seed=2, smooth=2)
+
+
+def test_energies_and_averages(mpx):
+    s = MagnetSpec(size=(20, 12, 2), cellsize=(2e-9, 2e-9, 2e-9), msat=8e5, aex=1e-11, ku1=3e5,
+                   anisU=(1, 1, 0), dmi={"xxz": 1e-3, "yyz": 1e-3}, world_bias=(0.01, 0, 0.02))
+    m0 = random_m(s.shape, seed=9, smooth=2)
+    ow, q = s.oracle_world(m0)
+    world, magnet = s.product(mpx, m0)
+    for quantity, prop in [(abi.Q_EXCHANGE_ENERGY_DENSITY, "exchange_energy"),
+                           (abi.Q_DMI_ENERGY_DENSITY, "dmi_energy"),
+                           (abi.Q_ANISOTROPY_ENERGY_DENSITY, "anisotropy_energy"),
+                           (abi.Q_ZEEMAN_ENERGY_DENSITY, "zeeman_energy"),
+                           (abi.Q_DEMAG_ENERGY_DENSITY, "demag_energy"),
+                           (abi.Q_TOTAL_ENERGY_DENSITY, "total_energy")]:
+        got = getattr(magnet, prop).eval()
+        want = ow.energy(q, quantity)
+        assert got == pytest.approx(want, rel=1e-5, abs=1e-30), prop
+    np.testing.assert_allclose(magnet.magnetization.average(), ow.average(q, abi.Q_MAGNETIZATION), atol=1e-6)
+    np.testing.assert_allclose(magnet.effective_field.average(), ow.average(q, abi.Q_EFFECTIVE_FIELD),
+                               atol=1e-5 * np.max(np.abs(ow.eval(q, abi.Q_EFFECTIVE_FIELD))))
+
+
+def _macrospin_exact(t, m0, hz, damping):
+    mx, my, mz = m0
+    theta0 = np.arccos(mz / np.sqrt(mx**2 + my**2 + mz**2))
+    phi0 = np.arctan(my / mx)
+    freq = GAMMALL * hz / (1 + damping**2)
+    phi = phi0 + freq * t
+    theta = np.pi - 2 * np.arctan(np.exp(damping * freq * t) * np.tan(np.pi / 2 - theta0 / 2))
+    return {"mx": np.sin(theta) * np.cos(phi), "my": np.sin(theta) * np.sin(phi), "mz": np.cos(theta)}
+
+
+@pytest.mark.parametrize("method", ["Heun", "BogackiShampine", "CashKarp", "Fehlberg", "DormandPrince"])
+def test_solve_single_system(mpx, method):
+    # test/test_timesolver.py:90-122, through the mumaxplus-style API
+    world = mpx.World(cellsize=(1, 1, 1))
+    magnet = mpx.Ferromagnet(world, grid=mpx.Grid((1, 1, 1)))
+    magnet.enable_demag = False
+    magnet.magnetization = (1, 0, 0)
+    magnet.alpha = 0.2
+    world.bias_magnetic_field = (0, 0, 0.11)
+    world.timesolver.set_method(method)
+    tps = np.linspace(0, 5e-10, 20)
+    out = world.timesolver.solve(tps, {
+        "mx": lambda: magnet.magnetization.average()[0],
+        "my": lambda: magnet.magnetization.average()[1],
+        "mz": lambda: magnet.magnetization.average()[2],
+    })
+    exact = _macrospin_exact(tps, (1, 0, 0), 0.11, 0.2)
+    for mc in ("mx", "my", "mz"):
+        assert np.max(np.abs(np.array(out[mc]) - exact[mc])) < 1e-4
+
+
+def test_fixed_timestep_and_setters(mpx):
+    world = mpx.World(cellsize=(1, 1, 1))
+    ts = world.timesolver
+    assert ts.time == 0.0
+    ts.time = 1e-9
+    assert ts.time == pytest.approx(1e-9)
+    ts.time = 0.0
+    assert ts.adaptive_timestep is True
+    ts.adaptive_timestep = False
+    ts.timestep = 2.3e-9
+    ts.steps(103)
+    assert ts.time == pytest.approx(103 * 2.3e-9, rel=1e-5)
+    for bad in ("", "asdf"):
+        with pytest.raises(ValueError):
+            ts.set_method(bad)
+    with pytest.raises(TypeError):
+        ts.set_method(2)
+
+
+@pytest.mark.parametrize("method", ["DormandPrince", "Fehlberg"])
+def test_film_trajectory_vs_oracle(mpx, method):
+    # <m>(t) of a small film with exchange + demag + Zeeman vs the FP64 oracle
+    s = MagnetSpec(size=(32, 16, 1), cellsize=(3e-9, 3e-9, 3e-9), msat=8.6e5, aex=1.3e-11, alpha=0.02,
+                   world_bias=(-0.030, 0.005, 0.0))
+    m0 = random_m(s.shape, seed=1, smooth=3)
+    ow, q = s.oracle_world(m0)
+    ow.set_method(method)
+    world, magnet = s.product(mpx, m0)
+    world.timesolver.set_method(method)
+    dt0 = ow.sensible_timestep()
+    ow.timestep = dt0
+    world.timesolver.timestep = dt0
+    worst = 0.0
+    for k in range(1, 9):
+        tp = k * 25e-12
+        ow.run(tp - ow.time)
+        world.timesolver._e.run(world._group, tp - world.timesolver.time)
+        a = np.array(magnet.magnetization.average())
+        b = np.array(ow.average(q, abi.Q_MAGNETIZATION))
+        worst = max(worst, float(np.max(np.abs(a - b))))
+    assert worst < 1e-4, worst
+    assert world.timesolver.time == pytest.approx(ow.time, rel=1e-12)
+
+
+def test_two_groups_one_engine_match_alone(mpx):
+    """A group advanced beside another group gives the same result as alone."""
+    from mumaxplus_b200._engine import Engine
+
+    def build(eng, size, seed, bias):
+        s = MagnetSpec(size=size, cellsize=(3e-9, 3e-9, 3e-9), msat=8e5, aex=1.3e-11, alpha=0.1,
+                       world_bias=(0, 0, 0))
+        s.bias = bias
+        g = eng.group_create()
+        keep = []
+        mid = eng.magnet_add(g, s.desc(keep))
+        eng.set_m(mid, random_m(s.shape, seed=seed, smooth=2))
+        p = eng.solver_params(g)
+        p.method = abi.RK_METHODS["DormandPrince"]
+        eng.set_solver_params(g, p)
+        eng.set_timestep(g, 1e-13)
+        return g, mid, s.shape
+
+    alone = Engine()
+    ga, ma, shape_a = build(alone, (24, 20, 1), 3, (0.02, 0, 0.05))
+    alone.group_start(ga, 30e-12)
+    while True:
+        alone.advance(8)
+        done, running = alone.poll()
+        if running == 0:
+            break
+    ref = alone.get_m(ma, (3, *shape_a))
+
+    mixed = Engine()
+    g1, m1, _ = build(mixed, (24, 20, 1), 3, (0.02, 0, 0.05))
+    g2, m2, shape2 = build(mixed, (40, 8, 2), 4, (0, 0.03, 0))
+    mixed.group_start(g1, 30e-12)
+    mixed.group_start(g2, 45e-12)
+    while True:
+        mixed.advance(8)
+        done, running = mixed.poll()
+        if running == 0:
+            break
+    got = mixed.get_m(m1, (3, *shape_a))
+    assert np.array_equal(got, ref)
+    assert mixed.get_time(g1) == pytest.approx(30e-12, rel=1e-12)
+    assert mixed.get_time(g2) == pytest.approx(45e-12, rel=1e-12)
+
+
+def test_nan_state_fails_cleanly(mpx):
+    world = mpx.World(cellsize=(1e-9, 1e-9, 1e-9))
+    magnet = mpx.Ferromagnet(world, mpx.Grid((4, 4, 1)))
+    magnet.enable_demag = False
+    magnet.aex = 1e-11
+    magnet.alpha = 0.1
+    magnet.msat = float("nan")
+    world.timesolver.timestep = 1e-13
+    with pytest.raises(RuntimeError):
+        world.timesolver.run(1e-12)
+    # the engine stays usable afterwards
+    magnet.msat = 8e5
+    magnet.magnetization = (1, 0.1, 0)
+    world.timesolver.timestep = 1e-13
+    world.timesolver.run(1e-12)
+    assert world.timesolver.time == pytest.approx(1e-12, rel=1e-9)

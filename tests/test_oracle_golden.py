@@ -1,0 +1,217 @@
+"""Pins the CPU FP64 oracle against the known answers the reference's own tests
+hold for this path (CPU only, no GPU).
+
+  exchange     test/test_exchange.py:6-46     numpy Laplacian, Neumann edges
+  DMI          test/test_interfacialdmi.py     numpy, open boundaries
+  anisotropy   test/test_anisotropy.py:15-57   numpy uniaxial field / energy
+  demag        test/test_demag.py:6-45         numpy FFT of the real-space kernel
+  stray field  test/test_strayfield.py:57-84   FFT vs direct sum, with PBC
+  time solver  test/test_timesolver.py:19-169  analytic macrospin precession, all 5 methods
+  PBC          test/test_PBC.py:14-91          <m> after 1 ns vs the mumax3 value
+"""
+import numpy as np
+import pytest
+
+import oracle as O
+from spec import MagnetSpec, max_rel, random_m
+
+abi = O.abi
+GAMMALL = 1.7595e11
+
+
+def test_newell_cube_self_demag():
+    # a cube's self-demag tensor is 1/3 on the diagonal, 0 off the diagonal
+    for c in range(3):
+        assert O.newell(c, 0, 0, 0, (1e-9, 1e-9, 1e-9)) == pytest.approx(1 / 3, rel=1e-12)
+    for c in range(3, 6):
+        assert O.newell(c, 0, 0, 0, (1e-9, 1e-9, 1e-9)) == 0.0
+    # trace of the self term is 1 for any cell shape
+    cs = (1e-9, 2e-9, 3.1e-9)
+    tr = sum(O.newell(c, 0, 0, 0, cs) for c in range(3))
+    assert tr == pytest.approx(1.0, rel=1e-10)
+
+
+def test_newell_far_field_dipole():
+    # far away the tensor tends to the point dipole V/(4 pi r^3) (3 r r / r^2 - 1)
+    cs = (1e-9, 1e-9, 1e-9)
+    x = 12
+    nxx = O.newell(0, x, 0, 0, cs)
+    assert nxx == pytest.approx(-2.0 / (4 * np.pi * x**3), rel=2e-2)
+
+
+def _exchange_numpy(m, cellsize, aex, msat):
+    # test/test_exchange.py:6-31 (Neumann: the missing neighbour adds nothing)
+    h = np.zeros(m.shape)
+    for ax, c in ((1, cellsize[2]), (2, cellsize[1]), (3, cellsize[0])):
+        for shift in (1, -1):
+            m_ = np.roll(m, shift, axis=ax)
+            sl = [slice(None)] * 4
+            sl[ax] = slice(1, None) if shift == 1 else slice(0, -1)
+            h[tuple(sl)] += (m_ - m)[tuple(sl)] / c**2
+    return 2 * aex * h / msat
+
+
+def test_exchange_neumann_vs_numpy():
+    s = MagnetSpec(size=(16, 16, 4), cellsize=(1e3, 2e3, 3e3), aex=3.2e7, msat=5.4, enable_demag=False)
+    m0 = random_m(s.shape, seed=11)
+    w, q = s.oracle_world(m0)
+    m = w.get_m(q)
+    wanted = _exchange_numpy(m, s.cellsize, s.aex, s.msat)
+    got = w.eval(q, abi.Q_EXCHANGE_FIELD)
+    assert np.max(np.abs(got - wanted) / np.abs(wanted)) < 1e-9
+
+
+def _idmi_numpy(m, cs, Dxxz, Dyyz, msat):
+    # test/test_interfacialdmi.py:8-43 (open boundaries)
+    X, Y, Z = 0, 1, 2
+    h = np.zeros(m.shape)
+    m_ = np.roll(m, 1, axis=3)
+    h[X][:, :, 1:] -= Dxxz * m_[Z][:, :, 1:] / cs[0]
+    h[Z][:, :, 1:] += Dxxz * m_[X][:, :, 1:] / cs[0]
+    m_ = np.roll(m, -1, axis=3)
+    h[X][:, :, 0:-1] += Dxxz * m_[Z][:, :, 0:-1] / cs[0]
+    h[Z][:, :, 0:-1] -= Dxxz * m_[X][:, :, 0:-1] / cs[0]
+    m_ = np.roll(m, 1, axis=2)
+    h[Y][:, 1:, :] -= Dyyz * m_[Z][:, 1:, :] / cs[1]
+    h[Z][:, 1:, :] += Dyyz * m_[Y][:, 1:, :] / cs[1]
+    m_ = np.roll(m, -1, axis=2)
+    h[Y][:, 0:-1, :] += Dyyz * m_[Z][:, 0:-1, :] / cs[1]
+    h[Z][:, 0:-1, :] -= Dyyz * m_[Y][:, 0:-1, :] / cs[1]
+    return h / msat
+
+
+def test_interfacial_dmi_openbc_vs_numpy():
+    s = MagnetSpec(size=(4, 5, 3), cellsize=(1.1, 2.0, 3.2), msat=3.1, dmi={"xxz": 7.1, "yyz": -7.1},
+                   enable_openbc=True, enable_demag=False)
+    w, q = s.oracle_world(random_m(s.shape, seed=3))
+    m = w.get_m(q)
+    wanted = _idmi_numpy(m, s.cellsize, 7.1, -7.1, 3.1)
+    got = w.eval(q, abi.Q_DMI_FIELD)
+    assert np.max(np.abs(got - wanted) / np.abs(wanted)) < 1e-9
+
+
+def test_uniaxial_anisotropy_vs_numpy():
+    s = MagnetSpec(size=(16, 32, 4), cellsize=(1e-9, 2e-9, 4e-9), msat=800e3, ku1=4.1e6, ku2=2.1e6,
+                   anisU=(0.3, 0.4, 1.0), enable_demag=False)
+    w, q = s.oracle_world(random_m(s.shape, seed=5))
+    m = w.get_m(q)
+    u = np.array([0.3, 0.4, 1.0]) / np.linalg.norm([0.3, 0.4, 1.0])
+    mu = np.einsum("c...,c->...", m, u)
+    wanted = (2 * 4.1e6 * mu + 4 * 2.1e6 * mu**3)[None] * u[:, None, None, None] / 800e3
+    assert max_rel(w.eval(q, abi.Q_ANISOTROPY_FIELD), wanted) < 1e-12
+    e_wanted = -4.1e6 * mu**2 - 2.1e6 * mu**4
+    assert np.max(np.abs(w.eval(q, abi.Q_ANISOTROPY_ENERGY_DENSITY)[0] - e_wanted)) < 1e-6 * np.max(np.abs(e_wanted))
+    E = w.energy(q, abi.Q_ANISOTROPY_ENERGY_DENSITY)
+    assert E == pytest.approx(np.sum(e_wanted) * 1e-9 * 2e-9 * 4e-9, rel=1e-10)
+
+
+def _demag_numpy(kernel, mag):
+    # test/test_demag.py:6-36: numpy FFT convolution on the reference kernel grid,
+    # cropping the LAST n cells of the padded result
+    pad = [(0, kernel.shape[i + 1] - mag.shape[i + 1]) for i in range(3)]
+    m = np.pad(mag, ((0, 0), *pad), "constant")
+    m = np.fft.fftn(m, axes=(1, 2, 3))
+    kxx, kyy, kzz, kxy, kxz, kyz = np.fft.fftn(kernel, axes=(1, 2, 3))
+    hx = np.fft.ifftn(m[0] * kxx + m[1] * kxy + m[2] * kxz)
+    hy = np.fft.ifftn(m[0] * kxy + m[1] * kyy + m[2] * kyz)
+    hz = np.fft.ifftn(m[0] * kxz + m[1] * kyz + m[2] * kzz)
+    h = -1.25663706212e-6 * np.array([hx, hy, hz]).real
+    return h[:, (h.shape[1] - mag.shape[1]):, (h.shape[2] - mag.shape[2]):, (h.shape[3] - mag.shape[3]):]
+
+
+def test_demag_vs_numpy_fft_of_reference_kernel_layout():
+    s = MagnetSpec(size=(16, 4, 3), cellsize=(1e-9, 1e-9, 1e-9), msat=1.0)
+    w, q = s.oracle_world(random_m(s.shape, seed=7))
+    kernel = w.demag_kernel(q)
+    assert kernel.shape == (6, 5, 8, 32)  # 2n-1, padded to even when above 5
+    wanted = _demag_numpy(kernel, 1.0 * w.get_m(q))
+    got = w.eval(q, abi.Q_DEMAG_FIELD)
+    assert max_rel(got, wanted) < 1e-12
+
+
+@pytest.mark.parametrize("pbc", [None, (1, 2, 0)])
+@pytest.mark.parametrize("size", [(17, 4, 1), (8, 10, 2), (6, 7, 5)])
+def test_demag_fft_vs_direct_sum(size, pbc):
+    # test/test_strayfield.py:57-84 (same source and destination grid)
+    kw = dict(size=size, cellsize=(1e-9, 2e-9, 3.1e-9), msat=800e3)
+    if pbc is not None:
+        kw.update(mastergrid_size=tuple(size[a] if pbc[a] else 0 for a in range(3)), pbc=pbc)
+    s = MagnetSpec(**kw)
+    w, q = s.oracle_world(random_m(s.shape, seed=17))
+    assert max_rel(w.eval(q, abi.Q_DEMAG_FIELD), w.demag_brute(q)) < 1e-10
+
+
+def test_demag_with_geometry_and_regions_vs_direct_sum():
+    geom = np.ones((2, 9, 11), dtype=bool)
+    geom[:, 3:6, 4:8] = False
+    s = MagnetSpec(size=(11, 9, 2), cellsize=(2e-9, 2e-9, 1e-9), msat=np.linspace(3e5, 9e5, 198).reshape(2, 9, 11),
+                   geometry=geom)
+    w, q = s.oracle_world(random_m(s.shape, seed=19))
+    got, wanted = w.eval(q, abi.Q_DEMAG_FIELD), w.demag_brute(q)
+    assert max_rel(got, wanted) < 1e-12
+    assert np.all(got[:, ~geom] == 0)
+
+
+def _macrospin_exact(t, m0, hz, damping):
+    # test/test_timesolver.py:19-29 analytic LLG precession about z
+    mx, my, mz = m0
+    theta0 = np.arccos(mz / np.sqrt(mx**2 + my**2 + mz**2))
+    phi0 = np.arctan(my / mx)
+    freq = GAMMALL * hz / (1 + damping**2)
+    phi = phi0 + freq * t
+    theta = np.pi - 2 * np.arctan(np.exp(damping * freq * t) * np.tan(np.pi / 2 - theta0 / 2))
+    return np.array([np.sin(theta) * np.cos(phi), np.sin(theta) * np.sin(phi), np.cos(theta)])
+
+
+@pytest.mark.parametrize("method", list(abi.RK_METHODS))
+def test_macrospin_vs_analytic(method):
+    s = MagnetSpec(size=(1, 1, 1), cellsize=(1, 1, 1), alpha=0.2, enable_demag=False, world_bias=(0, 0, 0.11))
+    w, q = s.oracle_world(np.array([1, 0, 0], np.float32).reshape(3, 1, 1, 1))
+    w.set_method(method)
+    w.timestep = w.sensible_timestep()
+    tps = np.linspace(0, 5e-10, 20)
+    got = []
+    for tp in tps:
+        w.run(tp - w.time)
+        got.append(w.get_m(q)[:, 0, 0, 0])
+    exact = _macrospin_exact(tps, (1, 0, 0), 0.11, 0.2)
+    assert np.max(np.abs(np.array(got).T - exact)) < 1e-4
+
+
+def test_fixed_timestep_time_accumulation():
+    # test/test_timesolver.py:80-86
+    s = MagnetSpec(size=(1, 1, 1), cellsize=(1, 1, 1), enable_demag=False)
+    w, q = s.oracle_world()
+    w.set_solver(adaptive=0)
+    w.timestep = 2.3e-9
+    w.steps(103)
+    assert w.time == pytest.approx(103 * 2.3e-9, rel=1e-5)
+
+
+def _pbc_rectangle_geometry(nx, ny, corners=False):
+    # test/test_PBC.py:34-51: Rectangle(nx/2 c, ny/2 c) centred in the box,
+    # repeated; cells at positions i*c.  Inside: nx/4 <= i < 3nx/4 (and y alike).
+    ix = np.arange(nx)
+    iy = np.arange(ny)
+    if corners:
+        ix = (ix - nx // 2) % nx
+        iy = (iy - ny // 2) % ny
+    inx = (ix >= nx // 4) & (ix < 3 * nx // 4)
+    iny = (iy >= ny // 4) & (iy < 3 * ny // 4)
+    return (iny[:, None] & inx[None, :])[None]
+
+
+@pytest.mark.slow
+def test_pbc_run_center_matches_mumax3_golden():
+    # test/test_PBC.py:77-82: <m> after 1 ns, mumax3 value, relative error < 1e-3
+    nx, ny, c = 128, 64, 5e-9
+    s = MagnetSpec(size=(nx, ny, 1), cellsize=(c, c, c), mastergrid_size=(nx, ny, 0), pbc=(2, 2, 0),
+                   geometry=_pbc_rectangle_geometry(nx, ny), msat=1000e3, aex=10e-12, alpha=1.0)
+    m0 = np.zeros((3, 1, ny, nx), np.float32)
+    m0[0], m0[1], m0[2] = 1.0, 0.1, 0.01
+    w, q = s.oracle_world(m0)
+    w.timestep = w.sensible_timestep()
+    w.run(1e-9)
+    avg = w.average(q, abi.Q_MAGNETIZATION)
+    wanted = np.array([0.89947968, 0.23352228, -0.00010287])
+    assert np.linalg.norm(np.array(avg) - wanted) / np.linalg.norm(wanted) < 1e-3

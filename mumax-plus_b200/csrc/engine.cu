@@ -557,6 +557,30 @@ mpx_status load_params(mpx_engine* e, Magnet* m, const mpx_magnet_desc* d) {
   if (d->enable_openbc) terms |= FLAG_OPENBC;
   D.terms = terms;
   for (int c = 0; c < 3; ++c) D.wb[c] = (float)e->wb[c];
+  // fast path: every parameter uniform, no geometry, no regions
+  bool uniform = !d->geometry && !d->regions;
+  for (const mpx_scalar* s : {&d->msat, &d->aex, &d->alpha, &d->ku1, &d->ku2, &d->frozen_spins})
+    uniform = uniform && !s->cells;
+  for (int c = 0; c < 9; ++c) uniform = uniform && !d->dmi[c].cells;
+  uniform = uniform && !d->anis_u.cells && !d->bias_magnetic_field.cells;
+  D.fast = uniform ? 1 : 0;
+  if (uniform) {
+    const float a = D.aex.u, ms = D.msat.u;
+    for (int ax = 0; ax < 3; ++ax) D.fe[ax] = (2 * a) * D.w[ax];  // 2 A w, as physics/exchange.cu:100
+    for (int c = 0; c < 9; ++c) D.fd[c] = D.dmi[c].u;
+    D.fa = a;
+    D.finv_2a = (a == 0.0f) ? 0.0f : 0.5f / a;
+    D.finv_ms = (ms == 0.0f) ? 0.0f : 1.0f / ms;
+    D.fk1 = D.ku1.u;
+    D.fk2 = D.ku2.u;
+    const float ux = D.anisU.u[0], uy = D.anisU.u[1], uz = D.anisU.u[2];
+    const float nu = std::sqrt(ux * ux + uy * uy + uz * uz);
+    const float s = (nu == 0.0f) ? 0.0f : 1.0f / nu;
+    D.fu[0] = s * ux;
+    D.fu[1] = s * uy;
+    D.fu[2] = s * uz;
+    for (int c = 0; c < 3; ++c) D.fb[c] = (terms & FLAG_MAGNET_BIAS) ? D.wb[c] + D.bias.u[c] : D.wb[c];
+  }
   return MPX_OK;
 }
 
@@ -600,6 +624,7 @@ mpx_status setup_magnet(mpx_engine* e, Magnet* m, const mpx_magnet_desc* d, bool
     D.cs[a] = (float)d->cellsize[a];
     const float c = (float)d->cellsize[a];
     D.w[a] = 1.0f / (c * c);
+    D.inv_cs[a] = 1.0f / c;
   }
   D.N = D.n[0] * D.n[1] * D.n[2];
   D.group = m->group;
@@ -1012,6 +1037,7 @@ mpx_status mpx_engine_set_world_bias(mpx_engine* e, const double b[3]) {
     const bool mb = (m->dev.terms & FLAG_MAGNET_BIAS) != 0;
     if (wb0 && !mb) m->dev.terms &= ~TERM_EXT;
     else m->dev.terms |= TERM_EXT;
+    for (int c = 0; c < 3; ++c) m->dev.fb[c] = mb ? m->dev.wb[c] + m->dev.bias.u[c] : m->dev.wb[c];
     MPX_TRY(upload_magnet_desc(e, m));
   }
   for (auto& g : e->groups)

@@ -35,19 +35,41 @@ __device__ __forceinline__ float2 cconj(float2 a) { return make_float2(a.x, -a.y
 __device__ __forceinline__ int pidx(int i) { return i + (i >> 4); }
 __host__ __device__ constexpr int plen(int L) { return L + (L >> 4); }
 
-// exp(DIR * 2 pi i e / L) from a shared-memory table of the L forward
-// twiddles exp(-2 pi i e / L) (DIR = -1 forward, +1 inverse)
+// Twiddle of entry e of a per-pass shared-memory table (DIR = -1 forward, +1 inverse)
 template <int DIR>
 __device__ __forceinline__ float2 twiddle_raw(const float2* tw, int e) {
   const float2 w = tw[e];
   return DIR < 0 ? w : make_float2(w.x, -w.y);
 }
 
-// Fill a shared-memory table of the L = 2^logL twiddles from the global
-// 4096-entry table (the caller synchronises before use).
+// log2 radix of pass i (of ceil(logL/maxlr) passes) for a 2^logL transform
+__host__ __device__ __forceinline__ int fft_npass(int logL, int maxlr) { return (logL + maxlr - 1) / maxlr; }
+__host__ __device__ __forceinline__ int fft_pass_lr(int logL, int maxlr, int i) {
+  const int p = fft_npass(logL, maxlr);
+  const int base = logL / p, extra = logL - base * p;
+  return base + (i < extra ? 1 : 0);
+}
+
+// Fill the shared-memory twiddle table of the Stockham plan of a 2^logL
+// transform (radices up to 2^MAXLR) from the global 4096-entry table.  The
+// pass with sub-transform size Ns and radix R keeps W_{Ns R}^{r k} at
+// (Ns - 1) + k (R - 1) + (r - 1), so lanes with consecutive k read
+// consecutive (R-1)-strided entries, free of bank conflicts.  L - 1 entries;
+// the caller synchronises before use.
+template <int MAXLR>
 __device__ __forceinline__ void load_twiddles(float2* dst, const float2* __restrict__ tw4096, int logL) {
-  const int L = 1 << logL;
-  for (int e = threadIdx.x; e < L; e += blockDim.x) dst[e] = __ldg(&tw4096[e << (TW_LOG - logL)]);
+  const int p = fft_npass(logL, MAXLR);
+  int logNs = 0;
+  for (int i = 0; i < p; ++i) {
+    const int lr = fft_pass_lr(logL, MAXLR, i);
+    const int Rm1 = (1 << lr) - 1, Ns = 1 << logNs;
+    const int shift = TW_LOG - logNs - lr;
+    for (int t = threadIdx.x; t < Ns * Rm1; t += blockDim.x) {
+      const int k = t / Rm1, r = t - k * Rm1 + 1;
+      dst[Ns - 1 + t] = __ldg(&tw4096[(r * k) << shift]);
+    }
+    logNs += lr;
+  }
 }
 
 // cos(2 pi m / 16), m = 0..4 (decimal expansions of the constants)
@@ -128,7 +150,7 @@ __device__ __forceinline__ void stockham_pass(float2* buf, int logL, int logNs, 
   const int nb = 1 << lognb;
   const int total = ncols << lognb;
   const int Ns = 1 << logNs;
-  const int twshift = logL - logNs - LR;  // tw holds the 2^logL twiddles of this length
+  const float2* twp = tw + (Ns - 1);  // this pass's twiddles, [k][r-1]
   float2 v[BPT][R];
 #pragma unroll
   for (int q = 0; q < BPT; ++q) {
@@ -150,7 +172,7 @@ __device__ __forceinline__ void stockham_pass(float2* buf, int logL, int logNs, 
       const int k = j & (Ns - 1);
       if (logNs > 0) {
 #pragma unroll
-        for (int r = 1; r < R; ++r) v[q][r] = cmul(v[q][r], twiddle_raw<DIR>(tw, (r * k) << twshift));
+        for (int r = 1; r < R; ++r) v[q][r] = cmul(v[q][r], twiddle_raw<DIR>(twp, k * (R - 1) + (r - 1)));
       }
       dft_reg<R, DIR>(v[q]);
       const int o = ((j - k) << LR) + k;
@@ -159,14 +181,6 @@ __device__ __forceinline__ void stockham_pass(float2* buf, int logL, int logNs, 
     }
   }
   __syncthreads();
-}
-
-// log2 radix of pass i (of ceil(logL/MAXLR) passes) for a 2^logL transform
-__device__ __forceinline__ int fft_npass(int logL, int maxlr) { return (logL + maxlr - 1) / maxlr; }
-__device__ __forceinline__ int fft_pass_lr(int logL, int maxlr, int i) {
-  const int p = fft_npass(logL, maxlr);
-  const int base = logL / p, extra = logL - base * p;
-  return base + (i < extra ? 1 : 0);
 }
 
 // In-place FFT of `ncols` padded columns of length 2^logL with radices up to

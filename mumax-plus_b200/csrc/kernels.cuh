@@ -121,7 +121,7 @@ __global__ void __launch_bounds__(512, 2) k_xfwd(const MagnetDev* __restrict__ m
   const float* x0 = M.buf[G.map[0]];
   const int rowbase = nx * (y0 + ny * z);
   float2* tws = sm + (ty + nzrows) * cs;  // twiddles of length L
-  load_twiddles(tws, tw, logL);
+  load_twiddles<3>(tws, tw, logL);
 
 #pragma unroll 2
   for (int e = threadIdx.x; e < (ty << logL); e += blockDim.x) {
@@ -315,7 +315,7 @@ __global__ void __launch_bounds__(384) k_yz(const MagnetDev* __restrict__ mags, 
   float2* D = sm;  // [3*nz] padded columns of length Py
   const int ncol = 3 * nz;
   float2* tws = sm + ncol * cs;  // twiddles of length Py
-  load_twiddles(tws, tw, logPy);
+  load_twiddles<4>(tws, tw, logPy);
   // slab load: 8 independent read-only loads in flight per thread
   const int total = ncol << logPy;
   for (int e0 = threadIdx.x; e0 < total; e0 += 8 * blockDim.x) {
@@ -374,7 +374,13 @@ __device__ __forceinline__ void epilogue_cell(const MagnetDev& M, const GroupDev
     float3 k = f3(0, 0, 0);
     if (ing && M.frozen.at(i) == 0.0f) {
       float3 h = f3(0, 0, 0);
-      if (M.msat.at(i) != 0.0f) {
+      if (M.fast) {
+        const LocalOut lo = local_terms_fast(M, m, x, y, z, mc);
+        h = lo.exch;
+        h = h + lo.anis;
+        h = h + lo.ext;
+        h = h + lo.dmi;
+      } else if (M.msat.at(i) != 0.0f) {
         const LocalOut lo = local_terms(M, m, x, y, z, i, mc, TERM_EXCH | TERM_DMI | TERM_ANIS | TERM_EXT);
         h = lo.exch;
         h = h + lo.anis;
@@ -418,7 +424,9 @@ __device__ __forceinline__ void epilogue_cell(const MagnetDev& M, const GroupDev
   const float ms = M.msat.at(i);
   LocalOut lo;
   lo.exch = lo.anis = lo.ext = lo.dmi = f3(0, 0, 0);
-  if (ms != 0.0f) {
+  if (M.fast) {
+    lo = local_terms_fast(M, m, x, y, z, mc);
+  } else if (ms != 0.0f) {
     lo = local_terms(M, m, x, y, z, i, mc, TERM_EXCH | TERM_DMI | TERM_ANIS | TERM_EXT);
   } else if (M.terms & TERM_EXT) {
     lo.ext = local_terms(M, m, x, y, z, i, mc, TERM_EXT).ext;
@@ -495,7 +503,7 @@ __global__ void __launch_bounds__(512, 2) k_xinv(const MagnetDev* __restrict__ m
   const int Fh = M.Fh;
   float2* rows_z = sm + ty * cs;
   float2* tws = sm + (ty + nzrows) * cs;  // twiddles of length L
-  load_twiddles(tws, tw, logL);
+  load_twiddles<3>(tws, tw, logL);
   const float2* __restrict__ S = M.spec;
   const size_t cstride = (size_t)nz * ny;
   // rebuild full-length Hermitian rows: Z = A + iB

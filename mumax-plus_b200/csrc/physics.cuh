@@ -50,6 +50,7 @@ struct MagnetDev {
   int mg[3], mgo[3]; // mastergrid size / origin (size 0: no wrap)
   float cs[3];       // cell size
   float w[3];        // 1/cellsize^2
+  float inv_cs[3];   // 1/cellsize (divisions by the finite difference become products)
   const unsigned char* __restrict__ geom;  // NULL: all cells in geometry
   const unsigned* __restrict__ reg;        // NULL: region 0
   DScalar msat, aex, alpha, ku1, ku2, frozen;
@@ -67,6 +68,14 @@ struct MagnetDev {
   float2* spec;      // spectrum S[kx][c][z][y]
   const float* __restrict__ kspec;  // kernel spectrum [kx][kz'][kcomp][ky']
   float* buf[9];     // field buffers (3N floats each); roles given by the group map
+  // Fast path: every parameter uniform, no geometry, no regions.  Set on the
+  // host together with the precomputed uniform values below.
+  int fast;
+  float fe[3];       // 2 A w[axis]: exchange coefficient per axis
+  float fd[9];       // uniform DMI tensor, MPX_DMI_* order
+  float fu[3];       // normalised uniaxial axis
+  float fb[3];       // world bias + magnet bias
+  float fa, finv_2a, finv_ms, fk1, fk2;
 };
 
 // Solve-group state (time integration); lives in a device array.
@@ -166,8 +175,14 @@ __device__ __forceinline__ LocalOut local_terms(const MagnetDev& M, const float*
   const bool openbc = (M.terms & FLAG_OPENBC) != 0;
   const bool do_exch = (mask & TERM_EXCH) && (M.terms & TERM_EXCH);
   const bool do_dmi = (mask & TERM_DMI) && (M.terms & TERM_DMI);
+  // Divisions by Ms, 2A and the finite difference are products with
+  // reciprocals (one division per cell): IEEE division takes a slow path on
+  // subnormal operands, which the in-plane components of a nearly uniform
+  // state produce (results agree to 1 ulp per operation).
+  const float inv_ms = 1.0f / ms;
   if (do_exch || do_dmi) {
     const float a = M.aex.at(i);
+    const float inv_2a = (a == 0.0f) ? 0.0f : 0.5f / a;
     const bool dmi_open = (a == 0.0f) ? true : openbc;
     float3 he = f3(0, 0, 0), hd = f3(0, 0, 0);
 #pragma unroll
@@ -182,6 +197,7 @@ __device__ __forceinline__ LocalOut local_terms(const MagnetDev& M, const float*
       const int j = (nc >= 0) ? xx + M.n[0] * (yy + M.n[1] * zz) : -1;
       const bool nin = (nc >= 0) && in_geom(M, j);
       const float delta = d * M.cs[axis];
+      const float inv_delta = d * M.inv_cs[axis];
       const int nx_ = axis == 0, ny_ = axis == 1, nz_ = axis == 2;
       // ---- exchange (physics/exchange.cu:58-102)
       if (do_exch) {
@@ -205,7 +221,7 @@ __device__ __forceinline__ LocalOut local_terms(const MagnetDev& M, const float*
               a_ = a;
             } else {
               const float3 G = get_gamma(M, i, nx_, ny_, nz_, mc);
-              m_ = mc + delta * (G / (2 * a));
+              m_ = mc + delta * (inv_2a * G);
               a_ = a;
             }
           }
@@ -234,18 +250,18 @@ __device__ __forceinline__ LocalOut local_terms(const MagnetDev& M, const float*
           float3 m_;
           if (!nin && !dmi_open) {
             const float3 G = get_gamma(M, i, nx_, ny_, nz_, mc);
-            m_ = mc + delta * (G / (2 * a));
+            m_ = mc + delta * (inv_2a * G);
           } else {
             m_ = ldg3(m, N, jj);
           }
-          hd.x += (Dxy * m_.y + Dxz * m_.z) / delta;
-          hd.y += (Dyx * m_.x + Dyz * m_.z) / delta;
-          hd.z += (Dzx * m_.x + Dzy * m_.y) / delta;
+          hd.x += (Dxy * m_.y + Dxz * m_.z) * inv_delta;
+          hd.y += (Dyx * m_.x + Dyz * m_.z) * inv_delta;
+          hd.z += (Dzx * m_.x + Dzy * m_.y) * inv_delta;
         }
       }
     }
-    if (do_exch) o.exch = he / ms;
-    if (do_dmi) o.dmi = hd / ms;
+    if (do_exch) o.exch = inv_ms * he;
+    if (do_dmi) o.dmi = inv_ms * hd;
   }
   if ((mask & TERM_ANIS) && (M.terms & TERM_ANIS)) {  // physics/anisotropy.cu:45-54
     float3 u = M.anisU.at(i, N);
@@ -254,13 +270,75 @@ __device__ __forceinline__ LocalOut local_terms(const MagnetDev& M, const float*
     u = s * u;
     const float k1 = M.ku1.at(i), k2 = M.ku2.at(i);
     const float mu = dot3(mc, u);
-    o.anis = ((2 * k1 * mu + 4 * k2 * mu * mu * mu) * u) / ms;
+    o.anis = inv_ms * ((2 * k1 * mu + 4 * k2 * mu * mu * mu) * u);
   }
   if ((mask & TERM_EXT) && (M.terms & TERM_EXT)) {  // physics/zeeman.cu:64-68
     float3 b = f3(M.wb[0], M.wb[1], M.wb[2]);
     if (M.terms & FLAG_MAGNET_BIAS) b = b + M.bias.at(i, N);
     o.ext = b;
   }
+  return o;
+}
+
+// The same local terms when every parameter is uniform and there is no
+// geometry mask and no region map (MagnetDev::fast): the harmonic means reduce
+// to the uniform values, all neighbours inside the grid are in the geometry,
+// and the per-axis exchange coefficients, DMI tensor, normalised anisotropy
+// axis and total bias field are precomputed.
+__device__ __forceinline__ float3 gamma_uniform(const float* D, int axis, float3 m) {
+  // physics/dmi.hpp:53-69 with normal e_axis and uniform tensor D
+  if (axis == 0) return f3(-D[0] * m.y - D[1] * m.z, D[0] * m.x - D[2] * m.z, D[1] * m.x + D[2] * m.y);
+  if (axis == 1) return f3(-D[4] * m.z - D[3] * m.y, D[3] * m.x - D[5] * m.z, D[5] * m.y + D[4] * m.x);
+  return f3(-D[6] * m.y - D[7] * m.z, -D[8] * m.z + D[6] * m.x, D[7] * m.x + D[8] * m.y);
+}
+
+__device__ __forceinline__ LocalOut local_terms_fast(const MagnetDev& M, const float* __restrict__ m, int x, int y,
+                                                     int z, float3 mc) {
+  LocalOut o;
+  o.exch = o.anis = o.ext = o.dmi = f3(0, 0, 0);
+  const int N = M.N;
+  const bool openbc = (M.terms & FLAG_OPENBC) != 0;
+  const bool do_exch = (M.terms & TERM_EXCH) != 0;
+  const bool do_dmi = (M.terms & TERM_DMI) != 0;
+  if (do_exch || do_dmi) {
+    const float a = M.fa;
+    const bool dmi_open = (a == 0.0f) || openbc;
+    const bool neumann = !openbc && a != 0.0f;
+    float3 he = f3(0, 0, 0), hd = f3(0, 0, 0);
+#pragma unroll
+    for (int r = 0; r < 6; ++r) {
+      const int axis = r >> 1;
+      const int d = (r & 1) ? 1 : -1;
+      int xx = x, yy = y, zz = z, nc;
+      if (axis == 0) { nc = nb_coord(x, d, M.n[0], M.o[0], M.mg[0], M.mgo[0]); xx = nc; }
+      else if (axis == 1) { nc = nb_coord(y, d, M.n[1], M.o[1], M.mg[1], M.mgo[1]); yy = nc; }
+      else { nc = nb_coord(z, d, M.n[2], M.o[2], M.mg[2], M.mgo[2]); zz = nc; }
+      const bool nin = nc >= 0;
+      float3 m_ = mc;
+      if (nin) {
+        m_ = ldg3(m, N, xx + M.n[0] * (yy + M.n[1] * zz));
+      } else if (neumann) {  // ghost cell m + Gamma/(2A) delta
+        const float3 G = gamma_uniform(M.fd, axis, mc);
+        m_ = mc + (d * M.cs[axis]) * (M.finv_2a * G);
+      }
+      if (do_exch && (nin || neumann)) he = he + M.fe[axis] * (m_ - mc);
+      if (do_dmi && (nin || !dmi_open)) {
+        const float Dxy = M.fd[3 * axis], Dxz = M.fd[3 * axis + 1], Dyz = M.fd[3 * axis + 2];
+        const float inv_delta = d * M.inv_cs[axis];
+        hd.x += (Dxy * m_.y + Dxz * m_.z) * inv_delta;
+        hd.y += (-Dxy * m_.x + Dyz * m_.z) * inv_delta;
+        hd.z += (-Dxz * m_.x - Dyz * m_.y) * inv_delta;
+      }
+    }
+    if (do_exch) o.exch = M.finv_ms * he;
+    if (do_dmi) o.dmi = M.finv_ms * hd;
+  }
+  if (M.terms & TERM_ANIS) {
+    const float3 u = f3(M.fu[0], M.fu[1], M.fu[2]);
+    const float mu = dot3(mc, u);
+    o.anis = M.finv_ms * ((2 * M.fk1 * mu + 4 * M.fk2 * mu * mu * mu) * u);
+  }
+  if (M.terms & TERM_EXT) o.ext = f3(M.fb[0], M.fb[1], M.fb[2]);
   return o;
 }
 

@@ -350,7 +350,7 @@ int x_threads(const Magnet* m) {
   int rows = m->ty + (m->ty + 1) / 2;
   int t = (rows * m->P[0] + 7) / 8;  // 8 values per thread in the x FFTs
   t = ((t + 31) / 32) * 32;
-  return std::min(512, std::max(256, t));
+  return std::min(X_THREADS_MAX, std::max(256, t));
 }
 
 mpx_status rebuild_tables(mpx_engine* e) {
@@ -641,8 +641,9 @@ mpx_status setup_magnet(mpx_engine* e, Magnet* m, const mpx_magnet_desc* d, bool
   D.kcomp = (m->P[2] == 1) ? 4 : 6;
   m->ty = std::min(4, D.n[1]);
   if (m->demag) {
-    if (m->P[0] > MAX_FFT || m->P[1] > MAX_FFT)
-      return fail(MPX_ERR_UNSUPPORTED, "demag: padded FFT length above 4096 (grid side > 2048)");
+    if (m->P[0] > X_VPT * X_THREADS_MAX || m->P[1] > std::min(MAX_FFT, YZ_VPT * YZ_THREADS))
+      return fail(MPX_ERR_UNSUPPORTED, "demag: padded FFT length above 2048 along x or 4096 along y "
+                                       "(grid side above 1024 along x or 2048 along y)");
     if (m->P[2] > 16) return fail(MPX_ERR_UNSUPPORTED, "demag: nz > 8 is not implemented by the fused y/z pass");
     if (yz_smem(m) > SMEM_DYN_MAX)
       return fail(MPX_ERR_UNSUPPORTED, "demag: 3*nz*Py complex values exceed shared memory (nz*Py > 9472)");

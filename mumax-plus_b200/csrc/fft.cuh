@@ -139,27 +139,43 @@ __device__ __forceinline__ void dft_reg(float2 (&v)[R]) {
   Dft<R, DIR>::run(v);
 }
 
-// One Stockham pass of radix 2^LR over `ncols` padded columns of length 2^logL
-// (column c at buf + c*cs), each thread holding VPT values.
-// Requires ncols*L <= VPT*blockDim.x.
-template <int LR, int DIR, int VPT>
-__device__ __forceinline__ void stockham_pass(float2* buf, int logL, int logNs, int ncols, int cs,
-                                              const float2* __restrict__ tw) {
+// Compile-time Stockham plan of a 2^LOGL transform with radices up to 2^MAXLR:
+// ceil(LOGL/MAXLR) passes, the larger radices first.
+template <int LOGL, int MAXLR>
+struct Plan {
+  static constexpr int P = (LOGL + MAXLR - 1) / MAXLR;
+  static constexpr int lr(int i) { return LOGL / P + (i < LOGL - (LOGL / P) * P ? 1 : 0); }
+  static constexpr int logns(int i) { return i == 0 ? 0 : logns(i - 1) + lr(i - 1); }
+};
+
+// padded offset of element i + r*S relative to pidx(i) when S is a multiple of 16
+template <int S>
+__device__ __forceinline__ constexpr int pstride() { return S + (S >> 4); }
+
+// One Stockham pass (radix 2^LR, sub-transform size 2^LOGNS) over `ncols`
+// padded columns of length 2^LOGL (column c at buf + c*cs), VPT values per
+// thread.  Requires ncols*L <= VPT*blockDim.x.  Strides that are multiples of
+// 16 turn every padded address of a butterfly into a constant offset.
+template <int LOGL, int LR, int LOGNS, int DIR, int VPT>
+__device__ __forceinline__ void stockham_pass(float2* buf, int ncols, int cs, const float2* tw) {
   constexpr int R = 1 << LR, BPT = VPT / R;
-  const int lognb = logL - LR;
-  const int nb = 1 << lognb;
-  const int total = ncols << lognb;
-  const int Ns = 1 << logNs;
-  const float2* twp = tw + (Ns - 1);  // this pass's twiddles, [k][r-1]
+  constexpr int LOGNB = LOGL - LR, NB = 1 << LOGNB, NS = 1 << LOGNS;
+  const int total = ncols << LOGNB;
   float2 v[BPT][R];
 #pragma unroll
   for (int q = 0; q < BPT; ++q) {
     const int b = threadIdx.x + q * blockDim.x;
     if (b < total) {
-      const float2* base = buf + (b >> lognb) * cs;
-      const int j = b & (nb - 1);
+      const int j = b & (NB - 1);
+      const int c0 = (b >> LOGNB) * cs;
+      if constexpr (NB % 16 == 0) {
+        const int o0 = c0 + pidx(j);
 #pragma unroll
-      for (int r = 0; r < R; ++r) v[q][r] = base[pidx(j + (r << lognb))];
+        for (int r = 0; r < R; ++r) v[q][r] = buf[o0 + r * pstride<NB>()];
+      } else {
+#pragma unroll
+        for (int r = 0; r < R; ++r) v[q][r] = buf[c0 + pidx(j + r * NB)];
+      }
     }
   }
   __syncthreads();
@@ -167,47 +183,68 @@ __device__ __forceinline__ void stockham_pass(float2* buf, int logL, int logNs, 
   for (int q = 0; q < BPT; ++q) {
     const int b = threadIdx.x + q * blockDim.x;
     if (b < total) {
-      float2* base = buf + (b >> lognb) * cs;
-      const int j = b & (nb - 1);
-      const int k = j & (Ns - 1);
-      if (logNs > 0) {
+      const int j = b & (NB - 1);
+      const int c0 = (b >> LOGNB) * cs;
+      const int k = j & (NS - 1);
+      if constexpr (LOGNS > 0) {
+        const int t0 = (NS - 1) + k * (R - 1) - 1;  // this pass's twiddles, [k][r-1]
 #pragma unroll
-        for (int r = 1; r < R; ++r) v[q][r] = cmul(v[q][r], twiddle_raw<DIR>(twp, k * (R - 1) + (r - 1)));
+        for (int r = 1; r < R; ++r) v[q][r] = cmul(v[q][r], twiddle_raw<DIR>(tw, t0 + r));
       }
       dft_reg<R, DIR>(v[q]);
       const int o = ((j - k) << LR) + k;
+      if constexpr (NS % 16 == 0) {
+        const int o0 = c0 + pidx(o);
 #pragma unroll
-      for (int r = 0; r < R; ++r) base[pidx(o + (r << logNs))] = v[q][r];
+        for (int r = 0; r < R; ++r) buf[o0 + r * pstride<NS>()] = v[q][r];
+      } else if constexpr (NS == 1 && R == 16) {  // o = 16 j: padded 17 j + r
+        const int o0 = c0 + 17 * j;
+#pragma unroll
+        for (int r = 0; r < R; ++r) buf[o0 + r] = v[q][r];
+      } else {
+#pragma unroll
+        for (int r = 0; r < R; ++r) buf[c0 + pidx(o + r * NS)] = v[q][r];
+      }
     }
   }
   __syncthreads();
 }
 
-// In-place FFT of `ncols` padded columns of length 2^logL with radices up to
-// 2^MAXLR and 2^MAXLR values per thread (ncols*L <= 2^MAXLR*blockDim.x).
-// All threads of the block must call it.
-template <int DIR, int MAXLR>
-__device__ void fft_cols(float2* buf, int logL, int ncols, int cs, const float2* __restrict__ tw) {
-  constexpr int VPT = 1 << MAXLR;
-  if (logL == 0) return;
-  const int p = fft_npass(logL, MAXLR);
-  int logNs = 0;
-  for (int i = 0; i < p; ++i) {
-    const int lr = fft_pass_lr(logL, MAXLR, i);
-    if (lr == 1) stockham_pass<1, DIR, VPT>(buf, logL, logNs, ncols, cs, tw);
-    else if (lr == 2) stockham_pass<2, DIR, VPT>(buf, logL, logNs, ncols, cs, tw);
-    else if (lr == 3 || MAXLR == 3) stockham_pass<(MAXLR >= 3 ? 3 : 2), DIR, VPT>(buf, logL, logNs, ncols, cs, tw);
-    else stockham_pass<(MAXLR >= 4 ? 4 : 2), DIR, VPT>(buf, logL, logNs, ncols, cs, tw);
-    logNs += lr;
+template <int LOGL, int MAXLR, int PASS, int DIR>
+__device__ __forceinline__ void fft_passes(float2* buf, int ncols, int cs, const float2* tw) {
+  using PL = Plan<LOGL, MAXLR>;
+  if constexpr (PASS < PL::P) {
+    stockham_pass<LOGL, PL::lr(PASS), PL::logns(PASS), DIR, (1 << MAXLR)>(buf, ncols, cs, tw);
+    fft_passes<LOGL, MAXLR, PASS + 1, DIR>(buf, ncols, cs, tw);
   }
 }
 
-// FFT of many padded columns, in groups that fit 2^MAXLR values per thread.
+// FFT of many padded columns of length 2^LOGL, in groups that fit 2^MAXLR
+// values per thread.  All threads of the block must call it.
+template <int LOGL, int MAXLR, int DIR>
+__device__ __forceinline__ void fft_many_ct(float2* buf, int ncols, int cs, const float2* tw) {
+  const int per = max(1, ((1 << MAXLR) * (int)blockDim.x) >> LOGL);
+  for (int c0 = 0; c0 < ncols; c0 += per) fft_passes<LOGL, MAXLR, 0, DIR>(buf + c0 * cs, min(per, ncols - c0), cs, tw);
+}
+
+// Runtime length dispatch (2^logL <= 4096).
 template <int DIR, int MAXLR>
-__device__ void fft_many(float2* buf, int logL, int ncols, int cs, const float2* __restrict__ tw) {
-  if (logL == 0) return;
-  const int per = max(1, ((1 << MAXLR) * (int)blockDim.x) >> logL);
-  for (int c0 = 0; c0 < ncols; c0 += per) fft_cols<DIR, MAXLR>(buf + c0 * cs, logL, min(per, ncols - c0), cs, tw);
+__device__ __forceinline__ void fft_many(float2* buf, int logL, int ncols, int cs, const float2* tw) {
+  switch (logL) {
+    case 1: fft_many_ct<1, MAXLR, DIR>(buf, ncols, cs, tw); break;
+    case 2: fft_many_ct<2, MAXLR, DIR>(buf, ncols, cs, tw); break;
+    case 3: fft_many_ct<3, MAXLR, DIR>(buf, ncols, cs, tw); break;
+    case 4: fft_many_ct<4, MAXLR, DIR>(buf, ncols, cs, tw); break;
+    case 5: fft_many_ct<5, MAXLR, DIR>(buf, ncols, cs, tw); break;
+    case 6: fft_many_ct<6, MAXLR, DIR>(buf, ncols, cs, tw); break;
+    case 7: fft_many_ct<7, MAXLR, DIR>(buf, ncols, cs, tw); break;
+    case 8: fft_many_ct<8, MAXLR, DIR>(buf, ncols, cs, tw); break;
+    case 9: fft_many_ct<9, MAXLR, DIR>(buf, ncols, cs, tw); break;
+    case 10: fft_many_ct<10, MAXLR, DIR>(buf, ncols, cs, tw); break;
+    case 11: fft_many_ct<11, MAXLR, DIR>(buf, ncols, cs, tw); break;
+    case 12: fft_many_ct<12, MAXLR, DIR>(buf, ncols, cs, tw); break;
+    default: break;  // logL == 0: identity
+  }
 }
 
 }  // namespace mpx

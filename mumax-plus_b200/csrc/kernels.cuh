@@ -34,6 +34,13 @@ struct TableauDev {
 };
 __constant__ TableauDev c_tab;
 
+// Block size bounds: the x passes hold 8 FFT values per thread, so a block of
+// X_THREADS_MAX threads covers transforms of up to 8*X_THREADS_MAX points; the
+// y/z pass holds 16 per thread.
+constexpr int X_THREADS_MAX = 384;
+constexpr int X_VPT = 8;
+constexpr int YZ_VPT = 16;
+
 // Work item of the row-tile kernels: magnet slot, z, first row y0, rows in tile (<= 4).
 // Work item of k_yz: magnet slot, kx (in z).
 struct Work {
@@ -103,7 +110,7 @@ __device__ __forceinline__ int tile_row(int e, int n) { return (e >= n) + (e >= 
 // smem: padded rows [ty] for (Mx + i My) of each row, then [(ty+1)/2] for
 // (Mz(y) + i Mz(y+1)).
 template <bool COMBINE>
-__global__ void __launch_bounds__(512, 2) k_xfwd(const MagnetDev* __restrict__ mags, const GroupDev* __restrict__ groups,
+__global__ void __launch_bounds__(X_THREADS_MAX, 2) k_xfwd(const MagnetDev* __restrict__ mags, const GroupDev* __restrict__ groups,
                                               const Work* __restrict__ work, int stage, int gate,
                                               const float* __restrict__ msrc_override,
                                               const float2* __restrict__ tw) {
@@ -488,7 +495,7 @@ __device__ __forceinline__ void epilogue_cell(const MagnetDev& M, const GroupDev
 }
 
 // ------------------------------------------------------------------ k_xinv
-__global__ void __launch_bounds__(512, 2) k_xinv(const MagnetDev* __restrict__ mags, GroupDev* __restrict__ groups,
+__global__ void __launch_bounds__(X_THREADS_MAX, 2) k_xinv(const MagnetDev* __restrict__ mags, GroupDev* __restrict__ groups,
                                               const Work* __restrict__ work, EpiArgs ea,
                                               const float2* __restrict__ tw) {
   extern __shared__ float2 sm[];

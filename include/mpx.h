@@ -249,6 +249,25 @@ mpx_status mpx_advance(mpx_engine* e, int attempts);
  * of groups still running into *n_running. */
 mpx_status mpx_poll(mpx_engine* e, int* done, int cap, int* n_done, int* n_running);
 
+/* ---- allocation-free reduction ------------------------------------------ */
+/* No counterpart in the reference.  For callers that may not allocate device
+ * memory (a monitoring hook inside another application's loop, held to a fixed
+ * device-memory budget, that must not add a cudaMalloc's synchronisation or
+ * out-of-memory failure).  Reduces a field the caller holds on the current
+ * device -- `field` is SoA, ncomp components of `ncells` floats, `geometry`
+ * optional (NULL = all cells) -- over the cells in the geometry: op 0 =
+ * per-component sum, op 1 = max |v| (in out[0]); FP64 accumulation, the same
+ * kernels as mpx_average / mpx_max_norm.  Allocates nothing: its scratch is a
+ * static device array of 6168 bytes (256 block partials x 3 + 3 results) that
+ * every GPU loading the library holds until exit.  ncells must be in
+ * [1, 715827882] and ncomp in [1, 3]; larger sizes are rejected with
+ * MPX_ERR_INVALID.  The first call on a device looks up the array's device
+ * address (set-up); make that first call before any stream capture.  All calls
+ * share the array: calls that overlap on the GPU race.  Blocks until `out` is
+ * written; `stream` NULL = the legacy default stream. */
+mpx_status mpx_reduce_noalloc(const float* field, int ncells, int ncomp, const unsigned char* geometry, int op,
+                              void* stream, double out[3]);
+
 #ifdef __cplusplus
 }
 #endif

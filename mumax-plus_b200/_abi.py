@@ -162,6 +162,7 @@ SIGNATURES = {
     "mpx_group_start": (I, [E, I, C.c_double, C.c_double]),
     "mpx_advance": (I, [E, I]),
     "mpx_poll": (I, [E, P_I, I, P_I, P_I]),
+    "mpx_reduce_noalloc": (I, [C.c_void_p, I, I, C.c_void_p, I, C.c_void_p, P_D]),
 }
 
 

@@ -13,6 +13,7 @@
 #include <cstdint>
 #include <cstring>
 #include <memory>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -1594,3 +1595,66 @@ mpx_status mpx_poll(mpx_engine* e, int* done, int cap, int* n_done, int* n_runni
 }
 
 }  // extern "C"
+
+// ============================================ allocation-free reduction
+// mpx_reduce_noalloc is for callers that may not allocate device memory: a
+// diagnostic or monitoring hook running inside another application's time
+// loop, whose host gave it a fixed device-memory budget (its own pool, no
+// cudaMalloc of its own) and which must not add the device-wide
+// synchronisation or the out-of-memory failure a cudaMalloc can bring.  It is
+// the sum / max-norm reduction of mpx_average / mpx_max_norm, with the block
+// partials and the result kept in the static array below instead of in
+// engine-allocated memory, over a field the caller already holds on the device.
+namespace {
+
+constexpr int NOALLOC_BLOCKS = 256;   // fixed grid of the partial pass (256 threads each)
+constexpr int NOALLOC_RESULT = NOALLOC_BLOCKS * 3;
+constexpr long long NOALLOC_MAX_CELLS = 0x7fffffffLL / 3;  // 32-bit cell indices of 3 components
+
+// 256 blocks x 3 partials + 3 results = 6168 bytes.  It is part of the
+// library's device image: every GPU that loads libmpx.so holds it until the
+// process exits.  All calls share it.
+static __device__ __align__(256) double g_noalloc_scratch[NOALLOC_RESULT + 3];
+
+std::mutex g_noalloc_mutex;
+double* g_noalloc_ptr[128] = {nullptr};  // device address of the array, per device
+
+}  // namespace
+
+extern "C" mpx_status mpx_reduce_noalloc(const float* field, int ncells, int ncomp,
+                                         const unsigned char* geometry, int op, void* stream,
+                                         double out[3]) {
+  if (!field || !out) return fail(MPX_ERR_INVALID, "mpx_reduce_noalloc: null field or output");
+  if (ncomp < 1 || ncomp > 3) return fail(MPX_ERR_INVALID, "mpx_reduce_noalloc: ncomp must be 1, 2 or 3");
+  if (op != 0 && op != 1) return fail(MPX_ERR_INVALID, "mpx_reduce_noalloc: op must be 0 (sum) or 1 (max norm)");
+  if (ncells < 1 || (long long)ncells > NOALLOC_MAX_CELLS)
+    return fail(MPX_ERR_INVALID, "mpx_reduce_noalloc: ncells must be in [1, " + std::to_string(NOALLOC_MAX_CELLS) +
+                                     "]");
+  int dev = -1;
+  CUDA_TRY(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 128) return fail(MPX_ERR_RANGE, "mpx_reduce_noalloc: device index out of range");
+  double* scratch = nullptr;
+  {
+    // set-up, once per device with that device current: the array's name is a
+    // host-side stand-in, the kernels need its device address
+    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+    if (!g_noalloc_ptr[dev]) {
+      void* p = nullptr;
+      CUDA_TRY(cudaGetSymbolAddress(&p, g_noalloc_scratch));
+      g_noalloc_ptr[dev] = static_cast<double*>(p);
+    }
+    scratch = g_noalloc_ptr[dev];
+  }
+  cudaStream_t s = (cudaStream_t)stream;
+  // every partial slot the final pass reads is written by this call's partial
+  // pass, and the final pass overwrites the results: nothing needs clearing
+  k_reduce_partial<<<NOALLOC_BLOCKS, 256, 0, s>>>(field, ncells, ncomp, geometry, op, scratch);
+  k_reduce_final<<<1, 32, 0, s>>>(scratch, NOALLOC_BLOCKS, op, scratch + NOALLOC_RESULT);
+  cudaError_t st = cudaGetLastError();
+  if (st != cudaSuccess) return fail(MPX_ERR_CUDA, std::string("mpx_reduce_noalloc: ") + cudaGetErrorString(st));
+  CUDA_TRY(cudaMemcpyAsync(out, scratch + NOALLOC_RESULT, sizeof(double) * 3, cudaMemcpyDeviceToHost, s));
+  CUDA_TRY(cudaStreamSynchronize(s));
+  for (int c = ncomp; c < 3; ++c)
+    if (op == 0) out[c] = 0.0;
+  return MPX_OK;
+}

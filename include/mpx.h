@@ -190,8 +190,18 @@ mpx_status mpx_group_info_get(mpx_engine* e, int group, mpx_group_info* out);
 
 /* ---- magnets ------------------------------------------------------------ */
 /* Adds a ferromagnet to `group`; builds its FP64 Newell kernel spectrum when
- * demag is enabled.  Initial magnetization is +x until set. */
+ * demag is enabled.  The initial magnetization is random unit vectors seeded by
+ * the magnet id (the reference seeds with the clock, ferromagnet.cpp:62-76);
+ * an adaptive group's time step becomes the sensible one for that state
+ * (core/timesolver.cpp:49-52). */
 mpx_status mpx_magnet_add(mpx_engine* e, int group, const mpx_magnet_desc* d, int* magnet);
+/* Device bytes mpx_magnet_add would take for `d`: *resident stays allocated
+ * until the magnet is removed (state buffers, spectra, per-cell parameters,
+ * work tables); *transient is the extra peak while it is added (the FP64
+ * kernel construction buffers).  No engine or device needed; used to admit
+ * solves against a memory budget.  No counterpart in the reference, which
+ * allocates from its pool as fields are needed (core/gpumemorypool.cu). */
+mpx_status mpx_magnet_bytes(const mpx_magnet_desc* d, int64_t* resident, int64_t* transient);
 /* Re-reads all parameters; rebuilds the demag kernel only when the cell size,
  * geometry-independent grid data, mastergrid or PBC changed. */
 mpx_status mpx_magnet_update(mpx_engine* e, int magnet, const mpx_magnet_desc* d);
@@ -242,7 +252,9 @@ mpx_status mpx_solver_run(mpx_engine* e, int group, double duration);
  * group then advances with every mpx_advance call until it finishes. */
 mpx_status mpx_group_start(mpx_engine* e, int group, double duration, double torque_stop);
 /* Enqueues `attempts` Runge-Kutta attempts for every armed group (asynchronous,
- * CUDA-graph replay; finished groups skip their work on the device). */
+ * CUDA-graph replay).  Only the magnets of started groups are in the launch
+ * tables; a group that finishes on the device skips its work until the next
+ * mpx_poll takes it out of the tables. */
 mpx_status mpx_advance(mpx_engine* e, int attempts);
 /* Waits for enqueued work; writes up to `cap` ids of groups that finished
  * since the last poll into done[] and their count into *n_done, and the number

@@ -141,6 +141,7 @@ SIGNATURES = {
     "mpx_magnet_add": (I, [E, I, C.c_void_p, P_I]),
     "mpx_magnet_update": (I, [E, I, C.c_void_p]),
     "mpx_magnet_remove": (I, [E, I]),
+    "mpx_magnet_bytes": (I, [C.c_void_p, P_I64, P_I64]),
     "mpx_magnet_set_m": (I, [E, I, C.c_void_p, I]),
     "mpx_magnet_get_m": (I, [E, I, C.c_void_p, I]),
     "mpx_eval": (I, [E, I, I, C.c_void_p, I]),

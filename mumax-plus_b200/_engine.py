@@ -223,3 +223,10 @@ class Engine:
         nd, nr = C.c_int(), C.c_int()
         check(lib().mpx_poll(self._h, done, cap, C.byref(nd), C.byref(nr)))
         return [done[i] for i in range(nd.value)], nr.value
+
+
+def magnet_bytes(desc):
+    """(resident, transient) device bytes that adding `desc` takes (no GPU needed)."""
+    res, tr = C.c_int64(), C.c_int64()
+    check(_abi.load().mpx_magnet_bytes(C.byref(desc), C.byref(res), C.byref(tr)))
+    return res.value, tr.value

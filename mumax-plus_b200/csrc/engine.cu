@@ -132,7 +132,8 @@ struct Magnet {
   std::vector<void*> allocs;  // per-magnet device allocations (params, masks, buffers...)
   int64_t bytes = 0;
   bool demag = false;
-  int ty = 4;
+  int ty = 4;    // rows per x-pass tile
+  int nkx = 1;   // consecutive kx per y/z block
   int P[3] = {1, 1, 1};
   // kernel-defining geometry (rebuild the spectrum when it changes)
   int kkey_n[3], kkey_mg[3], kkey_pbc[3];
@@ -154,6 +155,7 @@ struct Group {
   int slot = -1;
   mpx_solver_params sp{MPX_RK_FEHLBERG, 1, 1e-5, 0.8, 0.5, 2.0, 0.01, 1e-14};
   std::vector<int> magnets;
+  bool active = false;  // started and not yet seen finished: its magnets are in the attempt tables
 };
 
 }  // namespace
@@ -161,6 +163,10 @@ struct Group {
 struct mpx_engine {
   int device = 0;
   cudaStream_t own = nullptr, stream = nullptr;
+  // stream-ordered pool for everything a magnet owns (kept reserved when freed,
+  // so adding and removing solves neither synchronises the device nor returns
+  // memory to the driver)
+  cudaMemPool_t pool = nullptr;
   std::vector<std::unique_ptr<Magnet>> mags;
   std::vector<std::unique_ptr<Group>> groups;
   MagnetDev* d_mags = nullptr;
@@ -207,15 +213,29 @@ struct DeviceGuard {
   }
 };
 
-mpx_status dalloc(mpx_engine* e, Magnet* m, void** p, size_t bytes) {
+// Stream-ordered allocation from the engine's pool (usable by every later
+// operation on the engine's stream).
+mpx_status palloc(mpx_engine* e, void** p, size_t bytes) {
   *p = nullptr;
   if (bytes == 0) return MPX_OK;
-  cudaError_t st = cudaMalloc(p, bytes);
+  cudaError_t st = cudaMallocFromPoolAsync(p, bytes, e->pool, e->stream);
   if (st != cudaSuccess) {
     cudaGetLastError();
+    *p = nullptr;
     return fail(MPX_ERR_NOMEM, "device allocation of " + std::to_string(bytes) + " bytes failed: " +
                                    cudaGetErrorString(st));
   }
+  return MPX_OK;
+}
+// Stream-ordered release: the memory returns to the pool once the work queued
+// before it on the engine's stream has finished.
+void pfree(mpx_engine* e, void* p) {
+  if (p) cudaFreeAsync(p, e->stream);
+}
+
+mpx_status dalloc(mpx_engine* e, Magnet* m, void** p, size_t bytes) {
+  MPX_TRY(palloc(e, p, bytes));
+  if (!*p) return MPX_OK;
   if (m) {
     m->allocs.push_back(*p);
     m->bytes += (int64_t)bytes;
@@ -225,7 +245,7 @@ mpx_status dalloc(mpx_engine* e, Magnet* m, void** p, size_t bytes) {
 }
 
 void free_magnet(mpx_engine* e, Magnet* m) {
-  for (void* p : m->allocs) cudaFree(p);
+  for (void* p : m->allocs) pfree(e, p);
   e->bytes -= m->bytes;
   m->allocs.clear();
   m->bytes = 0;
@@ -234,16 +254,16 @@ void free_magnet(mpx_engine* e, Magnet* m) {
 // Frees every device allocation of a magnet.
 void release_all(mpx_engine* e, Magnet* m) {
   free_magnet(e, m);
-  if (m->fields) cudaFree(m->fields);
-  if (m->spec) cudaFree(m->spec);
-  if (m->kspec) cudaFree(m->kspec);
+  pfree(e, m->fields);
+  pfree(e, m->spec);
+  pfree(e, m->kspec);
   e->bytes -= m->fields_bytes + m->spec_bytes + m->kspec_bytes;
   m->fields = nullptr;
   m->spec = nullptr;
   m->kspec = nullptr;
   m->fields_bytes = m->spec_bytes = m->kspec_bytes = 0;
-  if (m->d_tiles) cudaFree(m->d_tiles);
-  if (m->d_kxw) cudaFree(m->d_kxw);
+  pfree(e, m->d_tiles);
+  pfree(e, m->d_kxw);
   m->d_tiles = nullptr;
   m->d_kxw = nullptr;
 }
@@ -307,20 +327,22 @@ mpx_status ensure_group_capacity(mpx_engine* e, int slot) {
 
 mpx_status ensure_scratch(mpx_engine* e, size_t bytes) {
   if (bytes <= e->scratch_bytes) return MPX_OK;
-  if (e->d_scratch) cudaFree(e->d_scratch);
+  pfree(e, e->d_scratch);
   e->d_scratch = nullptr;
   e->scratch_bytes = 0;
-  CUDA_TRY(cudaMalloc(&e->d_scratch, bytes));
+  MPX_TRY(palloc(e, (void**)&e->d_scratch, bytes));
   e->scratch_bytes = bytes;
   return MPX_OK;
 }
 
+// Replaces *d by a device copy of v (stream-ordered: kernels queued before
+// still read the old table, which returns to the pool after them).
 template <typename T>
 mpx_status upload_vec(mpx_engine* e, Work** d, const std::vector<T>& v) {
-  if (*d) cudaFree(*d);
+  pfree(e, *d);
   *d = nullptr;
   if (v.empty()) return MPX_OK;
-  CUDA_TRY(cudaMalloc(d, sizeof(T) * v.size()));
+  MPX_TRY(palloc(e, (void**)d, sizeof(T) * v.size()));
   CUDA_TRY(cudaMemcpyAsync(*d, v.data(), sizeof(T) * v.size(), cudaMemcpyHostToDevice, e->stream));
   CUDA_TRY(cudaStreamSynchronize(e->stream));
   return MPX_OK;
@@ -330,9 +352,23 @@ mpx_status upload_vec(mpx_engine* e, Work** d, const std::vector<T>& v) {
 int x_smem(const Magnet* m) {
   return ((m->ty + (m->ty + 1) / 2) * plen(m->P[0]) + m->P[0]) * (int)sizeof(float2);
 }
-int yz_smem(const Magnet* m) { return (3 * m->dev.n[2] * plen(m->P[1]) + m->P[1]) * (int)sizeof(float2); }
+int yz_smem(const Magnet* m) {
+  return (m->nkx * 3 * m->dev.n[2] * plen(m->P[1]) + m->P[1]) * (int)sizeof(float2);
+}
 int yz_class(const Magnet* m) { return ilog2(m->P[2]); }
 constexpr int YZ_THREADS = 384;
+
+// Tile shapes.  Row tiles: about 4096 points of the padded x transform per
+// tile (4 rows from Px = 1024 up; up to TY_MAX rows of short transforms), or
+// of the row itself without demag.  y/z blocks: enough consecutive kx that a
+// block holds about YZ_VPT * YZ_THREADS points of y transforms.
+int choose_ty(int ny, int len) {
+  const int t = len >= 1024 ? 4 : std::min(TY_MAX, std::max(1, 4096 / len));
+  return std::max(1, std::min(t, ny));
+}
+int choose_nkx(int nz, int Py, int Fh) {
+  return std::max(1, std::min(Fh, (YZ_VPT * YZ_THREADS) / (3 * nz * Py)));
+}
 
 // k_yz<PZ> launch for one z-length class
 mpx_status launch_yz(mpx_engine* e, int cls, const Work* work, int n, int smem, int stage, int gate) {
@@ -351,7 +387,7 @@ int x_threads(const Magnet* m) {
   int rows = m->ty + (m->ty + 1) / 2;
   int t = (rows * m->P[0] + 7) / 8;  // 8 values per thread in the x FFTs
   t = ((t + 31) / 32) * 32;
-  return std::min(X_THREADS_MAX, std::max(256, t));
+  return std::min(X_THREADS_MAX, std::max(64, t));
 }
 
 mpx_status rebuild_tables(mpx_engine* e) {
@@ -359,9 +395,12 @@ mpx_status rebuild_tables(mpx_engine* e) {
   e->smem_x = 0;
   e->nt_x = 256;
   for (int c = 0; c < 5; ++c) e->smem_yz[c] = 0;
+  // only the magnets of started groups: finished and idle solves cost no blocks
   for (auto& mp : e->mags) {
     if (!mp) continue;
     Magnet* m = mp.get();
+    const Group* g = (m->group >= 0 && m->group < (int)e->groups.size()) ? e->groups[m->group].get() : nullptr;
+    if (!g || !g->active) continue;
     if (m->demag) {
       const int cls = yz_class(m);
       td.insert(td.end(), m->tiles.begin(), m->tiles.end());
@@ -400,13 +439,12 @@ mpx_status build_kernel_spectrum(mpx_engine* e, Magnet* m) {
   const long long PP = (long long)m->P[0] * m->P[1] * m->P[2];
   double* oct = nullptr;
   double2 *f0 = nullptr, *f1 = nullptr;
-  CUDA_TRY(cudaMalloc(&oct, sizeof(double) * 6 * noct));
-  cudaError_t st = cudaMalloc(&f0, sizeof(double2) * PP);
-  if (st == cudaSuccess) st = cudaMalloc(&f1, sizeof(double2) * PP);
-  if (st != cudaSuccess) {
-    cudaGetLastError();
-    cudaFree(oct);
-    if (f0) cudaFree(f0);
+  mpx_status ast = palloc(e, (void**)&oct, sizeof(double) * 6 * noct);
+  if (ast == MPX_OK) ast = palloc(e, (void**)&f0, sizeof(double2) * PP);
+  if (ast == MPX_OK) ast = palloc(e, (void**)&f1, sizeof(double2) * PP);
+  if (ast != MPX_OK) {
+    pfree(e, oct);
+    pfree(e, f0);
     return fail(MPX_ERR_NOMEM, "demag kernel construction: out of device memory");
   }
   const int grid = 148 * 8;
@@ -430,11 +468,11 @@ mpx_status build_kernel_spectrum(mpx_engine* e, Magnet* m) {
     k_kernel_extract<<<grid, 256, 0, e->stream>>>(m->kspec, in, kc, kcomp, m->P[0], m->P[1], m->P[2], pref);
     e->launches++;
   }
-  st = cudaGetLastError();
+  cudaError_t st = cudaGetLastError();
+  pfree(e, oct);
+  pfree(e, f0);
+  pfree(e, f1);
   cudaError_t st2 = cudaStreamSynchronize(e->stream);
-  cudaFree(oct);
-  cudaFree(f0);
-  cudaFree(f1);
   if (st != cudaSuccess) return fail(MPX_ERR_CUDA, std::string("kernel build launch: ") + cudaGetErrorString(st));
   if (st2 != cudaSuccess) return fail(MPX_ERR_CUDA, std::string("kernel build: ") + cudaGetErrorString(st2));
   m->kspec_ready = true;
@@ -598,14 +636,14 @@ mpx_status setup_magnet(mpx_engine* e, Magnet* m, const mpx_magnet_desc* d, bool
                   m->kkey_cs[a] == d->cellsize[a];
   }
   // release parameter allocations (everything except fields/spec/kspec which are tracked separately)
-  for (void* p : m->allocs) cudaFree(p);
+  for (void* p : m->allocs) pfree(e, p);
   e->bytes -= m->bytes;
   m->allocs.clear();
   m->bytes = 0;
   if (!same_grid) {
-    if (old_fields) cudaFree(old_fields);
-    if (old_spec) cudaFree(old_spec);
-    if (old_kspec) cudaFree(old_kspec);
+    pfree(e, old_fields);
+    pfree(e, old_spec);
+    pfree(e, old_kspec);
     e->bytes -= m->fields_bytes + m->spec_bytes + m->kspec_bytes;
     m->fields_bytes = m->spec_bytes = m->kspec_bytes = 0;
     m->fields = nullptr;
@@ -640,7 +678,8 @@ mpx_status setup_magnet(mpx_engine* e, Magnet* m, const mpx_magnet_desc* d, bool
   }
   D.Fh = m->P[0] / 2 + 1;
   D.kcomp = (m->P[2] == 1) ? 4 : 6;
-  m->ty = std::min(4, D.n[1]);
+  m->ty = choose_ty(D.n[1], m->demag ? m->P[0] : D.n[0]);
+  m->nkx = m->demag ? choose_nkx(D.n[2], m->P[1], D.Fh) : 1;
   if (m->demag) {
     if (m->P[0] > X_VPT * X_THREADS_MAX || m->P[1] > std::min(MAX_FFT, YZ_VPT * YZ_THREADS))
       return fail(MPX_ERR_UNSUPPORTED, "demag: padded FFT length above 2048 along x or 4096 along y "
@@ -690,10 +729,10 @@ mpx_status setup_magnet(mpx_engine* e, Magnet* m, const mpx_magnet_desc* d, bool
   for (int z = 0; z < D.n[2]; ++z)
     for (int y0 = 0; y0 < D.n[1]; y0 += m->ty) m->tiles.push_back(Work{m->slot, z, y0, std::min(m->ty, D.n[1] - y0)});
   if (m->demag)
-    for (int kx = 0; kx < D.Fh; ++kx) m->kxw.push_back(Work{m->slot, kx, 0, 0});
+    for (int kx = 0; kx < D.Fh; kx += m->nkx) m->kxw.push_back(Work{m->slot, kx, std::min(m->nkx, D.Fh - kx), 0});
   {
-    cudaFree(m->d_tiles);
-    cudaFree(m->d_kxw);
+    pfree(e, m->d_tiles);
+    pfree(e, m->d_kxw);
     m->d_tiles = nullptr;
     m->d_kxw = nullptr;
     MPX_TRY(upload_vec(e, &m->d_tiles, m->tiles));
@@ -894,6 +933,10 @@ mpx_status drive_group(mpx_engine* e, Group* g) {
     MPX_TRY(run_attempts(e, g->sp.method, chunk));
     GroupDev G;
     MPX_TRY(read_group(e, g->slot, &G));
+    if (G.status != GS_RUNNING) {
+      g->active = false;
+      e->tables_dirty = true;
+    }
     if (G.status == GS_FAILED) {
       G.status = GS_IDLE;
       G.finished_flag = 0;
@@ -907,24 +950,6 @@ mpx_status drive_group(mpx_engine* e, Group* g) {
       return MPX_OK;
     }
     chunk = std::min(chunk * 2, 16);
-  }
-}
-
-// Random unit vectors for a new magnet (the reference seeds its generator with
-// the clock, ferromagnet.cpp:62-76; here the seed is the magnet slot).
-void initial_random(std::vector<float>& m, int N, int seed) {
-  uint64_t s = 0x9E3779B97F4A7C15ull * (uint64_t)(seed + 1) + 12345;
-  auto next = [&]() {
-    s ^= s << 13;
-    s ^= s >> 7;
-    s ^= s << 17;
-    return (double)(s >> 11) * (1.0 / 9007199254740992.0);
-  };
-  m.resize(3 * (size_t)N);
-  for (size_t i = 0; i < m.size(); ++i) {  // Box-Muller
-    double u1 = next(), u2 = next();
-    if (u1 < 1e-300) u1 = 1e-300;
-    m[i] = (float)(std::sqrt(-2.0 * std::log(u1)) * std::cos(2 * M_PI * u2));
   }
 }
 
@@ -968,6 +993,17 @@ mpx_status mpx_engine_create(int device, mpx_engine** out) {
   e->device = device;
   CUDA_TRY(cudaStreamCreateWithFlags(&e->own, cudaStreamNonBlocking));
   e->stream = e->own;
+  {
+    cudaMemPoolProps props;
+    std::memset(&props, 0, sizeof(props));
+    props.allocType = cudaMemAllocationTypePinned;
+    props.handleTypes = cudaMemHandleTypeNone;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = device;
+    CUDA_TRY(cudaMemPoolCreate(&e->pool, &props));
+    uint64_t keep = UINT64_MAX;
+    CUDA_TRY(cudaMemPoolSetAttribute(e->pool, cudaMemPoolAttrReleaseThreshold, &keep));
+  }
   // twiddle table exp(-2 pi i k / 4096), computed in FP64
   std::vector<float2> tw(TW_N);
   for (int k = 0; k < TW_N; ++k) {
@@ -1005,10 +1041,12 @@ mpx_status mpx_engine_destroy(mpx_engine* e) {
   cudaFree(e->d_tw);
   cudaFree(e->d_red);
   cudaFree(e->d_redout);
-  cudaFree(e->d_scratch);
-  cudaFree(e->d_t_demag);
-  for (int c = 0; c < 5; ++c) cudaFree(e->d_kx_demag[c]);
-  cudaFree(e->d_t_local);
+  pfree(e, e->d_scratch);
+  pfree(e, e->d_t_demag);
+  for (int c = 0; c < 5; ++c) pfree(e, e->d_kx_demag[c]);
+  pfree(e, e->d_t_local);
+  cudaStreamSynchronize(e->stream);
+  if (e->pool) cudaMemPoolDestroy(e->pool);
   if (e->own) cudaStreamDestroy(e->own);
   delete e;
   return MPX_OK;
@@ -1016,6 +1054,9 @@ mpx_status mpx_engine_destroy(mpx_engine* e) {
 
 mpx_status mpx_engine_set_stream(mpx_engine* e, void* stream) {
   if (!e) return fail(MPX_ERR_INVALID, "null engine");
+  DeviceGuard guard(e->device);
+  // pool allocations and frees are ordered on the old stream: let them finish
+  CUDA_TRY(cudaStreamSynchronize(e->stream));
   e->stream = stream ? (cudaStream_t)stream : e->own;
   return MPX_OK;
 }
@@ -1145,12 +1186,14 @@ mpx_status mpx_magnet_add(mpx_engine* e, int group, const mpx_magnet_desc* d, in
     g_last_error = msg;
     return st;
   }
-  // initial magnetisation: normalised random vectors
-  std::vector<float> m0;
-  initial_random(m0, m->dev.N, slot);
-  const size_t bytes = sizeof(float) * m0.size();
-  MPX_TRY(ensure_scratch(e, bytes));
-  CUDA_TRY(cudaMemcpyAsync(e->d_scratch, m0.data(), bytes, cudaMemcpyHostToDevice, e->stream));
+  // initial magnetisation: normalised random vectors, generated on the device
+  // (the reference seeds its generator with the clock, ferromagnet.cpp:62-76;
+  // here the seed is the magnet slot)
+  const int n3 = 3 * m->dev.N;
+  MPX_TRY(ensure_scratch(e, sizeof(float) * (size_t)n3));
+  k_random_normal<<<std::min((n3 + 255) / 256, 148 * 16), 256, 0, e->stream>>>(
+      e->d_scratch, n3, 0x5DEECE66Dull * (unsigned long long)(slot + 1));
+  e->launches++;
   Magnet* mp = m.get();
   e->mags[slot] = std::move(m);
   g->magnets.push_back(slot);
@@ -1182,11 +1225,46 @@ mpx_status mpx_magnet_update(mpx_engine* e, int magnet, const mpx_magnet_desc* d
   return MPX_OK;
 }
 
+mpx_status mpx_magnet_bytes(const mpx_magnet_desc* d, int64_t* resident, int64_t* transient) {
+  if (!resident || !transient) return fail(MPX_ERR_INVALID, "null argument");
+  MPX_TRY(validate_desc(d));
+  const int64_t N = (int64_t)d->size[0] * d->size[1] * d->size[2];
+  int64_t res = 4 * 9 * 3 * N;  // state, stage and scratch buffers (setup_magnet)
+  for (const mpx_scalar* sc : {&d->msat, &d->aex, &d->alpha, &d->ku1, &d->ku2, &d->frozen_spins})
+    if (sc->cells) res += 4 * N;
+  for (int c = 0; c < 9; ++c)
+    if (d->dmi[c].cells) res += 4 * N;
+  if (d->anis_u.cells) res += 12 * N;
+  if (d->bias_magnetic_field.cells) res += 12 * N;
+  if (d->geometry) res += N;
+  if (d->regions) res += 4 * N;
+  const int64_t L = (int64_t)d->lut_regions * (d->lut_regions - 1) / 2;
+  if (L > 0) res += 4 * L * ((d->inter_exchange_lut ? 1 : 0) + (d->scale_exchange_lut ? 1 : 0));
+  const bool demag = d->enable_demag && !scalar_zero(d->msat);
+  const int ty = choose_ty(d->size[1], demag ? padded(d->size[0]) : d->size[0]);
+  res += (int64_t)sizeof(Work) * d->size[2] * ((d->size[1] + ty - 1) / ty);
+  int64_t tr = 12 * N;  // initial random state (engine scratch)
+  if (demag) {
+    int P[3];
+    for (int a = 0; a < 3; ++a) P[a] = padded(d->size[a]);
+    const int64_t Fh = P[0] / 2 + 1;
+    const int kc = (P[2] == 1) ? 4 : 6;
+    res += 8 * Fh * 3 * d->size[1] * d->size[2];                 // spectrum S[kx][c][z][y]
+    res += 4 * Fh * (P[1] / 2 + 1) * (P[2] / 2 + 1) * kc;        // kernel spectrum
+    const int nkx = choose_nkx(d->size[2], P[1], (int)Fh);
+    res += (int64_t)sizeof(Work) * ((Fh + nkx - 1) / nkx);       // y/z work items
+    tr += 8 * 6 * N + 2 * 16 * (int64_t)P[0] * P[1] * P[2];    // FP64 octant + two transform buffers
+  }
+  *resident = res;
+  *transient = tr;
+  return MPX_OK;
+}
+
 mpx_status mpx_magnet_remove(mpx_engine* e, int magnet) {
   Magnet* m = get_mag(e, magnet);
   if (!m) return fail(MPX_ERR_RANGE, "no such magnet");
   DeviceGuard guard(e->device);
-  cudaStreamSynchronize(e->stream);
+  // frees are stream-ordered: attempts queued before still see the buffers
   Group* g = get_group(e, m->group);
   if (g) g->magnets.erase(std::remove(g->magnets.begin(), g->magnets.end(), magnet), g->magnets.end());
   release_all(e, m);
@@ -1372,12 +1450,12 @@ mpx_status mpx_demag_kernel(mpx_engine* e, int magnet, float* out, int dims[3]) 
   }
   const size_t KK = (size_t)K[0] * K[1] * K[2];
   float* d = nullptr;
-  CUDA_TRY(cudaMalloc(&d, sizeof(float) * 6 * KK));
+  MPX_TRY(palloc(e, (void**)&d, sizeof(float) * 6 * KK));
   k_newell_reflayout<<<148 * 8, 128, 0, e->stream>>>(d, g, K[0], K[1], K[2], O[0], O[1], O[2]);
   e->launches++;
   cudaError_t st = cudaMemcpyAsync(out, d, sizeof(float) * 6 * KK, cudaMemcpyDeviceToHost, e->stream);
+  pfree(e, d);
   if (st == cudaSuccess) st = cudaStreamSynchronize(e->stream);
-  cudaFree(d);
   if (st != cudaSuccess) return fail(MPX_ERR_CUDA, cudaGetErrorString(st));
   return MPX_OK;
 }
@@ -1503,6 +1581,10 @@ static mpx_status start_group(mpx_engine* e, Group* g, int mode, long long nstep
   }
   G.status = GS_RUNNING;
   MPX_TRY(write_group(e, g->slot, &G));
+  if (!g->active) {
+    g->active = true;
+    e->tables_dirty = true;
+  }
   return MPX_OK;
 }
 
@@ -1580,6 +1662,10 @@ mpx_status mpx_poll(mpx_engine* e, int* done, int cap, int* n_done, int* n_runni
   for (int i = 0; i < ng; ++i) {
     if (!e->groups[i]) continue;
     if (G[i].status == GS_RUNNING) nr++;
+    if (G[i].status != GS_RUNNING && e->groups[i]->active) {  // drop it from the attempt tables
+      e->groups[i]->active = false;
+      e->tables_dirty = true;
+    }
     if (G[i].finished_flag && nd < cap) {
       if (done) done[nd] = i;
       nd++;

@@ -41,8 +41,9 @@ constexpr int X_THREADS_MAX = 384;
 constexpr int X_VPT = 8;
 constexpr int YZ_VPT = 16;
 
-// Work item of the row-tile kernels: magnet slot, z, first row y0, rows in tile (<= 4).
-// Work item of k_yz: magnet slot, kx (in z).
+// Work item of the row-tile kernels: magnet slot, z, first row y0, rows in tile (<= TY_MAX).
+// Work item of k_yz: magnet slot, first kx (in z), number of consecutive kx (in y0).
+constexpr int TY_MAX = 16;
 struct Work {
   int mag, z, y0, ty;
 };
@@ -103,8 +104,18 @@ __device__ __forceinline__ float3 combine_cell(const MagnetDev& M, const GroupDe
   return f3(v.x * inv, v.y * inv, v.z * inv);
 }
 
-// row index within a tile of at most 4 rows of length n, without division
-__device__ __forceinline__ int tile_row(int e, int n) { return (e >= n) + (e >= 2 * n) + (e >= 3 * n); }
+// Row index e / n within a tile of at most TY_MAX rows of length n, without
+// an integer division: a float estimate of (e + 1/2) / n (exact unless n is
+// very large) corrected by one step either way.
+__device__ __forceinline__ int tile_row(int e, int n, float rn) {
+  int r = (int)(((float)e + 0.5f) * rn);
+  r -= (r * n > e) ? 1 : 0;
+  r += ((r + 1) * n <= e) ? 1 : 0;
+  return r;
+}
+
+// log2 of the power of two >= ty (ty <= TY_MAX): row slots of a tile
+__device__ __forceinline__ int tile_log(int ty) { return ty <= 1 ? 0 : 32 - __clz(ty - 1); }
 
 // ------------------------------------------------------------------ k_xfwd
 // smem: padded rows [ty] for (Mx + i My) of each row, then [(ty+1)/2] for
@@ -160,10 +171,11 @@ __global__ void __launch_bounds__(X_THREADS_MAX, 2) k_xfwd(const MagnetDev* __re
   // unpack the two real transforms of each complex row and store the half spectrum
   const int Fh = M.Fh;
   float2* S = M.spec;
-  for (int e = threadIdx.x; e < Fh * 12; e += blockDim.x) {
-    const int yl = e & 3;
+  const int tyl = tile_log(ty);
+  for (int e = threadIdx.x; e < (Fh * 3) << tyl; e += blockDim.x) {
+    const int yl = e & ((1 << tyl) - 1);
     if (yl >= ty) continue;
-    const int rest = e >> 2;
+    const int rest = e >> tyl;
     const int c = rest % 3, kx = rest / 3;
     const float2* Z = (c < 2) ? (sm + yl * cs) : (sm + (ty + (yl >> 1)) * cs);
     const float2 zk = Z[pidx(kx)];
@@ -315,12 +327,12 @@ __global__ void __launch_bounds__(384) k_yz(const MagnetDev* __restrict__ mags, 
   __shared__ GroupDev G;
   const Work wk = work[blockIdx.x];
   if (!load_descs(M, G, mags, groups, wk.mag, gate, stage)) return;
-  const int kx = wk.z;
+  const int kx0 = wk.z, nkx = wk.y0;
   const int ny = M.n[1], nz = M.n[2];
   const int logPy = M.logP[1], Py = 1 << logPy, cs = plen(Py);
-  float2* S = M.spec + (size_t)kx * 3 * nz * ny;
-  float2* D = sm;  // [3*nz] padded columns of length Py
-  const int ncol = 3 * nz;
+  float2* S = M.spec + (size_t)kx0 * 3 * nz * ny;  // the nkx slabs are consecutive
+  float2* D = sm;  // [nkx][3*nz] padded columns of length Py
+  const int ncol = nkx * 3 * nz;
   float2* tws = sm + ncol * cs;  // twiddles of length Py
   load_twiddles<4>(tws, tw, logPy);
   // slab load: 8 independent read-only loads in flight per thread
@@ -342,9 +354,16 @@ __global__ void __launch_bounds__(384) k_yz(const MagnetDev* __restrict__ mags, 
   __syncthreads();
   fft_many<-1, 4>(D, logPy, ncol, cs, tws);
   if constexpr (PZ == 1) {
-    for (int ky = threadIdx.x; ky < Py; ky += blockDim.x) zstage_single(D, cs, M, kx, ky, Py);
+    for (int t = threadIdx.x; t < nkx << logPy; t += blockDim.x) {
+      const int j = t >> logPy;
+      zstage_single(D + j * 3 * cs, cs, M, kx0 + j, t & (Py - 1), Py);
+    }
   } else {
-    for (int t = threadIdx.x; t < 2 * Py; t += blockDim.x) zstage_pair<PZ>(D, cs, M, kx, t >> 1, t & 1, nz, Py);
+    // lanes 2u and 2u+1 share one (kx, ky): the even and odd kz halves
+    for (int t = threadIdx.x; t < (2 * nkx) << logPy; t += blockDim.x) {
+      const int u = t >> 1, j = u >> logPy;
+      zstage_pair<PZ>(D + j * 3 * nz * cs, cs, M, kx0 + j, u & (Py - 1), t & 1, nz, Py);
+    }
   }
   __syncthreads();
   fft_many<1, 4>(D, logPy, ncol, cs, tws);
@@ -514,9 +533,10 @@ __global__ void __launch_bounds__(X_THREADS_MAX, 2) k_xinv(const MagnetDev* __re
   const float2* __restrict__ S = M.spec;
   const size_t cstride = (size_t)nz * ny;
   // rebuild full-length Hermitian rows: Z = A + iB
+  const int tyl = tile_log(ty);
 #pragma unroll 2
-  for (int e = threadIdx.x; e < Fh * 4; e += blockDim.x) {
-    const int yl = e & 3, kx = e >> 2;
+  for (int e = threadIdx.x; e < Fh << tyl; e += blockDim.x) {
+    const int yl = e & ((1 << tyl) - 1), kx = e >> tyl;
     if (yl >= ty) continue;
     const size_t base = (size_t)kx * 3 * cstride + (size_t)z * ny + y0 + yl;
     float2 A = __ldg(S + base), B = __ldg(S + base + cstride);
@@ -544,8 +564,9 @@ __global__ void __launch_bounds__(X_THREADS_MAX, 2) k_xinv(const MagnetDev* __re
   const float* m = ea.msrc ? ea.msrc : stage_m(M, G, ea.stage);
   double en = 0.0, tn = 0.0;
   const int rowbase = nx * (y0 + ny * z);
+  const float rn = 1.0f / (float)nx;
   for (int e = threadIdx.x; e < ty * nx; e += blockDim.x) {
-    const int yl = tile_row(e, nx), x = e - yl * nx;
+    const int yl = tile_row(e, nx, rn), x = e - yl * nx;
     const int i = rowbase + e;
     float3 bd = f3(0, 0, 0);
     if (in_geom(M, i)) {
@@ -572,8 +593,9 @@ __global__ void __launch_bounds__(256) k_local(const MagnetDev* __restrict__ mag
   const float* m = ea.msrc ? ea.msrc : stage_m(M, G, ea.stage);
   double en = 0.0, tn = 0.0;
   const int rowbase = nx * (wk.y0 + ny * wk.z);
+  const float rn = 1.0f / (float)nx;
   for (int e = threadIdx.x; e < wk.ty * nx; e += blockDim.x) {
-    const int yl = tile_row(e, nx), x = e - yl * nx;
+    const int yl = tile_row(e, nx, rn), x = e - yl * nx;
     double a = 0.0, b = 0.0;
     epilogue_cell(M, G, ea, m, x, wk.y0 + yl, wk.z, rowbase + e, f3(0, 0, 0), a, b);
     en = (a > en || a != a) ? a : en;
@@ -753,6 +775,21 @@ __global__ void k_normalize_into(float* dst, const float* __restrict__ src, int 
   dst[i] = x;
   dst[N + i] = y;
   dst[2 * N + i] = z;
+}
+
+// n normal(0,1) numbers for the initial magnetisation of a new magnet: the
+// splitmix64 finaliser of (seed, index) (Steele, Lea and Flood, OOPSLA 2014)
+// gives two 24-bit uniforms, turned into one normal by Box-Muller.
+__global__ void k_random_normal(float* __restrict__ out, int n, unsigned long long seed) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    unsigned long long z = seed + 0x9E3779B97F4A7C15ull * (unsigned long long)(i + 1);
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    z ^= z >> 31;
+    const float u1 = (float)((unsigned)(z >> 40) + 1u) * (1.0f / 16777216.0f);  // (0, 1]
+    const float u2 = (float)(unsigned)(z & 0xFFFFFFull) * (1.0f / 16777216.0f);  // [0, 1)
+    out[i] = sqrtf(-2.0f * logf(u1)) * cospif(2.0f * u2);
+  }
 }
 
 }  // namespace mpx

@@ -149,9 +149,11 @@ class _Pacer:
         return self.n
 
 
-def relax_batch(batch, instances, duration=2e-9, torque_stop=1e-4, fetch=True):
+def relax_batch(batch, instances, duration=2e-9, torque_stop=1e-4, fetch=True, trace=None):
     """Add every instance, start them all, advance until all have finished.
-    Returns (solves, seconds of the integration loop, seconds of set-up)."""
+    Returns (solves, seconds of the integration loop, seconds of set-up).
+    `trace`, a list, receives (seconds, attempts, solves running, cells
+    running) at every poll."""
     t0 = time.perf_counter()
     solves = [batch.add(w, key=i) for i, w in enumerate(instances)]
     batch.engine.synchronize()
@@ -161,15 +163,21 @@ def relax_batch(batch, instances, duration=2e-9, torque_stop=1e-4, fetch=True):
     pacer = _Pacer()
     t0 = time.perf_counter()
     running = len(solves)
+    cells = sum(s.cells for s in solves)
+    attempts = 0
     while running:
         n = pacer.n
         ta = time.perf_counter()
         batch.advance(n)
         done, running = batch.poll()
         pacer.update(n, time.perf_counter() - ta)
+        attempts += n
         for s in done:
             batch.finish(s, fetch=fetch)
             s.t_done = time.perf_counter() - t0
+            cells -= s.cells
+        if trace is not None:
+            trace.append((time.perf_counter() - t0, attempts, running, cells))
     return solves, time.perf_counter() - t0, t_setup
 
 

@@ -186,16 +186,19 @@ struct mpx_engine {
   Work* d_kx_demag[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
   int n_kx_demag[5] = {0, 0, 0, 0, 0};
   int smem_yz[5] = {0, 0, 0, 0, 0};
+  int maxpy_yz[5] = {0, 0, 0, 0, 0};  // longest y transform of each class
   int smem_x = 0, nt_x = 256;
   bool any_nodemag = false;
   int64_t bytes = 0;
   int64_t launches = 0;
   double wb[3] = {0, 0, 0};
   int tab_method = -1;
-  // CUDA graph of one attempt
-  cudaGraphExec_t graph = nullptr;
+  // CUDA graphs of one attempt: every stage, and (FSAL methods) without
+  // stage 0, whose torque k0 is the last stage of the previous step
+  cudaGraphExec_t graph = nullptr, graph_nok0 = nullptr;
   int graph_method = -1;
   bool graph_dirty = true;
+  bool need_stage0 = true;  // some started group may lack a valid k0
 };
 
 namespace {
@@ -283,6 +286,7 @@ mpx_status read_group(mpx_engine* e, int g, GroupDev* out) {
   return MPX_OK;
 }
 mpx_status write_group(mpx_engine* e, int g, const GroupDev* in) {
+  if (!in->k0_valid) e->need_stage0 = true;  // the next attempt must evaluate k0
   CUDA_TRY(cudaMemcpyAsync(e->d_groups + g, in, sizeof(GroupDev), cudaMemcpyHostToDevice, e->stream));
   CUDA_TRY(cudaStreamSynchronize(e->stream));
   return MPX_OK;
@@ -350,7 +354,7 @@ mpx_status upload_vec(mpx_engine* e, Work** d, const std::vector<T>& v) {
 
 // dynamic shared memory: padded rows / columns plus the twiddle table of the length
 int x_smem(const Magnet* m) {
-  return ((m->ty + (m->ty + 1) / 2) * plen(m->P[0]) + m->P[0]) * (int)sizeof(float2);
+  return ((m->ty + (m->ty + 1) / 2) * xstride(m->P[0]) + m->P[0]) * (int)sizeof(float2);
 }
 int yz_smem(const Magnet* m) {
   return (m->nkx * 3 * m->dev.n[2] * plen(m->P[1]) + m->P[1]) * (int)sizeof(float2);
@@ -371,15 +375,19 @@ int choose_nkx(int nz, int Py, int Fh) {
 }
 
 // k_yz<PZ> launch for one z-length class
-mpx_status launch_yz(mpx_engine* e, int cls, const Work* work, int n, int smem, int stage, int gate) {
+// (the radix-8 variant for z lengths up to 8 when every y length of the class is <= 2048)
+mpx_status launch_yz(mpx_engine* e, int cls, const Work* work, int n, int smem, int stage, int gate, int max_py) {
   if (n <= 0) return MPX_OK;
+  const bool r8 = max_py <= 2048;
+#define MPX_YZ(PZ, LR) k_yz<PZ, LR><<<n, YZ_THREADS, smem, e->stream>>>(e->d_mags, e->d_groups, work, stage, gate, e->d_tw)
   switch (cls) {
-    case 0: k_yz<1><<<n, YZ_THREADS, smem, e->stream>>>(e->d_mags, e->d_groups, work, stage, gate, e->d_tw); break;
-    case 1: k_yz<2><<<n, YZ_THREADS, smem, e->stream>>>(e->d_mags, e->d_groups, work, stage, gate, e->d_tw); break;
-    case 2: k_yz<4><<<n, YZ_THREADS, smem, e->stream>>>(e->d_mags, e->d_groups, work, stage, gate, e->d_tw); break;
-    case 3: k_yz<8><<<n, YZ_THREADS, smem, e->stream>>>(e->d_mags, e->d_groups, work, stage, gate, e->d_tw); break;
-    default: k_yz<16><<<n, YZ_THREADS, smem, e->stream>>>(e->d_mags, e->d_groups, work, stage, gate, e->d_tw); break;
+    case 0: if (r8) MPX_YZ(1, 3); else MPX_YZ(1, 4); break;
+    case 1: if (r8) MPX_YZ(2, 3); else MPX_YZ(2, 4); break;
+    case 2: if (r8) MPX_YZ(4, 3); else MPX_YZ(4, 4); break;
+    case 3: if (r8) MPX_YZ(8, 3); else MPX_YZ(8, 4); break;
+    default: MPX_YZ(16, 4); break;
   }
+#undef MPX_YZ
   e->launches++;
   return MPX_OK;
 }
@@ -394,7 +402,7 @@ mpx_status rebuild_tables(mpx_engine* e) {
   std::vector<Work> td, tl, kd[5];
   e->smem_x = 0;
   e->nt_x = 256;
-  for (int c = 0; c < 5; ++c) e->smem_yz[c] = 0;
+  for (int c = 0; c < 5; ++c) e->smem_yz[c] = e->maxpy_yz[c] = 0;
   // only the magnets of started groups: finished and idle solves cost no blocks
   for (auto& mp : e->mags) {
     if (!mp) continue;
@@ -407,6 +415,7 @@ mpx_status rebuild_tables(mpx_engine* e) {
       kd[cls].insert(kd[cls].end(), m->kxw.begin(), m->kxw.end());
       e->smem_x = std::max(e->smem_x, x_smem(m));
       e->smem_yz[cls] = std::max(e->smem_yz[cls], yz_smem(m));
+      e->maxpy_yz[cls] = std::max(e->maxpy_yz[cls], m->P[1]);
       e->nt_x = std::max(e->nt_x, x_threads(m));
     } else {
       tl.insert(tl.end(), m->tiles.begin(), m->tiles.end());
@@ -787,7 +796,7 @@ mpx_status eval_into(mpx_engine* e, Magnet* m, int q, float* out) {
   if (m->demag && needs_demag) {
     const int sx = x_smem(m), syz = yz_smem(m), nt = x_threads(m);
     k_xfwd<false><<<ntile, nt, sx, e->stream>>>(e->d_mags, e->d_groups, m->d_tiles, 0, 0, nullptr, e->d_tw);
-    MPX_TRY(launch_yz(e, yz_class(m), m->d_kxw, (int)m->kxw.size(), syz, 0, 0));
+    MPX_TRY(launch_yz(e, yz_class(m), m->d_kxw, (int)m->kxw.size(), syz, 0, 0, m->P[1]));
     k_xinv<<<ntile, nt, sx, e->stream>>>(e->d_mags, e->d_groups, m->d_tiles, ea, e->d_tw);
     e->launches += 2;
   } else {
@@ -798,9 +807,9 @@ mpx_status eval_into(mpx_engine* e, Magnet* m, int q, float* out) {
 }
 
 // One Runge-Kutta attempt for every running group (core/rungekutta.cpp:39-83).
-mpx_status launch_attempt(mpx_engine* e, const TableauDev& T) {
+mpx_status launch_attempt(mpx_engine* e, const TableauDev& T, int first_stage) {
   const int S = T.S;
-  for (int s = 0; s < S; ++s) {
+  for (int s = first_stage; s < S; ++s) {
     EpiArgs ea;
     ea.mode = EPI_STAGE;
     ea.stage = s;
@@ -816,7 +825,8 @@ mpx_status launch_attempt(mpx_engine* e, const TableauDev& T) {
       else
         k_xfwd<true><<<e->n_t_demag, e->nt_x, e->smem_x, e->stream>>>(e->d_mags, e->d_groups, e->d_t_demag, s, 1,
                                                                       nullptr, e->d_tw);
-      for (int c = 0; c < 5; ++c) MPX_TRY(launch_yz(e, c, e->d_kx_demag[c], e->n_kx_demag[c], e->smem_yz[c], s, 1));
+      for (int c = 0; c < 5; ++c)
+        MPX_TRY(launch_yz(e, c, e->d_kx_demag[c], e->n_kx_demag[c], e->smem_yz[c], s, 1, e->maxpy_yz[c]));
       k_xinv<<<e->n_t_demag, e->nt_x, e->smem_x, e->stream>>>(e->d_mags, e->d_groups, e->d_t_demag, ea, e->d_tw);
       e->launches += 2;
     }
@@ -851,44 +861,63 @@ mpx_status prepare_run(mpx_engine* e, int method) {
   return MPX_OK;
 }
 
-// Replays `n` attempts (through a CUDA graph of one attempt).
+// Captures one attempt (from `first_stage` on) as an executable graph.
+mpx_status capture_attempt(mpx_engine* e, const TableauDev& T, int first_stage, cudaGraphExec_t* out) {
+  if (*out) {
+    cudaGraphExecDestroy(*out);
+    *out = nullptr;
+  }
+  cudaGraph_t g = nullptr;
+  CUDA_TRY(cudaStreamBeginCapture(e->stream, cudaStreamCaptureModeThreadLocal));
+  const int64_t before = e->launches;
+  mpx_status st = launch_attempt(e, T, first_stage);
+  cudaError_t ce = cudaStreamEndCapture(e->stream, &g);
+  e->launches = before;
+  if (st != MPX_OK) {
+    if (g) cudaGraphDestroy(g);
+    return st;
+  }
+  if (ce != cudaSuccess) return fail(MPX_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(ce));
+  ce = cudaGraphInstantiate(out, g, 0);
+  cudaGraphDestroy(g);
+  if (ce != cudaSuccess) return fail(MPX_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(ce));
+  return MPX_OK;
+}
+
+// Kernel launches of one attempt from `first_stage` on (for the launch counter).
+int attempt_launches(const mpx_engine* e, const TableauDev& T, int first_stage) {
+  const int S = T.S, ns = S - first_stage;
+  int nyz = 0;
+  for (int c = 0; c < 5; ++c) nyz += e->n_kx_demag[c] > 0 ? 1 : 0;
+  int per = 1;  // controller
+  if (e->n_t_demag > 0) per += (2 + nyz) * ns + (T.fsal ? 0 : 1);
+  if (e->n_t_local > 0) per += ns + (ns - (first_stage == 0 ? 1 : 0)) + (T.fsal ? 0 : 1);
+  return per;
+}
+
+// Replays `n` attempts through the CUDA graphs of one attempt.  With an FSAL
+// method only the first attempt after a state change evaluates stage 0 (every
+// started group then holds its k0); the others replay the graph without it.
 mpx_status run_attempts(mpx_engine* e, int method, int n) {
   MPX_TRY(prepare_run(e, method));
   const TableauDev T = make_tableau(method);
   if (e->graph_dirty || e->graph_method != method || !e->graph) {
-    if (e->graph) {
-      cudaGraphExecDestroy(e->graph);
-      e->graph = nullptr;
+    MPX_TRY(capture_attempt(e, T, 0, &e->graph));
+    if (T.fsal) {
+      MPX_TRY(capture_attempt(e, T, 1, &e->graph_nok0));
+    } else if (e->graph_nok0) {
+      cudaGraphExecDestroy(e->graph_nok0);
+      e->graph_nok0 = nullptr;
     }
-    cudaGraph_t g = nullptr;
-    CUDA_TRY(cudaStreamBeginCapture(e->stream, cudaStreamCaptureModeThreadLocal));
-    const int64_t before = e->launches;
-    mpx_status st = launch_attempt(e, T);
-    cudaError_t ce = cudaStreamEndCapture(e->stream, &g);
-    e->launches = before;
-    if (st != MPX_OK) {
-      if (g) cudaGraphDestroy(g);
-      return st;
-    }
-    if (ce != cudaSuccess) return fail(MPX_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(ce));
-    ce = cudaGraphInstantiate(&e->graph, g, 0);
-    cudaGraphDestroy(g);
-    if (ce != cudaSuccess) return fail(MPX_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(ce));
     e->graph_method = method;
     e->graph_dirty = false;
   }
-  // launches per attempt (for the launch counter)
-  int per = 1;
-  {
-    const int S = T.S;
-    int nyz = 0;
-    for (int c = 0; c < 5; ++c) nyz += e->n_kx_demag[c] > 0 ? 1 : 0;
-    if (e->n_t_demag > 0) per += (2 + nyz) * S + (T.fsal ? 0 : 1);
-    if (e->n_t_local > 0) per += S + (S - 1) + (T.fsal ? 0 : 1);
-  }
+  const int per_full = attempt_launches(e, T, 0), per_nok0 = attempt_launches(e, T, 1);
   for (int i = 0; i < n; ++i) {
-    CUDA_TRY(cudaGraphLaunch(e->graph, e->stream));
-    e->launches += per;
+    const bool full = e->need_stage0 || !e->graph_nok0;
+    CUDA_TRY(cudaGraphLaunch(full ? e->graph : e->graph_nok0, e->stream));
+    e->launches += full ? per_full : per_nok0;
+    e->need_stage0 = false;
   }
   return MPX_OK;
 }
@@ -1016,8 +1045,9 @@ mpx_status mpx_engine_create(int device, mpx_engine** out) {
   CUDA_TRY(cudaMalloc(&e->d_redout, sizeof(double) * 3));
   // large dynamic shared memory and the max-shared carveout for the FFT kernels
   const void* fft_kernels[] = {(const void*)k_xfwd<false>, (const void*)k_xfwd<true>, (const void*)k_xinv,
-                               (const void*)k_yz<1>, (const void*)k_yz<2>, (const void*)k_yz<4>,
-                               (const void*)k_yz<8>, (const void*)k_yz<16>};
+                               (const void*)k_yz<1, 4>, (const void*)k_yz<2, 4>, (const void*)k_yz<4, 4>,
+                               (const void*)k_yz<8, 4>, (const void*)k_yz<16, 4>, (const void*)k_yz<1, 3>,
+                               (const void*)k_yz<2, 3>, (const void*)k_yz<4, 3>, (const void*)k_yz<8, 3>};
   for (const void* k : fft_kernels) {
     cudaFuncAttributes fa;
     CUDA_TRY(cudaFuncGetAttributes(&fa, k));
@@ -1034,6 +1064,7 @@ mpx_status mpx_engine_destroy(mpx_engine* e) {
   DeviceGuard guard(e->device);
   cudaStreamSynchronize(e->stream);
   if (e->graph) cudaGraphExecDestroy(e->graph);
+  if (e->graph_nok0) cudaGraphExecDestroy(e->graph_nok0);
   for (auto& m : e->mags)
     if (m) release_all(e, m.get());
   cudaFree(e->d_mags);
@@ -1398,7 +1429,7 @@ mpx_status mpx_profile_eval(mpx_engine* e, int magnet, int reps, double ms[4]) {
       CUDA_TRY(cudaEventRecord(ev[0], e->stream));
       k_xfwd<false><<<ntile, nt, sx, e->stream>>>(e->d_mags, e->d_groups, m->d_tiles, 0, 0, nullptr, e->d_tw);
       CUDA_TRY(cudaEventRecord(ev[1], e->stream));
-      MPX_TRY(launch_yz(e, yz_class(m), m->d_kxw, (int)m->kxw.size(), syz, 0, 0));
+      MPX_TRY(launch_yz(e, yz_class(m), m->d_kxw, (int)m->kxw.size(), syz, 0, 0, m->P[1]));
       CUDA_TRY(cudaEventRecord(ev[2], e->stream));
       k_xinv<<<ntile, nt, sx, e->stream>>>(e->d_mags, e->d_groups, m->d_tiles, ea, e->d_tw);
       CUDA_TRY(cudaEventRecord(ev[3], e->stream));

@@ -34,6 +34,10 @@ __device__ __forceinline__ float2 cconj(float2 a) { return make_float2(a.x, -a.y
 // padded shared-memory index and padded column length
 __device__ __forceinline__ int pidx(int i) { return i + (i >> 4); }
 __host__ __device__ constexpr int plen(int L) { return L + (L >> 4); }
+// Row stride of the x passes: the padded length plus 4 complex values, so that
+// consecutive rows start 8 banks apart (the row unpack and gather read the same
+// x of several rows at once).
+__host__ __device__ constexpr int xstride(int L) { return plen(L) + 4; }
 
 // Twiddle of entry e of a per-pass shared-memory table (DIR = -1 forward, +1 inverse)
 template <int DIR>

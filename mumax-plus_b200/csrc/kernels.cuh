@@ -132,7 +132,7 @@ __global__ void __launch_bounds__(X_THREADS_MAX, 2) k_xfwd(const MagnetDev* __re
   if (!load_descs(M, G, mags, groups, wk.mag, gate, stage)) return;
   const int z = wk.z, y0 = wk.y0, ty = wk.ty;
   const int nx = M.n[0], ny = M.n[1], nz = M.n[2], N = M.N;
-  const int logL = M.logP[0], L = 1 << logL, cs = plen(L);
+  const int logL = M.logP[0], L = 1 << logL, cs = xstride(L);
   const int nzrows = (ty + 1) >> 1;
   const float* src = msrc_override ? msrc_override : stage_m(M, G, stage);
   float* xs = M.buf[G.map[1]];
@@ -318,8 +318,12 @@ __device__ __forceinline__ void zstage_single(float2* D, int cs, const MagnetDev
   D[2 * cs + pky] = v2;
 }
 
-template <int PZ>
-__global__ void __launch_bounds__(384) k_yz(const MagnetDev* __restrict__ mags, const GroupDev* __restrict__ groups,
+// MAXLR = 4: radix-16 passes, 16 values per thread (y lengths up to 4096, one
+// 384-thread block per SM by registers); MAXLR = 3: radix-8 passes, 8 values
+// per thread, two blocks per SM (y lengths up to 2048, z length up to 8).
+template <int PZ, int MAXLR>
+__global__ void __launch_bounds__(384, MAXLR == 3 ? 2 : 1)
+    k_yz(const MagnetDev* __restrict__ mags, const GroupDev* __restrict__ groups,
                                             const Work* __restrict__ work, int stage, int gate,
                                             const float2* __restrict__ tw) {
   extern __shared__ float2 sm[];
@@ -334,7 +338,7 @@ __global__ void __launch_bounds__(384) k_yz(const MagnetDev* __restrict__ mags, 
   float2* D = sm;  // [nkx][3*nz] padded columns of length Py
   const int ncol = nkx * 3 * nz;
   float2* tws = sm + ncol * cs;  // twiddles of length Py
-  load_twiddles<4>(tws, tw, logPy);
+  load_twiddles<MAXLR>(tws, tw, logPy);
   // slab load: 8 independent read-only loads in flight per thread
   const int total = ncol << logPy;
   for (int e0 = threadIdx.x; e0 < total; e0 += 8 * blockDim.x) {
@@ -352,7 +356,7 @@ __global__ void __launch_bounds__(384) k_yz(const MagnetDev* __restrict__ mags, 
     }
   }
   __syncthreads();
-  fft_many<-1, 4>(D, logPy, ncol, cs, tws);
+  fft_many<-1, MAXLR>(D, logPy, ncol, cs, tws);
   if constexpr (PZ == 1) {
     for (int t = threadIdx.x; t < nkx << logPy; t += blockDim.x) {
       const int j = t >> logPy;
@@ -366,7 +370,7 @@ __global__ void __launch_bounds__(384) k_yz(const MagnetDev* __restrict__ mags, 
     }
   }
   __syncthreads();
-  fft_many<1, 4>(D, logPy, ncol, cs, tws);
+  fft_many<1, MAXLR>(D, logPy, ncol, cs, tws);
   for (int e = threadIdx.x; e < (ncol << logPy); e += blockDim.x) {
     const int col = e >> logPy, y = e & (Py - 1);
     if (y < ny) S[col * ny + y] = D[col * cs + pidx(y)];
@@ -524,7 +528,7 @@ __global__ void __launch_bounds__(X_THREADS_MAX, 2) k_xinv(const MagnetDev* __re
   if (!load_descs(M, G, mags, groups, wk.mag, ea.gate, ea.stage)) return;
   const int z = wk.z, y0 = wk.y0, ty = wk.ty;
   const int nx = M.n[0], ny = M.n[1], nz = M.n[2];
-  const int logL = M.logP[0], L = 1 << logL, cs = plen(L);
+  const int logL = M.logP[0], L = 1 << logL, cs = xstride(L);
   const int nzrows = (ty + 1) >> 1;
   const int Fh = M.Fh;
   float2* rows_z = sm + ty * cs;

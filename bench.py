@@ -36,9 +36,18 @@ def parse():
     ap.add_argument("--steps", type=int, default=30)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=["multilayer", "film", "precision"], default="multilayer")
+    ap.add_argument("--workload", choices=["multilayer", "film", "precision", "batched", "serving"],
+                    default="multilayer")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=8)
+    # batched / served forms
+    ap.add_argument("--duration", type=float, default=0.2e-9,
+                    help="batched: simulated seconds per relaxation (the full problem runs 2 ns)")
+    ap.add_argument("--plain-every", type=int, default=8,
+                    help="batched: the plain form runs every k-th instance")
+    ap.add_argument("--rate", type=float, default=1.0, help="serving: Poisson arrival rate (requests/s)")
+    ap.add_argument("--seconds", type=float, default=30.0, help="serving: length of the arrival window (s)")
+    ap.add_argument("--budget-gb", type=float, default=150.0, help="serving: device-memory budget")
     return ap.parse_args()
 
 
@@ -149,10 +158,53 @@ def cpu_baseline(w, n_evals=1):
     }
 
 
+def run_reference_many(args):
+    """CPU FP64 oracle on a bounded sample of the batched / served solves: one
+    effective-field evaluation per sampled solve, scaled by the 7 evaluations of
+    one reference Dormand-Prince step."""
+    import oracle as O
+    from mumaxplus_b200 import batch as B
+    from mumaxplus_b200 import workloads as Wl
+
+    if args.workload == "batched":
+        ws = Wl.batch_instances(256)[::32]
+    else:
+        ws = Wl.serving_requests(rate=2.0, seconds=4.0)[:6]
+    t_tot, cells = 0.0, 0
+    for k in range(args.warmup + args.steps):
+        w = ws[k % len(ws)]
+        keep = []
+        ow = O.OracleWorld()
+        q = ow.add_magnet(B.solve_desc(w, keep))
+        ow.set_m(q, w["m0"]())
+        ow.eval(q, O.abi.Q_DEMAG_FIELD)  # kernel construction, untimed
+        t0 = time.time()
+        ow.eval(q, O.abi.Q_EFFECTIVE_FIELD)
+        if k >= args.warmup:
+            t_tot += time.time() - t0
+            cells += Wl.ncells(w)
+    value = cells / (GAMMA_EVALS_REFERENCE_DP * t_tot)
+    sample = (f"{args.steps} FP64 effective-field evaluations of {args.workload} solves ({cells} cells), "
+              f"scaled by {GAMMA_EVALS_REFERENCE_DP} evaluations per reference Dormand-Prince step")
+    line = {
+        "impl": "reference", "metric": "cell-updates/s", "value": value, "unit": "cell-updates/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * GAMMA_EVALS_REFERENCE_DP * t_tot / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": args.workload, "method": "DormandPrince", "parallelism": "host cores (OpenMP)"},
+        "cpu_baseline": {"value": value, "unit": "cell-updates/s", "cores": os.cpu_count(), "kind": "port",
+                         "sample": sample},
+        "e2e": {"value": value, "unit": "cell-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
+    if args.workload in ("batched", "serving"):
+        return run_reference_many(args)
     w = workload(args.workload)
     from mumaxplus_b200 import workloads as Wl
     import oracle as O
@@ -324,10 +376,176 @@ def run_ours(args):
         dist.destroy_process_group()
 
 
+def _dist_setup():
+    import torch
+
+    world_size = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    torch.cuda.set_device(local)
+    if world_size > 1:
+        import datetime
+
+        import torch.distributed as dist_mod
+
+        dist = dist_mod
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    return world_size, rank, local, dist
+
+
+def _max_over_ranks(dist, value, device):
+    if dist is None:
+        return value
+    import torch
+
+    t = torch.tensor([value], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def run_batched(args):
+    """Relaxation batch: 256 solves of side 32-256 (nz 1 or 2) advanced together
+    vs the same solves one at a time (the plain form, on every k-th instance).
+    Under torchrun each rank runs its own copy of the batch (independent solves,
+    no collective on the data path)."""
+    import torch
+
+    from mumaxplus_b200 import batch as B
+    from mumaxplus_b200 import workloads as Wl
+
+    world_size, rank, local, dist = _dist_setup()
+    dev = torch.device("cuda", local)
+    insts = Wl.batch_instances(256)
+    wb = B.Batch(device=local)  # warm-up: first graph captures, pool growth
+    B.relax_batch(wb, insts[: max(1, args.warmup)], duration=2e-12, torque_stop=1e-4)
+    del wb
+    sampler = ClockSampler(local)
+    sampler.start()
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize(dev)
+    b = B.Batch(device=local)
+    l0 = b.engine.launch_count()
+    t0 = time.perf_counter()
+    solves, t_run, t_setup = B.relax_batch(b, insts, duration=args.duration, torque_stop=1e-4)
+    t_e2e = time.perf_counter() - t0
+    launches = b.engine.launch_count() - l0
+    clocks = sampler.stop()
+    upd = sum(s.cells * s.steps for s in solves)
+    t_run_max = _max_over_ranks(dist, t_run, dev)
+    t_e2e_max = _max_over_ranks(dist, t_e2e, dev)
+    # the plain form: the same solves one at a time (one solve resident)
+    k = max(1, args.plain_every)
+    sub = insts[::k]
+    psol, p_run, p_setup = B.run_plain(B.Batch(device=local), sub, duration=args.duration, torque_stop=1e-4)
+    p_upd = sum(s.cells * s.steps for s in psol)
+    same = {s.key: s for s in solves}
+    worst = max(float(np.max(np.abs(same[k * i].m - p.m))) for i, p in enumerate(psol))
+    if rank == 0:
+        value = world_size * upd / t_run_max
+        plain = p_upd / p_run
+        steps = [s.steps for s in solves]
+        line = {
+            "metric": "cell-updates/s", "value": value, "unit": "cell-updates/s", "n_gpus": world_size,
+            "steps": int(sum(steps)), "warmup": args.warmup, "ms_per_step": 1e3 * t_run_max / max(1, max(steps)),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "batch_256_relax", "instances": len(insts),
+                       "cells": int(sum(s.cells for s in solves)), "duration_s": args.duration,
+                       "torque_stop_T": 1e-4, "method": "DormandPrince 1e-5",
+                       "parallelism": f"independent batch per rank x{world_size}" if world_size > 1 else "single GPU",
+                       "l2": "state + spectra of the batch ~ 2 GB, larger than L2"},
+            "batched": {"cell_updates": upd, "seconds": t_run, "setup_seconds": t_setup,
+                        "solves_per_s": len(solves) / t_run,
+                        "steps_min_median_max": [int(min(steps)), float(np.median(steps)), int(max(steps))],
+                        "stopped_on_torque": int(sum(1 for s in solves if s.sim_time < 0.999 * args.duration)),
+                        "failed": int(sum(s.failed for s in solves))},
+            "plain": {"instances": len(sub), "cell_updates": p_upd, "seconds": p_run, "setup_seconds": p_setup,
+                      "value": plain, "unit": "cell-updates/s"},
+            "batched_over_plain": value / world_size / plain,
+            "max_abs_dm_batched_vs_plain": worst,
+            "e2e": {"value": world_size * upd / t_e2e_max, "unit": "cell-updates/s",
+                    "h2d_bytes_per_step": int(sum(12 * s.cells for s in solves)),
+                    "d2h_bytes_per_step": int(sum(12 * s.cells for s in solves)),
+                    "note": "one step = the whole batch: host m0 in, kernel construction, integration, host m out"},
+            "gpu_launches": int(launches),
+            "clocks": clocks,
+        }
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def run_serving(args):
+    """Open-loop Poisson request stream served by continuous batching, vs the
+    same requests served one at a time (the plain form: one solve resident)."""
+    import torch
+
+    from mumaxplus_b200 import batch as B
+    from mumaxplus_b200 import workloads as Wl
+
+    world_size, rank, local, dist = _dist_setup()
+    dev = torch.device("cuda", local)
+    reqs = Wl.serving_requests(rate=args.rate, seconds=args.seconds, seed=5 + rank)
+    budget = args.budget_gb * 1e9
+    wb = B.Batch(device=local)  # warm-up
+    B.relax_batch(wb, [dict(r) for r in reqs[: max(1, args.warmup)]], duration=2e-12, torque_stop=0.0)
+    del wb
+    sampler = ClockSampler(local)
+    sampler.start()
+    if dist is not None:
+        dist.barrier()
+    b = B.Batch(device=local)
+    l0 = b.engine.launch_count()
+    t0 = time.perf_counter()
+    served = B.Server(b, budget).run(reqs)
+    span = time.perf_counter() - t0
+    launches = b.engine.launch_count() - l0
+    clocks = sampler.stop()
+    span_max = _max_over_ranks(dist, span, dev)
+    t0 = time.perf_counter()
+    plain = B.Server(B.Batch(device=local), budget, max_active=1).run(reqs)
+    p_span = time.perf_counter() - t0
+    p50, p99 = B.latency_stats(served)
+    q50, q99 = B.latency_stats(plain)
+    upd = sum(s.cells * s.steps for s in served)
+    p_upd = sum(s.cells * s.steps for s in plain)
+    by = {s.key: s for s in plain}
+    worst = max((float(np.max(np.abs(s.m - by[s.key].m))) for s in served if s.key in by), default=0.0)
+    if rank == 0:
+        per_req = int(sum(12 * s.cells for s in served) / max(1, len(served)))
+        line = {
+            "metric": "solves/s", "value": world_size * len(served) / span_max, "unit": "solves/s",
+            "n_gpus": world_size, "steps": int(sum(s.steps for s in served)), "warmup": args.warmup,
+            "ms_per_step": None, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic",
+            "config": {"workload": "serving_poisson", "rate_per_s": args.rate, "window_s": args.seconds,
+                       "requests": len(reqs), "budget_gb": args.budget_gb, "method": "DormandPrince 1e-5"},
+            "served": {"p50_s": p50, "p99_s": p99, "makespan_s": span, "cell_updates_per_s": upd / span},
+            "plain": {"p50_s": q50, "p99_s": q99, "makespan_s": p_span, "solves_per_s": len(plain) / p_span,
+                      "cell_updates_per_s": p_upd / p_span},
+            "max_abs_dm_served_vs_plain": worst,
+            "e2e": {"value": world_size * len(served) / span_max, "unit": "solves/s",
+                    "h2d_bytes_per_step": per_req, "d2h_bytes_per_step": per_req,
+                    "note": "per request: host m0 in, host m out; latency from arrival to result on the host"},
+            "gpu_launches": int(launches),
+            "clocks": clocks,
+        }
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         run_reference(args)
+    elif args.workload == "batched":
+        run_batched(args)
+    elif args.workload == "serving":
+        run_serving(args)
     else:
         run_ours(args)
 

@@ -538,6 +538,71 @@ def run_serving(args):
         dist.destroy_process_group()
 
 
+def run_precision(args):
+    """Precision form: demag-only field of 1024x1024x4 random unit vectors
+    (padded FFT 2048x2048x8) against the FP64 oracle, per cell
+    |dB| / |B_ref| over cells with |B_ref| > 1e-6 max|B_ref|, and the
+    evaluation rate of the field on the GPU."""
+    import torch
+
+    import mumaxplus_b200 as mpx
+    import oracle as O
+    from mumaxplus_b200 import workloads as Wl
+
+    world_size, rank, local, dist = _dist_setup()
+    w = Wl.precision()
+    N = Wl.ncells(w)
+    world, magnet = Wl.build(mpx, w, device=local)
+    eng = magnet._engine
+    q = mpx._abi.Q_DEMAG_FIELD
+    shape = (3, *magnet.grid.shape)
+    got = eng.eval(magnet._id, q, shape).astype(np.float64)
+    stream = torch.cuda.Stream(device=local)
+    eng.set_stream(stream.cuda_stream)
+    for _ in range(max(3, args.warmup)):
+        eng.eval_only(magnet._id, q)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        eng.eval_only(magnet._id, q)
+    e1.record(stream)
+    torch.cuda.synchronize(local)
+    ms = e0.elapsed_time(e1) / args.steps
+    ms = _max_over_ranks(dist, ms, torch.device("cuda", local))
+    kms = eng.profile_eval(magnet._id, reps=5)
+    if rank == 0:
+        keep = []
+        ow = O.OracleWorld()
+        oq = ow.add_magnet(Wl.desc(w, keep))
+        ow.set_m(oq, w["m0"]())
+        t0 = time.time()
+        want = ow.eval(oq, O.abi.Q_DEMAG_FIELD)
+        t_oracle = time.time() - t0
+        nref = np.linalg.norm(want, axis=0)
+        mask = nref > 1e-6 * nref.max()
+        rel = np.linalg.norm(got - want, axis=0)[mask] / nref[mask]
+        line = {
+            "metric": "B_demag max relative error vs FP64", "value": float(rel.max()), "unit": "relative",
+            "n_gpus": world_size, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+            "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": w["name"], "fft_padding": "2048x2048x8", "dft": "FP32 shared-memory Stockham",
+                       "cells_compared": int(mask.sum())},
+            "rms_relative_error": float(np.sqrt(np.mean(rel * rel))),
+            "max_abs_error_over_max_field": float(np.abs(got - want).max() / np.abs(want).max()),
+            "evals_per_s": world_size * 1e3 / ms, "cell_evals_per_s": world_size * N * 1e3 / ms,
+            "kernel_ms": {"k_xfwd": kms[0], "k_yz": kms[1], "k_xinv": kms[2]},
+            "oracle_seconds": t_oracle,
+            "e2e": {"value": float(rel.max()), "unit": "relative", "h2d_bytes_per_step": 12 * N,
+                    "d2h_bytes_per_step": 12 * N},
+            "gpu_launches": 3 * args.steps,
+        }
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -546,6 +611,8 @@ def main():
         run_batched(args)
     elif args.workload == "serving":
         run_serving(args)
+    elif args.workload == "precision":
+        run_precision(args)
     else:
         run_ours(args)
 

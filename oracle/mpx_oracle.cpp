@@ -282,6 +282,7 @@ struct Magnet {
   int P[3] = {1, 1, 1};
   std::vector<cd> khat[6];
   bool kready = false;
+  std::vector<double> ext_oct;  // octant supplied by the caller (replaces kernel_octant when set)
 
   int idx(int x, int y, int z) const { return x + n[0] * (y + n[1] * z); }
   V3 mv(int i) const { return {m[i], m[(size_t)N + i], m[2 * (size_t)N + i]}; }
@@ -578,7 +579,10 @@ void build_demag_kernel(Magnet& mg) {
   const int px = mg.P[0], py = mg.P[1], pz = mg.P[2];
   const size_t PP = (size_t)px * py * pz;
   std::vector<double> oct;
-  kernel_octant(mg.n, mg.mg, mg.pbc, mg.cs, oct);
+  if (!mg.ext_oct.empty())
+    oct = mg.ext_oct;
+  else
+    kernel_octant(mg.n, mg.mg, mg.pbc, mg.cs, oct);
   const size_t noct = (size_t)mg.n[0] * mg.n[1] * mg.n[2];
   auto rel = [](int i, int P, int n) -> int {  // circular index -> displacement, or INT32_MIN if unused
     if (i <= n - 1) return i;
@@ -1052,6 +1056,18 @@ int ox_eval(ox_world* wp, int q, int quantity, double* out) {
     default: g_err = "unknown quantity"; return MPX_ERR_INVALID;
   }
   std::memcpy(out, h.data(), sizeof(double) * h.size());
+  return MPX_OK;
+}
+
+// Test hook: use the given real-space kernel octant (6 components x n cells,
+// displacements r >= 0, layout [c][z][y][x]) instead of building one, so that
+// the convolution arithmetic can be compared apart from kernel construction.
+int ox_set_kernel_octant(ox_world* wp, int q, const double* oct) {
+  World& w = *reinterpret_cast<World*>(wp);
+  Magnet& mg = w.mags.at(q);
+  const size_t noct = (size_t)mg.n[0] * mg.n[1] * mg.n[2];
+  mg.ext_oct.assign(oct, oct + 6 * noct);
+  mg.kready = false;
   return MPX_OK;
 }
 

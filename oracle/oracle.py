@@ -60,6 +60,7 @@ def lib():
         L.ox_eval.argtypes = [V, C.c_int, C.c_int, C.c_void_p]
         L.ox_demag_brute.argtypes = [V, C.c_int, C.c_void_p]
         L.ox_demag_kernel.argtypes = [V, C.c_int, C.c_void_p, C.POINTER(C.c_int)]
+        L.ox_set_kernel_octant.argtypes = [V, C.c_int, C.c_void_p]
         L.ox_newell.restype = C.c_double
         L.ox_newell.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double]
         L.ox_average.argtypes = [V, C.c_int, C.c_int, P_D]
@@ -146,6 +147,11 @@ class OracleWorld:
         out = np.empty((6, dims[2], dims[1], dims[0]), dtype=np.float64)
         self._check(lib().ox_demag_kernel(self._h, q, out.ctypes.data, dims))
         return out
+
+    def set_kernel_octant(self, q, oct):
+        """Use a given kernel octant (6, nz, ny, nx) of displacements r >= 0."""
+        a = np.ascontiguousarray(oct, dtype=np.float64)
+        self._check(lib().ox_set_kernel_octant(self._h, q, a.ctypes.data))
 
     def average(self, q, quantity):
         out = (C.c_double * 3)()

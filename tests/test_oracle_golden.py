@@ -215,3 +215,23 @@ def test_pbc_run_center_matches_mumax3_golden():
     avg = w.average(q, abi.Q_MAGNETIZATION)
     wanted = np.array([0.89947968, 0.23352228, -0.00010287])
     assert np.linalg.norm(np.array(avg) - wanted) / np.linalg.norm(wanted) < 1e-3
+
+
+def test_oracle_external_kernel_octant_reproduces_own(oracle):
+    """The external-kernel hook (used to compare convolution arithmetic apart
+    from kernel construction): feeding back the oracle's own real-space kernel
+    octant reproduces its demag field (to the FP64 rounding by which the
+    direct 27-point evaluation of the exported kernel differs from the shared
+    lattice evaluation of the octant)."""
+    s = MagnetSpec(size=(20, 12, 3), cellsize=(2e-9, 3e-9, 1.5e-9), msat=7e5)
+    m0 = random_m(s.shape, seed=9, smooth=1)
+    ow, q = s.oracle_world(m0)
+    want = ow.eval(q, oracle.abi.Q_DEMAG_FIELD)
+    K = ow.demag_kernel(q)  # reference layout, origin -(n-1)-pad per axis
+    nx, ny, nz = s.size
+    o = [K.shape[3] - nx, K.shape[2] - ny, K.shape[1] - nz]  # index of displacement 0
+    oct = K[:, o[2]:, o[1]:, o[0]:]
+    ow2, q2 = s.oracle_world(m0)
+    ow2.set_kernel_octant(q2, oct)
+    got = ow2.eval(q2, oracle.abi.Q_DEMAG_FIELD)
+    assert np.max(np.abs(got - want)) <= 1e-10 * np.max(np.abs(want))

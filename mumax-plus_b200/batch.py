@@ -285,6 +285,21 @@ class Server:
         return finished
 
 
+def shard(instances, rank, world_size):
+    """Instances of this rank when independent solves are spread over
+    `world_size` GPUs: greedy longest-processing-time bin packing on the cells
+    of each solve (the device work of a step is about proportional to them),
+    deterministic on every rank.  Returns the instance indices, in order."""
+    order = sorted(range(len(instances)), key=lambda i: (-workloads.ncells(instances[i]), i))
+    load = [0] * world_size
+    owner = [0] * len(instances)
+    for i in order:
+        r = min(range(world_size), key=lambda k: (load[k], k))
+        owner[i] = r
+        load[r] += workloads.ncells(instances[i])
+    return [i for i in range(len(instances)) if owner[i] == rank]
+
+
 def latency_stats(solves):
     """p50 / p99 latency (seconds from arrival to result) of finished solves."""
     lat = np.array([s.t_done - s.arrival for s in solves if s.t_done is not None and s.arrival is not None])

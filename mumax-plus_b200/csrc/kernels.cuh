@@ -320,7 +320,9 @@ __device__ __forceinline__ void zstage_single(float2* D, int cs, const MagnetDev
 
 // MAXLR = 4: radix-16 passes, 16 values per thread (y lengths up to 4096, one
 // 384-thread block per SM by registers); MAXLR = 3: radix-8 passes, 8 values
-// per thread, two blocks per SM (y lengths up to 2048, z length up to 8).
+// per thread, two blocks per SM (y lengths up to 2048, z length up to 8).  At
+// z length 16 the radix-8 form measured slower (more passes, and the z stage
+// needs 128 registers, so at most 512 threads).
 template <int PZ, int MAXLR>
 __global__ void __launch_bounds__(384, MAXLR == 3 ? 2 : 1)
     k_yz(const MagnetDev* __restrict__ mags, const GroupDev* __restrict__ groups,

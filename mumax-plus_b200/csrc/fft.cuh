@@ -160,7 +160,11 @@ __device__ __forceinline__ constexpr int pstride() { return S + (S >> 4); }
 // padded columns of length 2^LOGL (column c at buf + c*cs), VPT values per
 // thread.  Requires ncols*L <= VPT*blockDim.x.  Strides that are multiples of
 // 16 turn every padded address of a butterfly into a constant offset.
-template <int LOGL, int LR, int LOGNS, int DIR, int VPT>
+// ZIN (first pass only): the upper half of each column is zero padding, so the
+// butterfly inputs r >= R/2 (indices >= L/2) are not loaded.  ZOUT (last pass
+// only): the caller reads only the lower half, so the outputs r >= R/2 are
+// neither stored nor, once dead, computed.
+template <int LOGL, int LR, int LOGNS, int DIR, int VPT, bool ZIN, bool ZOUT>
 __device__ __forceinline__ void stockham_pass(float2* buf, int ncols, int cs, const float2* tw) {
   constexpr int R = 1 << LR, BPT = VPT / R;
   constexpr int LOGNB = LOGL - LR, NB = 1 << LOGNB, NS = 1 << LOGNS;
@@ -172,14 +176,17 @@ __device__ __forceinline__ void stockham_pass(float2* buf, int ncols, int cs, co
     if (b < total) {
       const int j = b & (NB - 1);
       const int c0 = (b >> LOGNB) * cs;
+      constexpr int RL = ZIN ? R / 2 : R;  // inputs that are loaded
       if constexpr (NB % 16 == 0) {
         const int o0 = c0 + pidx(j);
 #pragma unroll
-        for (int r = 0; r < R; ++r) v[q][r] = buf[o0 + r * pstride<NB>()];
+        for (int r = 0; r < RL; ++r) v[q][r] = buf[o0 + r * pstride<NB>()];
       } else {
 #pragma unroll
-        for (int r = 0; r < R; ++r) v[q][r] = buf[c0 + pidx(j + r * NB)];
+        for (int r = 0; r < RL; ++r) v[q][r] = buf[c0 + pidx(j + r * NB)];
       }
+#pragma unroll
+      for (int r = RL; r < R; ++r) v[q][r] = make_float2(0.f, 0.f);
     }
   }
   __syncthreads();
@@ -197,56 +204,61 @@ __device__ __forceinline__ void stockham_pass(float2* buf, int ncols, int cs, co
       }
       dft_reg<R, DIR>(v[q]);
       const int o = ((j - k) << LR) + k;
+      constexpr int RS = ZOUT ? R / 2 : R;  // outputs that are stored
       if constexpr (NS % 16 == 0) {
         const int o0 = c0 + pidx(o);
 #pragma unroll
-        for (int r = 0; r < R; ++r) buf[o0 + r * pstride<NS>()] = v[q][r];
+        for (int r = 0; r < RS; ++r) buf[o0 + r * pstride<NS>()] = v[q][r];
       } else if constexpr (NS == 1 && R == 16) {  // o = 16 j: padded 17 j + r
         const int o0 = c0 + 17 * j;
 #pragma unroll
-        for (int r = 0; r < R; ++r) buf[o0 + r] = v[q][r];
+        for (int r = 0; r < RS; ++r) buf[o0 + r] = v[q][r];
       } else {
 #pragma unroll
-        for (int r = 0; r < R; ++r) buf[c0 + pidx(o + r * NS)] = v[q][r];
+        for (int r = 0; r < RS; ++r) buf[c0 + pidx(o + r * NS)] = v[q][r];
       }
     }
   }
   __syncthreads();
 }
 
-template <int LOGL, int MAXLR, int PASS, int DIR>
+// PRUNE: bit 0 = the upper half of every input column is zero (not read),
+// bit 1 = only the lower half of every output column is used (not written).
+template <int LOGL, int MAXLR, int PASS, int DIR, int PRUNE>
 __device__ __forceinline__ void fft_passes(float2* buf, int ncols, int cs, const float2* tw) {
   using PL = Plan<LOGL, MAXLR>;
   if constexpr (PASS < PL::P) {
-    stockham_pass<LOGL, PL::lr(PASS), PL::logns(PASS), DIR, (1 << MAXLR)>(buf, ncols, cs, tw);
-    fft_passes<LOGL, MAXLR, PASS + 1, DIR>(buf, ncols, cs, tw);
+    stockham_pass<LOGL, PL::lr(PASS), PL::logns(PASS), DIR, (1 << MAXLR), (PRUNE & 1) && PASS == 0,
+                  (PRUNE & 2) && PASS == PL::P - 1>(buf, ncols, cs, tw);
+    fft_passes<LOGL, MAXLR, PASS + 1, DIR, PRUNE>(buf, ncols, cs, tw);
   }
 }
 
 // FFT of many padded columns of length 2^LOGL, in groups that fit 2^MAXLR
 // values per thread.  All threads of the block must call it.
-template <int LOGL, int MAXLR, int DIR>
+template <int LOGL, int MAXLR, int DIR, int PRUNE>
 __device__ __forceinline__ void fft_many_ct(float2* buf, int ncols, int cs, const float2* tw) {
   const int per = max(1, ((1 << MAXLR) * (int)blockDim.x) >> LOGL);
-  for (int c0 = 0; c0 < ncols; c0 += per) fft_passes<LOGL, MAXLR, 0, DIR>(buf + c0 * cs, min(per, ncols - c0), cs, tw);
+  for (int c0 = 0; c0 < ncols; c0 += per)
+    fft_passes<LOGL, MAXLR, 0, DIR, PRUNE>(buf + c0 * cs, min(per, ncols - c0), cs, tw);
 }
 
 // Runtime length dispatch (2^logL <= 4096).
-template <int DIR, int MAXLR>
+template <int DIR, int MAXLR, int PRUNE = 0>
 __device__ __forceinline__ void fft_many(float2* buf, int logL, int ncols, int cs, const float2* tw) {
   switch (logL) {
-    case 1: fft_many_ct<1, MAXLR, DIR>(buf, ncols, cs, tw); break;
-    case 2: fft_many_ct<2, MAXLR, DIR>(buf, ncols, cs, tw); break;
-    case 3: fft_many_ct<3, MAXLR, DIR>(buf, ncols, cs, tw); break;
-    case 4: fft_many_ct<4, MAXLR, DIR>(buf, ncols, cs, tw); break;
-    case 5: fft_many_ct<5, MAXLR, DIR>(buf, ncols, cs, tw); break;
-    case 6: fft_many_ct<6, MAXLR, DIR>(buf, ncols, cs, tw); break;
-    case 7: fft_many_ct<7, MAXLR, DIR>(buf, ncols, cs, tw); break;
-    case 8: fft_many_ct<8, MAXLR, DIR>(buf, ncols, cs, tw); break;
-    case 9: fft_many_ct<9, MAXLR, DIR>(buf, ncols, cs, tw); break;
-    case 10: fft_many_ct<10, MAXLR, DIR>(buf, ncols, cs, tw); break;
-    case 11: fft_many_ct<11, MAXLR, DIR>(buf, ncols, cs, tw); break;
-    case 12: fft_many_ct<12, MAXLR, DIR>(buf, ncols, cs, tw); break;
+    case 1: fft_many_ct<1, MAXLR, DIR, PRUNE>(buf, ncols, cs, tw); break;
+    case 2: fft_many_ct<2, MAXLR, DIR, PRUNE>(buf, ncols, cs, tw); break;
+    case 3: fft_many_ct<3, MAXLR, DIR, PRUNE>(buf, ncols, cs, tw); break;
+    case 4: fft_many_ct<4, MAXLR, DIR, PRUNE>(buf, ncols, cs, tw); break;
+    case 5: fft_many_ct<5, MAXLR, DIR, PRUNE>(buf, ncols, cs, tw); break;
+    case 6: fft_many_ct<6, MAXLR, DIR, PRUNE>(buf, ncols, cs, tw); break;
+    case 7: fft_many_ct<7, MAXLR, DIR, PRUNE>(buf, ncols, cs, tw); break;
+    case 8: fft_many_ct<8, MAXLR, DIR, PRUNE>(buf, ncols, cs, tw); break;
+    case 9: fft_many_ct<9, MAXLR, DIR, PRUNE>(buf, ncols, cs, tw); break;
+    case 10: fft_many_ct<10, MAXLR, DIR, PRUNE>(buf, ncols, cs, tw); break;
+    case 11: fft_many_ct<11, MAXLR, DIR, PRUNE>(buf, ncols, cs, tw); break;
+    case 12: fft_many_ct<12, MAXLR, DIR, PRUNE>(buf, ncols, cs, tw); break;
     default: break;  // logL == 0: identity
   }
 }

@@ -141,9 +141,12 @@ __global__ void __launch_bounds__(X_THREADS_MAX, 2) k_xfwd(const MagnetDev* __re
   float2* tws = sm + (ty + nzrows) * cs;  // twiddles of length L
   load_twiddles<3>(tws, tw, logL);
 
+  // only the lower half of each row: the upper half (x >= L/2 >= nx) is zero
+  // padding that the pruned first FFT pass does not read
+  const int logLh = logL > 0 ? logL - 1 : 0;
 #pragma unroll 2
-  for (int e = threadIdx.x; e < (ty << logL); e += blockDim.x) {
-    const int yl = e >> logL, x = e & (L - 1);
+  for (int e = threadIdx.x; e < (ty << logLh); e += blockDim.x) {
+    const int yl = e >> logLh, x = e & ((1 << logLh) - 1);
     float3 Mv = f3(0, 0, 0);
     if (x < nx) {
       const int i = rowbase + yl * nx + x;
@@ -166,7 +169,7 @@ __global__ void __launch_bounds__(X_THREADS_MAX, 2) k_xfwd(const MagnetDev* __re
     if ((ty & 1) && yl == ty - 1) zr[1] = 0.0f;
   }
   __syncthreads();
-  fft_many<-1, 3>(sm, logL, ty + nzrows, cs, tws);
+  fft_many<-1, 3, 1>(sm, logL, ty + nzrows, cs, tws);
 
   // unpack the two real transforms of each complex row and store the half spectrum
   const int Fh = M.Fh;
@@ -341,24 +344,27 @@ __global__ void __launch_bounds__(384, MAXLR == 3 ? 2 : 1)
   const int ncol = nkx * 3 * nz;
   float2* tws = sm + ncol * cs;  // twiddles of length Py
   load_twiddles<MAXLR>(tws, tw, logPy);
-  // slab load: 8 independent read-only loads in flight per thread
-  const int total = ncol << logPy;
+  // slab load: 8 independent read-only loads in flight per thread; only the
+  // lower half of each column (y < Py/2, of which y >= ny is zero padding),
+  // which is all the pruned first FFT pass reads
+  const int logPyh = logPy > 0 ? logPy - 1 : 0;
+  const int total = ncol << logPyh;
   for (int e0 = threadIdx.x; e0 < total; e0 += 8 * blockDim.x) {
     float2 r[8];
 #pragma unroll
     for (int u = 0; u < 8; ++u) {
       const int e = e0 + u * blockDim.x;
-      const int col = e >> logPy, y = e & (Py - 1);
+      const int col = e >> logPyh, y = e & ((1 << logPyh) - 1);
       r[u] = (e < total && y < ny) ? __ldg(S + col * ny + y) : make_float2(0.f, 0.f);
     }
 #pragma unroll
     for (int u = 0; u < 8; ++u) {
       const int e = e0 + u * blockDim.x;
-      if (e < total) D[(e >> logPy) * cs + pidx(e & (Py - 1))] = r[u];
+      if (e < total) D[(e >> logPyh) * cs + pidx(e & ((1 << logPyh) - 1))] = r[u];
     }
   }
   __syncthreads();
-  fft_many<-1, MAXLR>(D, logPy, ncol, cs, tws);
+  fft_many<-1, MAXLR, 1>(D, logPy, ncol, cs, tws);
   if constexpr (PZ == 1) {
     for (int t = threadIdx.x; t < nkx << logPy; t += blockDim.x) {
       const int j = t >> logPy;
@@ -372,7 +378,7 @@ __global__ void __launch_bounds__(384, MAXLR == 3 ? 2 : 1)
     }
   }
   __syncthreads();
-  fft_many<1, MAXLR>(D, logPy, ncol, cs, tws);
+  fft_many<1, MAXLR, 2>(D, logPy, ncol, cs, tws);  // only y < ny <= Py/2 is written back
   for (int e = threadIdx.x; e < (ncol << logPy); e += blockDim.x) {
     const int col = e >> logPy, y = e & (Py - 1);
     if (y < ny) S[col * ny + y] = D[col * cs + pidx(y)];
@@ -565,7 +571,7 @@ __global__ void __launch_bounds__(X_THREADS_MAX, 2) k_xinv(const MagnetDev* __re
     }
   }
   __syncthreads();
-  fft_many<1, 3>(sm, logL, ty + nzrows, cs, tws);
+  fft_many<1, 3, 2>(sm, logL, ty + nzrows, cs, tws);  // only x < nx <= L/2 is used
 
   const float* m = ea.msrc ? ea.msrc : stage_m(M, G, ea.stage);
   double en = 0.0, tn = 0.0;

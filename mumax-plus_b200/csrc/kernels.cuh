@@ -94,11 +94,19 @@ __device__ __forceinline__ float3 combine_cell(const MagnetDev& M, const GroupDe
   const int N = M.N;
   float3 v = ldg3(M.buf[G.map[0]], N, i);
   const int nj = final_b1 ? c_tab.S : stage;
-  for (int j = 0; j < nj; ++j) {
-    const double co = final_b1 ? c_tab.b1[j] : c_tab.a[stage][j];
-    const float cf = (float)(G.dt * co);
-    const float3 k = ldg3(M.buf[G.map[2 + j]], N, i);
-    v = f3(v.x + cf * k.x, v.y + cf * k.y, v.z + cf * k.z);
+  // unrolled over the 7 possible stages (predicated), so that the loads of all
+  // k_j are in flight together; the sum keeps the order j = 0, 1, ...
+  float3 k[7];
+#pragma unroll
+  for (int j = 0; j < 7; ++j)
+    if (j < nj) k[j] = ldg3(M.buf[G.map[2 + j]], N, i);
+#pragma unroll
+  for (int j = 0; j < 7; ++j) {
+    if (j < nj) {
+      const double co = final_b1 ? c_tab.b1[j] : c_tab.a[stage][j];
+      const float cf = (float)(G.dt * co);
+      v = f3(v.x + cf * k[j].x, v.y + cf * k[j].y, v.z + cf * k[j].z);
+    }
   }
   const float inv = rsqrtf(v.x * v.x + v.y * v.y + v.z * v.z);
   return f3(v.x * inv, v.y * inv, v.z * inv);
@@ -544,30 +552,39 @@ __global__ void __launch_bounds__(X_THREADS_MAX, 2) k_xinv(const MagnetDev* __re
   load_twiddles<3>(tws, tw, logL);
   const float2* __restrict__ S = M.spec;
   const size_t cstride = (size_t)nz * ny;
-  // rebuild full-length Hermitian rows: Z = A + iB
+  // rebuild full-length Hermitian rows: Z = A + iB.  Lanes e (kx = e >> tyl,
+  // row yl = e & (2^tyl - 1), rows fastest) each load their x, y and z values;
+  // the z value of the odd row comes from the next lane by a shuffle, so every
+  // lane issues its three loads together and all lanes run the same trip count.
   const int tyl = tile_log(ty);
+  const int total = Fh << tyl;
 #pragma unroll 2
-  for (int e = threadIdx.x; e < Fh << tyl; e += blockDim.x) {
+  for (int e0 = 0; e0 < total; e0 += blockDim.x) {
+    const int e = e0 + threadIdx.x;
     const int yl = e & ((1 << tyl) - 1), kx = e >> tyl;
-    if (yl >= ty) continue;
+    const bool act = e < total && yl < ty;
     const size_t base = (size_t)kx * 3 * cstride + (size_t)z * ny + y0 + yl;
-    float2 A = __ldg(S + base), B = __ldg(S + base + cstride);
+    float2 A = make_float2(0.f, 0.f), B = A, Cz = A;
+    if (act) {
+      A = __ldg(S + base);
+      B = __ldg(S + base + cstride);
+      Cz = __ldg(S + base + 2 * cstride);
+    }
+    const float dx = __shfl_down_sync(0xffffffffu, Cz.x, 1), dy = __shfl_down_sync(0xffffffffu, Cz.y, 1);
+    if (!act) continue;
     const bool edge = (kx == 0) || (2 * kx == L);
     if (edge) {
       A.y = 0.f;
       B.y = 0.f;
+      Cz.y = 0.f;
     }
     sm[yl * cs + pidx(kx)] = make_float2(A.x - B.y, A.y + B.x);
     if (kx > 0 && 2 * kx < L) sm[yl * cs + pidx(L - kx)] = make_float2(A.x + B.y, -A.y + B.x);
     if ((yl & 1) == 0) {
-      float2 C = __ldg(S + base + 2 * cstride);
-      float2 Dv = (yl + 1 < ty) ? __ldg(S + base + 2 * cstride + 1) : make_float2(0.f, 0.f);
-      if (edge) {
-        C.y = 0.f;
-        Dv.y = 0.f;
-      }
-      rows_z[(yl >> 1) * cs + pidx(kx)] = make_float2(C.x - Dv.y, C.y + Dv.x);
-      if (kx > 0 && 2 * kx < L) rows_z[(yl >> 1) * cs + pidx(L - kx)] = make_float2(C.x + Dv.y, -C.y + Dv.x);
+      float2 Dv = (yl + 1 < ty) ? make_float2(dx, dy) : make_float2(0.f, 0.f);
+      if (edge) Dv.y = 0.f;
+      rows_z[(yl >> 1) * cs + pidx(kx)] = make_float2(Cz.x - Dv.y, Cz.y + Dv.x);
+      if (kx > 0 && 2 * kx < L) rows_z[(yl >> 1) * cs + pidx(L - kx)] = make_float2(Cz.x + Dv.y, -Cz.y + Dv.x);
     }
   }
   __syncthreads();

@@ -305,6 +305,9 @@ __device__ __forceinline__ LocalOut local_terms_fast(const MagnetDev& M, const f
     const bool dmi_open = (a == 0.0f) || openbc;
     const bool neumann = !openbc && a != 0.0f;
     float3 he = f3(0, 0, 0), hd = f3(0, 0, 0);
+    // all six neighbour loads first (independent, in flight together), then the sums
+    float3 mn[6];
+    bool nin[6];
 #pragma unroll
     for (int r = 0; r < 6; ++r) {
       const int axis = r >> 1;
@@ -313,16 +316,20 @@ __device__ __forceinline__ LocalOut local_terms_fast(const MagnetDev& M, const f
       if (axis == 0) { nc = nb_coord(x, d, M.n[0], M.o[0], M.mg[0], M.mgo[0]); xx = nc; }
       else if (axis == 1) { nc = nb_coord(y, d, M.n[1], M.o[1], M.mg[1], M.mgo[1]); yy = nc; }
       else { nc = nb_coord(z, d, M.n[2], M.o[2], M.mg[2], M.mgo[2]); zz = nc; }
-      const bool nin = nc >= 0;
-      float3 m_ = mc;
-      if (nin) {
-        m_ = ldg3(m, N, xx + M.n[0] * (yy + M.n[1] * zz));
-      } else if (neumann) {  // ghost cell m + Gamma/(2A) delta
+      nin[r] = nc >= 0;
+      mn[r] = nin[r] ? ldg3(m, N, xx + M.n[0] * (yy + M.n[1] * zz)) : mc;
+    }
+#pragma unroll
+    for (int r = 0; r < 6; ++r) {
+      const int axis = r >> 1;
+      const int d = (r & 1) ? 1 : -1;
+      float3 m_ = mn[r];
+      if (!nin[r] && neumann) {  // ghost cell m + Gamma/(2A) delta
         const float3 G = gamma_uniform(M.fd, axis, mc);
         m_ = mc + (d * M.cs[axis]) * (M.finv_2a * G);
       }
-      if (do_exch && (nin || neumann)) he = he + M.fe[axis] * (m_ - mc);
-      if (do_dmi && (nin || !dmi_open)) {
+      if (do_exch && (nin[r] || neumann)) he = he + M.fe[axis] * (m_ - mc);
+      if (do_dmi && (nin[r] || !dmi_open)) {
         const float Dxy = M.fd[3 * axis], Dxz = M.fd[3 * axis + 1], Dyz = M.fd[3 * axis + 2];
         const float inv_delta = d * M.inv_cs[axis];
         hd.x += (Dxy * m_.y + Dxz * m_.z) * inv_delta;

@@ -246,6 +246,20 @@ mpx_status mpx_solver_step(mpx_engine* e, int group);
 mpx_status mpx_solver_steps(mpx_engine* e, int group, int nsteps);
 mpx_status mpx_solver_run(mpx_engine* e, int group, double duration);
 
+/* Minimizer::exec (physics/minimizer.cu:73-160): steepest descent on the
+ * damping torque with Barzilai-Borwein step sizes over the group's magnets,
+ * until the last nsamples x (number of magnets) largest per-cell changes of m
+ * are all <= tol.  The time and time step are left as they were. */
+mpx_status mpx_minimize(mpx_engine* e, int group, double tol, int nsamples);
+/* Relaxer::exec (physics/relaxer.cpp:88-174): adaptive Fehlberg steps of the
+ * damping torque (no precession) while the total energy decreases, then, with a
+ * negative threshold, lowering the maximum error by sqrt(2) down to tol while the
+ * summed squared torque decreases; with a positive threshold, lowering it each time
+ * every magnet's maximum torque is at or below the threshold.  Restores the solver
+ * settings, time and time step afterwards (an adaptive solver then takes the
+ * sensible time step).  threshold == 0 is MPX_ERR_INVALID. */
+mpx_status mpx_relax(mpx_engine* e, int group, double tol, double threshold);
+
 /* ---- many groups at once (batched / served forms) ----------------------- */
 /* Arms `group` to run for `duration` seconds, or until max|torque|/gamma_LL
  * drops below torque_stop tesla (torque_stop <= 0 disables that test).  The

@@ -160,6 +160,8 @@ SIGNATURES = {
     "mpx_solver_step": (I, [E, I]),
     "mpx_solver_steps": (I, [E, I, I]),
     "mpx_solver_run": (I, [E, I, C.c_double]),
+    "mpx_minimize": (I, [E, I, C.c_double, I]),
+    "mpx_relax": (I, [E, I, C.c_double, C.c_double]),
     "mpx_group_start": (I, [E, I, C.c_double, C.c_double]),
     "mpx_advance": (I, [E, I]),
     "mpx_poll": (I, [E, P_I, I, P_I, P_I]),

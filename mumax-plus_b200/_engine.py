@@ -211,6 +211,12 @@ class Engine:
     def run(self, g, duration):
         check(lib().mpx_solver_run(self._h, int(g), float(duration)))
 
+    def minimize(self, g, tol=1e-6, nsamples=10):
+        check(lib().mpx_minimize(self._h, int(g), float(tol), int(nsamples)))
+
+    def relax(self, g, tol=1e-9, threshold=-1.0):
+        check(lib().mpx_relax(self._h, int(g), float(tol), float(threshold)))
+
     # -- batched
     def group_start(self, g, duration, torque_stop=0.0):
         check(lib().mpx_group_start(self._h, int(g), float(duration), float(torque_stop)))

@@ -12,6 +12,7 @@
 #include <cmath>
 #include <cstdint>
 #include <cstring>
+#include <deque>
 #include <memory>
 #include <mutex>
 #include <string>
@@ -156,6 +157,7 @@ struct Group {
   mpx_solver_params sp{MPX_RK_FEHLBERG, 1, 1e-5, 0.8, 0.5, 2.0, 0.01, 1e-14};
   std::vector<int> magnets;
   bool active = false;  // started and not yet seen finished: its magnets are in the attempt tables
+  int torque_kind = 0;  // 0: LLG torque, 1: damping torque (during relax), mirrors GroupDev::torque_kind
 };
 
 }  // namespace
@@ -933,7 +935,7 @@ mpx_status sensible_timestep(mpx_engine* e, Group* g, double* out) {
     Magnet* m = get_mag(e, id);
     const int N = m->dev.N;
     MPX_TRY(ensure_scratch(e, sizeof(float) * 3 * (size_t)N));
-    MPX_TRY(eval_into(e, m, MPX_Q_TORQUE, e->d_scratch));
+    MPX_TRY(eval_into(e, m, g->torque_kind ? MPX_Q_DAMPING_TORQUE : MPX_Q_TORQUE, e->d_scratch));
     const int nb = 256;
     k_reduce_partial<<<nb, 256, 0, e->stream>>>(e->d_scratch, N, 3, m->geom, 1, e->d_red);
     k_reduce_final<<<1, 32, 0, e->stream>>>(e->d_red, nb, 1, e->d_redout);
@@ -1042,7 +1044,7 @@ mpx_status mpx_engine_create(int device, mpx_engine** out) {
   CUDA_TRY(cudaMalloc(&e->d_tw, sizeof(float2) * TW_N));
   CUDA_TRY(cudaMemcpy(e->d_tw, tw.data(), sizeof(float2) * TW_N, cudaMemcpyHostToDevice));
   CUDA_TRY(cudaMalloc(&e->d_red, sizeof(double) * 3 * 1024));
-  CUDA_TRY(cudaMalloc(&e->d_redout, sizeof(double) * 3));
+  CUDA_TRY(cudaMalloc(&e->d_redout, sizeof(double) * 4));  // 3 reduction results, or the 4 of k_min_final
   // large dynamic shared memory and the max-shared carveout for the FFT kernels
   const void* fft_kernels[] = {(const void*)k_xfwd<false>, (const void*)k_xfwd<true>, (const void*)k_xinv,
                                (const void*)k_yz<1, 4>, (const void*)k_yz<2, 4>, (const void*)k_yz<4, 4>,
@@ -1641,6 +1643,205 @@ mpx_status mpx_solver_run(mpx_engine* e, int group, double duration) {
   MPX_TRY(start_group(e, g, 0, 0, duration, 0.0, &none));
   if (none) return MPX_OK;
   return drive_group(e, g);
+}
+
+// ------------------------------------------------ minimize / relax
+// Sum over the group's magnets of the squared norm of the damping torque
+// (physics/relaxer.cpp calcTorque: dotSum(torque, torque)), or its largest
+// per-cell norm per magnet.
+static mpx_status damping_torque_reduce(mpx_engine* e, Magnet* m, int op, double* out) {
+  double r[3];
+  MPX_TRY(reduce_quantity(e, m, MPX_Q_DAMPING_TORQUE, op, r));
+  *out = r[0];
+  return MPX_OK;
+}
+
+static mpx_status group_energy(mpx_engine* e, Group* g, double* out) {
+  double E = 0;
+  for (int id : g->magnets) {
+    double v;
+    MPX_TRY(mpx_energy(e, id, MPX_Q_TOTAL_ENERGY_DENSITY, &v));
+    E += v;
+  }
+  *out = E;
+  return MPX_OK;
+}
+
+static mpx_status group_torque_sq(mpx_engine* e, Group* g, double* out) {
+  double t = 0;
+  for (int id : g->magnets) {
+    double v;
+    MPX_TRY(damping_torque_reduce(e, get_mag(e, id), 2, &v));
+    t += v;
+  }
+  *out = t;
+  return MPX_OK;
+}
+
+// Iteration bound of the minimize / relax loops, which the reference runs
+// without one: a solve that has not converged by then fails instead of hanging.
+constexpr long long RELAX_MAX_STEPS = 10000000;
+
+mpx_status mpx_minimize(mpx_engine* e, int group, double tol, int nsamples) {
+  Group* g = get_group(e, group);
+  if (!g) return fail(MPX_ERR_RANGE, "no such group");
+  if (nsamples <= 0) return fail(MPX_ERR_INVALID, "nsamples must be positive");
+  if (g->magnets.empty()) return MPX_OK;
+  DeviceGuard guard(e->device);
+  GroupDev G;
+  MPX_TRY(read_group(e, group, &G));
+  std::vector<Magnet*> ms;
+  for (int id : g->magnets) ms.push_back(get_mag(e, id));
+  // scratch roles among the stage buffers (the stage values are recomputed after)
+  int t0 = 2, t1 = 3;
+  const int m0 = 4, m1 = 5;
+  for (Magnet* m : ms) MPX_TRY(eval_into(e, m, MPX_Q_DAMPING_TORQUE, m->dev.buf[G.map[t0]]));
+  const size_t nkeep = (size_t)nsamples * ms.size();
+  std::vector<double> step(ms.size(), 1e-14);
+  std::deque<double> diffs;
+  const int nb = 256;
+  for (long long n = 0;; ++n) {
+    if (diffs.size() >= nkeep) {  // Minimizer::converged
+      bool conv = true;
+      for (double d : diffs) conv = conv && (d <= tol);
+      if (conv) break;
+    }
+    if (n >= RELAX_MAX_STEPS) return fail(MPX_ERR_RUNTIME, "minimize did not converge");
+    for (size_t j = 0; j < ms.size(); ++j) {
+      MagnetDev& D = ms[j]->dev;
+      k_min_step<<<std::min((D.N + 255) / 256, 148 * 8), 256, 0, e->stream>>>(
+          D.buf[G.map[0]], D.buf[G.map[m0]], D.buf[G.map[m1]], D.buf[G.map[t0]], D.N, (float)step[j], ms[j]->geom);
+      e->launches++;
+    }
+    for (Magnet* m : ms) MPX_TRY(eval_into(e, m, MPX_Q_DAMPING_TORQUE, m->dev.buf[G.map[t1]]));
+    for (size_t j = 0; j < ms.size(); ++j) {
+      MagnetDev& D = ms[j]->dev;
+      k_min_partial<<<nb, 256, 0, e->stream>>>(D.buf[G.map[m0]], D.buf[G.map[m1]], D.buf[G.map[t0]],
+                                               D.buf[G.map[t1]], D.N, e->d_red);
+      k_min_final<<<1, 32, 0, e->stream>>>(e->d_red, nb, e->d_redout);
+      e->launches += 2;
+      MPX_TRY(check_launch(e, "minimize"));
+      double r[4];
+      CUDA_TRY(cudaMemcpyAsync(r, e->d_redout, sizeof(r), cudaMemcpyDeviceToHost, e->stream));
+      CUDA_TRY(cudaStreamSynchronize(e->stream));
+      // Barzilai-Borwein step size, alternating its two forms
+      const double nom = (n % 2 == 0) ? r[0] : r[1], div = (n % 2 == 0) ? r[1] : r[2];
+      step[j] = (div == 0.0) ? 1e-14 : nom / div;
+      diffs.push_back(r[3]);
+      if (diffs.size() > nkeep) diffs.pop_front();
+    }
+    std::swap(t0, t1);
+  }
+  G.k0_valid = 0;
+  return write_group(e, group, &G);
+}
+
+mpx_status mpx_relax(mpx_engine* e, int group, double tol, double threshold) {
+  Group* g = get_group(e, group);
+  if (!g) return fail(MPX_ERR_RANGE, "no such group");
+  if (threshold == 0.0) return fail(MPX_ERR_INVALID, "The relax threshold should not be zero.");
+  if (g->magnets.empty()) return MPX_OK;
+  DeviceGuard guard(e->device);
+  const mpx_solver_params saved = g->sp;
+  GroupDev G;
+  MPX_TRY(read_group(e, group, &G));
+  const double t_saved = G.t, dt_saved = G.dt;
+  // adaptive Fehlberg on the damping torque, starting from the sensible step for it
+  mpx_solver_params p = saved;
+  p.method = MPX_RK_FEHLBERG;
+  p.adaptive = 1;
+  g->sp = p;
+  g->torque_kind = 1;
+  fill_group_params(G, p);
+  G.torque_kind = 1;
+  G.k0_valid = 0;
+  MPX_TRY(write_group(e, group, &G));
+  double dt;
+  MPX_TRY(sensible_timestep(e, g, &dt));
+  MPX_TRY(mpx_solver_set_timestep(e, group, dt));
+  auto set_max_error = [&](double err) -> mpx_status {
+    g->sp.max_error = err;
+    GroupDev H;
+    MPX_TRY(read_group(e, group, &H));
+    H.max_error = err;
+    return write_group(e, group, &H);
+  };
+  mpx_status st = MPX_OK;
+  long long nsteps = 0;
+  auto steps3 = [&]() -> mpx_status {
+    nsteps += 3;
+    if (nsteps > RELAX_MAX_STEPS) return fail(MPX_ERR_RUNTIME, "relax did not converge");
+    return mpx_solver_steps(e, group, 3);
+  };
+  do {
+    // energy phase (physics/relaxer.cpp): steps of 3 while the energy decreases
+    double E0, E1;
+    if ((st = group_energy(e, g, &E0)) != MPX_OK) break;
+    if ((st = steps3()) != MPX_OK) break;
+    if ((st = group_energy(e, g, &E1)) != MPX_OK) break;
+    while (E1 < E0) {
+      if ((st = steps3()) != MPX_OK) break;
+      E0 = E1;
+      if ((st = group_energy(e, g, &E1)) != MPX_OK) break;
+    }
+    if (st != MPX_OK) break;
+    double err = g->sp.max_error;
+    if (threshold < 0) {  // torque phase: lower the error while the torque decreases
+      double tq0, tq1;
+      if ((st = group_torque_sq(e, g, &tq1)) != MPX_OK) break;
+      while (err > tol && st == MPX_OK) {
+        err /= std::sqrt(2.0);
+        if ((st = set_max_error(err)) != MPX_OK) break;
+        if ((st = steps3()) != MPX_OK) break;
+        tq0 = tq1;
+        if ((st = group_torque_sq(e, g, &tq1)) != MPX_OK) break;
+        while (tq1 < tq0) {
+          if ((st = steps3()) != MPX_OK) break;
+          tq0 = tq1;
+          if ((st = group_torque_sq(e, g, &tq1)) != MPX_OK) break;
+        }
+      }
+    } else {  // until every magnet's max torque is at or below the threshold, then lower the error
+      while (err > tol && st == MPX_OK) {
+        bool conv = true;
+        for (int id : g->magnets) {
+          double mx;
+          if ((st = damping_torque_reduce(e, get_mag(e, id), 1, &mx)) != MPX_OK) break;
+          if (mx > threshold) {
+            conv = false;
+            break;
+          }
+        }
+        if (st != MPX_OK) break;
+        if (conv) {
+          err /= std::sqrt(2.0);
+          if ((st = set_max_error(err)) != MPX_OK) break;
+        }
+        st = steps3();
+      }
+    }
+  } while (false);
+  const std::string msg = g_last_error;
+  // restore the solver (physics/relaxer.cpp: method, error, adaptivity, time,
+  // time step, then the equations, which for an adaptive solver recompute the
+  // sensible time step of the LLG torque)
+  g->sp = saved;
+  g->torque_kind = 0;
+  GroupDev R;
+  MPX_TRY(read_group(e, group, &R));
+  fill_group_params(R, saved);
+  R.torque_kind = 0;
+  R.k0_valid = 0;
+  R.t = t_saved;
+  R.dt = dt_saved;
+  MPX_TRY(write_group(e, group, &R));
+  if (saved.adaptive) {
+    double dt2;
+    MPX_TRY(sensible_timestep(e, g, &dt2));
+    MPX_TRY(mpx_solver_set_timestep(e, group, dt2));
+  }
+  if (st != MPX_OK) g_last_error = msg;
+  return st;
 }
 
 mpx_status mpx_group_start(mpx_engine* e, int group, double duration, double torque_stop) {

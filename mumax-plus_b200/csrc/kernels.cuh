@@ -436,7 +436,7 @@ __device__ __forceinline__ void epilogue_cell(const MagnetDev& M, const GroupDev
         h = local_terms(M, m, x, y, z, i, mc, TERM_EXT).ext;
       }
       h = h + bdemag;
-      k = llg_torque(mc, h, M.alpha.at(i));
+      k = G.torque_kind ? damping_torque(mc, h) : llg_torque(mc, h, M.alpha.at(i));
     }
     store3(M.buf[G.map[2 + ea.stage]], N, i, k);
     if (ea.fsal_err && ing) {
@@ -497,7 +497,7 @@ __device__ __forceinline__ void epilogue_cell(const MagnetDev& M, const GroupDev
       if (M.frozen.at(i) == 0.0f) r = llg_torque(mc, h, M.alpha.at(i));
       break;
     case 9:
-      if (M.frozen.at(i) == 0.0f) r = (-GAMMA_LL) * cross3(mc, cross3(mc, h));
+      if (M.frozen.at(i) == 0.0f) r = damping_torque(mc, h);
       break;
     case 10: s = (M.terms & TERM_EXCH) ? -0.5f * ms * dot3(mc, lo.exch) : 0.f; break;
     case 11: s = (M.terms & TERM_DMI) ? -0.5f * ms * dot3(mc, lo.dmi) : 0.f; break;
@@ -750,6 +750,11 @@ __global__ void k_reduce_partial(const float* __restrict__ a, int N, int ncomp,
     if (geom && !geom[i]) continue;
     if (op == 0) {
       for (int c = 0; c < ncomp; ++c) acc[c] += (double)a[(size_t)c * N + i];
+    } else if (op == 2) {  // sum of squared norms (dotSum(a, a), core/reduce.cu)
+      for (int c = 0; c < ncomp; ++c) {
+        const double v = a[(size_t)c * N + i];
+        acc[0] += v * v;
+      }
     } else {
       double s = 0;
       for (int c = 0; c < ncomp; ++c) {
@@ -765,7 +770,7 @@ __global__ void k_reduce_partial(const float* __restrict__ a, int N, int ncomp,
   for (int s = blockDim.x / 2; s > 0; s >>= 1) {
     if (threadIdx.x < s)
       for (int c = 0; c < 3; ++c) {
-        if (op == 0) sh[c][threadIdx.x] += sh[c][threadIdx.x + s];
+        if (op != 1) sh[c][threadIdx.x] += sh[c][threadIdx.x + s];
         else {
           const double o = sh[c][threadIdx.x + s];
           if (o > sh[c][threadIdx.x] || o != o) sh[c][threadIdx.x] = o;
@@ -783,7 +788,7 @@ __global__ void k_reduce_final(const double* __restrict__ partial, int nblocks, 
   for (int b = 0; b < nblocks; ++b)
     for (int c = 0; c < 3; ++c) {
       const double v = partial[b * 3 + c];
-      if (op == 0) r[c] += v;
+      if (op != 1) r[c] += v;
       else if (v > r[c] || v != v) r[c] = v;
     }
   for (int c = 0; c < 3; ++c) out[c] = r[c];
@@ -819,6 +824,76 @@ __global__ void k_random_normal(float* __restrict__ out, int n, unsigned long lo
     const float u2 = (float)(unsigned)(z & 0xFFFFFFull) * (1.0f / 16777216.0f);  // [0, 1)
     out[i] = sqrtf(-2.0f * logf(u1)) * cospif(2.0f * u2);
   }
+}
+
+// ------------------------------------------------------------- minimizer
+// One steepest-descent step of physics/minimizer.cu (k_step): from the state m0
+// and its damping torque t0, m1 = ((4 - dt^2 t0^2) m0 + 4 dt t0) / (4 + dt^2 t0^2)
+// over every cell of the grid; m0 and the unnormalised m1 are kept for the
+// Barzilai-Borwein step size, the state becomes m1 normalised inside the
+// geometry (the reference's magnetization()->set(m1)).
+__global__ void k_min_step(float* __restrict__ state, float* __restrict__ m0_out, float* __restrict__ m1_out,
+                           const float* __restrict__ t0, int N, float dt, const unsigned char* __restrict__ geom) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x) {
+    const float3 m0 = load3(state, N, i), t = load3(t0, N, i);
+    const float t2 = dt * dt * dot3(t, t);
+    const float inv = 1.0f / (4.0f + t2);
+    const float3 m1 = f3(((4.0f - t2) * m0.x + 4.0f * dt * t.x) * inv, ((4.0f - t2) * m0.y + 4.0f * dt * t.y) * inv,
+                         ((4.0f - t2) * m0.z + 4.0f * dt * t.z) * inv);
+    store3(m0_out, N, i, m0);
+    store3(m1_out, N, i, m1);
+    float3 n = m1;
+    if (!geom || geom[i]) {
+      const float r = rsqrtf(dot3(m1, m1));
+      n = f3(m1.x * r, m1.y * r, m1.z * r);
+    }
+    store3(state, N, i, n);
+  }
+}
+
+// Block partials (FP64) of dm.dm, dm.dt, dt.dt and max|dm| with dm = m1 - m0 and
+// dt = t0 - t1 (physics/minimizer.cu: BarzilianBorweinStepSize, maxVecNorm(dm)).
+__global__ void k_min_partial(const float* __restrict__ m0, const float* __restrict__ m1, const float* __restrict__ t0,
+                              const float* __restrict__ t1, int N, double* __restrict__ partial) {
+  __shared__ double sh[4][256];
+  double a = 0, b = 0, c = 0, mx = 0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x) {
+    const float3 p = load3(m0, N, i), q = load3(m1, N, i), u = load3(t0, N, i), v = load3(t1, N, i);
+    const float3 dm = f3(q.x - p.x, q.y - p.y, q.z - p.z);
+    const float3 dt = f3(u.x - v.x, u.y - v.y, u.z - v.z);
+    const double mm = (double)dm.x * dm.x + (double)dm.y * dm.y + (double)dm.z * dm.z;
+    a += mm;
+    b += (double)dm.x * dt.x + (double)dm.y * dt.y + (double)dm.z * dt.z;
+    c += (double)dt.x * dt.x + (double)dt.y * dt.y + (double)dt.z * dt.z;
+    const double n = sqrt(mm);
+    mx = (n > mx || n != n) ? n : mx;
+  }
+  sh[0][threadIdx.x] = a;
+  sh[1][threadIdx.x] = b;
+  sh[2][threadIdx.x] = c;
+  sh[3][threadIdx.x] = mx;
+  __syncthreads();
+  for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+    if (threadIdx.x < s) {
+      for (int k = 0; k < 3; ++k) sh[k][threadIdx.x] += sh[k][threadIdx.x + s];
+      const double o = sh[3][threadIdx.x + s];
+      if (o > sh[3][threadIdx.x] || o != o) sh[3][threadIdx.x] = o;
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0)
+    for (int k = 0; k < 4; ++k) partial[blockIdx.x * 4 + k] = sh[k][0];
+}
+
+__global__ void k_min_final(const double* __restrict__ partial, int nblocks, double* __restrict__ out) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  double r[4] = {0, 0, 0, 0};
+  for (int b = 0; b < nblocks; ++b) {
+    for (int k = 0; k < 3; ++k) r[k] += partial[b * 4 + k];
+    const double v = partial[b * 4 + 3];
+    if (v > r[3] || v != v) r[3] = v;
+  }
+  for (int k = 0; k < 4; ++k) out[k] = r[k];
 }
 
 }  // namespace mpx

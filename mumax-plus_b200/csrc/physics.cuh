@@ -91,6 +91,7 @@ struct GroupDev {
   int k0_valid;
   int finished_flag;  // set when the group finished, cleared by the host poll
   int map[9];     // buffer roles: [0] x0 (state), [1] xs (stage / new state), [2+s] k_s
+  int torque_kind;  // right-hand side of the stages: 0 LLG torque, 1 damping torque only (relax)
 };
 
 enum { GS_IDLE = 0, GS_RUNNING = 1, GS_FINISHED = 2, GS_FAILED = 3 };
@@ -354,6 +355,11 @@ __device__ __forceinline__ float3 llg_torque(float3 m, float3 h, float a) {
   const float3 mxh = cross3(m, h);
   const float3 mxmxh = cross3(m, mxh);
   return (-GAMMA_LL / (1 + a * a)) * (mxh + a * mxmxh);
+}
+
+// physics/torque.cu:58-76 (k_dampingtorque): the relax torque -gamma_LL m x (m x h)
+__device__ __forceinline__ float3 damping_torque(float3 m, float3 h) {
+  return (-GAMMA_LL) * cross3(m, cross3(m, h));
 }
 
 }  // namespace mpx

@@ -48,6 +48,7 @@ class Ferromagnet:
         self._regions = self._mask(regions, "regions")
         self._engine = world._engine
         self._group = world._group
+        self._relax_threshold = -1.0
         self._suspend = True
         ch = self._update
         self._msat = Parameter(self, "msat", "A/m", 1, 1.0, ch)
@@ -372,12 +373,34 @@ class Ferromagnet:
     def total_energy(self):
         return self._energy(_abi.Q_TOTAL_ENERGY_DENSITY, "total_energy")
 
-    # ------------------------------------------------------------- not on the path
+    # ------------------------------------------------------------- energy minima
     def minimize(self, tol=1e-6, nsamples=10):
-        raise NotImplementedError("minimize() is not implemented on the accelerated path yet")
+        """Minimize the total energy (mumaxplus/ferromagnet.py:144-164): steepest
+        descent on the damping torque with Barzilai-Borwein steps until the last
+        `nsamples` largest changes of m are all <= tol.  In a world with several
+        magnets every magnet of the world takes part."""
+        self._engine.minimize(self._group, tol, nsamples)
 
     def relax(self, tol=1e-9):
-        raise NotImplementedError("relax() is not implemented on the accelerated path yet")
+        """Relax to an energy minimum (mumaxplus/ferromagnet.py:166-192): time
+        evolution without precession while the energy decreases, then while the
+        torque decreases, lowering the solver's maximum error down to `tol`."""
+        if tol >= 1e-5:
+            warnings.warn("The set tolerance is greater than or equal to the default value"
+                           + " used for the timesolver (1e-5). Using this value results"
+                           + " in no torque minimization, only energy minimization.", UserWarning)
+        self._engine.relax(self._group, tol, self._relax_threshold)
+
+    @property
+    def RelaxTorqueThreshold(self):
+        """Threshold torque for relax (default -1: relax until the torque is
+        steady or increasing; positive: until the max torque is <= it)."""
+        return self._relax_threshold
+
+    @RelaxTorqueThreshold.setter
+    def RelaxTorqueThreshold(self, value):
+        assert value != 0, "The relax threshold should not be zero."
+        self._relax_threshold = float(value)
 
 
 def _pad_lut(lut, n, uniform):

@@ -29,6 +29,7 @@ class World:
         self._mastergrid = Grid(mastergrid.size, mastergrid.origin)
         self._engine = Engine(device)
         self._group = self._engine.group_create()
+        self._relax_threshold = -1.0
         self._magnets = {}
         self._bias = (0.0, 0.0, 0.0)
         self._unnamed = 1
@@ -176,7 +177,24 @@ class World:
         self._update_all()
 
     def relax(self, tol=1e-9):
-        raise NotImplementedError("relax() is not implemented on the accelerated path yet")
+        """Relax all magnets of the world to an energy minimum
+        (mumaxplus/world.py:117-141, physics/relaxer.cpp)."""
+        if tol >= 1e-5:
+            warnings.warn("The set tolerance is greater than or equal to the default value"
+                           + " used for the timesolver (1e-5). Using this value results"
+                           + " in no torque minimization, only energy minimization.", UserWarning)
+        self._engine.relax(self._group, tol, self._relax_threshold)
 
     def minimize(self, tol=1e-6, nsamples=10):
-        raise NotImplementedError("minimize() is not implemented on the accelerated path yet")
+        """Minimize the total energy of the world (mumaxplus/world.py:95-115)."""
+        self._engine.minimize(self._group, tol, nsamples)
+
+    @property
+    def RelaxTorqueThreshold(self):
+        """Threshold torque for relax (default -1, see Ferromagnet.RelaxTorqueThreshold)."""
+        return self._relax_threshold
+
+    @RelaxTorqueThreshold.setter
+    def RelaxTorqueThreshold(self, value):
+        assert value != 0, "The relax threshold should not be zero."
+        self._relax_threshold = float(value)

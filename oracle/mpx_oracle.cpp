@@ -20,6 +20,7 @@
 // kernel-grid layout (physics/strayfieldkernel.cu:80-99, strayfieldfft.cu:75-100).
 
 #include <cmath>
+#include <deque>
 #include <complex>
 #include <cstdint>
 #include <cstring>
@@ -685,6 +686,7 @@ struct World {
   mpx_solver_params sp{MPX_RK_FEHLBERG, 1, 1e-5, 0.8, 0.5, 2.0, 0.01, 1e-14};
   double t = 0, dt = 0;
   int64_t steps = 0, rejected = 0, evals = 0;
+  bool relax_torque = false;  // the equations use the damping torque (physics/relaxer.cpp)
 };
 
 // physics/effectivefield.cpp:15-28 (terms added in this order)
@@ -874,7 +876,7 @@ double sensible_timestep(World& w) {
   double gmax = 0;
   for (auto& mg : w.mags) {
     std::vector<double> tq;
-    torque(w, mg, tq);
+    torque(w, mg, tq, w.relax_torque);
     gmax = std::max(gmax, max_norm(mg, tq));
   }
   if (gmax == 0) return w.sp.sensible_timestep_default;
@@ -920,7 +922,7 @@ void rk_step(World& w) {
         }
         set_normalized(mg, xs);
       }
-      for (size_t q = 0; q < w.mags.size(); ++q) torque(w, w.mags[q], k[q][s]);  // setStageK
+      for (size_t q = 0; q < w.mags.size(); ++q) torque(w, w.mags[q], k[q][s], w.relax_torque);  // setStageK
     }
     w.t = t0 + dt;
     for (size_t q = 0; q < w.mags.size(); ++q) {  // setFinalX
@@ -1181,6 +1183,168 @@ int ox_run(ox_world* wp, double duration) {
   w.dt = stop - w.t;
   int st = solver_step(w);
   if (!w.sp.adaptive) w.dt = old;
+  return st;
+}
+
+
+// physics/minimizer.cu:73-160 (Minimizer::exec): steepest descent on the damping
+// torque with Barzilai-Borwein step sizes, all magnets of the world.
+int ox_minimize(ox_world* wp, double tol, int nsamples) {
+  World& w = *reinterpret_cast<World*>(wp);
+  const size_t nm = w.mags.size();
+  if (nm == 0) return MPX_OK;
+  const size_t nkeep = (size_t)nsamples * nm;
+  std::vector<std::vector<double>> t0(nm), t1(nm);
+  std::vector<double> step(nm, 1e-14);
+  std::deque<double> diffs;
+  for (size_t q = 0; q < nm; ++q) torque(w, w.mags[q], t0[q], true);
+  for (long long n = 0;; ++n) {
+    if (diffs.size() >= nkeep) {
+      bool conv = true;
+      for (double d : diffs) conv = conv && d <= tol;
+      if (conv) break;
+    }
+    if (n >= 10000000) {
+      g_err = "minimize did not converge";
+      return MPX_ERR_RUNTIME;
+    }
+    std::vector<std::vector<double>> m0(nm), m1(nm);
+    for (size_t q = 0; q < nm; ++q) {  // k_step
+      Magnet& mg = w.mags[q];
+      const int N = mg.N;
+      m0[q] = mg.m;
+      m1[q].assign(3 * (size_t)N, 0.0);
+      const double dt = step[q];
+      for (int i = 0; i < N; ++i) {
+        V3 a = mg.mv(i), t{t0[q][i], t0[q][(size_t)N + i], t0[q][2 * (size_t)N + i]};
+        const double t2 = dt * dt * dot(t, t);
+        const V3 b = (1.0 / (4 + t2)) * ((4 - t2) * a + (4 * dt) * t);
+        m1[q][i] = b.x;
+        m1[q][(size_t)N + i] = b.y;
+        m1[q][2 * (size_t)N + i] = b.z;
+      }
+      mg.m = m1[q];
+      set_normalized(mg, m1[q]);
+    }
+    for (size_t q = 0; q < nm; ++q) torque(w, w.mags[q], t1[q], true);
+    for (size_t q = 0; q < nm; ++q) {
+      const int N = w.mags[q].N;
+      double dmdm = 0, dmdt = 0, dtdt = 0, mx = 0;
+      for (int i = 0; i < N; ++i) {
+        double s = 0;
+        for (int c = 0; c < 3; ++c) {
+          const size_t k = (size_t)c * N + i;
+          const double dm = m1[q][k] - m0[q][k], dtq = t0[q][k] - t1[q][k];
+          dmdm += dm * dm;
+          dmdt += dm * dtq;
+          dtdt += dtq * dtq;
+          s += dm * dm;
+        }
+        mx = std::max(mx, std::sqrt(s));
+      }
+      const double nom = (n % 2 == 0) ? dmdm : dmdt, div = (n % 2 == 0) ? dmdt : dtdt;
+      step[q] = (div == 0.0) ? 1e-14 : nom / div;
+      diffs.push_back(mx);
+      if (diffs.size() > nkeep) diffs.pop_front();
+    }
+    std::swap(t0, t1);
+  }
+  return MPX_OK;
+}
+
+// physics/relaxer.cpp:88-174 (Relaxer::exec) for all magnets of the world.
+int ox_relax(ox_world* wp, double tol, double threshold) {
+  World& w = *reinterpret_cast<World*>(wp);
+  if (threshold == 0.0) {
+    g_err = "The relax threshold should not be zero.";
+    return MPX_ERR_INVALID;
+  }
+  if (w.mags.empty()) return MPX_OK;
+  const mpx_solver_params saved = w.sp;
+  const double t_saved = w.t, dt_saved = w.dt;
+  w.sp.adaptive = 1;
+  w.sp.method = MPX_RK_FEHLBERG;
+  w.relax_torque = true;
+  w.dt = sensible_timestep(w);
+  auto energy = [&]() {
+    double E = 0;
+    for (size_t q = 0; q < w.mags.size(); ++q) {
+      double v;
+      ox_energy(wp, (int)q, MPX_Q_TOTAL_ENERGY_DENSITY, &v);
+      E += v;
+    }
+    return E;
+  };
+  auto torque_sq = [&]() {
+    double s = 0;
+    for (auto& mg : w.mags) {
+      std::vector<double> t;
+      torque(w, mg, t, true);
+      for (int i = 0; i < mg.N; ++i)
+        if (mg.in_geom(i))
+          for (int c = 0; c < 3; ++c) s += t[(size_t)c * mg.N + i] * t[(size_t)c * mg.N + i];
+    }
+    return s;
+  };
+  int st = MPX_OK;
+  long long nsteps = 0;
+  auto steps3 = [&]() {
+    nsteps += 3;
+    if (nsteps > 10000000) {
+      g_err = "relax did not converge";
+      return (int)MPX_ERR_RUNTIME;
+    }
+    return ox_steps(wp, 3);
+  };
+  do {
+    double E0 = energy();
+    if ((st = steps3())) break;
+    double E1 = energy();
+    while (E1 < E0) {
+      if ((st = steps3())) break;
+      E0 = E1;
+      E1 = energy();
+    }
+    if (st) break;
+    double err = w.sp.max_error;
+    if (threshold < 0) {
+      double tq1 = torque_sq(), tq0;
+      while (err > tol && !st) {
+        err /= std::sqrt(2.0);
+        w.sp.max_error = err;
+        if ((st = steps3())) break;
+        tq0 = tq1;
+        tq1 = torque_sq();
+        while (tq1 < tq0) {
+          if ((st = steps3())) break;
+          tq0 = tq1;
+          tq1 = torque_sq();
+        }
+      }
+    } else {
+      while (err > tol && !st) {
+        bool conv = true;
+        for (auto& mg : w.mags) {
+          std::vector<double> t;
+          torque(w, mg, t, true);
+          if (max_norm(mg, t) > threshold) {
+            conv = false;
+            break;
+          }
+        }
+        if (conv) {
+          err /= std::sqrt(2.0);
+          w.sp.max_error = err;
+        }
+        st = steps3();
+      }
+    }
+  } while (false);
+  w.sp = saved;
+  w.relax_torque = false;
+  w.t = t_saved;
+  w.dt = dt_saved;
+  if (saved.adaptive) w.dt = sensible_timestep(w);
   return st;
 }
 

@@ -61,6 +61,8 @@ def lib():
         L.ox_demag_brute.argtypes = [V, C.c_int, C.c_void_p]
         L.ox_demag_kernel.argtypes = [V, C.c_int, C.c_void_p, C.POINTER(C.c_int)]
         L.ox_set_kernel_octant.argtypes = [V, C.c_int, C.c_void_p]
+        L.ox_minimize.argtypes = [V, C.c_double, C.c_int]
+        L.ox_relax.argtypes = [V, C.c_double, C.c_double]
         L.ox_newell.restype = C.c_double
         L.ox_newell.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double]
         L.ox_average.argtypes = [V, C.c_int, C.c_int, P_D]
@@ -207,6 +209,12 @@ class OracleWorld:
 
     def steps(self, n):
         self._check(lib().ox_steps(self._h, int(n)))
+
+    def minimize(self, tol=1e-6, nsamples=10):
+        self._check(lib().ox_minimize(self._h, float(tol), int(nsamples)))
+
+    def relax(self, tol=1e-9, threshold=-1.0):
+        self._check(lib().ox_relax(self._h, float(tol), float(threshold)))
 
     def run(self, duration):
         self._check(lib().ox_run(self._h, float(duration)))

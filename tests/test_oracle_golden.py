@@ -235,3 +235,64 @@ def test_oracle_external_kernel_octant_reproduces_own(oracle):
     ow2.set_kernel_octant(q2, oct)
     got = ow2.eval(q2, oracle.abi.Q_DEMAG_FIELD)
     assert np.max(np.abs(got - want)) <= 1e-10 * np.max(np.abs(want))
+
+
+def sp2_coercivity(make, minimize, set_field, m_sum):
+    """Standard problem 2 in the small-particle limit, the protocol of the
+    reference's test/test_standardproblem2_coercivity.py:14-66: one cell of
+    L x d x t = 0.5 x 0.1 x 0.01 exchange lengths, minimize from (1,1,1), then
+    raise a field along -(1,1,1) in steps of 5e-5 Msat until m flips; returns
+    the interpolated relative coercive field."""
+    d = 0.1
+    t, L = 0.1 * d, 5.0 * d
+    msat, aex, mu0 = 800e3, 13e-12, 1.25663706212e-6
+    lex = np.sqrt(2 * aex / (mu0 * msat ** 2))
+    make((L * lex, d * lex, t * lex), msat, aex)
+    minimize()
+    hdir = -np.ones(3) / np.sqrt(3)
+    h1 = 0.05
+    set_field(mu0 * h1 * msat * hdir)
+    minimize()
+    m1 = m_sum()
+    h0, m0 = 0.0, None
+    while m1 > 0:
+        h0, m0 = h1, m1
+        h1 += 0.00005
+        set_field(mu0 * h1 * msat * hdir)
+        minimize()
+        m1 = m_sum()
+    return (m0 * h1 - m1 * h0) / (m0 - m1)
+
+
+def test_oracle_minimize_sp2_coercivity_golden(oracle):
+    """Known answer of the reference test: H_c / Msat = 0.057069478 (1e-5)."""
+    st = {}
+
+    def make(cs, msat, aex):
+        s = MagnetSpec(size=(1, 1, 1), cellsize=cs, msat=msat, aex=aex)
+        ow, q = s.oracle_world(np.ones((3, 1, 1, 1), np.float32))
+        st.update(ow=ow, q=q)
+
+    rhc = sp2_coercivity(make, lambda: st["ow"].minimize(1e-6, 10),
+                         lambda b: st["ow"].set_world_bias(tuple(b)),
+                         lambda: float(np.sum(st["ow"].average(st["q"], oracle.abi.Q_MAGNETIZATION))))
+    assert abs(0.057069478 - rhc) < 1e-5, rhc
+
+
+def test_oracle_relax_reaches_the_minimum_of_a_uniaxial_film(oracle):
+    """relax from a tilted state of a film with a strong uniaxial axis and a
+    field along it ends aligned with the axis, with the solver's time, time step
+    and settings restored."""
+    s = MagnetSpec(size=(8, 6, 1), cellsize=(2e-9, 2e-9, 2e-9), msat=8e5, aex=1e-11, alpha=0.1, ku1=5e5,
+                   anisU=(0.0, 0.0, 1.0), world_bias=(0.0, 0.0, 0.05), enable_demag=False)
+    m0 = np.zeros((3, 1, 6, 8), np.float32)
+    m0[0], m0[2] = 0.6, 0.8
+    ow, q = s.oracle_world(m0)
+    ow.set_method("DormandPrince")
+    ow.timestep = 1e-13
+    ow.time = 3e-12
+    ow.relax(1e-9)
+    m = np.array(ow.average(q, oracle.abi.Q_MAGNETIZATION))
+    assert m[2] > 1 - 1e-6
+    assert ow.time == 3e-12
+    assert oracle.abi.RK_NAMES[ow.solver.method] == "DormandPrince"

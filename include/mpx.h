@@ -140,6 +140,10 @@ typedef struct {
   const float* scale_exchange_lut;
   int enable_demag;             /* default 1                                    */
   int enable_openbc;            /* default 0                                    */
+  /* cubic anisotropy (physics/anisotropy.cu:57-106); used when the uniaxial
+   * term is assured zero, as in the reference */
+  mpx_scalar kc1, kc2, kc3;     /* J/m^3                                        */
+  mpx_vector anis_c1, anis_c2;  /* cubic axes (normalised per cell; c3 = c1 x c2) */
 } mpx_magnet_desc;
 
 /* Time-solver settings (core/timesolver.hpp:74-82 defaults in brackets). */

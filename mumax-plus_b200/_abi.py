@@ -86,6 +86,11 @@ class MagnetDesc(C.Structure):
         ("scale_exchange_lut", C.POINTER(C.c_float)),
         ("enable_demag", C.c_int),
         ("enable_openbc", C.c_int),
+        ("kc1", Scalar),
+        ("kc2", Scalar),
+        ("kc3", Scalar),
+        ("anis_c1", Vector),
+        ("anis_c2", Vector),
     ]
 
 

@@ -551,6 +551,11 @@ mpx_status load_params(mpx_engine* e, Magnet* m, const mpx_magnet_desc* d) {
   MPX_TRY(load_scalar(e, m, &D.frozen, d->frozen_spins, N));
   MPX_TRY(load_vector(e, m, &D.anisU, d->anis_u, N));
   MPX_TRY(load_vector(e, m, &D.bias, d->bias_magnetic_field, N));
+  MPX_TRY(load_scalar(e, m, &D.kc1, d->kc1, N));
+  MPX_TRY(load_scalar(e, m, &D.kc2, d->kc2, N));
+  MPX_TRY(load_scalar(e, m, &D.kc3, d->kc3, N));
+  MPX_TRY(load_vector(e, m, &D.anisC1, d->anis_c1, N));
+  MPX_TRY(load_vector(e, m, &D.anisC2, d->anis_c2, N));
   for (int c = 0; c < 9; ++c) MPX_TRY(load_scalar(e, m, &D.dmi[c], d->dmi[c], N));
   D.inter_u = (float)d->inter_exchange;
   D.scale_u = (float)d->scale_exchange;
@@ -599,7 +604,12 @@ mpx_status load_params(mpx_engine* e, Magnet* m, const mpx_magnet_desc* d) {
   bool dmi0 = true;
   for (int c = 0; c < 9; ++c) dmi0 = dmi0 && scalar_zero(d->dmi[c]);
   if (!(dmi0 || msat0)) terms |= TERM_DMI;
-  if (!((scalar_zero(d->ku1) && scalar_zero(d->ku2)) || vector_zero(d->anis_u) || msat0)) terms |= TERM_ANIS;
+  // physics/anisotropy.cu:9-23: uniaxial unless assured zero, else cubic unless assured zero
+  const bool uni0 = (scalar_zero(d->ku1) && scalar_zero(d->ku2)) || vector_zero(d->anis_u) || msat0;
+  const bool cub0 = (scalar_zero(d->kc1) && scalar_zero(d->kc2) && scalar_zero(d->kc3)) ||
+                    (vector_zero(d->anis_c1) && vector_zero(d->anis_c2)) || msat0;
+  if (!uni0) terms |= TERM_ANIS;
+  else if (!cub0) terms |= TERM_ANIS | FLAG_CUBIC;
   const bool wb0 = e->wb[0] == 0 && e->wb[1] == 0 && e->wb[2] == 0;
   if (!(wb0 && vector_zero(d->bias_magnetic_field))) terms |= TERM_EXT;
   if (!vector_zero(d->bias_magnetic_field)) terms |= FLAG_MAGNET_BIAS;
@@ -609,10 +619,11 @@ mpx_status load_params(mpx_engine* e, Magnet* m, const mpx_magnet_desc* d) {
   for (int c = 0; c < 3; ++c) D.wb[c] = (float)e->wb[c];
   // fast path: every parameter uniform, no geometry, no regions
   bool uniform = !d->geometry && !d->regions;
-  for (const mpx_scalar* s : {&d->msat, &d->aex, &d->alpha, &d->ku1, &d->ku2, &d->frozen_spins})
+  for (const mpx_scalar* s : {&d->msat, &d->aex, &d->alpha, &d->ku1, &d->ku2, &d->frozen_spins, &d->kc1, &d->kc2,
+                               &d->kc3})
     uniform = uniform && !s->cells;
   for (int c = 0; c < 9; ++c) uniform = uniform && !d->dmi[c].cells;
-  uniform = uniform && !d->anis_u.cells && !d->bias_magnetic_field.cells;
+  uniform = uniform && !d->anis_u.cells && !d->bias_magnetic_field.cells && !d->anis_c1.cells && !d->anis_c2.cells;
   D.fast = uniform ? 1 : 0;
   if (uniform) {
     const float a = D.aex.u, ms = D.msat.u;
@@ -630,6 +641,24 @@ mpx_status load_params(mpx_engine* e, Magnet* m, const mpx_magnet_desc* d) {
     D.fu[1] = s * uy;
     D.fu[2] = s * uz;
     for (int c = 0; c < 3; ++c) D.fb[c] = (terms & FLAG_MAGNET_BIAS) ? D.wb[c] + D.bias.u[c] : D.wb[c];
+    // cubic axes: normalised c1, c2 and c3 = c1 x c2 (not renormalised), as the reference kernel
+    float c1[3], c2[3];
+    for (int k = 0; k < 2; ++k) {
+      const float* u = k == 0 ? D.anisC1.u : D.anisC2.u;
+      const float n = std::sqrt(u[0] * u[0] + u[1] * u[1] + u[2] * u[2]);
+      const float sc = (n == 0.0f) ? 0.0f : 1.0f / n;
+      float* o = k == 0 ? c1 : c2;
+      for (int c = 0; c < 3; ++c) o[c] = sc * u[c];
+    }
+    const float c3[3] = {c1[1] * c2[2] - c1[2] * c2[1], c1[2] * c2[0] - c1[0] * c2[2], c1[0] * c2[1] - c1[1] * c2[0]};
+    for (int c = 0; c < 3; ++c) {
+      D.fc[0][c] = c1[c];
+      D.fc[1][c] = c2[c];
+      D.fc[2][c] = c3[c];
+    }
+    D.fkc[0] = D.kc1.u;
+    D.fkc[1] = D.kc2.u;
+    D.fkc[2] = D.kc3.u;
   }
   return MPX_OK;
 }
@@ -1263,8 +1292,11 @@ mpx_status mpx_magnet_bytes(const mpx_magnet_desc* d, int64_t* resident, int64_t
   MPX_TRY(validate_desc(d));
   const int64_t N = (int64_t)d->size[0] * d->size[1] * d->size[2];
   int64_t res = 4 * 9 * 3 * N;  // state, stage and scratch buffers (setup_magnet)
-  for (const mpx_scalar* sc : {&d->msat, &d->aex, &d->alpha, &d->ku1, &d->ku2, &d->frozen_spins})
+  for (const mpx_scalar* sc : {&d->msat, &d->aex, &d->alpha, &d->ku1, &d->ku2, &d->frozen_spins, &d->kc1, &d->kc2,
+                                &d->kc3})
     if (sc->cells) res += 4 * N;
+  if (d->anis_c1.cells) res += 12 * N;
+  if (d->anis_c2.cells) res += 12 * N;
   for (int c = 0; c < 9; ++c)
     if (d->dmi[c].cells) res += 4 * N;
   if (d->anis_u.cells) res += 12 * N;

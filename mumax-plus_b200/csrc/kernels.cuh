@@ -504,7 +504,10 @@ __device__ __forceinline__ void epilogue_cell(const MagnetDev& M, const GroupDev
     case 12:
     case 15: {
       float ea_ = 0.f;
-      if ((M.terms & TERM_ANIS) && ms != 0.0f) {  // physics/anisotropy.cu:142-173
+      if ((M.terms & TERM_ANIS) && (M.terms & FLAG_CUBIC) && ms != 0.0f) {  // physics/anisotropy.cu:185-215
+        const float3 c1 = normalized3(M.anisC1.at(i, N)), c2 = normalized3(M.anisC2.at(i, N));
+        ea_ = cubic_energy(mc, c1, c2, cross3(c1, c2), M.kc1.at(i), M.kc2.at(i), M.kc3.at(i));
+      } else if ((M.terms & TERM_ANIS) && ms != 0.0f) {  // physics/anisotropy.cu:142-173
         float3 u = M.anisU.at(i, N);
         const float nu = sqrtf(dot3(u, u));
         u = ((nu == 0.0f) ? 0.0f : 1.0f / nu) * u;

@@ -26,7 +26,8 @@ constexpr double MU0_D = 1.25663706212e-6; // H/m
 // as the reference's *AssuredZero checks do).
 enum : unsigned {
   TERM_EXCH = 1u, TERM_DMI = 2u, TERM_ANIS = 4u, TERM_EXT = 8u, TERM_DEMAG = 16u,
-  FLAG_OPENBC = 256u, FLAG_MAGNET_BIAS = 512u
+  FLAG_OPENBC = 256u, FLAG_MAGNET_BIAS = 512u,
+  FLAG_CUBIC = 1024u  // the anisotropy term is cubic (uniaxial otherwise)
 };
 
 struct DScalar {  // uniform value or per-cell array
@@ -55,6 +56,8 @@ struct MagnetDev {
   const unsigned* __restrict__ reg;        // NULL: region 0
   DScalar msat, aex, alpha, ku1, ku2, frozen;
   DVector anisU, bias;
+  DScalar kc1, kc2, kc3;  // cubic anisotropy constants
+  DVector anisC1, anisC2; // cubic anisotropy axes
   DScalar dmi[9];  // xxy, xxz, xyz, yxy, yxz, yyz, zxy, zxz, zyz
   float inter_u, scale_u;
   const float* __restrict__ inter_lut;
@@ -76,6 +79,8 @@ struct MagnetDev {
   float fu[3];       // normalised uniaxial axis
   float fb[3];       // world bias + magnet bias
   float fa, finv_2a, finv_ms, fk1, fk2;
+  float fc[3][3];    // cubic axes c1, c2 (normalised) and c3 = c1 x c2
+  float fkc[3];      // cubic constants kc1, kc2, kc3
 };
 
 // Solve-group state (time integration); lives in a device array.
@@ -163,6 +168,37 @@ __device__ __forceinline__ float lut_value(const float* __restrict__ lut, float 
 // The local terms of the effective field of cell (x, y, z) = i, which is in the
 // geometry with msat != 0.  `mask` selects terms (TERM_*).  Each term is
 // computed on its own, then added in the reference's order.
+// a / |a|, or 0 for a zero vector (core/datatypes.hpp normalized)
+__device__ __forceinline__ float3 normalized3(float3 a) {
+  const float n = sqrtf(dot3(a, a));
+  const float s = (n == 0.0f) ? 0.0f : 1.0f / n;
+  return f3(s * a.x, s * a.y, s * a.z);
+}
+
+// physics/anisotropy.cu:57-106 (k_cubicanisotropyField): cubic anisotropy field of
+// axes c1, c2, c3 = c1 x c2 and constants kc1..kc3, times 1/Ms.
+__device__ __forceinline__ float3 cubic_field(float3 m, float3 c1, float3 c2, float3 c3, float kc1, float kc2,
+                                              float kc3, float inv_ms) {
+  const float a = dot3(c1, m), b = dot3(c2, m), c = dot3(c3, m);
+  const float a2 = a * a, b2 = b * b, c2_ = c * c;
+  const float f1 = -2 * kc1 * (b2 + c2_) * a - 2 * kc2 * (b2 * c2_) * a - 4 * kc3 * (b2 * b2 + c2_ * c2_) * (a2 * a);
+  const float f2 = -2 * kc1 * (a2 + c2_) * b - 2 * kc2 * (a2 * c2_) * b - 4 * kc3 * (a2 * a2 + c2_ * c2_) * (b2 * b);
+  const float f3_ = -2 * kc1 * (a2 + b2) * c - 2 * kc2 * (a2 * b2) * c - 4 * kc3 * (a2 * a2 + b2 * b2) * (c2_ * c);
+  return f3(inv_ms * (f1 * c1.x + f2 * c2.x + f3_ * c3.x), inv_ms * (f1 * c1.y + f2 * c2.y + f3_ * c3.y),
+            inv_ms * (f1 * c1.z + f2 * c2.z + f3_ * c3.z));
+}
+
+// physics/anisotropy.cu:185-215 (k_cubanisotropyEnergyDensity)
+__device__ __forceinline__ float cubic_energy(float3 m, float3 c1, float3 c2, float3 c3, float kc1, float kc2,
+                                              float kc3) {
+  const float a = dot3(c1, m), b = dot3(c2, m), c = dot3(c3, m);
+  const float a2 = a * a, b2 = b * b, c2_ = c * c;
+  float e = kc1 * (a2 * b2 + a2 * c2_ + b2 * c2_);
+  e += kc2 * a2 * b2 * c2_;
+  e += kc3 * (a2 * a2 * b2 * b2 + a2 * a2 * c2_ * c2_ + b2 * b2 * c2_ * c2_);
+  return e;
+}
+
 struct LocalOut {
   float3 exch, anis, ext, dmi;
 };
@@ -264,7 +300,10 @@ __device__ __forceinline__ LocalOut local_terms(const MagnetDev& M, const float*
     if (do_exch) o.exch = inv_ms * he;
     if (do_dmi) o.dmi = inv_ms * hd;
   }
-  if ((mask & TERM_ANIS) && (M.terms & TERM_ANIS)) {  // physics/anisotropy.cu:45-54
+  if ((mask & TERM_ANIS) && (M.terms & TERM_ANIS) && (M.terms & FLAG_CUBIC)) {  // physics/anisotropy.cu:57-106
+    const float3 c1 = normalized3(M.anisC1.at(i, N)), c2 = normalized3(M.anisC2.at(i, N));
+    o.anis = cubic_field(mc, c1, c2, cross3(c1, c2), M.kc1.at(i), M.kc2.at(i), M.kc3.at(i), inv_ms);
+  } else if ((mask & TERM_ANIS) && (M.terms & TERM_ANIS)) {  // physics/anisotropy.cu:45-54
     float3 u = M.anisU.at(i, N);
     const float nu = sqrtf(dot3(u, u));
     const float s = (nu == 0.0f) ? 0.0f : 1.0f / nu;
@@ -341,7 +380,10 @@ __device__ __forceinline__ LocalOut local_terms_fast(const MagnetDev& M, const f
     if (do_exch) o.exch = M.finv_ms * he;
     if (do_dmi) o.dmi = M.finv_ms * hd;
   }
-  if (M.terms & TERM_ANIS) {
+  if ((M.terms & TERM_ANIS) && (M.terms & FLAG_CUBIC)) {
+    o.anis = cubic_field(mc, f3(M.fc[0][0], M.fc[0][1], M.fc[0][2]), f3(M.fc[1][0], M.fc[1][1], M.fc[1][2]),
+                         f3(M.fc[2][0], M.fc[2][1], M.fc[2][2]), M.fkc[0], M.fkc[1], M.fkc[2], M.finv_ms);
+  } else if (M.terms & TERM_ANIS) {
     const float3 u = f3(M.fu[0], M.fu[1], M.fu[2]);
     const float mu = dot3(mc, u);
     o.anis = M.finv_ms * ((2 * M.fk1 * mu + 4 * M.fk2 * mu * mu * mu) * u);

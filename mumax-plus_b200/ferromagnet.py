@@ -3,8 +3,8 @@
 The parameter bag follows physics/ferromagnet.cpp:18-60 (defaults msat = 1,
 everything else 0, scale_exchange = 1, demag on, open boundaries off).  Every
 quantity is evaluated by the CUDA engine; parameters of terms outside the
-accelerated path (cubic anisotropy, spin-transfer torque, temperature,
-magnetoelastics, ...) raise NotImplementedError when set to non-zero values.
+accelerated path (spin-transfer torque, temperature, magnetoelastics, ...)
+raise NotImplementedError when set to non-zero values.
 """
 import ctypes as C
 import warnings
@@ -59,13 +59,18 @@ class Ferromagnet:
         self._anisU = Parameter(self, "anisU", "", 3, (0.0, 0.0, 0.0), ch)
         self._bias = Parameter(self, "bias_magnetic_field", "T", 3, (0.0, 0.0, 0.0), ch)
         self._frozen = Parameter(self, "frozen_spins", "", 1, 0.0, ch)
+        self._kc1 = Parameter(self, "kc1", "J/m3", 1, 0.0, ch)
+        self._kc2 = Parameter(self, "kc2", "J/m3", 1, 0.0, ch)
+        self._kc3 = Parameter(self, "kc3", "J/m3", 1, 0.0, ch)
+        self._anisC1 = Parameter(self, "anisC1", "", 3, (0.0, 0.0, 0.0), ch)
+        self._anisC2 = Parameter(self, "anisC2", "", 3, (0.0, 0.0, 0.0), ch)
         self._dmi = DmiTensor(self, ch)
         self._inter_exchange = InterParameter(self, "inter_exchange", "J/m", 0.0, ch)
         self._scale_exchange = InterParameter(self, "scale_exchange", "", 1.0, ch)
         self._enable_demag = True
         self._enable_openbc = False
         self._unsupported = {}
-        for n, nc in (("kc1", 1), ("kc2", 1), ("kc3", 1), ("anisC1", 3), ("anisC2", 3), ("temperature", 1),
+        for n, nc in (("temperature", 1),
                       ("xi", 1), ("Lambda", 1), ("pol", 1), ("epsilon_prime", 1), ("jcur", 3),
                       ("fixed_layer", 3), ("B1", 1), ("B2", 1), ("conductivity", 1), ("amr_ratio", 1)):
             self._unsupported[n] = _Unsupported(self, n, "", nc, (0.0, 0.0, 0.0) if nc == 3 else 0.0)
@@ -122,6 +127,11 @@ class Ferromagnet:
         d.frozen_spins = self._frozen._scalar(keep)
         d.anis_u = self._anisU._vector(keep)
         d.bias_magnetic_field = self._bias._vector(keep)
+        d.kc1 = self._kc1._scalar(keep)
+        d.kc2 = self._kc2._scalar(keep)
+        d.kc3 = self._kc3._scalar(keep)
+        d.anis_c1 = self._anisC1._vector(keep)
+        d.anis_c2 = self._anisC2._vector(keep)
         for i, p in enumerate(self._dmi._list()):
             d.dmi[i] = p._scalar(keep)
         li, ls = self._inter_exchange._lut(), self._scale_exchange._lut()
@@ -248,6 +258,11 @@ class Ferromagnet:
     ku1 = _param_prop("_ku1")
     ku2 = _param_prop("_ku2")
     anisU = _param_prop("_anisU")
+    kc1 = _param_prop("_kc1")
+    kc2 = _param_prop("_kc2")
+    kc3 = _param_prop("_kc3")
+    anisC1 = _param_prop("_anisC1")
+    anisC2 = _param_prop("_anisC2")
     bias_magnetic_field = _param_prop("_bias")
     frozen_spins = _param_prop("_frozen")
 
@@ -419,6 +434,6 @@ def _unsupported_prop(name):
     return property(getter, setter)
 
 
-for _n in ("kc1", "kc2", "kc3", "anisC1", "anisC2", "temperature", "xi", "Lambda", "pol", "epsilon_prime",
+for _n in ("temperature", "xi", "Lambda", "pol", "epsilon_prime",
            "jcur", "fixed_layer", "B1", "B2", "conductivity", "amr_ratio"):
     setattr(Ferromagnet, _n, _unsupported_prop(_n))

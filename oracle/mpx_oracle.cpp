@@ -273,6 +273,8 @@ struct Magnet {
   std::vector<uint32_t> reg;
   Param msat, aex, alpha, ku1, ku2, frozen;
   VParam anisU, bias;
+  Param kc1, kc2, kc3;
+  VParam anisC1, anisC2;
   Param dmi[9];
   int lutn = 0;
   double inter_u = 0, scale_u = 1;
@@ -337,6 +339,11 @@ int load_magnet(Magnet& mg, const mpx_magnet_desc* d) {
   mg.frozen.load(d->frozen_spins, N);
   mg.anisU.load(d->anis_u, N);
   mg.bias.load(d->bias_magnetic_field, N);
+  mg.kc1.load(d->kc1, N);
+  mg.kc2.load(d->kc2, N);
+  mg.kc3.load(d->kc3, N);
+  mg.anisC1.load(d->anis_c1, N);
+  mg.anisC2.load(d->anis_c2, N);
   for (int c = 0; c < 9; ++c) mg.dmi[c].load(d->dmi[c], N);
   mg.lutn = d->lut_regions;
   int L = mg.lutn * (mg.lutn - 1) / 2;
@@ -384,9 +391,14 @@ bool dmi_zero(const Magnet& mg) {  // physics/dmi.cu:12-17
     if (!mg.dmi[c].zero()) return false;
   return true;
 }
-bool anis_zero(const Magnet& mg) {  // physics/anisotropy.cu:9-12 (uniaxial)
+bool uni_zero(const Magnet& mg) {  // physics/anisotropy.cu:9-12
   return (mg.ku1.zero() && mg.ku2.zero()) || mg.anisU.zero() || mg.msat.zero();
 }
+bool cubic_zero(const Magnet& mg) {  // physics/anisotropy.cu:14-18
+  return (mg.kc1.zero() && mg.kc2.zero() && mg.kc3.zero()) || (mg.anisC1.zero() && mg.anisC2.zero()) ||
+         mg.msat.zero();
+}
+bool anis_zero(const Magnet& mg) { return uni_zero(mg) && cubic_zero(mg); }  // :20-23
 bool external_zero(const Magnet& mg, const double wb[3]) {  // physics/zeeman.cu:37-51
   return wb[0] == 0 && wb[1] == 0 && wb[2] == 0 && mg.bias.zero();
 }
@@ -498,8 +510,23 @@ void anisotropy_field(const Magnet& mg, std::vector<double>& h) {
   const int N = mg.N;
   h.assign(3 * (size_t)N, 0.0);
   if (anis_zero(mg)) return;
+  const bool cubic = uni_zero(mg);  // uniaxial takes precedence (physics/anisotropy.cu:121-138)
   for (int i = 0; i < N; ++i) {
     if (!mg.in_geom(i) || mg.msat.at(i) == 0) continue;
+    if (cubic) {  // physics/anisotropy.cu:57-106
+      V3 c1 = normalized(mg.anisC1.at(i)), c2 = normalized(mg.anisC2.at(i)), c3 = cross(c1, c2), m = mg.mv(i);
+      double k1 = mg.kc1.at(i), k2 = mg.kc2.at(i), k3 = mg.kc3.at(i), Ms = mg.msat.at(i);
+      double a = dot(c1, m), b = dot(c2, m), c = dot(c3, m);
+      V3 hh = (-2 * k1 / Ms) * ((b * b + c * c) * a * c1 + (a * a + c * c) * b * c2 + (a * a + b * b) * c * c3) +
+              (-2 * k2 / Ms) * ((b * b * c * c) * a * c1 + (a * a * c * c) * b * c2 + (a * a * b * b) * c * c3) +
+              (-4 * k3 / Ms) * ((std::pow(b, 4) + std::pow(c, 4)) * std::pow(a, 3) * c1 +
+                                (std::pow(a, 4) + std::pow(c, 4)) * std::pow(b, 3) * c2 +
+                                (std::pow(a, 4) + std::pow(b, 4)) * std::pow(c, 3) * c3);
+      h[i] = hh.x;
+      h[(size_t)N + i] = hh.y;
+      h[2 * (size_t)N + i] = hh.z;
+      continue;
+    }
     V3 u = normalized(mg.anisU.at(i));
     V3 m = mg.mv(i);
     double k1 = mg.ku1.at(i), k2 = mg.ku2.at(i), Ms = mg.msat.at(i);
@@ -759,6 +786,13 @@ void energy_density(World& w, Magnet& mg, int q, std::vector<double>& e) {
       if (anis_zero(mg)) return;
       for (int i = 0; i < N; ++i) {
         if (!mg.in_geom(i) || mg.msat.at(i) == 0) continue;
+        if (uni_zero(mg)) {  // physics/anisotropy.cu:175-215 (cubic)
+          V3 c1 = normalized(mg.anisC1.at(i)), c2 = normalized(mg.anisC2.at(i)), c3 = cross(c1, c2), m = mg.mv(i);
+          double a2 = std::pow(dot(c1, m), 2), b2 = std::pow(dot(c2, m), 2), c2_ = std::pow(dot(c3, m), 2);
+          e[i] = mg.kc1.at(i) * (a2 * b2 + a2 * c2_ + b2 * c2_) + mg.kc2.at(i) * a2 * b2 * c2_ +
+                 mg.kc3.at(i) * (a2 * a2 * b2 * b2 + a2 * a2 * c2_ * c2_ + b2 * b2 * c2_ * c2_);
+          continue;
+        }
         V3 u = normalized(mg.anisU.at(i));
         double mu = dot(mg.mv(i), u), k1 = mg.ku1.at(i), k2 = mg.ku2.at(i);
         e[i] = -k1 * mu * mu - k2 * mu * mu * mu * mu;

@@ -28,6 +28,11 @@ class MagnetSpec:
     ku2: object = 0.0
     anisU: object = (0.0, 0.0, 0.0)
     bias: object = (0.0, 0.0, 0.0)
+    kc1: object = 0.0
+    kc2: object = 0.0
+    kc3: object = 0.0
+    anisC1: object = (0.0, 0.0, 0.0)
+    anisC2: object = (0.0, 0.0, 0.0)
     frozen: object = 0.0
     dmi: dict = field(default_factory=dict)
     inter_exchange: float = 0.0
@@ -99,6 +104,11 @@ class MagnetSpec:
         d.ku2 = self._scalar(self.ku2, keep)
         d.frozen_spins = self._scalar(self.frozen, keep)
         d.anis_u = self._vector(self.anisU, keep)
+        d.kc1 = self._scalar(self.kc1, keep)
+        d.kc2 = self._scalar(self.kc2, keep)
+        d.kc3 = self._scalar(self.kc3, keep)
+        d.anis_c1 = self._vector(self.anisC1, keep)
+        d.anis_c2 = self._vector(self.anisC2, keep)
         d.bias_magnetic_field = self._vector(self.bias, keep)
         for i, k in enumerate(abi.DMI_ORDER):
             d.dmi[i] = self._scalar(self.dmi.get(k, 0.0), keep)
@@ -145,6 +155,11 @@ class MagnetSpec:
         magnet.ku1 = self.ku1
         magnet.ku2 = self.ku2
         magnet.anisU = self.anisU
+        magnet.kc1 = self.kc1
+        magnet.kc2 = self.kc2
+        magnet.kc3 = self.kc3
+        magnet.anisC1 = self.anisC1
+        magnet.anisC2 = self.anisC2
         magnet.bias_magnetic_field = self.bias
         magnet.frozen_spins = self.frozen
         for k, v in self.dmi.items():

@@ -309,3 +309,23 @@ def test_nan_state_fails_cleanly(mpx):
     world.timesolver.timestep = 1e-13
     world.timesolver.run(1e-12)
     assert world.timesolver.time == pytest.approx(1e-12, rel=1e-9)
+
+
+@pytest.mark.parametrize("per_cell", [False, True])
+def test_cubic_anisotropy(mpx, per_cell):
+    """Cubic anisotropy field, energy density and torque (uniform parameters take
+    the specialised epilogue, per-cell ones the general one)."""
+    rng = np.random.default_rng(5)
+    shape = (2, 12, 20)
+    if per_cell:
+        c1 = rng.standard_normal((3, *shape)).astype(np.float32)
+        c2 = np.cross(c1, rng.standard_normal((3, *shape)), axis=0).astype(np.float32)
+        kc1 = rng.uniform(1e5, 5e6, shape).astype(np.float32)
+    else:
+        c1 = (1.0, 2.0, 0.5)
+        c2 = tuple(np.cross(c1, [0.3, -1.0, 2.0]))
+        kc1 = 4.1e6
+    s = MagnetSpec(size=(20, 12, 2), cellsize=(2e-9, 2e-9, 2e-9), msat=8e5, aex=1e-11, alpha=0.1, kc1=kc1,
+                   kc2=-2e5, kc3=3e4, anisC1=c1, anisC2=c2)
+    compare(s, mpx, [abi.Q_ANISOTROPY_FIELD, abi.Q_EFFECTIVE_FIELD, abi.Q_TORQUE, abi.Q_ANISOTROPY_ENERGY_DENSITY,
+                     abi.Q_TOTAL_ENERGY_DENSITY])

@@ -296,3 +296,46 @@ def test_oracle_relax_reaches_the_minimum_of_a_uniaxial_film(oracle):
     assert m[2] > 1 - 1e-6
     assert ow.time == 3e-12
     assert oracle.abi.RK_NAMES[ow.solver.method] == "DormandPrince"
+
+
+def _cubic_numpy(m, msat, kc, c1, c2):
+    """numpy restatement of the reference's cubic anisotropy field and energy
+    density (test/test_anisotropy.py:73-112, physics/anisotropy.cu:57-106)."""
+    c1 = c1 / np.linalg.norm(c1, axis=0)
+    c2 = c2 / np.linalg.norm(c2, axis=0)
+    c3 = np.cross(c1, c2, axis=0)
+    a, b, c = (np.sum(v * m, axis=0) for v in (c1, c2, c3))
+    k1, k2, k3 = kc
+    h = -2 / msat * (k1 * ((b**2 + c**2) * a * c1 + (a**2 + c**2) * b * c2 + (a**2 + b**2) * c * c3)
+                     + k2 * (b**2 * c**2 * a * c1 + a**2 * c**2 * b * c2 + a**2 * b**2 * c * c3)
+                     + 2 * k3 * ((b**4 + c**4) * a**3 * c1 + (a**4 + c**4) * b**3 * c2 + (a**4 + b**4) * c**3 * c3))
+    e = (k1 * (a**2 * b**2 + a**2 * c**2 + b**2 * c**2) + k2 * a**2 * b**2 * c**2
+         + k3 * (a**4 * b**4 + a**4 * c**4 + b**4 * c**4))
+    return h, e
+
+
+@pytest.mark.parametrize("per_cell", [False, True])
+def test_oracle_cubic_anisotropy_vs_numpy(oracle, per_cell):
+    rng = np.random.default_rng(21)
+    shape = (2, 5, 6)
+    m = random_m(shape, seed=3, smooth=0).astype(np.float64)
+    if per_cell:
+        c1 = rng.standard_normal((3, *shape)).astype(np.float32)
+        c2 = np.cross(c1, rng.standard_normal((3, *shape)), axis=0).astype(np.float32)
+        kc1 = rng.uniform(1e5, 5e6, shape).astype(np.float32)
+        c1v, c2v, kc1v = c1, c2, kc1
+    else:
+        c1 = np.array([1.0, 2.0, 0.5], np.float32)
+        c2 = np.cross(c1, [0.3, -1.0, 2.0]).astype(np.float32)
+        c1v = np.broadcast_to(c1[:, None, None, None], (3, *shape)).astype(np.float64)
+        c2v = np.broadcast_to(c2[:, None, None, None], (3, *shape)).astype(np.float64)
+        kc1 = kc1v = 4.1e6
+        c1, c2 = tuple(c1), tuple(c2)
+    s = MagnetSpec(size=(6, 5, 2), msat=8e5, kc1=kc1, kc2=-2e5, kc3=3e4, anisC1=c1, anisC2=c2, enable_demag=False)
+    ow, q = s.oracle_world(m.astype(np.float32))
+    mm = ow.get_m(q)
+    h, e = _cubic_numpy(mm, 8e5, (np.asarray(kc1v, np.float64), -2e5, 3e4), np.asarray(c1v, np.float64),
+                        np.asarray(c2v, np.float64))
+    np.testing.assert_allclose(ow.eval(q, oracle.abi.Q_ANISOTROPY_FIELD), h, rtol=1e-9, atol=1e-12 * np.abs(h).max())
+    np.testing.assert_allclose(ow.eval(q, oracle.abi.Q_ANISOTROPY_ENERGY_DENSITY)[0], e, rtol=1e-9,
+                               atol=1e-9 * np.abs(e).max())

@@ -144,6 +144,11 @@ typedef struct {
    * term is assured zero, as in the reference */
   mpx_scalar kc1, kc2, kc3;     /* J/m^3                                        */
   mpx_vector anis_c1, anis_c2;  /* cubic axes (normalised per cell; c3 = c1 x c2) */
+  /* stray fields between the magnets of one group (physics/zeeman.cu:70-88):
+   * Magnet::enableAsStrayFieldSource / Destination, inverted so that the
+   * zero default keeps both on */
+  int stray_source_off;
+  int stray_destination_off;
 } mpx_magnet_desc;
 
 /* Time-solver settings (core/timesolver.hpp:74-82 defaults in brackets). */

@@ -91,6 +91,8 @@ class MagnetDesc(C.Structure):
         ("kc3", Scalar),
         ("anis_c1", Vector),
         ("anis_c2", Vector),
+        ("stray_source_off", C.c_int),
+        ("stray_destination_off", C.c_int),
     ]
 
 

@@ -21,6 +21,7 @@
 #include "../../include/mpx.h"
 #include "kernels.cuh"
 #include "newell.cuh"
+#include "stray.cuh"
 
 using namespace mpx;
 
@@ -130,6 +131,12 @@ TableauDev make_tableau(int method) {
 struct Magnet {
   int slot = -1, group = -1;
   MagnetDev dev;
+  unsigned terms_base = 0;        // TERM_* / FLAG_* from the parameters, before stray fields
+  bool msat_zero = false;
+  bool stray_src = true, stray_dst = true;
+  int pbc_rep[3] = {0, 0, 0};
+  double cs_d[3] = {1, 1, 1};
+  float* hstray = nullptr;        // stray field of the other magnets (3N floats), when a destination
   std::vector<void*> allocs;  // per-magnet device allocations (params, masks, buffers...)
   int64_t bytes = 0;
   bool demag = false;
@@ -195,6 +202,14 @@ struct mpx_engine {
   int64_t launches = 0;
   double wb[3] = {0, 0, 0};
   int tab_method = -1;
+  // stray-field pairs (source -> destination magnet of one group)
+  struct Pair {
+    int src, dst;
+    float* k;
+    StrayTable tab;
+  };
+  std::vector<Pair> pairs;
+  bool pairs_dirty = true;
   // CUDA graphs of one attempt: every stage, and (FSAL methods) without
   // stage 0, whose torque k0 is the last stage of the previous step
   cudaGraphExec_t graph = nullptr, graph_nok0 = nullptr;
@@ -259,6 +274,9 @@ void free_magnet(mpx_engine* e, Magnet* m) {
 // Frees every device allocation of a magnet.
 void release_all(mpx_engine* e, Magnet* m) {
   free_magnet(e, m);
+  pfree(e, m->hstray);
+  m->hstray = nullptr;
+  e->pairs_dirty = true;
   pfree(e, m->fields);
   pfree(e, m->spec);
   pfree(e, m->kspec);
@@ -433,6 +451,83 @@ mpx_status rebuild_tables(mpx_engine* e) {
   e->n_t_local = (int)tl.size();
   e->tables_dirty = false;
   e->graph_dirty = true;
+  return MPX_OK;
+}
+
+// Stray-field pairs: every ordered pair (A, B) of distinct magnets of one group
+// with A an enabled source (msat not zero) and B an enabled destination gets
+// the FP32 table of the Newell tensor (built in FP64, PBC images included) of
+// their displacements; B gets a stray-field buffer and FLAG_STRAY.
+mpx_status rebuild_pairs(mpx_engine* e) {
+  for (auto& p : e->pairs) pfree(e, p.k);
+  e->pairs.clear();
+  std::vector<bool> is_dst(e->mags.size(), false);
+  for (auto& gp : e->groups) {
+    if (!gp) continue;
+    for (int b : gp->magnets)
+      for (int a : gp->magnets) {
+        if (a == b) continue;
+        Magnet* A = get_mag(e, a);
+        Magnet* B = get_mag(e, b);
+        if (!A->stray_src || A->msat_zero || !B->stray_dst) continue;
+        mpx_engine::Pair p;
+        p.src = a;
+        p.dst = b;
+        KernelGeom g;
+        for (int ax = 0; ax < 3; ++ax) {
+          p.tab.K[ax] = A->dev.n[ax] + B->dev.n[ax] - 1;
+          p.tab.O[ax] = B->dev.o[ax] - A->dev.o[ax] - (A->dev.n[ax] - 1);
+          g.n[ax] = B->dev.n[ax];
+          g.mg[ax] = B->dev.mg[ax];
+          g.pbc[ax] = B->pbc_rep[ax];
+          g.cs[ax] = B->cs_d[ax];
+        }
+        const size_t KK = (size_t)p.tab.K[0] * p.tab.K[1] * p.tab.K[2];
+        MPX_TRY(palloc(e, (void**)&p.k, sizeof(float) * 6 * KK));
+        k_newell_reflayout<<<148 * 8, 128, 0, e->stream>>>(p.k, g, p.tab.K[0], p.tab.K[1], p.tab.K[2], p.tab.O[0],
+                                                           p.tab.O[1], p.tab.O[2]);
+        e->launches++;
+        p.tab.k = p.k;
+        e->pairs.push_back(p);
+        is_dst[b] = true;
+      }
+  }
+  for (size_t i = 0; i < e->mags.size(); ++i) {
+    Magnet* m = e->mags[i].get();
+    if (!m) continue;
+    unsigned terms = m->terms_base;
+    if (is_dst[i]) {
+      if (!m->hstray) MPX_TRY(palloc(e, (void**)&m->hstray, sizeof(float) * 3 * (size_t)m->dev.N));
+      terms |= TERM_EXT | FLAG_STRAY;
+    } else if (m->hstray) {
+      pfree(e, m->hstray);
+      m->hstray = nullptr;
+    }
+    if (terms != m->dev.terms || m->dev.hstray != m->hstray) {
+      m->dev.terms = terms;
+      m->dev.hstray = m->hstray;
+      MPX_TRY(upload_magnet_desc(e, m));
+    }
+  }
+  e->pairs_dirty = false;
+  e->graph_dirty = true;
+  const cudaError_t ce = cudaGetLastError();
+  if (ce != cudaSuccess) return fail(MPX_ERR_CUDA, std::string("stray-field tables: ") + cudaGetErrorString(ce));
+  return MPX_OK;
+}
+
+// Stray fields of the sources of `dst` (all destinations when dst < 0) for `stage`.
+mpx_status launch_pairs(mpx_engine* e, int dst, int stage, int gate) {
+  std::vector<int> seen;
+  for (const auto& p : e->pairs) {
+    if (dst >= 0 && p.dst != dst) continue;
+    const bool add = std::find(seen.begin(), seen.end(), p.dst) != seen.end();
+    if (!add) seen.push_back(p.dst);
+    Magnet* B = get_mag(e, p.dst);
+    k_stray_pair<<<(B->dev.N + 255) / 256, 256, 0, e->stream>>>(e->d_mags, e->d_groups, p.src, p.dst, p.tab, stage,
+                                                                gate, add ? 1 : 0, B->hstray);
+    e->launches++;
+  }
   return MPX_OK;
 }
 
@@ -616,6 +711,11 @@ mpx_status load_params(mpx_engine* e, Magnet* m, const mpx_magnet_desc* d) {
   if (d->enable_demag && !msat0) terms |= TERM_DEMAG;
   if (d->enable_openbc) terms |= FLAG_OPENBC;
   D.terms = terms;
+  m->terms_base = terms;
+  m->msat_zero = msat0;
+  m->stray_src = !d->stray_source_off;
+  m->stray_dst = !d->stray_destination_off;
+  e->pairs_dirty = true;
   for (int c = 0; c < 3; ++c) D.wb[c] = (float)e->wb[c];
   // fast path: every parameter uniform, no geometry, no regions
   bool uniform = !d->geometry && !d->regions;
@@ -701,6 +801,8 @@ mpx_status setup_magnet(mpx_engine* e, Magnet* m, const mpx_magnet_desc* d, bool
     D.mg[a] = d->mastergrid_size[a];
     D.mgo[a] = d->mastergrid_origin[a];
     D.cs[a] = (float)d->cellsize[a];
+    m->pbc_rep[a] = d->pbc_repetitions[a];
+    m->cs_d[a] = d->cellsize[a];
     const float c = (float)d->cellsize[a];
     D.w[a] = 1.0f / (c * c);
     D.inv_cs[a] = 1.0f / c;
@@ -803,6 +905,7 @@ mpx_status check_launch(mpx_engine* e, const char* what) {
 // --------------------------------------------------- field evaluation
 // Evaluate quantity q of magnet m into the device buffer out.
 mpx_status eval_into(mpx_engine* e, Magnet* m, int q, float* out) {
+  if (e->pairs_dirty) MPX_TRY(rebuild_pairs(e));
   if (e->tables_dirty) MPX_TRY(rebuild_tables(e));
   const int N = m->dev.N;
   if (q == MPX_Q_MAGNETIZATION) {
@@ -824,6 +927,7 @@ mpx_status eval_into(mpx_engine* e, Magnet* m, int q, float* out) {
                             q == MPX_Q_LLG_TORQUE || q == MPX_Q_DAMPING_TORQUE || q == MPX_Q_DEMAG_ENERGY_DENSITY ||
                             q == MPX_Q_TOTAL_ENERGY_DENSITY);
   const int ntile = (int)m->tiles.size();
+  if (m->hstray) MPX_TRY(launch_pairs(e, m->slot, 0, 0));  // stray fields of the other magnets' states
   if (m->demag && needs_demag) {
     const int sx = x_smem(m), syz = yz_smem(m), nt = x_threads(m);
     k_xfwd<false><<<ntile, nt, sx, e->stream>>>(e->d_mags, e->d_groups, m->d_tiles, 0, 0, nullptr, e->d_tw);
@@ -849,6 +953,7 @@ mpx_status launch_attempt(mpx_engine* e, const TableauDev& T, int first_stage) {
     ea.gate = 1;
     ea.out = nullptr;
     ea.msrc = nullptr;
+    // stage states: combination fused into the x-forward pass, or k_combine
     if (e->n_t_demag > 0) {
       if (s == 0)
         k_xfwd<false><<<e->n_t_demag, e->nt_x, e->smem_x, e->stream>>>(e->d_mags, e->d_groups, e->d_t_demag, 0, 1,
@@ -856,16 +961,21 @@ mpx_status launch_attempt(mpx_engine* e, const TableauDev& T, int first_stage) {
       else
         k_xfwd<true><<<e->n_t_demag, e->nt_x, e->smem_x, e->stream>>>(e->d_mags, e->d_groups, e->d_t_demag, s, 1,
                                                                       nullptr, e->d_tw);
+      e->launches++;
+    }
+    if (e->n_t_local > 0 && s > 0) {
+      k_combine<<<e->n_t_local, 256, 0, e->stream>>>(e->d_mags, e->d_groups, e->d_t_local, s, 0);
+      e->launches++;
+    }
+    // stray fields of the stage states of the other magnets
+    MPX_TRY(launch_pairs(e, -1, s, 1));
+    if (e->n_t_demag > 0) {
       for (int c = 0; c < 5; ++c)
         MPX_TRY(launch_yz(e, c, e->d_kx_demag[c], e->n_kx_demag[c], e->smem_yz[c], s, 1, e->maxpy_yz[c]));
       k_xinv<<<e->n_t_demag, e->nt_x, e->smem_x, e->stream>>>(e->d_mags, e->d_groups, e->d_t_demag, ea, e->d_tw);
-      e->launches += 2;
+      e->launches++;
     }
     if (e->n_t_local > 0) {
-      if (s > 0) {
-        k_combine<<<e->n_t_local, 256, 0, e->stream>>>(e->d_mags, e->d_groups, e->d_t_local, s, 0);
-        e->launches++;
-      }
       k_local<<<e->n_t_local, 256, 0, e->stream>>>(e->d_mags, e->d_groups, e->d_t_local, ea);
       e->launches++;
     }
@@ -887,6 +997,7 @@ mpx_status launch_attempt(mpx_engine* e, const TableauDev& T, int first_stage) {
 }
 
 mpx_status prepare_run(mpx_engine* e, int method) {
+  if (e->pairs_dirty) MPX_TRY(rebuild_pairs(e));
   if (e->tables_dirty) MPX_TRY(rebuild_tables(e));
   MPX_TRY(upload_tableau(e, method));
   return MPX_OK;
@@ -920,7 +1031,7 @@ int attempt_launches(const mpx_engine* e, const TableauDev& T, int first_stage) 
   const int S = T.S, ns = S - first_stage;
   int nyz = 0;
   for (int c = 0; c < 5; ++c) nyz += e->n_kx_demag[c] > 0 ? 1 : 0;
-  int per = 1;  // controller
+  int per = 1 + (int)e->pairs.size() * ns;  // controller, stray-field pairs
   if (e->n_t_demag > 0) per += (2 + nyz) * ns + (T.fsal ? 0 : 1);
   if (e->n_t_local > 0) per += ns + (ns - (first_stage == 0 ? 1 : 0)) + (T.fsal ? 0 : 1);
   return per;
@@ -1139,9 +1250,11 @@ mpx_status mpx_engine_set_world_bias(mpx_engine* e, const double b[3]) {
     if (!mp) continue;
     Magnet* m = mp.get();
     for (int c = 0; c < 3; ++c) m->dev.wb[c] = (float)b[c];
-    const bool mb = (m->dev.terms & FLAG_MAGNET_BIAS) != 0;
-    if (wb0 && !mb) m->dev.terms &= ~TERM_EXT;
-    else m->dev.terms |= TERM_EXT;
+    const bool mb = (m->terms_base & FLAG_MAGNET_BIAS) != 0;
+    if (wb0 && !mb) m->terms_base &= ~TERM_EXT;
+    else m->terms_base |= TERM_EXT;
+    // stray fields keep the external term on
+    m->dev.terms = m->terms_base | (m->hstray ? (TERM_EXT | FLAG_STRAY) : 0u);
     for (int c = 0; c < 3; ++c) m->dev.fb[c] = mb ? m->dev.wb[c] + m->dev.bias.u[c] : m->dev.wb[c];
     MPX_TRY(upload_magnet_desc(e, m));
   }

@@ -27,7 +27,8 @@ constexpr double MU0_D = 1.25663706212e-6; // H/m
 enum : unsigned {
   TERM_EXCH = 1u, TERM_DMI = 2u, TERM_ANIS = 4u, TERM_EXT = 8u, TERM_DEMAG = 16u,
   FLAG_OPENBC = 256u, FLAG_MAGNET_BIAS = 512u,
-  FLAG_CUBIC = 1024u  // the anisotropy term is cubic (uniaxial otherwise)
+  FLAG_CUBIC = 1024u,  // the anisotropy term is cubic (uniaxial otherwise)
+  FLAG_STRAY = 2048u   // stray fields of other magnets in `hstray`
 };
 
 struct DScalar {  // uniform value or per-cell array
@@ -71,6 +72,7 @@ struct MagnetDev {
   float2* spec;      // spectrum S[kx][c][z][y]
   const float* __restrict__ kspec;  // kernel spectrum [kx][kz'][kcomp][ky']
   float* buf[9];     // field buffers (3N floats each); roles given by the group map
+  const float* hstray;  // stray field of the other magnets of the world (3N), or NULL
   // Fast path: every parameter uniform, no geometry, no regions.  Set on the
   // host together with the precomputed uniform values below.
   int fast;
@@ -315,6 +317,7 @@ __device__ __forceinline__ LocalOut local_terms(const MagnetDev& M, const float*
   if ((mask & TERM_EXT) && (M.terms & TERM_EXT)) {  // physics/zeeman.cu:64-68
     float3 b = f3(M.wb[0], M.wb[1], M.wb[2]);
     if (M.terms & FLAG_MAGNET_BIAS) b = b + M.bias.at(i, N);
+    if (M.terms & FLAG_STRAY) b = b + load3(M.hstray, N, i);
     o.ext = b;
   }
   return o;
@@ -388,7 +391,13 @@ __device__ __forceinline__ LocalOut local_terms_fast(const MagnetDev& M, const f
     const float mu = dot3(mc, u);
     o.anis = M.finv_ms * ((2 * M.fk1 * mu + 4 * M.fk2 * mu * mu * mu) * u);
   }
-  if (M.terms & TERM_EXT) o.ext = f3(M.fb[0], M.fb[1], M.fb[2]);
+  if (M.terms & TERM_EXT) {
+    o.ext = f3(M.fb[0], M.fb[1], M.fb[2]);
+    if (M.terms & FLAG_STRAY) {
+      const float3 s = load3(M.hstray, N, x + M.n[0] * (y + M.n[1] * z));
+      o.ext = f3(o.ext.x + s.x, o.ext.y + s.y, o.ext.z + s.z);
+    }
+  }
   return o;
 }
 

@@ -49,6 +49,8 @@ class Ferromagnet:
         self._engine = world._engine
         self._group = world._group
         self._relax_threshold = -1.0
+        self._stray_source = True
+        self._stray_destination = True
         self._suspend = True
         ch = self._update
         self._msat = Parameter(self, "msat", "A/m", 1, 1.0, ch)
@@ -132,6 +134,8 @@ class Ferromagnet:
         d.kc3 = self._kc3._scalar(keep)
         d.anis_c1 = self._anisC1._vector(keep)
         d.anis_c2 = self._anisC2._vector(keep)
+        d.stray_source_off = 0 if self._stray_source else 1
+        d.stray_destination_off = 0 if self._stray_destination else 1
         for i, p in enumerate(self._dmi._list()):
             d.dmi[i] = p._scalar(keep)
         li, ls = self._inter_exchange._lut(), self._scale_exchange._lut()
@@ -405,6 +409,28 @@ class Ferromagnet:
                            + " used for the timesolver (1e-5). Using this value results"
                            + " in no torque minimization, only energy minimization.", UserWarning)
         self._engine.relax(self._group, tol, self._relax_threshold)
+
+    @property
+    def enable_as_stray_field_source(self):
+        """Whether this magnet's stray field acts on the other magnets of the
+        world (mumaxplus/magnet.py:155-172; default True)."""
+        return self._stray_source
+
+    @enable_as_stray_field_source.setter
+    def enable_as_stray_field_source(self, value):
+        self._stray_source = bool(value)
+        self._update()
+
+    @property
+    def enable_as_stray_field_destination(self):
+        """Whether the stray fields of the other magnets of the world act on
+        this magnet (default True)."""
+        return self._stray_destination
+
+    @enable_as_stray_field_destination.setter
+    def enable_as_stray_field_destination(self, value):
+        self._stray_destination = bool(value)
+        self._update()
 
     @property
     def RelaxTorqueThreshold(self):

@@ -74,9 +74,6 @@ class World:
         return name
 
     def _register(self, magnet):
-        if self._magnets:
-            warnings.warn("stray fields between different magnets of one world are not included "
-                          "(each magnet only feels its own demag field)", UserWarning, stacklevel=3)
         self._magnets[magnet.name] = magnet
 
     def _update_all(self):

@@ -286,6 +286,7 @@ struct Magnet {
   std::vector<cd> khat[6];
   bool kready = false;
   std::vector<double> ext_oct;  // octant supplied by the caller (replaces kernel_octant when set)
+  bool stray_src_off = false, stray_dst_off = false;  // Magnet::enableAsStrayFieldSource/Destination
 
   int idx(int x, int y, int z) const { return x + n[0] * (y + n[1] * z); }
   V3 mv(int i) const { return {m[i], m[(size_t)N + i], m[2 * (size_t)N + i]}; }
@@ -320,6 +321,8 @@ int load_magnet(Magnet& mg, const mpx_magnet_desc* d) {
     if (d->size[a] <= 0) { g_err = "grid size must be positive"; return MPX_ERR_INVALID; }
     mg.n[a] = d->size[a];
     mg.o[a] = d->origin[a];
+    mg.stray_src_off = d->stray_source_off != 0;
+    mg.stray_dst_off = d->stray_destination_off != 0;
     mg.mg[a] = d->mastergrid_size[a];
     mg.mgo[a] = d->mastergrid_origin[a];
     mg.pbc[a] = d->pbc_repetitions[a];
@@ -716,6 +719,72 @@ struct World {
   bool relax_torque = false;  // the equations use the damping torque (physics/relaxer.cpp)
 };
 
+// physics/zeeman.cu:70-88: the destination receives the stray field of every
+// other enabled source of its world
+bool has_stray(const World& w, const Magnet& dst) {
+  if (dst.stray_dst_off) return false;
+  for (const Magnet& src : w.mags)
+    if (&src != &dst && !src.stray_src_off && !src.msat.zero()) return true;
+  return false;
+}
+
+// physics/strayfieldbrute.cu:15-57: B(r) = -mu0 sum_{r' in src} N(r - r') Ms m(r'),
+// r, r' world cell coordinates, the tensor (with PBC images) tabulated over the
+// displacements of the two grids; zero outside the destination's geometry.
+void add_stray(const World& w, const Magnet& dst, std::vector<double>& h) {
+  if (dst.stray_dst_off) return;
+  const int NB = dst.N;
+  for (const Magnet& src : w.mags) {
+    if (&src == &dst || src.stray_src_off || src.msat.zero()) continue;
+    int K[3], O[3];
+    for (int a = 0; a < 3; ++a) {
+      K[a] = src.n[a] + dst.n[a] - 1;
+      O[a] = dst.o[a] - src.o[a] - (src.n[a] - 1);
+    }
+    const size_t KK = (size_t)K[0] * K[1] * K[2];
+    std::vector<double> tab(6 * KK);
+#pragma omp parallel for collapse(2) schedule(dynamic)
+    for (int k = 0; k < K[2]; ++k)
+      for (int j = 0; j < K[1]; ++j)
+        for (int i = 0; i < K[0]; ++i) {
+          double v[6];
+          kernel_at(O[0] + i, O[1] + j, O[2] + k, dst.mg, dst.pbc, dst.cs, v);
+          const size_t p = ((size_t)k * K[1] + j) * K[0] + i;
+          for (int c = 0; c < 6; ++c) tab[c * KK + p] = v[c];
+        }
+    const int NA = src.N;
+#pragma omp parallel for schedule(static)
+    for (int ib = 0; ib < NB; ++ib) {
+      if (!dst.in_geom(ib)) continue;
+      const int bx = ib % dst.n[0], by = (ib / dst.n[0]) % dst.n[1], bz = ib / (dst.n[0] * dst.n[1]);
+      double hx = 0, hy = 0, hz = 0;
+      for (int ia = 0; ia < NA; ++ia) {
+        if (!src.in_geom(ia)) continue;
+        const int ax = ia % src.n[0], ay = (ia / src.n[0]) % src.n[1], az = ia / (src.n[0] * src.n[1]);
+        const size_t p = ((size_t)(dst.o[2] + bz - src.o[2] - az - O[2]) * K[1] +
+                          (dst.o[1] + by - src.o[1] - ay - O[1])) * K[0] +
+                         (dst.o[0] + bx - src.o[0] - ax - O[0]);
+        const double ms = src.msat.at(ia);
+        const V3 M = ms * src.mv(ia);
+        const double nxx = tab[p], nyy = tab[KK + p], nzz = tab[2 * KK + p];
+        const double nxy = tab[3 * KK + p], nxz = tab[4 * KK + p], nyz = tab[5 * KK + p];
+        hx -= nxx * M.x + nxy * M.y + nxz * M.z;
+        hy -= nxy * M.x + nyy * M.y + nyz * M.z;
+        hz -= nxz * M.x + nyz * M.y + nzz * M.z;
+      }
+      h[ib] += MU0 * hx;
+      h[(size_t)NB + ib] += MU0 * hy;
+      h[2 * (size_t)NB + ib] += MU0 * hz;
+    }
+  }
+}
+
+bool ext_zero(const World& w, const Magnet& mg) { return external_zero(mg, w.wb) && !has_stray(w, mg); }
+void ext_field(const World& w, const Magnet& mg, std::vector<double>& h) {
+  external_field(mg, w.wb, h);
+  add_stray(w, mg, h);
+}
+
 // physics/effectivefield.cpp:15-28 (terms added in this order)
 void effective_field(World& w, Magnet& mg, std::vector<double>& h) {
   const size_t n3 = 3 * (size_t)mg.N;
@@ -729,7 +798,7 @@ void effective_field(World& w, Magnet& mg, std::vector<double>& h) {
   };
   if (!exchange_zero(mg)) { exchange_field(mg, t); add(t); }
   if (!anis_zero(mg)) { anisotropy_field(mg, t); add(t); }
-  if (!external_zero(mg, w.wb)) { external_field(mg, w.wb, t); add(t); }
+  if (!ext_zero(w, mg)) { ext_field(w, mg, t); add(t); }
   if (!dmi_zero(mg)) { dmi_field(mg, t); add(t); }
   if (!demag_zero(mg)) { demag_field(mg, t); add(t); }
 }
@@ -777,8 +846,8 @@ void energy_density(World& w, Magnet& mg, int q, std::vector<double>& e) {
       if (dmi_zero(mg)) return;
       dmi_field(mg, h); from_field(0.5); return;
     case MPX_Q_ZEEMAN_ENERGY_DENSITY:
-      if (external_zero(mg, w.wb)) return;
-      external_field(mg, w.wb, h); from_field(1.0); return;
+      if (ext_zero(w, mg)) return;
+      ext_field(w, mg, h); from_field(1.0); return;
     case MPX_Q_DEMAG_ENERGY_DENSITY:
       if (demag_zero(mg)) return;
       demag_field(mg, h); from_field(0.5); return;
@@ -1078,7 +1147,7 @@ int ox_eval(ox_world* wp, int q, int quantity, double* out) {
     case MPX_Q_EXCHANGE_FIELD: exchange_field(mg, h); break;
     case MPX_Q_DMI_FIELD: dmi_field(mg, h); break;
     case MPX_Q_ANISOTROPY_FIELD: anisotropy_field(mg, h); break;
-    case MPX_Q_EXTERNAL_FIELD: external_field(mg, w.wb, h); break;
+    case MPX_Q_EXTERNAL_FIELD: ext_field(w, mg, h); break;
     case MPX_Q_DEMAG_FIELD: demag_field(mg, h); break;
     case MPX_Q_TORQUE:
     case MPX_Q_LLG_TORQUE: torque(w, mg, h); break;

@@ -33,6 +33,8 @@ class MagnetSpec:
     kc3: object = 0.0
     anisC1: object = (0.0, 0.0, 0.0)
     anisC2: object = (0.0, 0.0, 0.0)
+    stray_source: bool = True
+    stray_destination: bool = True
     frozen: object = 0.0
     dmi: dict = field(default_factory=dict)
     inter_exchange: float = 0.0
@@ -109,6 +111,8 @@ class MagnetSpec:
         d.kc3 = self._scalar(self.kc3, keep)
         d.anis_c1 = self._vector(self.anisC1, keep)
         d.anis_c2 = self._vector(self.anisC2, keep)
+        d.stray_source_off = 0 if self.stray_source else 1
+        d.stray_destination_off = 0 if self.stray_destination else 1
         d.bias_magnetic_field = self._vector(self.bias, keep)
         for i, k in enumerate(abi.DMI_ORDER):
             d.dmi[i] = self._scalar(self.dmi.get(k, 0.0), keep)

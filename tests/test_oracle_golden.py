@@ -339,3 +339,52 @@ def test_oracle_cubic_anisotropy_vs_numpy(oracle, per_cell):
     np.testing.assert_allclose(ow.eval(q, oracle.abi.Q_ANISOTROPY_FIELD), h, rtol=1e-9, atol=1e-12 * np.abs(h).max())
     np.testing.assert_allclose(ow.eval(q, oracle.abi.Q_ANISOTROPY_ENERGY_DENSITY)[0], e, rtol=1e-9,
                                atol=1e-9 * np.abs(e).max())
+
+
+def test_oracle_stray_field_between_magnets_equals_union_demag(oracle):
+    """Two magnets of one world: self demag (FFT) + stray field of the other
+    (direct sum over the tabulated tensor) equals the demag field of a single
+    magnet covering both, with the gap masked out (independent code paths of
+    the oracle, physics/zeeman.cu:70-88 vs strayfieldfft.cu)."""
+    cs = (2e-9, 3e-9, 2.5e-9)
+    A = MagnetSpec(size=(10, 6, 2), cellsize=cs, msat=8e5)
+    B = MagnetSpec(size=(7, 6, 2), origin=(13, 2, 0), cellsize=cs, msat=6e5)
+    mA = random_m(A.shape, seed=11, smooth=1)
+    mB = random_m(B.shape, seed=12, smooth=1)
+    ow = O.OracleWorld()
+    keep = []
+    qa = ow.add_magnet(A.desc(keep))
+    qb = ow.add_magnet(B.desc(keep))
+    ow.set_m(qa, mA)
+    ow.set_m(qb, mB)
+    got_b = ow.eval(qb, oracle.abi.Q_EFFECTIVE_FIELD)
+    got_a = ow.eval(qa, oracle.abi.Q_EFFECTIVE_FIELD)
+    # union grid 20 x 8 x 2 at the origin
+    nz, ny, nx = 2, 8, 20
+    geom = np.zeros((nz, ny, nx), np.uint8)
+    msat = np.zeros((nz, ny, nx), np.float32)
+    m = np.zeros((3, nz, ny, nx), np.float32)
+    m[0] = 1.0
+    geom[:, 0:6, 0:10] = 1
+    geom[:, 2:8, 13:20] = 1
+    msat[:, 0:6, 0:10] = 8e5
+    msat[:, 2:8, 13:20] = 6e5
+    m[:, :, 0:6, 0:10] = mA
+    m[:, :, 2:8, 13:20] = mB
+    U = MagnetSpec(size=(nx, ny, nz), cellsize=cs, msat=msat, geometry=geom)
+    ou, qu = U.oracle_world(m)
+    want = ou.eval(qu, oracle.abi.Q_EFFECTIVE_FIELD)
+    scale = np.abs(want).max()
+    assert np.abs(got_a - want[:, :, 0:6, 0:10]).max() < 1e-9 * scale
+    assert np.abs(got_b - want[:, :, 2:8, 13:20]).max() < 1e-9 * scale
+    # switches: B no longer receives, A no longer sends
+    B2 = MagnetSpec(size=(7, 6, 2), origin=(13, 2, 0), cellsize=cs, msat=6e5, stray_destination=False)
+    ow2 = O.OracleWorld()
+    qa2 = ow2.add_magnet(A.desc(keep))
+    qb2 = ow2.add_magnet(B2.desc(keep))
+    ow2.set_m(qa2, mA)
+    ow2.set_m(qb2, mB)
+    alone = O.OracleWorld()
+    ql = alone.add_magnet(B.desc(keep))
+    alone.set_m(ql, mB)
+    np.testing.assert_array_equal(ow2.eval(qb2, oracle.abi.Q_EFFECTIVE_FIELD), alone.eval(ql, oracle.abi.Q_EFFECTIVE_FIELD))

@@ -77,8 +77,11 @@ typedef enum {
   MPX_Q_ZEEMAN_ENERGY_DENSITY = 13,
   MPX_Q_DEMAG_ENERGY_DENSITY = 14,
   MPX_Q_TOTAL_ENERGY_DENSITY = 15,
-  MPX_Q_COUNT = 16
+  MPX_Q_SPIN_TRANSFER_TORQUE = 16,   /* physics/stt.cu:143-185 (Zhang-Li or Slonczewski), 1/s */
+  MPX_Q_COUNT = 17
 } mpx_quantity;
+/* energy densities are the scalar quantities; the others have 3 components */
+#define MPX_Q_IS_SCALAR(q) ((q) >= MPX_Q_EXCHANGE_ENERGY_DENSITY && (q) <= MPX_Q_TOTAL_ENERGY_DENSITY)
 
 /* Runge-Kutta methods (core/butchertableau.cpp). */
 typedef enum {
@@ -149,6 +152,14 @@ typedef struct {
    * zero default keeps both on */
   int stray_source_off;
   int stray_destination_off;
+  /* spin-transfer torque (physics/stt.cu; physics/ferromagnet.cpp:34-52 defaults) */
+  mpx_scalar pol, xi, lambda, epsilon_prime;
+  mpx_scalar free_layer_thickness;  /* m; the reference's default is nz * cellsize z */
+  mpx_vector jcur;                  /* A/m^2 */
+  mpx_vector fixed_layer;           /* Slonczewski polarisation direction p */
+  int fixed_layer_below;            /* 0: fixed layer on top (reference default) */
+  int zhang_li_off;                 /* enableZhangLiTorque, inverted */
+  int slonczewski_off;              /* enableSlonczewskiTorque, inverted */
 } mpx_magnet_desc;
 
 /* Time-solver settings (core/timesolver.hpp:74-82 defaults in brackets). */

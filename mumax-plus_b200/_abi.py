@@ -37,7 +37,8 @@ Q_ANISOTROPY_ENERGY_DENSITY = 12
 Q_ZEEMAN_ENERGY_DENSITY = 13
 Q_DEMAG_ENERGY_DENSITY = 14
 Q_TOTAL_ENERGY_DENSITY = 15
-Q_COUNT = 16
+Q_SPIN_TRANSFER_TORQUE = 16
+Q_COUNT = 17
 
 # Runge-Kutta methods, with the names of core/butchertableau.hpp
 RK_METHODS = {
@@ -93,6 +94,16 @@ class MagnetDesc(C.Structure):
         ("anis_c2", Vector),
         ("stray_source_off", C.c_int),
         ("stray_destination_off", C.c_int),
+        ("pol", Scalar),
+        ("xi", Scalar),
+        ("lambda_", Scalar),
+        ("epsilon_prime", Scalar),
+        ("free_layer_thickness", Scalar),
+        ("jcur", Vector),
+        ("fixed_layer", Vector),
+        ("fixed_layer_below", C.c_int),
+        ("zhang_li_off", C.c_int),
+        ("slonczewski_off", C.c_int),
     ]
 
 

@@ -651,6 +651,14 @@ mpx_status load_params(mpx_engine* e, Magnet* m, const mpx_magnet_desc* d) {
   MPX_TRY(load_scalar(e, m, &D.kc3, d->kc3, N));
   MPX_TRY(load_vector(e, m, &D.anisC1, d->anis_c1, N));
   MPX_TRY(load_vector(e, m, &D.anisC2, d->anis_c2, N));
+  MPX_TRY(load_scalar(e, m, &D.pol, d->pol, N));
+  MPX_TRY(load_scalar(e, m, &D.xi, d->xi, N));
+  MPX_TRY(load_scalar(e, m, &D.lambda_, d->lambda, N));
+  MPX_TRY(load_scalar(e, m, &D.epsp, d->epsilon_prime, N));
+  MPX_TRY(load_scalar(e, m, &D.flt, d->free_layer_thickness, N));
+  MPX_TRY(load_vector(e, m, &D.jcur, d->jcur, N));
+  MPX_TRY(load_vector(e, m, &D.fixl, d->fixed_layer, N));
+  D.fl_below = d->fixed_layer_below ? 1 : 0;
   for (int c = 0; c < 9; ++c) MPX_TRY(load_scalar(e, m, &D.dmi[c], d->dmi[c], N));
   D.inter_u = (float)d->inter_exchange;
   D.scale_u = (float)d->scale_exchange;
@@ -705,6 +713,14 @@ mpx_status load_params(mpx_engine* e, Magnet* m, const mpx_magnet_desc* d) {
                     (vector_zero(d->anis_c1) && vector_zero(d->anis_c2)) || msat0;
   if (!uni0) terms |= TERM_ANIS;
   else if (!cub0) terms |= TERM_ANIS | FLAG_CUBIC;
+  // physics/stt.cu:9-24: Slonczewski unless assured zero, else Zhang-Li unless assured zero
+  const bool j0 = vector_zero(d->jcur);
+  const bool zl0 = d->zhang_li_off || msat0 || j0 || scalar_zero(d->pol);
+  const bool sl0 = d->slonczewski_off || msat0 || j0 || scalar_zero(d->free_layer_thickness) ||
+                   vector_zero(d->fixed_layer) ||
+                   (scalar_zero(d->epsilon_prime) && (scalar_zero(d->lambda) || scalar_zero(d->pol)));
+  if (!sl0) terms |= FLAG_STT_SL;
+  else if (!zl0) terms |= FLAG_STT_ZL;
   const bool wb0 = e->wb[0] == 0 && e->wb[1] == 0 && e->wb[2] == 0;
   if (!(wb0 && vector_zero(d->bias_magnetic_field))) terms |= TERM_EXT;
   if (!vector_zero(d->bias_magnetic_field)) terms |= FLAG_MAGNET_BIAS;
@@ -1410,6 +1426,10 @@ mpx_status mpx_magnet_bytes(const mpx_magnet_desc* d, int64_t* resident, int64_t
     if (sc->cells) res += 4 * N;
   if (d->anis_c1.cells) res += 12 * N;
   if (d->anis_c2.cells) res += 12 * N;
+  for (const mpx_scalar* sc : {&d->pol, &d->xi, &d->lambda, &d->epsilon_prime, &d->free_layer_thickness})
+    if (sc->cells) res += 4 * N;
+  if (d->jcur.cells) res += 12 * N;
+  if (d->fixed_layer.cells) res += 12 * N;
   for (int c = 0; c < 9; ++c)
     if (d->dmi[c].cells) res += 4 * N;
   if (d->anis_u.cells) res += 12 * N;
@@ -1483,7 +1503,7 @@ mpx_status mpx_eval(mpx_engine* e, int magnet, int quantity, float* out, int on_
   if (!m || (!out && on_device != 2)) return fail(MPX_ERR_INVALID, "no such magnet / null output");
   if (quantity < 0 || quantity >= MPX_Q_COUNT) return fail(MPX_ERR_INVALID, "unknown quantity");
   DeviceGuard guard(e->device);
-  const int nc = quantity >= MPX_Q_EXCHANGE_ENERGY_DENSITY ? 1 : 3;
+  const int nc = MPX_Q_IS_SCALAR(quantity) ? 1 : 3;
   const size_t bytes = sizeof(float) * nc * (size_t)m->dev.N;
   float* dst = out;
   if (on_device == 2) {
@@ -1503,7 +1523,7 @@ mpx_status mpx_eval(mpx_engine* e, int magnet, int quantity, float* out, int on_
 }
 
 static mpx_status reduce_quantity(mpx_engine* e, Magnet* m, int quantity, int op, double out[3]) {
-  const int nc = quantity >= MPX_Q_EXCHANGE_ENERGY_DENSITY ? 1 : 3;
+  const int nc = MPX_Q_IS_SCALAR(quantity) ? 1 : 3;
   const int N = m->dev.N;
   MPX_TRY(ensure_scratch(e, sizeof(float) * 3 * (size_t)N));
   MPX_TRY(eval_into(e, m, quantity, e->d_scratch));
@@ -1524,7 +1544,7 @@ mpx_status mpx_average(mpx_engine* e, int magnet, int quantity, double out[3]) {
   DeviceGuard guard(e->device);
   double r[3];
   MPX_TRY(reduce_quantity(e, m, quantity, 0, r));
-  const int nc = quantity >= MPX_Q_EXCHANGE_ENERGY_DENSITY ? 1 : 3;
+  const int nc = MPX_Q_IS_SCALAR(quantity) ? 1 : 3;
   for (int c = 0; c < 3; ++c) out[c] = (c < nc && m->ngeo > 0) ? r[c] / m->ngeo : 0.0;
   return MPX_OK;
 }
@@ -1543,7 +1563,7 @@ mpx_status mpx_max_norm(mpx_engine* e, int magnet, int quantity, double* out) {
 mpx_status mpx_energy(mpx_engine* e, int magnet, int quantity, double* out) {
   Magnet* m = get_mag(e, magnet);
   if (!m || !out) return fail(MPX_ERR_INVALID, "no such magnet / null output");
-  if (quantity < MPX_Q_EXCHANGE_ENERGY_DENSITY || quantity >= MPX_Q_COUNT)
+  if (!MPX_Q_IS_SCALAR(quantity))
     return fail(MPX_ERR_INVALID, "energy needs an energy-density quantity");
   double avg[3];
   MPX_TRY(mpx_average(e, magnet, quantity, avg));

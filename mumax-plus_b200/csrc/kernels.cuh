@@ -437,6 +437,7 @@ __device__ __forceinline__ void epilogue_cell(const MagnetDev& M, const GroupDev
       }
       h = h + bdemag;
       k = G.torque_kind ? damping_torque(mc, h) : llg_torque(mc, h, M.alpha.at(i));
+      if (!G.torque_kind && (M.terms & (FLAG_STT_ZL | FLAG_STT_SL))) k = k + stt_torque(M, m, x, y, z, i, mc);
     }
     store3(M.buf[G.map[2 + ea.stage]], N, i, k);
     if (ea.fsal_err && ing) {
@@ -454,7 +455,7 @@ __device__ __forceinline__ void epilogue_cell(const MagnetDev& M, const GroupDev
   // ---- EPI_EVAL
   const int q = ea.quantity;
   float* out = ea.out;
-  const bool scalar = q >= 10;
+  const bool scalar = MPX_Q_IS_SCALAR(q);
   if (!ing) {
     if (scalar) {
       out[i] = 0.f;
@@ -492,9 +493,15 @@ __device__ __forceinline__ void epilogue_cell(const MagnetDev& M, const GroupDev
     case 4: r = lo.anis; break;
     case 5: r = lo.ext; break;
     case 6: r = bdemag; break;
-    case 7:
+    case 7:  // total torque: LLG + spin transfer (physics/torque.cu:78-90)
     case 8:
-      if (M.frozen.at(i) == 0.0f) r = llg_torque(mc, h, M.alpha.at(i));
+      if (M.frozen.at(i) == 0.0f) {
+        r = llg_torque(mc, h, M.alpha.at(i));
+        if (q == 7 && (M.terms & (FLAG_STT_ZL | FLAG_STT_SL))) r = r + stt_torque(M, m, x, y, z, i, mc);
+      }
+      break;
+    case 16:
+      if (M.frozen.at(i) == 0.0f && (M.terms & (FLAG_STT_ZL | FLAG_STT_SL))) r = stt_torque(M, m, x, y, z, i, mc);
       break;
     case 9:
       if (M.frozen.at(i) == 0.0f) r = damping_torque(mc, h);

@@ -28,7 +28,8 @@ enum : unsigned {
   TERM_EXCH = 1u, TERM_DMI = 2u, TERM_ANIS = 4u, TERM_EXT = 8u, TERM_DEMAG = 16u,
   FLAG_OPENBC = 256u, FLAG_MAGNET_BIAS = 512u,
   FLAG_CUBIC = 1024u,  // the anisotropy term is cubic (uniaxial otherwise)
-  FLAG_STRAY = 2048u   // stray fields of other magnets in `hstray`
+  FLAG_STRAY = 2048u,  // stray fields of other magnets in `hstray`
+  FLAG_STT_ZL = 4096u, FLAG_STT_SL = 8192u  // spin-transfer torque: Zhang-Li or Slonczewski
 };
 
 struct DScalar {  // uniform value or per-cell array
@@ -59,6 +60,9 @@ struct MagnetDev {
   DVector anisU, bias;
   DScalar kc1, kc2, kc3;  // cubic anisotropy constants
   DVector anisC1, anisC2; // cubic anisotropy axes
+  DScalar pol, xi, lambda_, epsp, flt;  // spin-transfer torque parameters
+  DVector jcur, fixl;
+  int fl_below;           // Slonczewski fixed layer below the free layer
   DScalar dmi[9];  // xxy, xxz, xyz, yxy, yxz, yyz, zxy, zxz, zyz
   float inter_u, scale_u;
   const float* __restrict__ inter_lut;
@@ -406,6 +410,59 @@ __device__ __forceinline__ float3 llg_torque(float3 m, float3 h, float a) {
   const float3 mxh = cross3(m, h);
   const float3 mxmxh = cross3(m, mxh);
   return (-GAMMA_LL / (1 + a * a)) * (mxh + a * mxmxh);
+}
+
+// physics/stt.cu:26-185: spin-transfer torque (1/s) of the cell, Zhang-Li (central
+// differences of m along the current, neighbours in the grid with msat != 0,
+// mastergrid wrap) or Slonczewski (current along z through a free layer).
+constexpr float MUB_F = 9.274009152e-24f, QE_F = 1.60217646e-19f, HBAR_F = 1.054571817e-34f;
+__device__ __noinline__ float3 stt_torque(const MagnetDev& M, const float* __restrict__ m, int x, int y, int z, int i,
+                                          float3 mc) {
+  const int N = M.N;
+  const float ms = M.msat.at(i), alpha = M.alpha.at(i);
+  if (M.terms & FLAG_STT_SL) {
+    const float jz = M.jcur.at(i, N).z;
+    const float pol = M.pol.at(i), lambda = M.lambda_.at(i), eps_p = M.epsp.at(i);
+    const float3 p = M.fixl.at(i, N);
+    float d = M.flt.at(i);
+    if (M.fl_below) d = -d;
+    if (ms == 0.f || jz == 0.f || d == 0.f || (p.x == 0.f && p.y == 0.f && p.z == 0.f) ||
+        (eps_p == 0.f && (lambda == 0.f || pol == 0.f)))
+      return f3(0.f, 0.f, 0.f);
+    const float B = (HBAR_F / QE_F) * jz / (ms * d);
+    const float l2 = lambda * lambda;
+    const float eps = pol * l2 / ((l2 + 1) + (l2 - 1) * dot3(mc, p));
+    const float3 pxm = cross3(p, mc);
+    const float3 mxpxm = cross3(mc, pxm);
+    const float s = (B / (1 + alpha * alpha)) * GAMMA_LL;
+    return f3(((eps + eps_p * alpha) * mxpxm.x + (eps_p - eps * alpha) * pxm.x) * s,
+              ((eps + eps_p * alpha) * mxpxm.y + (eps_p - eps * alpha) * pxm.y) * s,
+              ((eps + eps_p * alpha) * mxpxm.z + (eps_p - eps * alpha) * pxm.z) * s);
+  }
+  const float3 j = M.jcur.at(i, N);
+  const float pol = M.pol.at(i), xi = M.xi.at(i);
+  if (ms == 0.f || pol == 0.f || (j.x == 0.f && j.y == 0.f && j.z == 0.f)) return f3(0.f, 0.f, 0.f);
+  const float cu = MUB_F * pol / (QE_F * ms * (1 + xi * xi));
+  const float u[3] = {cu * j.x, cu * j.y, cu * j.z};
+  float3 hs = f3(0.f, 0.f, 0.f);
+  for (int axis = 0; axis < 3; ++axis)
+    for (int d = -1; d <= 1; d += 2) {
+      int xx = x, yy = y, zz = z, nc;
+      if (axis == 0) { nc = nb_coord(x, d, M.n[0], M.o[0], M.mg[0], M.mgo[0]); xx = nc; }
+      else if (axis == 1) { nc = nb_coord(y, d, M.n[1], M.o[1], M.mg[1], M.mgo[1]); yy = nc; }
+      else { nc = nb_coord(z, d, M.n[2], M.o[2], M.mg[2], M.mgo[2]); zz = nc; }
+      if (nc < 0) continue;
+      const int jn = xx + M.n[0] * (yy + M.n[1] * zz);
+      if (M.msat.at(jn) == 0.f) continue;
+      const float3 mn = load3(m, N, jn);
+      const float c = d * u[axis] / (2 * M.cs[axis]);
+      hs = f3(hs.x + c * mn.x, hs.y + c * mn.y, hs.z + c * mn.z);
+    }
+  const float3 mxh = cross3(mc, hs);
+  const float3 mxmxh = cross3(mc, mxh);
+  const float s = -1 / (1 + alpha * alpha);
+  return f3(s * ((1 + xi * alpha) * mxmxh.x + (xi - alpha) * mxh.x), s * ((1 + xi * alpha) * mxmxh.y + (xi - alpha) * mxh.y),
+            s * ((1 + xi * alpha) * mxmxh.z + (xi - alpha) * mxh.z));
 }
 
 // physics/torque.cu:58-76 (k_dampingtorque): the relax torque -gamma_LL m x (m x h)

@@ -66,15 +66,25 @@ class Ferromagnet:
         self._kc3 = Parameter(self, "kc3", "J/m3", 1, 0.0, ch)
         self._anisC1 = Parameter(self, "anisC1", "", 3, (0.0, 0.0, 0.0), ch)
         self._anisC2 = Parameter(self, "anisC2", "", 3, (0.0, 0.0, 0.0), ch)
+        # spin-transfer torque (physics/ferromagnet.cpp:34-52 defaults)
+        self._pol = Parameter(self, "pol", "", 1, 0.0, ch)
+        self._xi = Parameter(self, "xi", "", 1, 0.0, ch)
+        self._Lambda = Parameter(self, "Lambda", "", 1, 0.0, ch)
+        self._epsilon_prime = Parameter(self, "epsilon_prime", "", 1, 0.0, ch)
+        self._jcur = Parameter(self, "jcur", "A/m2", 3, (0.0, 0.0, 0.0), ch)
+        self._fixed_layer = Parameter(self, "fixed_layer", "", 3, (0.0, 0.0, 0.0), ch)
+        self._free_layer_thickness = Parameter(self, "free_layer_thickness", "m", 1,
+                                               float(self._grid.size[2] * world.cellsize[2]), ch)
+        self._fixed_layer_on_top = True
+        self._enable_zhang_li = True
+        self._enable_slonczewski = True
         self._dmi = DmiTensor(self, ch)
         self._inter_exchange = InterParameter(self, "inter_exchange", "J/m", 0.0, ch)
         self._scale_exchange = InterParameter(self, "scale_exchange", "", 1.0, ch)
         self._enable_demag = True
         self._enable_openbc = False
         self._unsupported = {}
-        for n, nc in (("temperature", 1),
-                      ("xi", 1), ("Lambda", 1), ("pol", 1), ("epsilon_prime", 1), ("jcur", 3),
-                      ("fixed_layer", 3), ("B1", 1), ("B2", 1), ("conductivity", 1), ("amr_ratio", 1)):
+        for n, nc in (("temperature", 1), ("B1", 1), ("B2", 1), ("conductivity", 1), ("amr_ratio", 1)):
             self._unsupported[n] = _Unsupported(self, n, "", nc, (0.0, 0.0, 0.0) if nc == 3 else 0.0)
         self._suspend = False
         self._id = self._engine.magnet_add(self._group, self._desc())
@@ -134,6 +144,16 @@ class Ferromagnet:
         d.kc3 = self._kc3._scalar(keep)
         d.anis_c1 = self._anisC1._vector(keep)
         d.anis_c2 = self._anisC2._vector(keep)
+        d.pol = self._pol._scalar(keep)
+        d.xi = self._xi._scalar(keep)
+        d.lambda_ = self._Lambda._scalar(keep)
+        d.epsilon_prime = self._epsilon_prime._scalar(keep)
+        d.free_layer_thickness = self._free_layer_thickness._scalar(keep)
+        d.jcur = self._jcur._vector(keep)
+        d.fixed_layer = self._fixed_layer._vector(keep)
+        d.fixed_layer_below = 0 if self._fixed_layer_on_top else 1
+        d.zhang_li_off = 0 if self._enable_zhang_li else 1
+        d.slonczewski_off = 0 if self._enable_slonczewski else 1
         d.stray_source_off = 0 if self._stray_source else 1
         d.stray_destination_off = 0 if self._stray_destination else 1
         for i, p in enumerate(self._dmi._list()):
@@ -263,6 +283,13 @@ class Ferromagnet:
     ku2 = _param_prop("_ku2")
     anisU = _param_prop("_anisU")
     kc1 = _param_prop("_kc1")
+    pol = _param_prop("_pol")
+    xi = _param_prop("_xi")
+    Lambda = _param_prop("_Lambda")
+    epsilon_prime = _param_prop("_epsilon_prime")
+    jcur = _param_prop("_jcur")
+    fixed_layer = _param_prop("_fixed_layer")
+    free_layer_thickness = _param_prop("_free_layer_thickness")
     kc2 = _param_prop("_kc2")
     kc3 = _param_prop("_kc3")
     anisC1 = _param_prop("_anisC1")
@@ -410,6 +437,25 @@ class Ferromagnet:
                            + " in no torque minimization, only energy minimization.", UserWarning)
         self._engine.relax(self._group, tol, self._relax_threshold)
 
+    def _flag(name, doc):
+        def getter(self):
+            return getattr(self, name)
+
+        def setter(self, value):
+            setattr(self, name, bool(value))
+            self._update()
+
+        return property(getter, setter, doc=doc)
+
+    fixed_layer_on_top = _flag("_fixed_layer_on_top", "Slonczewski fixed layer above the free layer (default True).")
+    enable_zhang_li_torque = _flag("_enable_zhang_li", "Zhang-Li spin-transfer torque on (default True).")
+    enable_slonczewski_torque = _flag("_enable_slonczewski", "Slonczewski spin-transfer torque on (default True).")
+
+    @property
+    def spin_transfer_torque(self):
+        """Spin-transfer torque (1/s), physics/stt.cu:143-185."""
+        return self._q(_abi.Q_SPIN_TRANSFER_TORQUE, "spintransfer_torque", "1/s")
+
     @property
     def enable_as_stray_field_source(self):
         """Whether this magnet's stray field acts on the other magnets of the
@@ -460,6 +506,5 @@ def _unsupported_prop(name):
     return property(getter, setter)
 
 
-for _n in ("temperature", "xi", "Lambda", "pol", "epsilon_prime",
-           "jcur", "fixed_layer", "B1", "B2", "conductivity", "amr_ratio"):
+for _n in ("temperature", "B1", "B2", "conductivity", "amr_ratio"):
     setattr(Ferromagnet, _n, _unsupported_prop(_n))

@@ -36,6 +36,9 @@ using cd = std::complex<double>;
 
 constexpr double GAMMALL = 1.7595e11;       // physics/constants.hpp:24 (DOUBLE)
 constexpr double MU0 = 1.25663706212e-6;    // physics/constants.hpp:26 (DOUBLE)
+constexpr double QE = 1.60217646e-19;       // physics/constants.hpp:26-30 (DOUBLE)
+constexpr double MUB = 9.2740091523e-24;
+constexpr double HBAR = 1.054571817e-34;
 
 thread_local std::string g_err;
 
@@ -275,6 +278,9 @@ struct Magnet {
   VParam anisU, bias;
   Param kc1, kc2, kc3;
   VParam anisC1, anisC2;
+  Param pol, xi, lambda, epsp, flt;
+  VParam jcur, fixl;
+  bool fl_below = false, zl_off = false, sl_off = false;
   Param dmi[9];
   int lutn = 0;
   double inter_u = 0, scale_u = 1;
@@ -347,6 +353,16 @@ int load_magnet(Magnet& mg, const mpx_magnet_desc* d) {
   mg.kc3.load(d->kc3, N);
   mg.anisC1.load(d->anis_c1, N);
   mg.anisC2.load(d->anis_c2, N);
+  mg.pol.load(d->pol, N);
+  mg.xi.load(d->xi, N);
+  mg.lambda.load(d->lambda, N);
+  mg.epsp.load(d->epsilon_prime, N);
+  mg.flt.load(d->free_layer_thickness, N);
+  mg.jcur.load(d->jcur, N);
+  mg.fixl.load(d->fixed_layer, N);
+  mg.fl_below = d->fixed_layer_below != 0;
+  mg.zl_off = d->zhang_li_off != 0;
+  mg.sl_off = d->slonczewski_off != 0;
   for (int c = 0; c < 9; ++c) mg.dmi[c].load(d->dmi[c], N);
   mg.lutn = d->lut_regions;
   int L = mg.lutn * (mg.lutn - 1) / 2;
@@ -803,8 +819,65 @@ void effective_field(World& w, Magnet& mg, std::vector<double>& h) {
   if (!demag_zero(mg)) { demag_field(mg, t); add(t); }
 }
 
+// physics/stt.cu:9-24
+bool zl_zero(const Magnet& mg) { return mg.zl_off || mg.msat.zero() || mg.jcur.zero() || mg.pol.zero(); }
+bool sl_zero(const Magnet& mg) {
+  return mg.sl_off || mg.msat.zero() || mg.jcur.zero() || mg.flt.zero() || mg.fixl.zero() ||
+         (mg.epsp.zero() && (mg.lambda.zero() || mg.pol.zero()));
+}
+
+// physics/stt.cu:26-185: spin-transfer torque, Slonczewski unless assured zero, else Zhang-Li
+void stt_torque(const Magnet& mg, std::vector<double>& tq) {
+  const int N = mg.N;
+  tq.assign(3 * (size_t)N, 0.0);
+  const bool sl = !sl_zero(mg), zl = !zl_zero(mg);
+  if (!sl && !zl) return;
+  for (int i = 0; i < N; ++i) {
+    if (!mg.in_geom(i) || mg.frozen.at(i) != 0) continue;
+    const V3 m = mg.mv(i);
+    const double ms = mg.msat.at(i), alpha = mg.alpha.at(i);
+    V3 t{0, 0, 0};
+    if (sl) {
+      const double jz = mg.jcur.at(i).z, pol = mg.pol.at(i), lambda = mg.lambda.at(i), eps_p = mg.epsp.at(i);
+      const V3 p = mg.fixl.at(i);
+      double d = mg.flt.at(i);
+      if (mg.fl_below) d = -d;
+      if (ms == 0 || jz == 0 || d == 0 || (p.x == 0 && p.y == 0 && p.z == 0) ||
+          (eps_p == 0 && (lambda == 0 || pol == 0)))
+        continue;
+      const double B = (HBAR / QE) * jz / (ms * d);
+      const double l2 = lambda * lambda;
+      const double eps = pol * l2 / ((l2 + 1) + (l2 - 1) * dot(m, p));
+      const V3 pxm = cross(p, m), mxpxm = cross(m, pxm);
+      t = ((B / (1 + alpha * alpha)) * GAMMALL) * ((eps + eps_p * alpha) * mxpxm + (eps_p - eps * alpha) * pxm);
+    } else {
+      const V3 j = mg.jcur.at(i);
+      const double pol = mg.pol.at(i), xi = mg.xi.at(i);
+      if (ms == 0 || pol == 0 || (j.x == 0 && j.y == 0 && j.z == 0)) continue;
+      const double cu = MUB * pol / (QE * ms * (1 + xi * xi));
+      const double u[3] = {cu * j.x, cu * j.y, cu * j.z};
+      const int x = i % mg.n[0], y = (i / mg.n[0]) % mg.n[1], z = i / (mg.n[0] * mg.n[1]);
+      V3 hs{0, 0, 0};
+      for (int axis = 0; axis < 3; ++axis)
+        for (int sg = -1; sg <= 1; sg += 2) {
+          int xx = x + (axis == 0 ? sg : 0), yy = y + (axis == 1 ? sg : 0), zz = z + (axis == 2 ? sg : 0);
+          mg.wrap_local(xx, yy, zz);
+          if (!mg.in_grid_local(xx, yy, zz)) continue;
+          const int jn = mg.idx(xx, yy, zz);
+          if (mg.msat.at(jn) == 0) continue;
+          hs = hs + (sg * u[axis] / (2 * mg.cs[axis])) * mg.mv(jn);
+        }
+      const V3 mxh = cross(m, hs), mxmxh = cross(m, mxh);
+      t = (-1 / (1 + alpha * alpha)) * ((1 + xi * alpha) * mxmxh + (xi - alpha) * mxh);
+    }
+    tq[i] = t.x;
+    tq[(size_t)N + i] = t.y;
+    tq[2 * (size_t)N + i] = t.z;
+  }
+}
+
 // physics/torque.cu:21-45 (LLG) and :58-77 (damping only)
-void torque(World& w, Magnet& mg, std::vector<double>& tq, bool damping_only = false) {
+void torque(World& w, Magnet& mg, std::vector<double>& tq, bool damping_only = false, bool with_stt = true) {
   std::vector<double> h;
   effective_field(w, mg, h);
   const int N = mg.N;
@@ -823,6 +896,11 @@ void torque(World& w, Magnet& mg, std::vector<double>& tq, bool damping_only = f
     tq[i] = t.x;
     tq[(size_t)N + i] = t.y;
     tq[2 * (size_t)N + i] = t.z;
+  }
+  if (!damping_only && with_stt && (!zl_zero(mg) || !sl_zero(mg))) {  // total torque = LLG + STT (torque.cu:78-90)
+    std::vector<double> s;
+    stt_torque(mg, s);
+    for (size_t k = 0; k < tq.size(); ++k) tq[k] += s[k];
   }
   w.evals++;
 }
@@ -1149,9 +1227,10 @@ int ox_eval(ox_world* wp, int q, int quantity, double* out) {
     case MPX_Q_ANISOTROPY_FIELD: anisotropy_field(mg, h); break;
     case MPX_Q_EXTERNAL_FIELD: ext_field(w, mg, h); break;
     case MPX_Q_DEMAG_FIELD: demag_field(mg, h); break;
-    case MPX_Q_TORQUE:
-    case MPX_Q_LLG_TORQUE: torque(w, mg, h); break;
+    case MPX_Q_TORQUE: torque(w, mg, h); break;
+    case MPX_Q_LLG_TORQUE: torque(w, mg, h, false, false); break;
     case MPX_Q_DAMPING_TORQUE: torque(w, mg, h, true); break;
+    case MPX_Q_SPIN_TRANSFER_TORQUE: stt_torque(mg, h); break;
     case MPX_Q_EXCHANGE_ENERGY_DENSITY:
     case MPX_Q_DMI_ENERGY_DENSITY:
     case MPX_Q_ANISOTROPY_ENERGY_DENSITY:
@@ -1220,7 +1299,7 @@ double ox_newell(int comp, int x, int y, int z, double cx, double cy, double cz)
 int ox_average(ox_world* wp, int q, int quantity, double out[3]) {
   World& w = *reinterpret_cast<World*>(wp);
   Magnet& mg = w.mags.at(q);
-  int nc = (quantity >= MPX_Q_EXCHANGE_ENERGY_DENSITY) ? 1 : 3;
+  int nc = MPX_Q_IS_SCALAR(quantity) ? 1 : 3;
   std::vector<double> h((size_t)nc * mg.N);
   int st = ox_eval(wp, q, quantity, h.data());
   if (st) return st;

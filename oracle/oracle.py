@@ -133,7 +133,7 @@ class OracleWorld:
         return out
 
     def eval(self, q, quantity):
-        nc = 1 if quantity >= abi.Q_EXCHANGE_ENERGY_DENSITY else 3
+        nc = 1 if abi.Q_EXCHANGE_ENERGY_DENSITY <= quantity <= abi.Q_TOTAL_ENERGY_DENSITY else 3
         out = np.empty((nc, *self._shapes[q]), dtype=np.float64)
         self._check(lib().ox_eval(self._h, q, int(quantity), out.ctypes.data))
         return out

@@ -35,6 +35,16 @@ class MagnetSpec:
     anisC2: object = (0.0, 0.0, 0.0)
     stray_source: bool = True
     stray_destination: bool = True
+    pol: object = 0.0
+    xi: object = 0.0
+    Lambda: object = 0.0
+    epsilon_prime: object = 0.0
+    free_layer_thickness: object = None  # None: nz * cellsize z (the reference's default)
+    jcur: object = (0.0, 0.0, 0.0)
+    fixed_layer: object = (0.0, 0.0, 0.0)
+    fixed_layer_on_top: bool = True
+    zhang_li: bool = True
+    slonczewski: bool = True
     frozen: object = 0.0
     dmi: dict = field(default_factory=dict)
     inter_exchange: float = 0.0
@@ -111,6 +121,17 @@ class MagnetSpec:
         d.kc3 = self._scalar(self.kc3, keep)
         d.anis_c1 = self._vector(self.anisC1, keep)
         d.anis_c2 = self._vector(self.anisC2, keep)
+        d.pol = self._scalar(self.pol, keep)
+        d.xi = self._scalar(self.xi, keep)
+        d.lambda_ = self._scalar(self.Lambda, keep)
+        d.epsilon_prime = self._scalar(self.epsilon_prime, keep)
+        flt = self.size[2] * self.cellsize[2] if self.free_layer_thickness is None else self.free_layer_thickness
+        d.free_layer_thickness = self._scalar(flt, keep)
+        d.jcur = self._vector(self.jcur, keep)
+        d.fixed_layer = self._vector(self.fixed_layer, keep)
+        d.fixed_layer_below = 0 if self.fixed_layer_on_top else 1
+        d.zhang_li_off = 0 if self.zhang_li else 1
+        d.slonczewski_off = 0 if self.slonczewski else 1
         d.stray_source_off = 0 if self.stray_source else 1
         d.stray_destination_off = 0 if self.stray_destination else 1
         d.bias_magnetic_field = self._vector(self.bias, keep)
@@ -164,6 +185,17 @@ class MagnetSpec:
         magnet.kc3 = self.kc3
         magnet.anisC1 = self.anisC1
         magnet.anisC2 = self.anisC2
+        magnet.pol = self.pol
+        magnet.xi = self.xi
+        magnet.Lambda = self.Lambda
+        magnet.epsilon_prime = self.epsilon_prime
+        if self.free_layer_thickness is not None:
+            magnet.free_layer_thickness = self.free_layer_thickness
+        magnet.jcur = self.jcur
+        magnet.fixed_layer = self.fixed_layer
+        magnet._fixed_layer_on_top = self.fixed_layer_on_top
+        magnet._enable_zhang_li = self.zhang_li
+        magnet._enable_slonczewski = self.slonczewski
         magnet.bias_magnetic_field = self.bias
         magnet.frozen_spins = self.frozen
         for k, v in self.dmi.items():

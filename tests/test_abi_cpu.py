@@ -66,6 +66,9 @@ int main(void) {
   P(mpx_magnet_desc, geometry) P(mpx_magnet_desc, regions) P(mpx_magnet_desc, msat)
   P(mpx_magnet_desc, anis_u) P(mpx_magnet_desc, bias_magnetic_field) P(mpx_magnet_desc, dmi)
   P(mpx_magnet_desc, lut_regions) P(mpx_magnet_desc, scale_exchange_lut) P(mpx_magnet_desc, enable_openbc)
+  P(mpx_magnet_desc, kc1) P(mpx_magnet_desc, anis_c2) P(mpx_magnet_desc, stray_destination_off)
+  P(mpx_magnet_desc, pol) P(mpx_magnet_desc, jcur) P(mpx_magnet_desc, fixed_layer_below)
+  P(mpx_magnet_desc, slonczewski_off)
   P(mpx_solver_params, max_error) P(mpx_solver_params, sensible_timestep_default)
   P(mpx_group_info, status) P(mpx_group_info, max_torque)
   return 0;

@@ -27,7 +27,7 @@ def compare(spec, mpx, quantities, seed=1, smooth=2, tol=FIELD_TOL):
     eng = magnet._engine
     worst = {}
     for quantity in quantities:
-        nc = 1 if quantity >= abi.Q_EXCHANGE_ENERGY_DENSITY else 3
+        nc = 1 if abi.Q_EXCHANGE_ENERGY_DENSITY <= quantity <= abi.Q_TOTAL_ENERGY_DENSITY else 3
         got = eng.eval(magnet._id, quantity, (nc, *spec.shape))
         want = ow.eval(q, quantity)
         if np.max(np.abs(want)) == 0:
@@ -329,3 +329,37 @@ def test_cubic_anisotropy(mpx, per_cell):
                    kc2=-2e5, kc3=3e4, anisC1=c1, anisC2=c2)
     compare(s, mpx, [abi.Q_ANISOTROPY_FIELD, abi.Q_EFFECTIVE_FIELD, abi.Q_TORQUE, abi.Q_ANISOTROPY_ENERGY_DENSITY,
                      abi.Q_TOTAL_ENERGY_DENSITY])
+
+
+@pytest.mark.parametrize("kind", ["zhangli", "zhangli_pbc", "slonczewski", "slonczewski_below"])
+def test_spin_transfer_torque(mpx, kind):
+    common = dict(size=(24, 12, 3), cellsize=(2e-9, 3e-9, 1e-9), msat=7e5, aex=1.1e-11, alpha=0.05)
+    if kind.startswith("zhangli"):
+        extra = dict(pbc=(1, 0, 0), mastergrid_size=(24, 0, 0)) if kind == "zhangli_pbc" else {}
+        s = MagnetSpec(**common, **extra, pol=0.6, xi=0.1, jcur=(2e11, -1e11, 5e10))
+    else:
+        s = MagnetSpec(**common, pol=0.5, Lambda=1.3, epsilon_prime=0.02, jcur=(0, 0, 3e11),
+                       fixed_layer=(1.0, 0.0, 1.0), fixed_layer_on_top=(kind == "slonczewski"))
+    compare(s, mpx, [abi.Q_SPIN_TRANSFER_TORQUE, abi.Q_LLG_TORQUE, abi.Q_TORQUE])
+
+
+def test_zhang_li_trajectory_vs_oracle(mpx):
+    s = MagnetSpec(size=(32, 8, 1), cellsize=(3e-9, 3e-9, 3e-9), msat=8e5, aex=1.3e-11, alpha=0.05, pol=0.7,
+                   xi=0.05, jcur=(5e11, 0.0, 0.0))
+    m0 = random_m(s.shape, seed=6, smooth=3)
+    ow, q = s.oracle_world(m0)
+    ow.set_method("DormandPrince")
+    world, magnet = s.product(mpx, m0)
+    world.timesolver.set_method("DormandPrince")
+    dt0 = ow.sensible_timestep()
+    ow.timestep = dt0
+    world.timesolver.timestep = dt0
+    worst = 0.0
+    for k in range(1, 5):
+        tp = k * 10e-12
+        ow.run(tp - ow.time)
+        world.timesolver._e.run(world._group, tp - world.timesolver.time)
+        a = np.array(magnet.magnetization.average())
+        b = np.array(ow.average(q, abi.Q_MAGNETIZATION))
+        worst = max(worst, float(np.max(np.abs(a - b))))
+    assert worst < 1e-4, worst

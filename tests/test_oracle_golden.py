@@ -388,3 +388,57 @@ def test_oracle_stray_field_between_magnets_equals_union_demag(oracle):
     ql = alone.add_magnet(B.desc(keep))
     alone.set_m(ql, mB)
     np.testing.assert_array_equal(ow2.eval(qb2, oracle.abi.Q_EFFECTIVE_FIELD), alone.eval(ql, oracle.abi.Q_EFFECTIVE_FIELD))
+
+
+def _stt_numpy(m, spec):
+    """numpy restatement of physics/stt.cu (k_ZhangLi with open edges, no
+    mastergrid; k_Slonczewski) for uniform parameters."""
+    QE, MUB, HBAR, G = 1.60217646e-19, 9.2740091523e-24, 1.054571817e-34, 1.7595e11
+    ms, alpha = spec.msat, spec.alpha
+    j = np.array(spec.jcur, float)
+    if spec.epsilon_prime or (spec.Lambda and spec.pol):  # Slonczewski
+        p = np.array(spec.fixed_layer, float)[:, None, None, None]
+        d = spec.size[2] * spec.cellsize[2] if spec.free_layer_thickness is None else spec.free_layer_thickness
+        d = d if spec.fixed_layer_on_top else -d
+        B = (HBAR / QE) * j[2] / (ms * d)
+        l2 = spec.Lambda ** 2
+        eps = spec.pol * l2 / ((l2 + 1) + (l2 - 1) * np.sum(m * p, axis=0))
+        pxm = np.cross(p, m, axis=0)
+        mxpxm = np.cross(m, pxm, axis=0)
+        return ((eps + spec.epsilon_prime * alpha) * mxpxm + (spec.epsilon_prime - eps * alpha) * pxm) \
+            * B / (1 + alpha ** 2) * G
+    xi = spec.xi
+    u = MUB * spec.pol / (QE * ms * (1 + xi ** 2)) * j
+    hs = np.zeros_like(m)
+    for ax, arr_ax in ((0, 3), (1, 2), (2, 1)):
+        n = m.shape[arr_ax]
+        for sg in (-1, 1):
+            shifted = np.zeros_like(m)
+            src = [slice(None)] * 4
+            dst = [slice(None)] * 4
+            if sg == 1:
+                src[arr_ax], dst[arr_ax] = slice(1, n), slice(0, n - 1)
+            else:
+                src[arr_ax], dst[arr_ax] = slice(0, n - 1), slice(1, n)
+            shifted[tuple(dst)] = m[tuple(src)]
+            hs += sg * u[ax] * shifted / (2 * spec.cellsize[ax])
+    mxh = np.cross(m, hs, axis=0)
+    mxmxh = np.cross(m, mxh, axis=0)
+    return -1 / (1 + alpha ** 2) * ((1 + xi * alpha) * mxmxh + (xi - alpha) * mxh)
+
+
+@pytest.mark.parametrize("kind", ["zhangli", "slonczewski", "slonczewski_below"])
+def test_oracle_spin_transfer_torque_vs_numpy(oracle, kind):
+    common = dict(size=(9, 7, 3), cellsize=(2e-9, 3e-9, 1e-9), msat=7e5, alpha=0.05, enable_demag=False)
+    if kind == "zhangli":
+        s = MagnetSpec(**common, pol=0.6, xi=0.1, jcur=(2e11, -1e11, 5e10))
+    else:
+        s = MagnetSpec(**common, pol=0.5, Lambda=1.3, epsilon_prime=0.02, jcur=(0, 0, 3e11),
+                       fixed_layer=(1.0, 0.0, 1.0), fixed_layer_on_top=(kind == "slonczewski"))
+    ow, q = s.oracle_world(random_m(s.shape, seed=4, smooth=1))
+    m = ow.get_m(q)
+    want = _stt_numpy(m, s)
+    got = ow.eval(q, oracle.abi.Q_SPIN_TRANSFER_TORQUE)
+    np.testing.assert_allclose(got, want, rtol=1e-9, atol=1e-12 * np.abs(want).max())
+    llg = ow.eval(q, oracle.abi.Q_LLG_TORQUE)
+    np.testing.assert_allclose(ow.eval(q, oracle.abi.Q_TORQUE), llg + got, rtol=1e-12, atol=1e-9)

@@ -160,6 +160,10 @@ typedef struct {
   int fixed_layer_below;            /* 0: fixed layer on top (reference default) */
   int zhang_li_off;                 /* enableZhangLiTorque, inverted */
   int slonczewski_off;              /* enableSlonczewskiTorque, inverted */
+  /* thermal noise (physics/thermalnoise.cu): temperature in K and the seed of
+   * the counter-based generator (the reference seeds cuRAND with the clock) */
+  mpx_scalar temperature;
+  uint64_t thermal_seed;
 } mpx_magnet_desc;
 
 /* Time-solver settings (core/timesolver.hpp:74-82 defaults in brackets). */

@@ -104,6 +104,8 @@ class MagnetDesc(C.Structure):
         ("fixed_layer_below", C.c_int),
         ("zhang_li_off", C.c_int),
         ("slonczewski_off", C.c_int),
+        ("temperature", Scalar),
+        ("thermal_seed", C.c_uint64),
     ]
 
 

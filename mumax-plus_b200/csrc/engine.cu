@@ -165,6 +165,7 @@ struct Group {
   std::vector<int> magnets;
   bool active = false;  // started and not yet seen finished: its magnets are in the attempt tables
   int torque_kind = 0;  // 0: LLG torque, 1: damping torque (during relax), mirrors GroupDev::torque_kind
+  int thermal = 0;      // mirrors GroupDev::thermal
 };
 
 }  // namespace
@@ -210,6 +211,7 @@ struct mpx_engine {
   };
   std::vector<Pair> pairs;
   bool pairs_dirty = true;
+  bool any_thermal = false;  // some started group has thermal noise: stage 0 is evaluated every attempt
   // CUDA graphs of one attempt: every stage, and (FSAL methods) without
   // stage 0, whose torque k0 is the last stage of the previous step
   cudaGraphExec_t graph = nullptr, graph_nok0 = nullptr;
@@ -441,6 +443,24 @@ mpx_status rebuild_tables(mpx_engine* e) {
       tl.insert(tl.end(), m->tiles.begin(), m->tiles.end());
     }
   }
+  // groups with thermal noise never reuse k0 (GroupDev::thermal, read by the controller)
+  e->any_thermal = false;
+  for (auto& gp : e->groups) {
+    if (!gp) continue;
+    int th = 0;
+    for (int id : gp->magnets) {
+      Magnet* mm = get_mag(e, id);
+      if (mm && (mm->dev.terms & FLAG_THERMAL)) th = 1;
+    }
+    if (th && gp->active) e->any_thermal = true;
+    if (th != gp->thermal) {
+      GroupDev G;
+      MPX_TRY(read_group(e, gp->slot, &G));
+      G.thermal = th;
+      MPX_TRY(write_group(e, gp->slot, &G));
+      gp->thermal = th;
+    }
+  }
   MPX_TRY(upload_vec(e, &e->d_t_demag, td));
   MPX_TRY(upload_vec(e, &e->d_t_local, tl));
   for (int c = 0; c < 5; ++c) {
@@ -659,6 +679,10 @@ mpx_status load_params(mpx_engine* e, Magnet* m, const mpx_magnet_desc* d) {
   MPX_TRY(load_vector(e, m, &D.jcur, d->jcur, N));
   MPX_TRY(load_vector(e, m, &D.fixl, d->fixed_layer, N));
   D.fl_below = d->fixed_layer_below ? 1 : 0;
+  MPX_TRY(load_scalar(e, m, &D.temp, d->temperature, N));
+  D.seed = d->thermal_seed;
+  // physics/thermalnoise.cu:60-66: 2 kB gamma_LL / cell volume (KB, GAMMALL of physics/constants.hpp)
+  D.noise_pref = (float)(2.0 * 1.38064852e-23 * 1.7595e11 / (d->cellsize[0] * d->cellsize[1] * d->cellsize[2]));
   for (int c = 0; c < 9; ++c) MPX_TRY(load_scalar(e, m, &D.dmi[c], d->dmi[c], N));
   D.inter_u = (float)d->inter_exchange;
   D.scale_u = (float)d->scale_exchange;
@@ -721,6 +745,7 @@ mpx_status load_params(mpx_engine* e, Magnet* m, const mpx_magnet_desc* d) {
                    (scalar_zero(d->epsilon_prime) && (scalar_zero(d->lambda) || scalar_zero(d->pol)));
   if (!sl0) terms |= FLAG_STT_SL;
   else if (!zl0) terms |= FLAG_STT_ZL;
+  if (!scalar_zero(d->temperature) && !msat0) terms |= FLAG_THERMAL;  // physics/thermalnoise.cu:16-18
   const bool wb0 = e->wb[0] == 0 && e->wb[1] == 0 && e->wb[2] == 0;
   if (!(wb0 && vector_zero(d->bias_magnetic_field))) terms |= TERM_EXT;
   if (!vector_zero(d->bias_magnetic_field)) terms |= FLAG_MAGNET_BIAS;
@@ -1072,7 +1097,7 @@ mpx_status run_attempts(mpx_engine* e, int method, int n) {
   }
   const int per_full = attempt_launches(e, T, 0), per_nok0 = attempt_launches(e, T, 1);
   for (int i = 0; i < n; ++i) {
-    const bool full = e->need_stage0 || !e->graph_nok0;
+    const bool full = e->need_stage0 || !e->graph_nok0 || e->any_thermal;
     CUDA_TRY(cudaGraphLaunch(full ? e->graph : e->graph_nok0, e->stream));
     e->launches += full ? per_full : per_nok0;
     e->need_stage0 = false;
@@ -1429,6 +1454,7 @@ mpx_status mpx_magnet_bytes(const mpx_magnet_desc* d, int64_t* resident, int64_t
   for (const mpx_scalar* sc : {&d->pol, &d->xi, &d->lambda, &d->epsilon_prime, &d->free_layer_thickness})
     if (sc->cells) res += 4 * N;
   if (d->jcur.cells) res += 12 * N;
+  if (d->temperature.cells) res += 4 * N;
   if (d->fixed_layer.cells) res += 12 * N;
   for (int c = 0; c < 9; ++c)
     if (d->dmi[c].cells) res += 4 * N;

@@ -438,6 +438,7 @@ __device__ __forceinline__ void epilogue_cell(const MagnetDev& M, const GroupDev
       h = h + bdemag;
       k = G.torque_kind ? damping_torque(mc, h) : llg_torque(mc, h, M.alpha.at(i));
       if (!G.torque_kind && (M.terms & (FLAG_STT_ZL | FLAG_STT_SL))) k = k + stt_torque(M, m, x, y, z, i, mc);
+      if (M.terms & FLAG_THERMAL) k = k + thermal_term(M, i, G.steps, G.dt);
     }
     store3(M.buf[G.map[2 + ea.stage]], N, i, k);
     if (ea.fsal_err && ing) {
@@ -710,7 +711,7 @@ __global__ void k_controller(GroupDev* __restrict__ groups, int ngroups) {
   }
   if (!success) {
     G.rejected++;
-    G.k0_valid = 1;
+    G.k0_valid = G.thermal ? 0 : 1;  // with noise k0 depends on dt (noise / sqrt(dt))
     return;
   }
   // accept: t = t0 + dt; x0 <- x_new; FSAL: k0 <- k_{S-1}
@@ -723,7 +724,7 @@ __global__ void k_controller(GroupDev* __restrict__ groups, int ngroups) {
     const int k0 = G.map[2];
     G.map[2] = G.map[2 + c_tab.S - 1];
     G.map[2 + c_tab.S - 1] = k0;
-    G.k0_valid = 1;
+    G.k0_valid = G.thermal ? 0 : 1;  // a new step draws new noise
   } else {
     G.k0_valid = 0;
   }

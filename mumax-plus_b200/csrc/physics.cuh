@@ -29,7 +29,8 @@ enum : unsigned {
   FLAG_OPENBC = 256u, FLAG_MAGNET_BIAS = 512u,
   FLAG_CUBIC = 1024u,  // the anisotropy term is cubic (uniaxial otherwise)
   FLAG_STRAY = 2048u,  // stray fields of other magnets in `hstray`
-  FLAG_STT_ZL = 4096u, FLAG_STT_SL = 8192u  // spin-transfer torque: Zhang-Li or Slonczewski
+  FLAG_STT_ZL = 4096u, FLAG_STT_SL = 8192u,  // spin-transfer torque: Zhang-Li or Slonczewski
+  FLAG_THERMAL = 16384u  // thermal noise (temperature not zero)
 };
 
 struct DScalar {  // uniform value or per-cell array
@@ -63,6 +64,9 @@ struct MagnetDev {
   DScalar pol, xi, lambda_, epsp, flt;  // spin-transfer torque parameters
   DVector jcur, fixl;
   int fl_below;           // Slonczewski fixed layer below the free layer
+  DScalar temp;           // temperature (K)
+  unsigned long long seed;  // thermal noise generator seed
+  float noise_pref;       // 2 kB gamma_LL / cell volume
   DScalar dmi[9];  // xxy, xxz, xyz, yxy, yxz, yyz, zxy, zxz, zyz
   float inter_u, scale_u;
   const float* __restrict__ inter_lut;
@@ -103,6 +107,7 @@ struct GroupDev {
   int finished_flag;  // set when the group finished, cleared by the host poll
   int map[9];     // buffer roles: [0] x0 (state), [1] xs (stage / new state), [2+s] k_s
   int torque_kind;  // right-hand side of the stages: 0 LLG torque, 1 damping torque only (relax)
+  int thermal;      // some magnet of the group has thermal noise: k0 is never reused
 };
 
 enum { GS_IDLE = 0, GS_RUNNING = 1, GS_FINISHED = 2, GS_FAILED = 3 };
@@ -463,6 +468,32 @@ __device__ __noinline__ float3 stt_torque(const MagnetDev& M, const float* __res
   const float s = -1 / (1 + alpha * alpha);
   return f3(s * ((1 + xi * alpha) * mxmxh.x + (xi - alpha) * mxh.x), s * ((1 + xi * alpha) * mxmxh.y + (xi - alpha) * mxh.y),
             s * ((1 + xi * alpha) * mxmxh.z + (xi - alpha) * mxh.z));
+}
+
+// Standard normal number of (seed, step, cell, component): splitmix64
+// finaliser (Steele, Lea and Flood, OOPSLA 2014) of the combined counter, two
+// 24-bit uniforms, Box-Muller.  The same step gives the same numbers in every
+// stage and every retried attempt (the reference evaluates the noise once per
+// step, core/rungekutta.cpp:94-98).
+__device__ __forceinline__ float thermal_normal(unsigned long long seed, long long step, int i, int c) {
+  unsigned long long z = seed ^ (0x9E3779B97F4A7C15ull * (unsigned long long)(step + 1));
+  z += 0xD1B54A32D192ED03ull * (unsigned long long)(3 * (long long)i + c + 1);
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  z ^= z >> 31;
+  const float u1 = (float)((unsigned)(z >> 40) + 1u) * (1.0f / 16777216.0f);
+  const float u2 = (float)(unsigned)(z & 0xFFFFFFull) * (1.0f / 16777216.0f);
+  return sqrtf(-2.0f * logf(u1)) * cospif(2.0f * u2);
+}
+
+// physics/thermalnoise.cu:20-43: the thermal field of the step times 1/sqrt(dt)
+// (added to every stage, core/rungekutta.cpp:100-106)
+__device__ __noinline__ float3 thermal_term(const MagnetDev& M, int i, long long step, double dt) {
+  const float ms = M.msat.at(i), T = M.temp.at(i), a = M.alpha.at(i);
+  if (ms == 0.f || T == 0.f) return f3(0.f, 0.f, 0.f);
+  const float s = sqrtf(M.noise_pref * a * T / ((1 + a * a) * ms)) * (float)(1.0 / sqrt(dt));
+  return f3(s * thermal_normal(M.seed, step, i, 0), s * thermal_normal(M.seed, step, i, 1),
+            s * thermal_normal(M.seed, step, i, 2));
 }
 
 // physics/torque.cu:58-76 (k_dampingtorque): the relax torque -gamma_LL m x (m x h)

@@ -7,6 +7,7 @@ accelerated path (spin-transfer torque, temperature, magnetoelastics, ...)
 raise NotImplementedError when set to non-zero values.
 """
 import ctypes as C
+import os as _os
 import warnings
 
 import numpy as _np
@@ -75,6 +76,9 @@ class Ferromagnet:
         self._fixed_layer = Parameter(self, "fixed_layer", "", 3, (0.0, 0.0, 0.0), ch)
         self._free_layer_thickness = Parameter(self, "free_layer_thickness", "m", 1,
                                                float(self._grid.size[2] * world.cellsize[2]), ch)
+        self._temperature = Parameter(self, "temperature", "K", 1, 0.0, ch)
+        # the reference seeds its generator from the clock (ferromagnet.cpp:79-81)
+        self._thermal_seed = int.from_bytes(_os.urandom(8), "little")
         self._fixed_layer_on_top = True
         self._enable_zhang_li = True
         self._enable_slonczewski = True
@@ -84,7 +88,7 @@ class Ferromagnet:
         self._enable_demag = True
         self._enable_openbc = False
         self._unsupported = {}
-        for n, nc in (("temperature", 1), ("B1", 1), ("B2", 1), ("conductivity", 1), ("amr_ratio", 1)):
+        for n, nc in (("B1", 1), ("B2", 1), ("conductivity", 1), ("amr_ratio", 1)):
             self._unsupported[n] = _Unsupported(self, n, "", nc, (0.0, 0.0, 0.0) if nc == 3 else 0.0)
         self._suspend = False
         self._id = self._engine.magnet_add(self._group, self._desc())
@@ -153,6 +157,8 @@ class Ferromagnet:
         d.fixed_layer = self._fixed_layer._vector(keep)
         d.fixed_layer_below = 0 if self._fixed_layer_on_top else 1
         d.zhang_li_off = 0 if self._enable_zhang_li else 1
+        d.temperature = self._temperature._scalar(keep)
+        d.thermal_seed = self._thermal_seed
         d.slonczewski_off = 0 if self._enable_slonczewski else 1
         d.stray_source_off = 0 if self._stray_source else 1
         d.stray_destination_off = 0 if self._stray_destination else 1
@@ -284,6 +290,7 @@ class Ferromagnet:
     anisU = _param_prop("_anisU")
     kc1 = _param_prop("_kc1")
     pol = _param_prop("_pol")
+    temperature = _param_prop("_temperature")
     xi = _param_prop("_xi")
     Lambda = _param_prop("_Lambda")
     epsilon_prime = _param_prop("_epsilon_prime")
@@ -452,6 +459,18 @@ class Ferromagnet:
     enable_slonczewski_torque = _flag("_enable_slonczewski", "Slonczewski spin-transfer torque on (default True).")
 
     @property
+    def thermal_seed(self):
+        """Seed of the thermal-noise generator (random at creation; set it for
+        reproducible runs).  The noise of a step is a function of the seed, the
+        step count, the cell and the component."""
+        return self._thermal_seed
+
+    @thermal_seed.setter
+    def thermal_seed(self, value):
+        self._thermal_seed = int(value) & 0xFFFFFFFFFFFFFFFF
+        self._update()
+
+    @property
     def spin_transfer_torque(self):
         """Spin-transfer torque (1/s), physics/stt.cu:143-185."""
         return self._q(_abi.Q_SPIN_TRANSFER_TORQUE, "spintransfer_torque", "1/s")
@@ -506,5 +525,5 @@ def _unsupported_prop(name):
     return property(getter, setter)
 
 
-for _n in ("temperature", "B1", "B2", "conductivity", "amr_ratio"):
+for _n in ("B1", "B2", "conductivity", "amr_ratio"):
     setattr(Ferromagnet, _n, _unsupported_prop(_n))

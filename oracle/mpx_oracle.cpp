@@ -281,6 +281,8 @@ struct Magnet {
   Param pol, xi, lambda, epsp, flt;
   VParam jcur, fixl;
   bool fl_below = false, zl_off = false, sl_off = false;
+  Param temp;
+  uint64_t seed = 0;
   Param dmi[9];
   int lutn = 0;
   double inter_u = 0, scale_u = 1;
@@ -363,6 +365,8 @@ int load_magnet(Magnet& mg, const mpx_magnet_desc* d) {
   mg.fl_below = d->fixed_layer_below != 0;
   mg.zl_off = d->zhang_li_off != 0;
   mg.sl_off = d->slonczewski_off != 0;
+  mg.temp.load(d->temperature, N);
+  mg.seed = d->thermal_seed;
   for (int c = 0; c < 9; ++c) mg.dmi[c].load(d->dmi[c], N);
   mg.lutn = d->lut_regions;
   int L = mg.lutn * (mg.lutn - 1) / 2;
@@ -1074,6 +1078,35 @@ void adapt_timestep(World& w, double corr) {
   w.dt *= corr;
 }
 
+// Standard normal number of (seed, step, cell, component), the generator of the
+// device path restated in FP64: splitmix64 finaliser of the combined counter,
+// two 24-bit uniforms, Box-Muller.
+double thermal_normal(uint64_t seed, long long step, int i, int c) {
+  uint64_t z = seed ^ (0x9E3779B97F4A7C15ull * (uint64_t)(step + 1));
+  z += 0xD1B54A32D192ED03ull * (uint64_t)(3 * (long long)i + c + 1);
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  z ^= z >> 31;
+  const double u1 = (double)((uint32_t)(z >> 40) + 1u) / 16777216.0;
+  const double u2 = (double)(uint32_t)(z & 0xFFFFFFull) / 16777216.0;
+  return std::sqrt(-2.0 * std::log(u1)) * std::cos(2.0 * M_PI * u2);
+}
+
+// physics/thermalnoise.cu:20-66: thermal field of step `step` (zero where T or Ms is 0)
+bool thermal_zero(const Magnet& mg) { return mg.temp.zero() || mg.msat.zero(); }
+void thermal_noise(const Magnet& mg, long long step, std::vector<double>& out) {
+  const int N = mg.N;
+  out.assign(3 * (size_t)N, 0.0);
+  const double pref = 2 * 1.38064852e-23 * GAMMALL / (mg.cs[0] * mg.cs[1] * mg.cs[2]);
+  for (int i = 0; i < N; ++i) {
+    if (!mg.in_geom(i)) continue;
+    const double ms = mg.msat.at(i), T = mg.temp.at(i), a = mg.alpha.at(i);
+    if (ms == 0 || T == 0) continue;
+    const double s = std::sqrt(pref * a * T / ((1 + a * a) * ms));
+    for (int c = 0; c < 3; ++c) out[(size_t)c * N + i] = s * thermal_normal(mg.seed, step, i, c);
+  }
+}
+
 // core/rungekutta.cpp:25-151
 void rk_step(World& w) {
   if (w.mags.empty()) {
@@ -1085,6 +1118,10 @@ void rk_step(World& w) {
   std::vector<std::vector<double>> x0(w.mags.size());
   for (size_t q = 0; q < w.mags.size(); ++q) x0[q] = w.mags[q].m;
   std::vector<std::vector<std::vector<double>>> k(w.mags.size(), std::vector<std::vector<double>>(T.S));
+  // noise of this step, the same for every stage and retry (core/rungekutta.cpp:94-106)
+  std::vector<std::vector<double>> noise(w.mags.size());
+  for (size_t q = 0; q < w.mags.size(); ++q)
+    if (!thermal_zero(w.mags[q])) thermal_noise(w.mags[q], w.steps, noise[q]);
   bool success = false;
   while (!success) {
     const double dt = w.dt;
@@ -1103,7 +1140,13 @@ void rk_step(World& w) {
         }
         set_normalized(mg, xs);
       }
-      for (size_t q = 0; q < w.mags.size(); ++q) torque(w, w.mags[q], k[q][s], w.relax_torque);  // setStageK
+      for (size_t q = 0; q < w.mags.size(); ++q) {  // setStageK
+        torque(w, w.mags[q], k[q][s], w.relax_torque);
+        if (!noise[q].empty()) {
+          const double f = 1 / std::sqrt(dt);
+          for (size_t c = 0; c < noise[q].size(); ++c) k[q][s][c] += f * noise[q][c];
+        }
+      }
     }
     w.t = t0 + dt;
     for (size_t q = 0; q < w.mags.size(); ++q) {  // setFinalX

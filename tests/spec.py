@@ -45,6 +45,8 @@ class MagnetSpec:
     fixed_layer_on_top: bool = True
     zhang_li: bool = True
     slonczewski: bool = True
+    temperature: object = 0.0
+    thermal_seed: int = 12345
     frozen: object = 0.0
     dmi: dict = field(default_factory=dict)
     inter_exchange: float = 0.0
@@ -132,6 +134,8 @@ class MagnetSpec:
         d.fixed_layer_below = 0 if self.fixed_layer_on_top else 1
         d.zhang_li_off = 0 if self.zhang_li else 1
         d.slonczewski_off = 0 if self.slonczewski else 1
+        d.temperature = self._scalar(self.temperature, keep)
+        d.thermal_seed = self.thermal_seed
         d.stray_source_off = 0 if self.stray_source else 1
         d.stray_destination_off = 0 if self.stray_destination else 1
         d.bias_magnetic_field = self._vector(self.bias, keep)
@@ -196,6 +200,8 @@ class MagnetSpec:
         magnet._fixed_layer_on_top = self.fixed_layer_on_top
         magnet._enable_zhang_li = self.zhang_li
         magnet._enable_slonczewski = self.slonczewski
+        magnet.temperature = self.temperature
+        magnet._thermal_seed = self.thermal_seed
         magnet.bias_magnetic_field = self.bias
         magnet.frozen_spins = self.frozen
         for k, v in self.dmi.items():

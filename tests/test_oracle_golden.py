@@ -442,3 +442,41 @@ def test_oracle_spin_transfer_torque_vs_numpy(oracle, kind):
     np.testing.assert_allclose(got, want, rtol=1e-9, atol=1e-12 * np.abs(want).max())
     llg = ow.eval(q, oracle.abi.Q_LLG_TORQUE)
     np.testing.assert_allclose(ow.eval(q, oracle.abi.Q_TORQUE), llg + got, rtol=1e-12, atol=1e-9)
+
+
+def _langevin(x):
+    return 1 / np.tanh(x) - 1 / x
+
+
+def thermal_macrospins(run_steps, mean_mz):
+    """Independent macrospins (no exchange, no demag) in B = 0.1 T along z at
+    20 K: after equilibration <m_z> follows the Langevin function of
+    x = Ms V B / (kB T) (Boltzmann statistics of a classical moment), which pins
+    the amplitude of the thermal field (physics/thermalnoise.cu:60-66)."""
+    ms, cs, b, temp = 8e5, 2e-9, 0.1, 20.0
+    x = ms * cs ** 3 * b / (1.38064852e-23 * temp)
+    spec = MagnetSpec(size=(32, 32, 2), cellsize=(cs, cs, cs), msat=ms, alpha=0.5, temperature=temp,
+                      world_bias=(0.0, 0.0, b), enable_demag=False)
+    run_steps(spec, 2000)  # equilibrate
+    samples = []
+    for _ in range(40):
+        run_steps(spec, 50)
+        samples.append(mean_mz())
+    return float(np.mean(samples)), _langevin(x)
+
+
+def test_oracle_thermal_noise_langevin(oracle):
+    st = {}
+
+    def run_steps(spec, n):
+        if "ow" not in st:
+            m0 = np.zeros((3, *spec.shape), np.float32)
+            m0[2] = 1.0
+            ow, q = spec.oracle_world(m0)
+            ow.set_solver(method=oracle.abi.RK_METHODS["Heun"], adaptive=0)
+            ow.timestep = 2e-13
+            st.update(ow=ow, q=q)
+        st["ow"].steps(n)
+
+    got, want = thermal_macrospins(run_steps, lambda: st["ow"].average(st["q"], oracle.abi.Q_MAGNETIZATION)[2])
+    assert abs(got - want) < 0.02, (got, want)

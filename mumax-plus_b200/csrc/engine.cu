@@ -22,6 +22,7 @@
 #include "kernels.cuh"
 #include "newell.cuh"
 #include "stray.cuh"
+#include "yzsplit.cuh"
 
 using namespace mpx;
 
@@ -142,6 +143,12 @@ struct Magnet {
   bool demag = false;
   int ty = 4;    // rows per x-pass tile
   int nkx = 1;   // consecutive kx per y/z block
+  bool split = false;        // y/z in three passes (k_ycols, k_zmul, k_ycols)
+  int ncy = 1, nkz = 1;      // columns per k_ycols block, ky per k_zmul block
+  float2* tspec = nullptr;
+  int64_t tspec_bytes = 0;
+  std::vector<Work> ycw, zmw;            // k_ycols / k_zmul work items
+  Work *d_ycw = nullptr, *d_zmw = nullptr;
   int P[3] = {1, 1, 1};
   // kernel-defining geometry (rebuild the spectrum when it changes)
   int kkey_n[3], kkey_mg[3], kkey_pbc[3];
@@ -197,6 +204,9 @@ struct mpx_engine {
   int n_kx_demag[5] = {0, 0, 0, 0, 0};
   int smem_yz[5] = {0, 0, 0, 0, 0};
   int maxpy_yz[5] = {0, 0, 0, 0, 0};  // longest y transform of each class
+  // split y/z path over all split magnets
+  Work *d_t_ycols = nullptr, *d_t_zmul = nullptr;
+  int n_t_ycols = 0, n_t_zmul = 0, smem_ycols = 0, smem_zmul = 0, maxpy_split = 0, maxpz_split = 0;
   int smem_x = 0, nt_x = 256;
   bool any_nodemag = false;
   int64_t bytes = 0;
@@ -279,6 +289,13 @@ void release_all(mpx_engine* e, Magnet* m) {
   pfree(e, m->hstray);
   m->hstray = nullptr;
   e->pairs_dirty = true;
+  pfree(e, m->tspec);
+  e->bytes -= m->tspec_bytes;
+  m->tspec = nullptr;
+  m->tspec_bytes = 0;
+  pfree(e, m->d_ycw);
+  pfree(e, m->d_zmw);
+  m->d_ycw = m->d_zmw = nullptr;
   pfree(e, m->fields);
   pfree(e, m->spec);
   pfree(e, m->kspec);
@@ -398,6 +415,30 @@ int choose_nkx(int nz, int Py, int Fh) {
 
 // k_yz<PZ> launch for one z-length class
 // (the radix-8 variant for z lengths up to 8 when every y length of the class is <= 2048)
+int ycols_smem(const Magnet* m) { return (m->ncy * plen(m->P[1]) + m->P[1]) * (int)sizeof(float2); }
+int zmul_smem(const Magnet* m) { return (3 * m->nkz * plen(m->P[2]) + m->P[2]) * (int)sizeof(float2); }
+
+// The three passes of the split y/z path (radix-8 forms when the lengths allow).
+mpx_status launch_split(mpx_engine* e, const Work* ycw, int nyc, const Work* zmw, int nzm, int smem_y, int smem_z,
+                        int max_py, int max_pz, int stage, int gate) {
+  if (nyc <= 0) return MPX_OK;
+  const bool ry = max_py <= 2048, rz = max_pz <= 2048;
+  if (ry)
+    k_ycols<-1, 3><<<nyc, YZ_THREADS, smem_y, e->stream>>>(e->d_mags, e->d_groups, ycw, stage, gate, e->d_tw);
+  else
+    k_ycols<-1, 4><<<nyc, YZ_THREADS, smem_y, e->stream>>>(e->d_mags, e->d_groups, ycw, stage, gate, e->d_tw);
+  if (rz)
+    k_zmul<3><<<nzm, YZ_THREADS, smem_z, e->stream>>>(e->d_mags, e->d_groups, zmw, stage, gate, e->d_tw);
+  else
+    k_zmul<4><<<nzm, YZ_THREADS, smem_z, e->stream>>>(e->d_mags, e->d_groups, zmw, stage, gate, e->d_tw);
+  if (ry)
+    k_ycols<1, 3><<<nyc, YZ_THREADS, smem_y, e->stream>>>(e->d_mags, e->d_groups, ycw, stage, gate, e->d_tw);
+  else
+    k_ycols<1, 4><<<nyc, YZ_THREADS, smem_y, e->stream>>>(e->d_mags, e->d_groups, ycw, stage, gate, e->d_tw);
+  e->launches += 3;
+  return MPX_OK;
+}
+
 mpx_status launch_yz(mpx_engine* e, int cls, const Work* work, int n, int smem, int stage, int gate, int max_py) {
   if (n <= 0) return MPX_OK;
   const bool r8 = max_py <= 2048;
@@ -421,7 +462,8 @@ int x_threads(const Magnet* m) {
 }
 
 mpx_status rebuild_tables(mpx_engine* e) {
-  std::vector<Work> td, tl, kd[5];
+  std::vector<Work> td, tl, kd[5], yc, zm;
+  e->smem_ycols = e->smem_zmul = e->maxpy_split = e->maxpz_split = 0;
   e->smem_x = 0;
   e->nt_x = 256;
   for (int c = 0; c < 5; ++c) e->smem_yz[c] = e->maxpy_yz[c] = 0;
@@ -432,12 +474,21 @@ mpx_status rebuild_tables(mpx_engine* e) {
     const Group* g = (m->group >= 0 && m->group < (int)e->groups.size()) ? e->groups[m->group].get() : nullptr;
     if (!g || !g->active) continue;
     if (m->demag) {
-      const int cls = yz_class(m);
       td.insert(td.end(), m->tiles.begin(), m->tiles.end());
-      kd[cls].insert(kd[cls].end(), m->kxw.begin(), m->kxw.end());
       e->smem_x = std::max(e->smem_x, x_smem(m));
-      e->smem_yz[cls] = std::max(e->smem_yz[cls], yz_smem(m));
-      e->maxpy_yz[cls] = std::max(e->maxpy_yz[cls], m->P[1]);
+      if (m->split) {
+        yc.insert(yc.end(), m->ycw.begin(), m->ycw.end());
+        zm.insert(zm.end(), m->zmw.begin(), m->zmw.end());
+        e->smem_ycols = std::max(e->smem_ycols, ycols_smem(m));
+        e->smem_zmul = std::max(e->smem_zmul, zmul_smem(m));
+        e->maxpy_split = std::max(e->maxpy_split, m->P[1]);
+        e->maxpz_split = std::max(e->maxpz_split, m->P[2]);
+      } else {
+        const int cls = yz_class(m);
+        kd[cls].insert(kd[cls].end(), m->kxw.begin(), m->kxw.end());
+        e->smem_yz[cls] = std::max(e->smem_yz[cls], yz_smem(m));
+        e->maxpy_yz[cls] = std::max(e->maxpy_yz[cls], m->P[1]);
+      }
       e->nt_x = std::max(e->nt_x, x_threads(m));
     } else {
       tl.insert(tl.end(), m->tiles.begin(), m->tiles.end());
@@ -463,6 +514,10 @@ mpx_status rebuild_tables(mpx_engine* e) {
   }
   MPX_TRY(upload_vec(e, &e->d_t_demag, td));
   MPX_TRY(upload_vec(e, &e->d_t_local, tl));
+  MPX_TRY(upload_vec(e, &e->d_t_ycols, yc));
+  MPX_TRY(upload_vec(e, &e->d_t_zmul, zm));
+  e->n_t_ycols = (int)yc.size();
+  e->n_t_zmul = (int)zm.size();
   for (int c = 0; c < 5; ++c) {
     MPX_TRY(upload_vec(e, &e->d_kx_demag[c], kd[c]));
     e->n_kx_demag[c] = (int)kd[c].size();
@@ -863,13 +918,20 @@ mpx_status setup_magnet(mpx_engine* e, Magnet* m, const mpx_magnet_desc* d, bool
   D.kcomp = (m->P[2] == 1) ? 4 : 6;
   m->ty = choose_ty(D.n[1], m->demag ? m->P[0] : D.n[0]);
   m->nkx = m->demag ? choose_nkx(D.n[2], m->P[1], D.Fh) : 1;
+  m->split = false;
   if (m->demag) {
     if (m->P[0] > X_VPT * X_THREADS_MAX || m->P[1] > std::min(MAX_FFT, YZ_VPT * YZ_THREADS))
       return fail(MPX_ERR_UNSUPPORTED, "demag: padded FFT length above 2048 along x or 4096 along y "
                                        "(grid side above 1024 along x or 2048 along y)");
-    if (m->P[2] > 16) return fail(MPX_ERR_UNSUPPORTED, "demag: nz > 8 is not implemented by the fused y/z pass");
-    if (yz_smem(m) > SMEM_DYN_MAX)
-      return fail(MPX_ERR_UNSUPPORTED, "demag: 3*nz*Py complex values exceed shared memory (nz*Py > 9472)");
+    // thick magnets (nz > 8) and long y transforms of many columns take the split y/z path
+    m->split = m->P[2] > 16 || yz_smem(m) > SMEM_DYN_MAX;
+    if (m->split) {
+      if (m->P[2] > MAX_FFT) return fail(MPX_ERR_UNSUPPORTED, "demag: padded FFT length above 4096 along z");
+      m->ncy = std::max(1, std::min(D.Fh * 3 * D.n[2], (YZ_VPT * YZ_THREADS) / m->P[1]));
+      m->nkz = std::max(1, std::min(m->P[1], (YZ_VPT * YZ_THREADS) / (3 * m->P[2])));
+      if (ycols_smem(m) > SMEM_DYN_MAX || zmul_smem(m) > SMEM_DYN_MAX)
+        return fail(MPX_ERR_UNSUPPORTED, "demag: y/z transforms exceed shared memory");
+    }
     if (x_smem(m) > SMEM_DYN_MAX) return fail(MPX_ERR_UNSUPPORTED, "demag: x-pass tile exceeds shared memory");
   }
   // field buffers (9 x 3N floats) and spectrum
@@ -888,6 +950,18 @@ mpx_status setup_magnet(mpx_engine* e, Magnet* m, const mpx_magnet_desc* d, bool
   }
   m->spec = old_spec;
   D.spec = old_spec;
+  // split path: the y-transformed spectrum (no state kept between evaluations)
+  pfree(e, m->tspec);
+  e->bytes -= m->tspec_bytes;
+  m->tspec = nullptr;
+  m->tspec_bytes = 0;
+  if (m->demag && m->split) {
+    const size_t tb = sizeof(float2) * (size_t)D.Fh * 3 * D.n[2] * m->P[1];
+    MPX_TRY(palloc(e, (void**)&m->tspec, tb));
+    m->tspec_bytes = (int64_t)tb;
+    e->bytes += (int64_t)tb;
+  }
+  D.tspec = m->tspec;
   const size_t kbytes = sizeof(float) * (size_t)D.Fh * (m->P[1] / 2 + 1) * (m->P[2] / 2 + 1) * D.kcomp;
   if (m->demag && !old_kspec) {
     MPX_TRY(dalloc(e, nullptr, (void**)&old_kspec, kbytes));
@@ -913,6 +987,15 @@ mpx_status setup_magnet(mpx_engine* e, Magnet* m, const mpx_magnet_desc* d, bool
     for (int y0 = 0; y0 < D.n[1]; y0 += m->ty) m->tiles.push_back(Work{m->slot, z, y0, std::min(m->ty, D.n[1] - y0)});
   if (m->demag)
     for (int kx = 0; kx < D.Fh; kx += m->nkx) m->kxw.push_back(Work{m->slot, kx, std::min(m->nkx, D.Fh - kx), 0});
+  m->ycw.clear();
+  m->zmw.clear();
+  if (m->demag && m->split) {
+    const int ncols = D.Fh * 3 * D.n[2];
+    for (int c0 = 0; c0 < ncols; c0 += m->ncy) m->ycw.push_back(Work{m->slot, c0, std::min(m->ncy, ncols - c0), 0});
+    for (int kx = 0; kx < D.Fh; ++kx)
+      for (int ky0 = 0; ky0 < m->P[1]; ky0 += m->nkz)
+        m->zmw.push_back(Work{m->slot, kx, ky0, std::min(m->nkz, m->P[1] - ky0)});
+  }
   {
     pfree(e, m->d_tiles);
     pfree(e, m->d_kxw);
@@ -920,6 +1003,8 @@ mpx_status setup_magnet(mpx_engine* e, Magnet* m, const mpx_magnet_desc* d, bool
     m->d_kxw = nullptr;
     MPX_TRY(upload_vec(e, &m->d_tiles, m->tiles));
     MPX_TRY(upload_vec(e, &m->d_kxw, m->kxw));
+    MPX_TRY(upload_vec(e, &m->d_ycw, m->ycw));
+    MPX_TRY(upload_vec(e, &m->d_zmw, m->zmw));
   }
   MPX_TRY(upload_magnet_desc(e, m));
   e->tables_dirty = true;
@@ -972,7 +1057,11 @@ mpx_status eval_into(mpx_engine* e, Magnet* m, int q, float* out) {
   if (m->demag && needs_demag) {
     const int sx = x_smem(m), syz = yz_smem(m), nt = x_threads(m);
     k_xfwd<false><<<ntile, nt, sx, e->stream>>>(e->d_mags, e->d_groups, m->d_tiles, 0, 0, nullptr, e->d_tw);
-    MPX_TRY(launch_yz(e, yz_class(m), m->d_kxw, (int)m->kxw.size(), syz, 0, 0, m->P[1]));
+    if (m->split)
+      MPX_TRY(launch_split(e, m->d_ycw, (int)m->ycw.size(), m->d_zmw, (int)m->zmw.size(), ycols_smem(m),
+                           zmul_smem(m), m->P[1], m->P[2], 0, 0));
+    else
+      MPX_TRY(launch_yz(e, yz_class(m), m->d_kxw, (int)m->kxw.size(), syz, 0, 0, m->P[1]));
     k_xinv<<<ntile, nt, sx, e->stream>>>(e->d_mags, e->d_groups, m->d_tiles, ea, e->d_tw);
     e->launches += 2;
   } else {
@@ -1013,6 +1102,8 @@ mpx_status launch_attempt(mpx_engine* e, const TableauDev& T, int first_stage) {
     if (e->n_t_demag > 0) {
       for (int c = 0; c < 5; ++c)
         MPX_TRY(launch_yz(e, c, e->d_kx_demag[c], e->n_kx_demag[c], e->smem_yz[c], s, 1, e->maxpy_yz[c]));
+      MPX_TRY(launch_split(e, e->d_t_ycols, e->n_t_ycols, e->d_t_zmul, e->n_t_zmul, e->smem_ycols, e->smem_zmul,
+                           e->maxpy_split, e->maxpz_split, s, 1));
       k_xinv<<<e->n_t_demag, e->nt_x, e->smem_x, e->stream>>>(e->d_mags, e->d_groups, e->d_t_demag, ea, e->d_tw);
       e->launches++;
     }
@@ -1072,6 +1163,7 @@ int attempt_launches(const mpx_engine* e, const TableauDev& T, int first_stage) 
   const int S = T.S, ns = S - first_stage;
   int nyz = 0;
   for (int c = 0; c < 5; ++c) nyz += e->n_kx_demag[c] > 0 ? 1 : 0;
+  if (e->n_t_ycols > 0) nyz += 3;
   int per = 1 + (int)e->pairs.size() * ns;  // controller, stray-field pairs
   if (e->n_t_demag > 0) per += (2 + nyz) * ns + (T.fsal ? 0 : 1);
   if (e->n_t_local > 0) per += ns + (ns - (first_stage == 0 ? 1 : 0)) + (T.fsal ? 0 : 1);
@@ -1230,7 +1322,9 @@ mpx_status mpx_engine_create(int device, mpx_engine** out) {
   const void* fft_kernels[] = {(const void*)k_xfwd<false>, (const void*)k_xfwd<true>, (const void*)k_xinv,
                                (const void*)k_yz<1, 4>, (const void*)k_yz<2, 4>, (const void*)k_yz<4, 4>,
                                (const void*)k_yz<8, 4>, (const void*)k_yz<16, 4>, (const void*)k_yz<1, 3>,
-                               (const void*)k_yz<2, 3>, (const void*)k_yz<4, 3>, (const void*)k_yz<8, 3>};
+                               (const void*)k_yz<2, 3>, (const void*)k_yz<4, 3>, (const void*)k_yz<8, 3>,
+                               (const void*)k_ycols<-1, 3>, (const void*)k_ycols<-1, 4>, (const void*)k_ycols<1, 3>,
+                               (const void*)k_ycols<1, 4>, (const void*)k_zmul<3>, (const void*)k_zmul<4>};
   for (const void* k : fft_kernels) {
     cudaFuncAttributes fa;
     CUDA_TRY(cudaFuncGetAttributes(&fa, k));
@@ -1477,6 +1571,13 @@ mpx_status mpx_magnet_bytes(const mpx_magnet_desc* d, int64_t* resident, int64_t
     res += 4 * Fh * (P[1] / 2 + 1) * (P[2] / 2 + 1) * kc;        // kernel spectrum
     const int nkx = choose_nkx(d->size[2], P[1], (int)Fh);
     res += (int64_t)sizeof(Work) * ((Fh + nkx - 1) / nkx);       // y/z work items
+    const int yzs = (d->size[2] * 3 * nkx * plen(P[1]) + P[1]) * (int)sizeof(float2);
+    if (P[2] > 16 || yzs > SMEM_DYN_MAX) {  // split y/z path: T and its work items
+      res += 8 * Fh * 3 * d->size[2] * P[1];
+      const int64_t ncy = std::max<int64_t>(1, std::min<int64_t>(Fh * 3 * d->size[2], (YZ_VPT * YZ_THREADS) / P[1]));
+      const int64_t nkz = std::max(1, std::min(P[1], (YZ_VPT * YZ_THREADS) / (3 * P[2])));
+      res += (int64_t)sizeof(Work) * ((Fh * 3 * d->size[2] + ncy - 1) / ncy + Fh * ((P[1] + nkz - 1) / nkz));
+    }
     tr += 8 * 6 * N + 2 * 16 * (int64_t)P[0] * P[1] * P[2];    // FP64 octant + two transform buffers
   }
   *resident = res;
@@ -1622,7 +1723,11 @@ mpx_status mpx_profile_eval(mpx_engine* e, int magnet, int reps, double ms[4]) {
       CUDA_TRY(cudaEventRecord(ev[0], e->stream));
       k_xfwd<false><<<ntile, nt, sx, e->stream>>>(e->d_mags, e->d_groups, m->d_tiles, 0, 0, nullptr, e->d_tw);
       CUDA_TRY(cudaEventRecord(ev[1], e->stream));
-      MPX_TRY(launch_yz(e, yz_class(m), m->d_kxw, (int)m->kxw.size(), syz, 0, 0, m->P[1]));
+      if (m->split)
+        MPX_TRY(launch_split(e, m->d_ycw, (int)m->ycw.size(), m->d_zmw, (int)m->zmw.size(), ycols_smem(m),
+                             zmul_smem(m), m->P[1], m->P[2], 0, 0));
+      else
+        MPX_TRY(launch_yz(e, yz_class(m), m->d_kxw, (int)m->kxw.size(), syz, 0, 0, m->P[1]));
       CUDA_TRY(cudaEventRecord(ev[2], e->stream));
       k_xinv<<<ntile, nt, sx, e->stream>>>(e->d_mags, e->d_groups, m->d_tiles, ea, e->d_tw);
       CUDA_TRY(cudaEventRecord(ev[3], e->stream));

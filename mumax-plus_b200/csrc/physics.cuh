@@ -78,6 +78,7 @@ struct MagnetDev {
   int logP[3], P[3], Fh;
   int kcomp;         // 6 (3-D kernel) or 4 (Pz == 1)
   float2* spec;      // spectrum S[kx][c][z][y]
+  float2* tspec;     // split y/z path: y-transformed spectrum T[kx][c][z][ky] (Py rows), else NULL
   const float* __restrict__ kspec;  // kernel spectrum [kx][kz'][kcomp][ky']
   float* buf[9];     // field buffers (3N floats each); roles given by the group map
   const float* hstray;  // stray field of the other magnets of the world (3N), or NULL

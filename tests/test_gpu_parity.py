@@ -363,3 +363,28 @@ def test_zhang_li_trajectory_vs_oracle(mpx):
         b = np.array(ow.average(q, abi.Q_MAGNETIZATION))
         worst = max(worst, float(np.max(np.abs(a - b))))
     assert worst < 1e-4, worst
+
+
+@pytest.mark.parametrize("size", [(16, 8, 16), (12, 6, 9), (8, 4, 33), (40, 7, 20), (24, 20, 12)])
+def test_demag_thick_magnets_split_path(mpx, size):
+    """nz > 8 takes the three-pass y/z path (k_ycols, k_zmul, k_ycols)."""
+    compare(MagnetSpec(size=size, cellsize=(1e-9, 2e-9, 1.5e-9), msat=8e5), mpx, [abi.Q_DEMAG_FIELD])
+
+
+def test_thick_magnet_pbc_and_trajectory(mpx):
+    s = MagnetSpec(size=(16, 12, 10), cellsize=(2e-9, 2e-9, 2e-9), msat=8e5, aex=1.3e-11, alpha=0.2,
+                   pbc=(1, 0, 1), mastergrid_size=(16, 0, 10), world_bias=(0.0, 0.01, 0.02))
+    compare(s, mpx, [abi.Q_DEMAG_FIELD, abi.Q_EFFECTIVE_FIELD])
+    m0 = random_m(s.shape, seed=9, smooth=3)
+    ow, q = s.oracle_world(m0)
+    ow.set_method("DormandPrince")
+    world, magnet = s.product(mpx, m0)
+    world.timesolver.set_method("DormandPrince")
+    dt0 = ow.sensible_timestep()
+    ow.timestep = dt0
+    world.timesolver.timestep = dt0
+    ow.run(10e-12)
+    world.timesolver._e.run(world._group, 10e-12)
+    a = np.array(magnet.magnetization.average())
+    b = np.array(ow.average(q, abi.Q_MAGNETIZATION))
+    assert float(np.max(np.abs(a - b))) < 1e-4

@@ -143,6 +143,7 @@ struct Magnet {
   bool demag = false;
   int ty = 4;    // rows per x-pass tile
   int nkx = 1;   // consecutive kx per y/z block
+  int ty_def = 4, nkx_def = 1;  // the shapes for a magnet launched with many others
   bool split = false;        // y/z in three passes (k_ycols, k_zmul, k_ycols)
   int ncy = 1, nkz = 1;      // columns per k_ycols block, ky per k_zmul block
   float2* tspec = nullptr;
@@ -461,7 +462,76 @@ int x_threads(const Magnet* m) {
   return std::min(X_THREADS_MAX, std::max(64, t));
 }
 
+// Tile shapes for magnets launched together: from each magnet's default
+// (about 4096 points per x tile, 6144 per y/z block), halve the rows per tile
+// and the kx per block, all magnets alike, while the launch would have fewer
+// than two blocks per SM; small single solves then spread over the GPU and
+// large batches keep their large tiles.
+constexpr int SHAPE_MIN_BLOCKS = 2 * 148;
+void plan_shapes(const std::vector<Magnet*>& ms, int* ty, int* nkx) {
+  std::vector<int> t(ms.size()), k(ms.size());
+  for (size_t i = 0; i < ms.size(); ++i) {
+    t[i] = ms[i]->ty_def;
+    k[i] = ms[i]->nkx_def;
+  }
+  for (;;) {
+    long long blocks = 0;
+    bool shrink = false;
+    for (size_t i = 0; i < ms.size(); ++i) {
+      blocks += (long long)ms[i]->dev.n[2] * ((ms[i]->dev.n[1] + t[i] - 1) / t[i]);
+      shrink = shrink || t[i] > 1;
+    }
+    if (blocks >= SHAPE_MIN_BLOCKS || !shrink) break;
+    for (auto& v : t) v = std::max(1, v / 2);
+  }
+  for (;;) {
+    long long blocks = 0;
+    bool shrink = false;
+    for (size_t i = 0; i < ms.size(); ++i) {
+      if (!ms[i]->demag || ms[i]->split) continue;
+      blocks += (ms[i]->dev.Fh + k[i] - 1) / k[i];
+      shrink = shrink || k[i] > 1;
+    }
+    if (blocks >= SHAPE_MIN_BLOCKS || !shrink) break;
+    for (auto& v : k) v = std::max(1, v / 2);
+  }
+  for (size_t i = 0; i < ms.size(); ++i) {
+    ty[i] = t[i];
+    nkx[i] = k[i];
+  }
+}
+
+// Rebuilds the row tiles and y/z work items of m for the given shapes, with its
+// own device tables (the per-magnet evaluation path).
+mpx_status retile(mpx_engine* e, Magnet* m, int ty, int nkx) {
+  const MagnetDev& D = m->dev;
+  m->ty = ty;
+  m->nkx = nkx;
+  m->tiles.clear();
+  m->kxw.clear();
+  for (int z = 0; z < D.n[2]; ++z)
+    for (int y0 = 0; y0 < D.n[1]; y0 += m->ty) m->tiles.push_back(Work{m->slot, z, y0, std::min(m->ty, D.n[1] - y0)});
+  if (m->demag)
+    for (int kx = 0; kx < D.Fh; kx += m->nkx) m->kxw.push_back(Work{m->slot, kx, std::min(m->nkx, D.Fh - kx), 0});
+  MPX_TRY(upload_vec(e, &m->d_tiles, m->tiles));
+  MPX_TRY(upload_vec(e, &m->d_kxw, m->kxw));
+  return MPX_OK;
+}
+
 mpx_status rebuild_tables(mpx_engine* e) {
+  {  // shapes for the set of magnets launched together
+    std::vector<Magnet*> act;
+    for (auto& mp : e->mags) {
+      if (!mp) continue;
+      const Group* g =
+          (mp->group >= 0 && mp->group < (int)e->groups.size()) ? e->groups[mp->group].get() : nullptr;
+      if (g && g->active) act.push_back(mp.get());
+    }
+    std::vector<int> ty(act.size()), nkx(act.size());
+    plan_shapes(act, ty.data(), nkx.data());
+    for (size_t i = 0; i < act.size(); ++i)
+      if (ty[i] != act[i]->ty || nkx[i] != act[i]->nkx) MPX_TRY(retile(e, act[i], ty[i], nkx[i]));
+  }
   std::vector<Work> td, tl, kd[5], yc, zm;
   e->smem_ycols = e->smem_zmul = e->maxpy_split = e->maxpz_split = 0;
   e->smem_x = 0;
@@ -916,8 +986,11 @@ mpx_status setup_magnet(mpx_engine* e, Magnet* m, const mpx_magnet_desc* d, bool
   }
   D.Fh = m->P[0] / 2 + 1;
   D.kcomp = (m->P[2] == 1) ? 4 : 6;
-  m->ty = choose_ty(D.n[1], m->demag ? m->P[0] : D.n[0]);
-  m->nkx = m->demag ? choose_nkx(D.n[2], m->P[1], D.Fh) : 1;
+  m->ty_def = choose_ty(D.n[1], m->demag ? m->P[0] : D.n[0]);
+  m->nkx_def = m->demag ? choose_nkx(D.n[2], m->P[1], D.Fh) : 1;
+  m->ty = m->ty_def;
+  m->nkx = m->nkx_def;
+  plan_shapes({m}, &m->ty, &m->nkx);  // alone (plain evaluations, single solves)
   m->split = false;
   if (m->demag) {
     if (m->P[0] > X_VPT * X_THREADS_MAX || m->P[1] > std::min(MAX_FFT, YZ_VPT * YZ_THREADS))
@@ -981,12 +1054,7 @@ mpx_status setup_magnet(mpx_engine* e, Magnet* m, const mpx_magnet_desc* d, bool
     MPX_TRY(build_kernel_spectrum(e, m));
   }
   // tiles
-  m->tiles.clear();
-  m->kxw.clear();
-  for (int z = 0; z < D.n[2]; ++z)
-    for (int y0 = 0; y0 < D.n[1]; y0 += m->ty) m->tiles.push_back(Work{m->slot, z, y0, std::min(m->ty, D.n[1] - y0)});
-  if (m->demag)
-    for (int kx = 0; kx < D.Fh; kx += m->nkx) m->kxw.push_back(Work{m->slot, kx, std::min(m->nkx, D.Fh - kx), 0});
+  MPX_TRY(retile(e, m, m->ty, m->nkx));
   m->ycw.clear();
   m->zmw.clear();
   if (m->demag && m->split) {
@@ -996,16 +1064,8 @@ mpx_status setup_magnet(mpx_engine* e, Magnet* m, const mpx_magnet_desc* d, bool
       for (int ky0 = 0; ky0 < m->P[1]; ky0 += m->nkz)
         m->zmw.push_back(Work{m->slot, kx, ky0, std::min(m->nkz, m->P[1] - ky0)});
   }
-  {
-    pfree(e, m->d_tiles);
-    pfree(e, m->d_kxw);
-    m->d_tiles = nullptr;
-    m->d_kxw = nullptr;
-    MPX_TRY(upload_vec(e, &m->d_tiles, m->tiles));
-    MPX_TRY(upload_vec(e, &m->d_kxw, m->kxw));
-    MPX_TRY(upload_vec(e, &m->d_ycw, m->ycw));
-    MPX_TRY(upload_vec(e, &m->d_zmw, m->zmw));
-  }
+  MPX_TRY(upload_vec(e, &m->d_ycw, m->ycw));
+  MPX_TRY(upload_vec(e, &m->d_zmw, m->zmw));
   MPX_TRY(upload_magnet_desc(e, m));
   e->tables_dirty = true;
   return MPX_OK;

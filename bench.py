@@ -445,6 +445,15 @@ def run_batched(args):
     p_upd = sum(s.cells * s.steps for s in psol)
     same = {s.key: s for s in solves}
     worst = max(float(np.max(np.abs(same[k * i].m - p.m))) for i, p in enumerate(psol))
+    # per-kernel time of one attempt stage over the whole started batch
+    kb = B.Batch(device=local)
+    started = [kb.add(w, key=i) for i, w in enumerate(insts)]
+    for s in started:
+        kb.start(s, 1e-9, 0.0)
+    kb.advance(2)
+    kb.poll()
+    kms = kb.engine.profile_attempt("DormandPrince", reps=5)
+    del kb, started
     if rank == 0:
         value = world_size * upd / t_run_max
         plain = p_upd / p_run
@@ -466,6 +475,9 @@ def run_batched(args):
             "plain": {"instances": len(sub), "cell_updates": p_upd, "seconds": p_run, "setup_seconds": p_setup,
                       "value": plain, "unit": "cell-updates/s"},
             "batched_over_plain": value / world_size / plain,
+            "stage_kernel_ms": {"combine+x_forward": kms[0], "stray_pairs": kms[1], "y_z": kms[2],
+                                "x_inverse+epilogue": kms[3], "note": "one stage (of 6 per accepted step) over all "
+                                                                      "256 started solves"},
             "max_abs_dm_batched_vs_plain": worst,
             "e2e": {"value": world_size * upd / t_e2e_max, "unit": "cell-updates/s",
                     "h2d_bytes_per_step": int(sum(12 * s.cells for s in solves)),

@@ -251,6 +251,15 @@ mpx_status mpx_energy(mpx_engine* e, int magnet, int quantity, double* out);
  * magnet does not use).  No reference counterpart (FieldQuantity::_bench times
  * the whole evaluation, mumaxplus/fieldquantity.py:111-118). */
 mpx_status mpx_profile_eval(mpx_engine* e, int magnet, int reps, double ms[4]);
+/* Measurement of the batched launches: times, with CUDA events, the kernels of
+ * stage 1 of one Runge-Kutta attempt over every started group (the launch
+ * tables of mpx_advance), `reps` times after one warm-up, without the step
+ * controller, and writes the mean milliseconds of [stage combination + x-forward
+ * (or k_combine), stray-field pairs, y/z passes (all z classes and the split
+ * path), x-inverse + epilogue (or k_local)].  Stage 1 only writes the stage
+ * state and k_1, which the next attempt recomputes; the solves do not advance.
+ * Needs the method the groups run with.  No reference counterpart. */
+mpx_status mpx_profile_attempt(mpx_engine* e, int method, int reps, double ms[4]);
 /* Real-space demag kernel, 6*K floats on the reference's kernel grid
  * (physics/strayfieldkernel.cu:80-99; bindings/wrap_magnet.cpp:56-59).
  * dims receives the kernel grid size (Kx, Ky, Kz). Pass out=NULL to query dims. */

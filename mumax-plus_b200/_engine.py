@@ -164,6 +164,13 @@ class Engine:
         check(lib().mpx_profile_eval(self._h, int(magnet), int(reps), out))
         return [out[i] for i in range(4)]
 
+    def profile_attempt(self, method="DormandPrince", reps=5):
+        """Mean ms of [combination + x-forward, stray pairs, y/z passes, x-inverse +
+        epilogue] of stage 1 over every started group."""
+        out = (C.c_double * 4)()
+        check(lib().mpx_profile_attempt(self._h, _abi.RK_METHODS[method], int(reps), out))
+        return [out[i] for i in range(4)]
+
     def demag_kernel(self, magnet):
         dims = (C.c_int * 3)()
         check(lib().mpx_demag_kernel(self._h, int(magnet), None, dims))

@@ -406,9 +406,14 @@ constexpr int YZ_THREADS = 384;
 // tile (4 rows from Px = 1024 up; up to TY_MAX rows of short transforms), or
 // of the row itself without demag.  y/z blocks: enough consecutive kx that a
 // block holds about YZ_VPT * YZ_THREADS points of y transforms.
+// Rows per tile are even (or the single row of ny = 1): the x passes pack the
+// z components of rows 2k and 2k+1 into one complex FFT, so tiles that start
+// on even rows give every magnet the same arithmetic whatever its tiling (the
+// same results alone and in any batch).
+int even_rows(int t, int ny) { return ny <= 1 ? 1 : std::max(2, t & ~1); }
 int choose_ty(int ny, int len) {
   const int t = len >= 1024 ? 4 : std::min(TY_MAX, std::max(1, 4096 / len));
-  return std::max(1, std::min(t, ny));
+  return even_rows(std::max(1, std::min(t, ny)), ny);
 }
 int choose_nkx(int nz, int Py, int Fh) {
   return std::max(1, std::min(Fh, (YZ_VPT * YZ_THREADS) / (3 * nz * Py)));
@@ -479,10 +484,10 @@ void plan_shapes(const std::vector<Magnet*>& ms, int* ty, int* nkx) {
     bool shrink = false;
     for (size_t i = 0; i < ms.size(); ++i) {
       blocks += (long long)ms[i]->dev.n[2] * ((ms[i]->dev.n[1] + t[i] - 1) / t[i]);
-      shrink = shrink || t[i] > 1;
+      shrink = shrink || t[i] > even_rows(1, ms[i]->dev.n[1]);
     }
     if (blocks >= SHAPE_MIN_BLOCKS || !shrink) break;
-    for (auto& v : t) v = std::max(1, v / 2);
+    for (size_t i = 0; i < ms.size(); ++i) t[i] = even_rows(t[i] / 2, ms[i]->dev.n[1]);
   }
   for (;;) {
     long long blocks = 0;
@@ -1755,6 +1760,58 @@ mpx_status mpx_energy(mpx_engine* e, int magnet, int quantity, double* out) {
   double avg[3];
   MPX_TRY(mpx_average(e, magnet, quantity, avg));
   *out = (double)m->dev.N * avg[0] * ((double)m->dev.cs[0] * m->dev.cs[1] * m->dev.cs[2]);
+  return MPX_OK;
+}
+
+mpx_status mpx_profile_attempt(mpx_engine* e, int method, int reps, double ms[4]) {
+  if (!e || !ms || reps <= 0) return fail(MPX_ERR_INVALID, "bad arguments");
+  if (method < 0 || method > MPX_RK_DORMAND_PRINCE) return fail(MPX_ERR_INVALID, "unknown method");
+  DeviceGuard guard(e->device);
+  MPX_TRY(prepare_run(e, method));
+  const int s = 1;
+  EpiArgs ea;
+  ea.mode = EPI_STAGE;
+  ea.stage = s;
+  ea.quantity = 0;
+  ea.fsal_err = 0;
+  ea.gate = 1;
+  ea.out = nullptr;
+  ea.msrc = nullptr;
+  cudaEvent_t ev[5];
+  for (auto& x : ev) CUDA_TRY(cudaEventCreate(&x));
+  double acc[4] = {0, 0, 0, 0};
+  for (int r = 0; r <= reps; ++r) {
+    CUDA_TRY(cudaEventRecord(ev[0], e->stream));
+    if (e->n_t_demag > 0)
+      k_xfwd<true><<<e->n_t_demag, e->nt_x, e->smem_x, e->stream>>>(e->d_mags, e->d_groups, e->d_t_demag, s, 1,
+                                                                    nullptr, e->d_tw);
+    if (e->n_t_local > 0)
+      k_combine<<<e->n_t_local, 256, 0, e->stream>>>(e->d_mags, e->d_groups, e->d_t_local, s, 0);
+    CUDA_TRY(cudaEventRecord(ev[1], e->stream));
+    MPX_TRY(launch_pairs(e, -1, s, 1));
+    CUDA_TRY(cudaEventRecord(ev[2], e->stream));
+    if (e->n_t_demag > 0) {
+      for (int c = 0; c < 5; ++c)
+        MPX_TRY(launch_yz(e, c, e->d_kx_demag[c], e->n_kx_demag[c], e->smem_yz[c], s, 1, e->maxpy_yz[c]));
+      MPX_TRY(launch_split(e, e->d_t_ycols, e->n_t_ycols, e->d_t_zmul, e->n_t_zmul, e->smem_ycols, e->smem_zmul,
+                           e->maxpy_split, e->maxpz_split, s, 1));
+    }
+    CUDA_TRY(cudaEventRecord(ev[3], e->stream));
+    if (e->n_t_demag > 0)
+      k_xinv<<<e->n_t_demag, e->nt_x, e->smem_x, e->stream>>>(e->d_mags, e->d_groups, e->d_t_demag, ea, e->d_tw);
+    if (e->n_t_local > 0) k_local<<<e->n_t_local, 256, 0, e->stream>>>(e->d_mags, e->d_groups, e->d_t_local, ea);
+    CUDA_TRY(cudaEventRecord(ev[4], e->stream));
+    CUDA_TRY(cudaEventSynchronize(ev[4]));
+    MPX_TRY(check_launch(e, "profile attempt"));
+    if (r > 0)
+      for (int k = 0; k < 4; ++k) {
+        float t;
+        CUDA_TRY(cudaEventElapsedTime(&t, ev[k], ev[k + 1]));
+        acc[k] += t;
+      }
+  }
+  for (auto& x : ev) cudaEventDestroy(x);
+  for (int k = 0; k < 4; ++k) ms[k] = acc[k] / reps;
   return MPX_OK;
 }
 

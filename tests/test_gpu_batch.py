@@ -117,3 +117,17 @@ def test_batch_solve_follows_oracle(mpx):
         ow.run(10e-12)
         want = ow.get_m(q)
         assert float(np.max(np.abs(got.m - want))) < 1e-4, w["name"]
+
+
+def test_same_result_with_small_and_large_tiles(mpx):
+    """Alone, a small solve runs with small tiles (the shape planner spreads it
+    over the GPU); in a large batch with the default large tiles.  Tiles start
+    on even rows, so the arithmetic and the result are the same."""
+    from mumaxplus_b200 import batch as B
+
+    w = _solve(7, (64, 30, 1), 3e-9, 8e5, 1.3e-11, 0.1, (0.02, 0.0, 0.05))
+    fill = [_solve(10 + k, (128, 96, 2), 3e-9, 7e5, 1.2e-11, 0.2, (0.0, 0.01, 0.02)) for k in range(30)]
+    (alone,), _, _ = B.run_plain(B.Batch(), [w], duration=15e-12, torque_stop=0.0)
+    mixed, _, _ = B.relax_batch(B.Batch(), [w] + fill, duration=15e-12, torque_stop=0.0)
+    assert alone.steps == mixed[0].steps
+    assert np.array_equal(alone.m, mixed[0].m)

@@ -309,8 +309,8 @@ def run_ours(args):
     for _ in range(k_e2e):
         eng.set_m(magnet._id, host_in)
         ts.step()
-        host_out[...] = eng.get_m(magnet._id, host_in.shape)
-        host_in[...] = host_out
+        eng.get_m(magnet._id, host_in.shape, out=host_out)  # pinned: direct DMA
+        host_in, host_out = host_out, host_in
     barrier()
     e2e_s = time.perf_counter() - t0
     e2e_value = world_size * N * k_e2e / e2e_s
@@ -471,7 +471,8 @@ def run_batched(args):
                         "solves_per_s": len(solves) / t_run,
                         "steps_min_median_max": [int(min(steps)), float(np.median(steps)), int(max(steps))],
                         "stopped_on_torque": int(sum(1 for s in solves if s.sim_time < 0.999 * args.duration)),
-                        "failed": int(sum(s.failed for s in solves))},
+                        "failed": int(sum(s.failed for s in solves)),
+                        "autotuned_shape_divisors": {"x": b.tuned[0], "y_z": b.tuned[1]}},
             "plain": {"instances": len(sub), "cell_updates": p_upd, "seconds": p_run, "setup_seconds": p_setup,
                       "value": plain, "unit": "cell-updates/s"},
             "batched_over_plain": value / world_size / plain,

@@ -260,6 +260,13 @@ mpx_status mpx_profile_eval(mpx_engine* e, int magnet, int reps, double ms[4]);
  * state and k_1, which the next attempt recomputes; the solves do not advance.
  * Needs the method the groups run with.  No reference counterpart. */
 mpx_status mpx_profile_attempt(mpx_engine* e, int method, int reps, double ms[4]);
+/* Shape autotuner for the started groups: times stage 1 of an attempt (as
+ * mpx_profile_attempt) with the default row-tile and y/z-block shapes divided by
+ * 1, 2, 4 and 8 (then the two-blocks-per-SM rule), and keeps the fastest divisor
+ * for the x passes and for the y/z passes while the started magnets keep more
+ * than half of the cells they had at tuning.  Call after one mpx_advance (k0 of the started solves valid).  The
+ * divisors chosen go to *div_x, *div_yz.  No reference counterpart. */
+mpx_status mpx_autotune(mpx_engine* e, int method, int* div_x, int* div_yz);
 /* Real-space demag kernel, 6*K floats on the reference's kernel grid
  * (physics/strayfieldkernel.cu:80-99; bindings/wrap_magnet.cpp:56-59).
  * dims receives the kernel grid size (Kx, Ky, Kz). Pass out=NULL to query dims. */

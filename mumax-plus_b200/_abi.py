@@ -171,6 +171,7 @@ SIGNATURES = {
     "mpx_demag_kernel": (I, [E, I, C.c_void_p, P_I]),
     "mpx_profile_eval": (I, [E, I, I, P_D]),
     "mpx_profile_attempt": (I, [E, I, I, P_D]),
+    "mpx_autotune": (I, [E, I, P_I, P_I]),
     "mpx_solver_set_params": (I, [E, I, C.POINTER(SolverParams)]),
     "mpx_solver_get_params": (I, [E, I, C.POINTER(SolverParams)]),
     "mpx_solver_set_time": (I, [E, I, C.c_double]),

@@ -123,8 +123,12 @@ class Engine:
     def set_m_device(self, magnet, dev_ptr):
         check(lib().mpx_magnet_set_m(self._h, int(magnet), C.c_void_p(dev_ptr), 1))
 
-    def get_m(self, magnet, shape):
-        out = np.empty(shape, dtype=np.float32)
+    def get_m(self, magnet, shape, out=None):
+        """Magnetization as (3, nz, ny, nx) float32; into `out` (e.g. a pinned
+        host buffer, for a direct DMA copy) when given."""
+        if out is None:
+            out = np.empty(shape, dtype=np.float32)
+        assert out.dtype == np.float32 and out.flags["C_CONTIGUOUS"] and out.shape == tuple(shape)
         check(lib().mpx_magnet_get_m(self._h, int(magnet), out.ctypes.data, 0))
         return out
 
@@ -170,6 +174,12 @@ class Engine:
         out = (C.c_double * 4)()
         check(lib().mpx_profile_attempt(self._h, _abi.RK_METHODS[method], int(reps), out))
         return [out[i] for i in range(4)]
+
+    def autotune(self, method="DormandPrince"):
+        """Pick the tile-shape divisors of the started groups by timing (returns (div_x, div_yz))."""
+        dx, dy = C.c_int(), C.c_int()
+        check(lib().mpx_autotune(self._h, _abi.RK_METHODS[method], C.byref(dx), C.byref(dy)))
+        return dx.value, dy.value
 
     def demag_kernel(self, magnet):
         dims = (C.c_int * 3)()

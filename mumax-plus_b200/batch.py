@@ -76,6 +76,7 @@ class Batch:
         self.max_error = float(max_error)
         self.solves = {}  # group id -> Solve
         self.resident = 0
+        self.tuned = (1, 1)  # tile-shape divisors chosen by the last autotune
 
     def add(self, w, key=None, m0=None):
         """Create the solve for workload `w` (magnet + group), set its initial
@@ -149,11 +150,13 @@ class _Pacer:
         return self.n
 
 
-def relax_batch(batch, instances, duration=2e-9, torque_stop=1e-4, fetch=True, trace=None):
+def relax_batch(batch, instances, duration=2e-9, torque_stop=1e-4, fetch=True, trace=None, autotune=True):
     """Add every instance, start them all, advance until all have finished.
     Returns (solves, seconds of the integration loop, seconds of set-up).
     `trace`, a list, receives (seconds, attempts, solves running, cells
-    running) at every poll."""
+    running) at every poll.  With `autotune` the tile shapes of the started
+    batch are chosen by timing after the first attempt (mpx_autotune); they
+    hold while the running solves keep more than half of the cells."""
     t0 = time.perf_counter()
     solves = [batch.add(w, key=i) for i, w in enumerate(instances)]
     batch.engine.synchronize()
@@ -165,6 +168,16 @@ def relax_batch(batch, instances, duration=2e-9, torque_stop=1e-4, fetch=True, t
     running = len(solves)
     cells = sum(s.cells for s in solves)
     attempts = 0
+    if autotune and running > 1:  # one attempt (k0 of every solve), then the tile shapes
+        batch.advance(1)
+        done, running = batch.poll()
+        attempts = 1
+        for s in done:
+            batch.finish(s, fetch=fetch)
+            s.t_done = time.perf_counter() - t0
+            cells -= s.cells
+        if running:
+            batch.tuned = batch.engine.autotune(_abi.RK_NAMES[batch.method])
     while running:
         n = pacer.n
         ta = time.perf_counter()

@@ -223,6 +223,9 @@ struct mpx_engine {
   std::vector<Pair> pairs;
   bool pairs_dirty = true;
   bool any_thermal = false;  // some started group has thermal noise: stage 0 is evaluated every attempt
+  // autotuned shape divisors and the launched set they belong to (mpx_autotune)
+  int tune_div_x = 1, tune_div_yz = 1;
+  long long tune_cells = 0;
   // CUDA graphs of one attempt: every stage, and (FSAL methods) without
   // stage 0, whose torque k0 is the last stage of the previous step
   cudaGraphExec_t graph = nullptr, graph_nok0 = nullptr;
@@ -473,11 +476,13 @@ int x_threads(const Magnet* m) {
 // than two blocks per SM; small single solves then spread over the GPU and
 // large batches keep their large tiles.
 constexpr int SHAPE_MIN_BLOCKS = 2 * 148;
-void plan_shapes(const std::vector<Magnet*>& ms, int* ty, int* nkx) {
+// div_x / div_yz (powers of two, from the autotuner; 1 otherwise) divide the
+// default shapes before the rule.
+void plan_shapes(const std::vector<Magnet*>& ms, int* ty, int* nkx, int div_x = 1, int div_yz = 1) {
   std::vector<int> t(ms.size()), k(ms.size());
   for (size_t i = 0; i < ms.size(); ++i) {
-    t[i] = ms[i]->ty_def;
-    k[i] = ms[i]->nkx_def;
+    t[i] = even_rows(ms[i]->ty_def / div_x, ms[i]->dev.n[1]);
+    k[i] = std::max(1, ms[i]->nkx_def / div_yz);
   }
   for (;;) {
     long long blocks = 0;
@@ -523,17 +528,28 @@ mpx_status retile(mpx_engine* e, Magnet* m, int ty, int nkx) {
   return MPX_OK;
 }
 
+// The magnets of started groups (launched together); returns their total cells.
+long long active_set(mpx_engine* e, std::vector<Magnet*>& act) {
+  act.clear();
+  for (auto& mp : e->mags) {
+    if (!mp) continue;
+    const Group* g = (mp->group >= 0 && mp->group < (int)e->groups.size()) ? e->groups[mp->group].get() : nullptr;
+    if (g && g->active) act.push_back(mp.get());
+  }
+  long long cells = 0;
+  for (Magnet* m : act) cells += m->dev.N;
+  return cells;
+}
+
 mpx_status rebuild_tables(mpx_engine* e) {
   {  // shapes for the set of magnets launched together
     std::vector<Magnet*> act;
-    for (auto& mp : e->mags) {
-      if (!mp) continue;
-      const Group* g =
-          (mp->group >= 0 && mp->group < (int)e->groups.size()) ? e->groups[mp->group].get() : nullptr;
-      if (g && g->active) act.push_back(mp.get());
-    }
+    const long long cells = active_set(e, act);
     std::vector<int> ty(act.size()), nkx(act.size());
-    plan_shapes(act, ty.data(), nkx.data());
+    // tuned divisors hold while the launched set keeps more than half of the cells
+    // it had when they were measured (solves of a batch finish one by one)
+    if (2 * cells <= e->tune_cells || cells > e->tune_cells) e->tune_div_x = e->tune_div_yz = 1;
+    plan_shapes(act, ty.data(), nkx.data(), e->tune_div_x, e->tune_div_yz);
     for (size_t i = 0; i < act.size(); ++i)
       if (ty[i] != act[i]->ty || nkx[i] != act[i]->nkx) MPX_TRY(retile(e, act[i], ty[i], nkx[i]));
   }
@@ -1812,6 +1828,40 @@ mpx_status mpx_profile_attempt(mpx_engine* e, int method, int reps, double ms[4]
   }
   for (auto& x : ev) cudaEventDestroy(x);
   for (int k = 0; k < 4; ++k) ms[k] = acc[k] / reps;
+  return MPX_OK;
+}
+
+mpx_status mpx_autotune(mpx_engine* e, int method, int* div_x, int* div_yz) {
+  if (!e) return fail(MPX_ERR_INVALID, "null engine");
+  DeviceGuard guard(e->device);
+  std::vector<Magnet*> act;
+  const long long cells = active_set(e, act);
+  int bx = 1, byz = 1;
+  if (!act.empty()) {
+    double tx_best = 1e300, tyz_best = 1e300;
+    for (int d : {1, 2, 4, 8}) {
+      e->tune_cells = cells;
+      e->tune_div_x = d;
+      e->tune_div_yz = d;
+      e->tables_dirty = true;
+      double ms[4];
+      MPX_TRY(mpx_profile_attempt(e, method, 3, ms));
+      if (ms[0] + ms[3] < tx_best) {
+        tx_best = ms[0] + ms[3];
+        bx = d;
+      }
+      if (ms[2] < tyz_best) {
+        tyz_best = ms[2];
+        byz = d;
+      }
+    }
+    e->tune_cells = cells;
+    e->tune_div_x = bx;
+    e->tune_div_yz = byz;
+    e->tables_dirty = true;
+  }
+  if (div_x) *div_x = bx;
+  if (div_yz) *div_yz = byz;
   return MPX_OK;
 }
 

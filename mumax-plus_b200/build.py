@@ -11,7 +11,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 SRC = os.path.join(HERE, "csrc", "engine.cu")
-HEADERS = [os.path.join(HERE, "csrc", f) for f in ("fft.cuh", "physics.cuh", "kernels.cuh", "newell.cuh")]
+HEADERS = [os.path.join(HERE, "csrc", f) for f in ("fft.cuh", "physics.cuh", "kernels.cuh", "newell.cuh", "stray.cuh", "yzsplit.cuh")]
 OUT = os.path.join(HERE, "libmpx.so")
 
 NVCC_FLAGS = [

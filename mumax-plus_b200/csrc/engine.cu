@@ -60,6 +60,7 @@ constexpr int MAX_FFT = 4096;
 constexpr int SMEM_MAX = 227 * 1024;
 // dynamic shared memory left next to the static descriptor copies of a block
 constexpr int SMEM_DYN_MAX = SMEM_MAX - 2048;
+constexpr int YZ_CLASSES = 10;  // k_yz launch classes (yz_class)
 
 // ------------------------------------------------------------ tableaus
 // core/butchertableau.cpp: Heun, Bogacki-Shampine, Cash-Karp, Fehlberg, Dormand-Prince
@@ -200,11 +201,10 @@ struct mpx_engine {
   bool tables_dirty = true;
   Work *d_t_demag = nullptr, *d_t_local = nullptr;
   int n_t_demag = 0, n_t_local = 0;
-  // k_yz work per z-length class (Pz = 1, 2, 4, 8, 16 -> class log2 Pz)
-  Work* d_kx_demag[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
-  int n_kx_demag[5] = {0, 0, 0, 0, 0};
-  int smem_yz[5] = {0, 0, 0, 0, 0};
-  int maxpy_yz[5] = {0, 0, 0, 0, 0};  // longest y transform of each class
+  // k_yz work per class (yz_class: the z length and whether Py > 2048)
+  Work* d_kx_demag[YZ_CLASSES] = {};
+  int n_kx_demag[YZ_CLASSES] = {};
+  int smem_yz[YZ_CLASSES] = {};
   // split y/z path over all split magnets
   Work *d_t_ycols = nullptr, *d_t_zmul = nullptr;
   int n_t_ycols = 0, n_t_zmul = 0, smem_ycols = 0, smem_zmul = 0, maxpy_split = 0, maxpz_split = 0;
@@ -402,7 +402,10 @@ int x_smem(const Magnet* m) {
 int yz_smem(const Magnet* m) {
   return (m->nkx * 3 * m->dev.n[2] * plen(m->P[1]) + m->P[1]) * (int)sizeof(float2);
 }
-int yz_class(const Magnet* m) { return ilog2(m->P[2]); }
+// k_yz class of a magnet: log2 Pz, plus 5 for y transforms longer than 2048
+// (which need the radix-16 form).  The FFT plan of a magnet depends on its own
+// lengths only, so it computes the same alone and in any batch.
+int yz_class(const Magnet* m) { return ilog2(m->P[2]) + (m->P[1] > 2048 ? 5 : 0); }
 constexpr int YZ_THREADS = 384;
 
 // Tile shapes.  Row tiles: about 4096 points of the padded x transform per
@@ -422,8 +425,6 @@ int choose_nkx(int nz, int Py, int Fh) {
   return std::max(1, std::min(Fh, (YZ_VPT * YZ_THREADS) / (3 * nz * Py)));
 }
 
-// k_yz<PZ> launch for one z-length class
-// (the radix-8 variant for z lengths up to 8 when every y length of the class is <= 2048)
 int ycols_smem(const Magnet* m) { return (m->ncy * plen(m->P[1]) + m->P[1]) * (int)sizeof(float2); }
 int zmul_smem(const Magnet* m) { return (3 * m->nkz * plen(m->P[2]) + m->P[2]) * (int)sizeof(float2); }
 
@@ -448,16 +449,22 @@ mpx_status launch_split(mpx_engine* e, const Work* ycw, int nyc, const Work* zmw
   return MPX_OK;
 }
 
-mpx_status launch_yz(mpx_engine* e, int cls, const Work* work, int n, int smem, int stage, int gate, int max_py) {
+// k_yz launch for one class: the radix-8 form for z lengths up to 8 and y
+// lengths up to 2048, else the radix-16 form (with warp columns for y length
+// 1024 at z length 16)
+mpx_status launch_yz(mpx_engine* e, int cls, const Work* work, int n, int smem, int stage, int gate) {
   if (n <= 0) return MPX_OK;
-  const bool r8 = max_py <= 2048;
 #define MPX_YZ(PZ, LR) k_yz<PZ, LR><<<n, YZ_THREADS, smem, e->stream>>>(e->d_mags, e->d_groups, work, stage, gate, e->d_tw)
   switch (cls) {
-    case 0: if (r8) MPX_YZ(1, 3); else MPX_YZ(1, 4); break;
-    case 1: if (r8) MPX_YZ(2, 3); else MPX_YZ(2, 4); break;
-    case 2: if (r8) MPX_YZ(4, 3); else MPX_YZ(4, 4); break;
-    case 3: if (r8) MPX_YZ(8, 3); else MPX_YZ(8, 4); break;
-    default: MPX_YZ(16, 4); break;
+    case 0: MPX_YZ(1, 3); break;
+    case 1: MPX_YZ(2, 3); break;
+    case 2: MPX_YZ(4, 3); break;
+    case 3: MPX_YZ(8, 3); break;
+    case 5: MPX_YZ(1, 4); break;
+    case 6: MPX_YZ(2, 4); break;
+    case 7: MPX_YZ(4, 4); break;
+    case 8: MPX_YZ(8, 4); break;
+    default: MPX_YZ(16, 4); break;  // 4 and 9 (z length 16; y lengths up to 1024 in warp columns)
   }
 #undef MPX_YZ
   e->launches++;
@@ -553,11 +560,11 @@ mpx_status rebuild_tables(mpx_engine* e) {
     for (size_t i = 0; i < act.size(); ++i)
       if (ty[i] != act[i]->ty || nkx[i] != act[i]->nkx) MPX_TRY(retile(e, act[i], ty[i], nkx[i]));
   }
-  std::vector<Work> td, tl, kd[5], yc, zm;
+  std::vector<Work> td, tl, kd[YZ_CLASSES], yc, zm;
   e->smem_ycols = e->smem_zmul = e->maxpy_split = e->maxpz_split = 0;
   e->smem_x = 0;
   e->nt_x = 256;
-  for (int c = 0; c < 5; ++c) e->smem_yz[c] = e->maxpy_yz[c] = 0;
+  for (int c = 0; c < YZ_CLASSES; ++c) e->smem_yz[c] = 0;
   // only the magnets of started groups: finished and idle solves cost no blocks
   for (auto& mp : e->mags) {
     if (!mp) continue;
@@ -578,7 +585,6 @@ mpx_status rebuild_tables(mpx_engine* e) {
         const int cls = yz_class(m);
         kd[cls].insert(kd[cls].end(), m->kxw.begin(), m->kxw.end());
         e->smem_yz[cls] = std::max(e->smem_yz[cls], yz_smem(m));
-        e->maxpy_yz[cls] = std::max(e->maxpy_yz[cls], m->P[1]);
       }
       e->nt_x = std::max(e->nt_x, x_threads(m));
     } else {
@@ -609,7 +615,7 @@ mpx_status rebuild_tables(mpx_engine* e) {
   MPX_TRY(upload_vec(e, &e->d_t_zmul, zm));
   e->n_t_ycols = (int)yc.size();
   e->n_t_zmul = (int)zm.size();
-  for (int c = 0; c < 5; ++c) {
+  for (int c = 0; c < YZ_CLASSES; ++c) {
     MPX_TRY(upload_vec(e, &e->d_kx_demag[c], kd[c]));
     e->n_kx_demag[c] = (int)kd[c].size();
   }
@@ -1142,7 +1148,7 @@ mpx_status eval_into(mpx_engine* e, Magnet* m, int q, float* out) {
       MPX_TRY(launch_split(e, m->d_ycw, (int)m->ycw.size(), m->d_zmw, (int)m->zmw.size(), ycols_smem(m),
                            zmul_smem(m), m->P[1], m->P[2], 0, 0));
     else
-      MPX_TRY(launch_yz(e, yz_class(m), m->d_kxw, (int)m->kxw.size(), syz, 0, 0, m->P[1]));
+      MPX_TRY(launch_yz(e, yz_class(m), m->d_kxw, (int)m->kxw.size(), syz, 0, 0));
     k_xinv<<<ntile, nt, sx, e->stream>>>(e->d_mags, e->d_groups, m->d_tiles, ea, e->d_tw);
     e->launches += 2;
   } else {
@@ -1181,8 +1187,8 @@ mpx_status launch_attempt(mpx_engine* e, const TableauDev& T, int first_stage) {
     // stray fields of the stage states of the other magnets
     MPX_TRY(launch_pairs(e, -1, s, 1));
     if (e->n_t_demag > 0) {
-      for (int c = 0; c < 5; ++c)
-        MPX_TRY(launch_yz(e, c, e->d_kx_demag[c], e->n_kx_demag[c], e->smem_yz[c], s, 1, e->maxpy_yz[c]));
+      for (int c = 0; c < YZ_CLASSES; ++c)
+        MPX_TRY(launch_yz(e, c, e->d_kx_demag[c], e->n_kx_demag[c], e->smem_yz[c], s, 1));
       MPX_TRY(launch_split(e, e->d_t_ycols, e->n_t_ycols, e->d_t_zmul, e->n_t_zmul, e->smem_ycols, e->smem_zmul,
                            e->maxpy_split, e->maxpz_split, s, 1));
       k_xinv<<<e->n_t_demag, e->nt_x, e->smem_x, e->stream>>>(e->d_mags, e->d_groups, e->d_t_demag, ea, e->d_tw);
@@ -1243,7 +1249,7 @@ mpx_status capture_attempt(mpx_engine* e, const TableauDev& T, int first_stage, 
 int attempt_launches(const mpx_engine* e, const TableauDev& T, int first_stage) {
   const int S = T.S, ns = S - first_stage;
   int nyz = 0;
-  for (int c = 0; c < 5; ++c) nyz += e->n_kx_demag[c] > 0 ? 1 : 0;
+  for (int c = 0; c < YZ_CLASSES; ++c) nyz += e->n_kx_demag[c] > 0 ? 1 : 0;
   if (e->n_t_ycols > 0) nyz += 3;
   int per = 1 + (int)e->pairs.size() * ns;  // controller, stray-field pairs
   if (e->n_t_demag > 0) per += (2 + nyz) * ns + (T.fsal ? 0 : 1);
@@ -1432,7 +1438,7 @@ mpx_status mpx_engine_destroy(mpx_engine* e) {
   cudaFree(e->d_redout);
   pfree(e, e->d_scratch);
   pfree(e, e->d_t_demag);
-  for (int c = 0; c < 5; ++c) pfree(e, e->d_kx_demag[c]);
+  for (int c = 0; c < YZ_CLASSES; ++c) pfree(e, e->d_kx_demag[c]);
   pfree(e, e->d_t_local);
   cudaStreamSynchronize(e->stream);
   if (e->pool) cudaMemPoolDestroy(e->pool);
@@ -1807,8 +1813,8 @@ mpx_status mpx_profile_attempt(mpx_engine* e, int method, int reps, double ms[4]
     MPX_TRY(launch_pairs(e, -1, s, 1));
     CUDA_TRY(cudaEventRecord(ev[2], e->stream));
     if (e->n_t_demag > 0) {
-      for (int c = 0; c < 5; ++c)
-        MPX_TRY(launch_yz(e, c, e->d_kx_demag[c], e->n_kx_demag[c], e->smem_yz[c], s, 1, e->maxpy_yz[c]));
+      for (int c = 0; c < YZ_CLASSES; ++c)
+        MPX_TRY(launch_yz(e, c, e->d_kx_demag[c], e->n_kx_demag[c], e->smem_yz[c], s, 1));
       MPX_TRY(launch_split(e, e->d_t_ycols, e->n_t_ycols, e->d_t_zmul, e->n_t_zmul, e->smem_ycols, e->smem_zmul,
                            e->maxpy_split, e->maxpz_split, s, 1));
     }
@@ -1894,7 +1900,7 @@ mpx_status mpx_profile_eval(mpx_engine* e, int magnet, int reps, double ms[4]) {
         MPX_TRY(launch_split(e, m->d_ycw, (int)m->ycw.size(), m->d_zmw, (int)m->zmw.size(), ycols_smem(m),
                              zmul_smem(m), m->P[1], m->P[2], 0, 0));
       else
-        MPX_TRY(launch_yz(e, yz_class(m), m->d_kxw, (int)m->kxw.size(), syz, 0, 0, m->P[1]));
+        MPX_TRY(launch_yz(e, yz_class(m), m->d_kxw, (int)m->kxw.size(), syz, 0, 0));
       CUDA_TRY(cudaEventRecord(ev[2], e->stream));
       k_xinv<<<ntile, nt, sx, e->stream>>>(e->d_mags, e->d_groups, m->d_tiles, ea, e->d_tw);
       CUDA_TRY(cudaEventRecord(ev[3], e->stream));

@@ -263,4 +263,118 @@ __device__ __forceinline__ void fft_many(float2* buf, int logL, int ncols, int c
   }
 }
 
+// ------------------------------------------------ one 1024-point column per warp
+// A 1024-point transform as 32 x 32 (four-step): with n = j + 32 r and
+// k = s + 32 t,  X[s + 32 t] = sum_j W32^{j t} W1024^{j s} sum_r x[j + 32 r] W32^{r s}.
+// Lane j does the inner 32-point DFT over r and the twiddle W1024^{j s}; one
+// transpose through the warp's column in shared memory; lane s does the outer
+// 32-point DFT over j.  Only __syncwarp, no block barrier.
+//
+// Column layout: element i at qidx(i) = i + i/32.  Lane j reading or writing
+// element j + 32 r, and lane s reading element j + 32 s, both touch 16
+// different 8-byte banks per half-warp.
+
+__device__ __forceinline__ int qidx(int i) { return i + (i >> 5); }
+__host__ __device__ constexpr int qlen(int L) { return L + (L >> 5); }
+
+// cos(2 pi m / 32), m = 0..8 (decimal expansions; the even entries equal c16)
+__host__ __device__ constexpr float c32(int m) {
+  return m == 0 ? 1.0f : m == 1 ? 0.980785280403230449126f : m == 2 ? 0.923879532511286756128f
+         : m == 3 ? 0.831469612302545237079f : m == 4 ? 0.707106781186547524401f
+         : m == 5 ? 0.555570233019602224743f : m == 6 ? 0.382683432365089771728f
+         : m == 7 ? 0.195090322016128267848f : 0.0f;
+}
+
+// Multiply by exp(DIR * 2 pi i M / 32), M a compile-time constant in [0, 32).
+template <int DIR, int M>
+__device__ __forceinline__ float2 rot32(float2 v) {
+  constexpr int q = M / 8, r = M % 8;
+  float2 a = v;
+  if (q == 1) a = DIR < 0 ? make_float2(v.y, -v.x) : make_float2(-v.y, v.x);
+  if (q == 2) a = make_float2(-v.x, -v.y);
+  if (q == 3) a = DIR < 0 ? make_float2(-v.y, v.x) : make_float2(v.y, -v.x);
+  if (r == 0) return a;
+  constexpr float c = c32(r), s = DIR * c32(8 - r);
+  return make_float2(a.x * c - a.y * s, a.x * s + a.y * c);
+}
+
+// Radix-2 decimation-in-time DFT of N register values (N = 1 .. 32),
+// unnormalised, natural order.  ZH: inputs N/2 .. N-1 are zero (never read;
+// the zeros stay zeros down the even / odd splits).  LO: only outputs
+// 0 .. N/2-1 are formed.
+template <int N, int DIR, bool ZH, bool LO>
+struct DftZ {
+  template <int K>
+  __device__ __forceinline__ static void combine(float2 (&v)[N], const float2 (&e)[N / 2], const float2 (&o)[N / 2]) {
+    if constexpr (K < N / 2) {
+      const float2 t = rot32<DIR, (K * (32 / N)) % 32>(o[K]);
+      v[K] = cadd(e[K], t);
+      if constexpr (!LO) v[K + N / 2] = csub(e[K], t);
+      combine<K + 1>(v, e, o);
+    }
+  }
+  __device__ __forceinline__ static void run(float2 (&v)[N]) {
+    float2 e[N / 2], o[N / 2];
+#pragma unroll
+    for (int i = 0; i < N / 2; ++i) {
+      e[i] = v[2 * i];
+      o[i] = v[2 * i + 1];
+    }
+    DftZ<N / 2, DIR, ZH, false>::run(e);
+    DftZ<N / 2, DIR, ZH, false>::run(o);
+    combine<0>(v, e, o);
+  }
+};
+template <int DIR, bool ZH, bool LO>
+struct DftZ<2, DIR, ZH, LO> {
+  __device__ __forceinline__ static void run(float2 (&v)[2]) {
+    if constexpr (ZH) {
+      v[1] = v[0];
+    } else {
+      const float2 a = v[0], b = v[1];
+      v[0] = cadd(a, b);
+      if constexpr (!LO) v[1] = csub(a, b);
+    }
+  }
+};
+template <int DIR, bool ZH, bool LO>
+struct DftZ<1, DIR, ZH, LO> {
+  __device__ __forceinline__ static void run(float2 (&)[1]) {}
+};
+
+// Twiddles W1024^{j s} of the four-step transform at [j * 31 + s - 1] (j in
+// [0, 32), s in [1, 32)): lanes j reading the same s hit 16 different banks.
+// 992 entries; the caller synchronises before use.
+__device__ __forceinline__ void load_tw1024(float2* dst, const float2* __restrict__ tw4096) {
+  for (int t = threadIdx.x; t < 32 * 31; t += blockDim.x) {
+    const int j = t / 31, s = t - j * 31 + 1;
+    dst[t] = __ldg(&tw4096[(j * s) << (TW_LOG - 10)]);
+  }
+}
+
+// Inner step of lane j: v = the 32 values x[j + 32 r] (r = 0..31; with ZH the
+// values r >= 16 are zero and unread); on return v[s] holds
+// W1024^{j s} sum_r x[j + 32 r] W32^{r s}.
+template <int DIR, bool ZH>
+__device__ __forceinline__ void four_step_inner(float2 (&v)[32], const float2* twj, int lane) {
+  DftZ<32, DIR, ZH, false>::run(v);
+  const float2* t = twj + lane * 31 - 1;
+#pragma unroll
+  for (int s = 1; s < 32; ++s) v[s] = cmul(v[s], twiddle_raw<DIR>(t, s));
+}
+
+// Transpose the inner results of the warp through column C (qidx layout) and
+// do the outer step: on return lane s holds X[s + 32 t] in v[t] (t < 16 only
+// with LO).  C is free again when this returns.
+template <int DIR, bool LO>
+__device__ __forceinline__ void four_step_outer(float2 (&v)[32], float2* C, int lane) {
+#pragma unroll
+  for (int s = 0; s < 32; ++s) C[lane + 33 * s] = v[s];  // element lane + 32 s
+  __syncwarp();
+#pragma unroll
+  for (int j = 0; j < 32; ++j) v[j] = C[j + 33 * lane];  // element j + 32 lane
+  __syncwarp();
+  DftZ<32, DIR, false, LO>::run(v);
+}
+
 }  // namespace mpx

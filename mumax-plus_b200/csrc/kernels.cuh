@@ -234,13 +234,14 @@ __device__ __forceinline__ void apply3(float2* v0, float2* v1, float2* v2, float
 // z stage of one ky, half = 0 / 1 computing the even / odd kz of the PZ-point
 // transform of nz <= PZ/2 inputs as a PZ/2-point transform (of x, or of
 // x[n] W_PZ^n); the partner lane holds the other half and the two inverse
-// halves are summed with one shuffle.
-template <int PZ>
+// halves are summed with one shuffle.  Q5: columns in the qidx layout of the
+// warp transforms (else pidx).
+template <int PZ, bool Q5 = false>
 __device__ __forceinline__ void zstage_pair(float2* D, int cs, const MagnetDev& M, int kx, int ky, int half, int nz,
                                             int Py) {
   constexpr int H = PZ / 2;
   float2 v[3][H];
-  const int pky = pidx(ky);
+  const int pky = Q5 ? qidx(ky) : pidx(ky);
   // kernel spectrum of this lane's kz values, issued before the transforms
   const int hy = Py / 2 + 1;
   const int kyp = min(ky, Py - ky);
@@ -329,6 +330,61 @@ __device__ __forceinline__ void zstage_single(float2* D, int cs, const MagnetDev
   D[2 * cs + pky] = v2;
 }
 
+// k_yz for y length 1024 (z length 16): every warp transforms whole columns in
+// registers (four-step 32 x 32), reading its columns of S straight into the
+// inner step and writing the y < ny outputs straight back; the block
+// synchronises only around the z stage.  Columns in the qidx layout.
+template <int PZ>
+__device__ __forceinline__ void yz_warp1024(const MagnetDev& M, int kx0, int nkx, float2* sm,
+                                            const float2* __restrict__ tw) {
+  constexpr int Py = 1024, cs = qlen(Py);
+  const int ny = M.n[1], nz = M.n[2];
+  const int ncol = nkx * 3 * nz;
+  float2* D = sm;
+  float2* twj = sm + ncol * cs;
+  load_tw1024(twj, tw);
+  __syncthreads();
+  float2* S = M.spec + (size_t)kx0 * 3 * nz * ny;
+  const int lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+  for (int col = threadIdx.x >> 5; col < ncol; col += nw) {
+    const float2* __restrict__ Sc = S + (size_t)col * ny;
+    float2 v[32];
+#pragma unroll
+    for (int r = 0; r < 16; ++r) {  // y = lane + 32 r < 512; y >= ny is zero padding
+      const int y = lane + 32 * r;
+      v[r] = (y < ny) ? __ldg(Sc + y) : make_float2(0.f, 0.f);
+    }
+#pragma unroll
+    for (int r = 16; r < 32; ++r) v[r] = make_float2(0.f, 0.f);
+    four_step_inner<-1, true>(v, twj, lane);
+    float2* C = D + col * cs;
+    four_step_outer<-1, false>(v, C, lane);
+#pragma unroll
+    for (int t = 0; t < 32; ++t) C[lane + 33 * t] = v[t];  // ky = lane + 32 t
+  }
+  __syncthreads();
+  // lanes 2u and 2u+1 share one (kx, ky): the even and odd kz halves
+  for (int t = threadIdx.x; t < (2 * nkx) << 10; t += blockDim.x) {
+    const int u = t >> 1, j = u >> 10;
+    zstage_pair<PZ, true>(D + j * 3 * nz * cs, cs, M, kx0 + j, u & (Py - 1), t & 1, nz, Py);
+  }
+  __syncthreads();
+  for (int col = threadIdx.x >> 5; col < ncol; col += nw) {
+    float2* C = D + col * cs;
+    float2 v[32];
+#pragma unroll
+    for (int r = 0; r < 32; ++r) v[r] = C[lane + 33 * r];  // ky = lane + 32 r
+    four_step_inner<1, false>(v, twj, lane);
+    four_step_outer<1, true>(v, C, lane);
+    float2* __restrict__ Sc = S + (size_t)col * ny;
+#pragma unroll
+    for (int t = 0; t < 16; ++t) {  // y = lane + 32 t < 512: only y < ny is kept
+      const int y = lane + 32 * t;
+      if (y < ny) Sc[y] = v[t];
+    }
+  }
+}
+
 // MAXLR = 4: radix-16 passes, 16 values per thread (y lengths up to 4096, one
 // 384-thread block per SM by registers); MAXLR = 3: radix-8 passes, 8 values
 // per thread, two blocks per SM (y lengths up to 2048, z length up to 8).  At
@@ -347,6 +403,12 @@ __global__ void __launch_bounds__(384, MAXLR == 3 ? 2 : 1)
   const int kx0 = wk.z, nkx = wk.y0;
   const int ny = M.n[1], nz = M.n[2];
   const int logPy = M.logP[1], Py = 1 << logPy, cs = plen(Py);
+  if constexpr (PZ == 16 && MAXLR == 4) {
+    if (logPy == 10) {
+      yz_warp1024<PZ>(M, kx0, nkx, sm, tw);
+      return;
+    }
+  }
   float2* S = M.spec + (size_t)kx0 * 3 * nz * ny;  // the nkx slabs are consecutive
   float2* D = sm;  // [nkx][3*nz] padded columns of length Py
   const int ncol = nkx * 3 * nz;

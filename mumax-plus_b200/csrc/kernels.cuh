@@ -606,6 +606,123 @@ __device__ __forceinline__ void epilogue_cell(const MagnetDev& M, const GroupDev
   else store3(out, N, i, r);
 }
 
+// ------------------------------------------------------- lean stage epilogue
+// Neighbour rows of a tile for the lean epilogue: for tile row yl the index of
+// x = 0 in the rows y-1, y+1, z-1, z+1 (-1: no neighbour there), and the x
+// neighbours of the first and the last cell of a row (nb_coord of each).
+struct NbRows {
+  int r[TY_MAX][4];
+  int xl, xr;
+};
+
+__device__ __forceinline__ void nb_rows_fill(NbRows& T, const MagnetDev& M, int y0, int ty, int z) {
+  for (int t = threadIdx.x; t < 4 * ty + 2; t += blockDim.x) {
+    if (t < 4 * ty) {
+      const int yl = t >> 2, q = t & 3, y = y0 + yl;
+      int yy = y, zz = z, nc;
+      if (q < 2) {
+        nc = nb_coord(y, q ? 1 : -1, M.n[1], M.o[1], M.mg[1], M.mgo[1]);
+        yy = nc;
+      } else {
+        nc = nb_coord(z, (q & 1) ? 1 : -1, M.n[2], M.o[2], M.mg[2], M.mgo[2]);
+        zz = nc;
+      }
+      T.r[yl][q] = nc >= 0 ? M.n[0] * (yy + M.n[1] * zz) : -1;
+    } else if (t == 4 * ty) {
+      T.xl = nb_coord(0, -1, M.n[0], M.o[0], M.mg[0], M.mgo[0]);
+    } else {
+      T.xr = nb_coord(M.n[0] - 1, 1, M.n[0], M.o[0], M.mg[0], M.mgo[0]);
+    }
+  }
+}
+
+// The lean epilogue applies to magnets on the fast path (uniform parameters,
+// no geometry) whose x range lies inside one mastergrid period, so that the
+// x neighbours of inner cells are x - 1 and x + 1.
+__device__ __forceinline__ bool lean_ok(const MagnetDev& M) {
+  const int off = M.o[0] - M.mgo[0];
+  return M.fast && !M.geom && (M.mg[0] == 0 || (off >= 0 && off + M.n[0] <= M.mg[0]));
+}
+
+// Right-hand side of one cell of a stage on the lean path: the arithmetic of
+// local_terms_fast and of the torque in epilogue_cell, in the same order,
+// with the neighbours taken from the block's row table.
+__device__ __forceinline__ float3 stage_cell_lean(const MagnetDev& M, const GroupDev& G, const NbRows& T,
+                                                  const float* __restrict__ m, int i, int x, int yl, int y, int z,
+                                                  float3 bdemag) {
+  const int N = M.N;
+  if (M.frozen.u != 0.0f) return f3(0.f, 0.f, 0.f);
+  const unsigned terms = M.terms;
+  const float3 mc = ldg3(m, N, i);
+  float3 exch = f3(0, 0, 0), dmi = f3(0, 0, 0), anis = f3(0, 0, 0), ext = f3(0, 0, 0);
+  const bool openbc = (terms & FLAG_OPENBC) != 0;
+  const bool do_exch = (terms & TERM_EXCH) != 0;
+  const bool do_dmi = (terms & TERM_DMI) != 0;
+  if (do_exch || do_dmi) {
+    const float a = M.fa;
+    const bool dmi_open = (a == 0.0f) || openbc;
+    const bool neumann = !openbc && a != 0.0f;
+    const int r0 = i - x;
+    int nb[6];
+    nb[0] = x > 0 ? i - 1 : (T.xl >= 0 ? r0 + T.xl : -1);
+    nb[1] = x < M.n[0] - 1 ? i + 1 : (T.xr >= 0 ? r0 + T.xr : -1);
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int b = T.r[yl][q];
+      nb[2 + q] = b >= 0 ? b + x : -1;
+    }
+    float3 mn[6];
+#pragma unroll
+    for (int r = 0; r < 6; ++r) mn[r] = nb[r] >= 0 ? ldg3(m, N, nb[r]) : mc;
+    float3 he = f3(0, 0, 0), hd = f3(0, 0, 0);
+#pragma unroll
+    for (int r = 0; r < 6; ++r) {
+      const int axis = r >> 1;
+      const int d = (r & 1) ? 1 : -1;
+      const bool nin = nb[r] >= 0;
+      float3 m_ = mn[r];
+      if (!nin && neumann) {  // ghost cell m + Gamma/(2A) delta
+        const float3 Gm = gamma_uniform(M.fd, axis, mc);
+        m_ = mc + (d * M.cs[axis]) * (M.finv_2a * Gm);
+      }
+      if (do_exch && (nin || neumann)) he = he + M.fe[axis] * (m_ - mc);
+      if (do_dmi && (nin || !dmi_open)) {
+        const float Dxy = M.fd[3 * axis], Dxz = M.fd[3 * axis + 1], Dyz = M.fd[3 * axis + 2];
+        const float inv_delta = d * M.inv_cs[axis];
+        hd.x += (Dxy * m_.y + Dxz * m_.z) * inv_delta;
+        hd.y += (-Dxy * m_.x + Dyz * m_.z) * inv_delta;
+        hd.z += (-Dxz * m_.x - Dyz * m_.y) * inv_delta;
+      }
+    }
+    if (do_exch) exch = M.finv_ms * he;
+    if (do_dmi) dmi = M.finv_ms * hd;
+  }
+  if ((terms & TERM_ANIS) && (terms & FLAG_CUBIC)) {
+    anis = cubic_field(mc, f3(M.fc[0][0], M.fc[0][1], M.fc[0][2]), f3(M.fc[1][0], M.fc[1][1], M.fc[1][2]),
+                       f3(M.fc[2][0], M.fc[2][1], M.fc[2][2]), M.fkc[0], M.fkc[1], M.fkc[2], M.finv_ms);
+  } else if (terms & TERM_ANIS) {
+    const float3 u = f3(M.fu[0], M.fu[1], M.fu[2]);
+    const float mu = dot3(mc, u);
+    anis = M.finv_ms * ((2 * M.fk1 * mu + 4 * M.fk2 * mu * mu * mu) * u);
+  }
+  if (terms & TERM_EXT) {
+    ext = f3(M.fb[0], M.fb[1], M.fb[2]);
+    if (terms & FLAG_STRAY) {
+      const float3 s = load3(M.hstray, N, i);
+      ext = f3(ext.x + s.x, ext.y + s.y, ext.z + s.z);
+    }
+  }
+  float3 h = exch;
+  h = h + anis;
+  h = h + ext;
+  h = h + dmi;
+  h = h + bdemag;
+  float3 k = G.torque_kind ? damping_torque(mc, h) : llg_torque(mc, h, M.alpha.u);
+  if (!G.torque_kind && (terms & (FLAG_STT_ZL | FLAG_STT_SL))) k = k + stt_torque(M, m, x, y, z, i, mc);
+  if (terms & FLAG_THERMAL) k = k + thermal_term(M, i, G.steps, G.dt);
+  return k;
+}
+
 // ------------------------------------------------------------------ k_xinv
 __global__ void __launch_bounds__(X_THREADS_MAX, 2) k_xinv(const MagnetDev* __restrict__ mags, GroupDev* __restrict__ groups,
                                               const Work* __restrict__ work, EpiArgs ea,
@@ -623,6 +740,13 @@ __global__ void __launch_bounds__(X_THREADS_MAX, 2) k_xinv(const MagnetDev* __re
   float2* rows_z = sm + ty * cs;
   float2* tws = sm + (ty + nzrows) * cs;  // twiddles of length L
   load_twiddles<3>(tws, tw, logL);
+  __shared__ NbRows T;
+  __shared__ float cf[8];  // FSAL error weights dt (b1 - b2) of the stages
+  const bool lean = ea.mode == EPI_STAGE && lean_ok(M);
+  if (lean) {
+    nb_rows_fill(T, M, y0, ty, z);
+    if (threadIdx.x < c_tab.S) cf[threadIdx.x] = (float)(G.dt * (c_tab.b1[threadIdx.x] - c_tab.b2[threadIdx.x]));
+  }
   const float2* __restrict__ S = M.spec;
   const size_t cstride = (size_t)nz * ny;
   // rebuild full-length Hermitian rows: Z = A + iB.  Lanes e (kx = e >> tyl,
@@ -667,6 +791,35 @@ __global__ void __launch_bounds__(X_THREADS_MAX, 2) k_xinv(const MagnetDev* __re
   double en = 0.0, tn = 0.0;
   const int rowbase = nx * (y0 + ny * z);
   const float rn = 1.0f / (float)nx;
+  if (lean) {
+    // squared error / torque norms: the maximum of the squares gives the same
+    // maximum norm after one square root per thread
+    const int N = M.N;
+    float* __restrict__ kout = M.buf[G.map[2 + ea.stage]];
+    for (int e = threadIdx.x; e < ty * nx; e += blockDim.x) {
+      const int yl = tile_row(e, nx, rn), x = e - yl * nx;
+      const int i = rowbase + e;
+      const float2 hxy = sm[yl * cs + pidx(x)];
+      const float2 hz2 = rows_z[(yl >> 1) * cs + pidx(x)];
+      const float3 bd = f3(hxy.x, hxy.y, (yl & 1) ? hz2.y : hz2.x);
+      const float3 k = stage_cell_lean(M, G, T, m, i, x, yl, y0 + yl, z, bd);
+      store3(kout, N, i, k);
+      if (ea.fsal_err) {
+        float3 er = f3(0, 0, 0);
+        for (int j = 0; j < c_tab.S; ++j) {
+          const float c = cf[j];
+          const float3 kj = (j == ea.stage) ? k : load3(M.buf[G.map[2 + j]], N, i);
+          er = f3(er.x + c * kj.x, er.y + c * kj.y, er.z + c * kj.z);
+        }
+        const double es = (double)er.x * er.x + (double)er.y * er.y + (double)er.z * er.z;
+        const double ts = (double)k.x * k.x + (double)k.y * k.y + (double)k.z * k.z;
+        en = (es > en || es != es) ? es : en;
+        tn = fmax(tn, ts);
+      }
+    }
+    if (ea.fsal_err) block_max2(sqrt(en), sqrt(tn), &groups[M.group].err_bits, &groups[M.group].tmax_bits);
+    return;
+  }
   for (int e = threadIdx.x; e < ty * nx; e += blockDim.x) {
     const int yl = tile_row(e, nx, rn), x = e - yl * nx;
     const int i = rowbase + e;

@@ -377,4 +377,28 @@ __device__ __forceinline__ void four_step_outer(float2 (&v)[32], float2* C, int 
   DftZ<32, DIR, false, LO>::run(v);
 }
 
+// 1024-point transforms of `nrows` rows in shared memory (row r at buf + r*cs,
+// qidx layout), one row per warp at a time, in place.  ZIN: the upper half of
+// every input row is zero padding (not read).  LO: only the lower half of every
+// output row is written.  No block barrier: the caller synchronises before (rows
+// and twiddles written) and after.
+template <int DIR, bool ZIN, bool LO>
+__device__ __forceinline__ void warp_rows1024(float2* buf, int nrows, int cs, const float2* twj) {
+  const int lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+  for (int row = threadIdx.x >> 5; row < nrows; row += nw) {
+    float2* R = buf + row * cs;
+    float2 v[32];
+#pragma unroll
+    for (int r = 0; r < 32; ++r) v[r] = (!ZIN || r < 16) ? R[lane + 33 * r] : make_float2(0.f, 0.f);
+    four_step_inner<DIR, ZIN>(v, twj, lane);
+    four_step_outer<DIR, LO>(v, R, lane);
+#pragma unroll
+    for (int t = 0; t < (LO ? 16 : 32); ++t) R[lane + 33 * t] = v[t];
+  }
+}
+
+// Padded index of the x rows: i + i/32 for 1024-point rows (warp transforms),
+// else pidx.
+__device__ __forceinline__ int xidx(int i, int sh) { return i + (i >> sh); }
+
 }  // namespace mpx

@@ -147,7 +147,10 @@ __global__ void __launch_bounds__(X_THREADS_MAX, 2) k_xfwd(const MagnetDev* __re
   const float* x0 = M.buf[G.map[0]];
   const int rowbase = nx * (y0 + ny * z);
   float2* tws = sm + (ty + nzrows) * cs;  // twiddles of length L
-  load_twiddles<3>(tws, tw, logL);
+  const bool wrow = logL == 10;  // 1024-point rows: one warp per row (four-step)
+  const int sh = wrow ? 5 : 4;
+  if (wrow) load_tw1024(tws, tw);
+  else load_twiddles<3>(tws, tw, logL);
 
   // only the lower half of each row: the upper half (x >= L/2 >= nx) is zero
   // padding that the pruned first FFT pass does not read
@@ -171,13 +174,18 @@ __global__ void __launch_bounds__(X_THREADS_MAX, 2) k_xfwd(const MagnetDev* __re
         store3(xs, N, i, load3(x0, N, i));
       }
     }
-    sm[yl * cs + pidx(x)] = make_float2(Mv.x, Mv.y);
-    float* zr = reinterpret_cast<float*>(sm + (ty + (yl >> 1)) * cs + pidx(x));
+    sm[yl * cs + xidx(x, sh)] = make_float2(Mv.x, Mv.y);
+    float* zr = reinterpret_cast<float*>(sm + (ty + (yl >> 1)) * cs + xidx(x, sh));
     zr[yl & 1] = Mv.z;
     if ((ty & 1) && yl == ty - 1) zr[1] = 0.0f;
   }
   __syncthreads();
-  fft_many<-1, 3, 1>(sm, logL, ty + nzrows, cs, tws);
+  if (wrow) {
+    warp_rows1024<-1, true, false>(sm, ty + nzrows, cs, tws);
+    __syncthreads();
+  } else {
+    fft_many<-1, 3, 1>(sm, logL, ty + nzrows, cs, tws);
+  }
 
   // unpack the two real transforms of each complex row and store the half spectrum
   const int Fh = M.Fh;
@@ -189,8 +197,8 @@ __global__ void __launch_bounds__(X_THREADS_MAX, 2) k_xfwd(const MagnetDev* __re
     const int rest = e >> tyl;
     const int c = rest % 3, kx = rest / 3;
     const float2* Z = (c < 2) ? (sm + yl * cs) : (sm + (ty + (yl >> 1)) * cs);
-    const float2 zk = Z[pidx(kx)];
-    const float2 zc = cconj(Z[pidx((L - kx) & (L - 1))]);
+    const float2 zk = Z[xidx(kx, sh)];
+    const float2 zc = cconj(Z[xidx((L - kx) & (L - 1), sh)]);
     float2 val;
     const bool second = (c == 1) || (c == 2 && (yl & 1));
     if (!second) {
@@ -739,7 +747,10 @@ __global__ void __launch_bounds__(X_THREADS_MAX, 2) k_xinv(const MagnetDev* __re
   const int Fh = M.Fh;
   float2* rows_z = sm + ty * cs;
   float2* tws = sm + (ty + nzrows) * cs;  // twiddles of length L
-  load_twiddles<3>(tws, tw, logL);
+  const bool wrow = logL == 10;  // 1024-point rows: one warp per row (four-step)
+  const int sh = wrow ? 5 : 4;
+  if (wrow) load_tw1024(tws, tw);
+  else load_twiddles<3>(tws, tw, logL);
   __shared__ NbRows T;
   __shared__ float cf[8];  // FSAL error weights dt (b1 - b2) of the stages
   const bool lean = ea.mode == EPI_STAGE && lean_ok(M);
@@ -775,17 +786,22 @@ __global__ void __launch_bounds__(X_THREADS_MAX, 2) k_xinv(const MagnetDev* __re
       B.y = 0.f;
       Cz.y = 0.f;
     }
-    sm[yl * cs + pidx(kx)] = make_float2(A.x - B.y, A.y + B.x);
-    if (kx > 0 && 2 * kx < L) sm[yl * cs + pidx(L - kx)] = make_float2(A.x + B.y, -A.y + B.x);
+    sm[yl * cs + xidx(kx, sh)] = make_float2(A.x - B.y, A.y + B.x);
+    if (kx > 0 && 2 * kx < L) sm[yl * cs + xidx(L - kx, sh)] = make_float2(A.x + B.y, -A.y + B.x);
     if ((yl & 1) == 0) {
       float2 Dv = (yl + 1 < ty) ? make_float2(dx, dy) : make_float2(0.f, 0.f);
       if (edge) Dv.y = 0.f;
-      rows_z[(yl >> 1) * cs + pidx(kx)] = make_float2(Cz.x - Dv.y, Cz.y + Dv.x);
-      if (kx > 0 && 2 * kx < L) rows_z[(yl >> 1) * cs + pidx(L - kx)] = make_float2(Cz.x + Dv.y, -Cz.y + Dv.x);
+      rows_z[(yl >> 1) * cs + xidx(kx, sh)] = make_float2(Cz.x - Dv.y, Cz.y + Dv.x);
+      if (kx > 0 && 2 * kx < L) rows_z[(yl >> 1) * cs + xidx(L - kx, sh)] = make_float2(Cz.x + Dv.y, -Cz.y + Dv.x);
     }
   }
   __syncthreads();
-  fft_many<1, 3, 2>(sm, logL, ty + nzrows, cs, tws);  // only x < nx <= L/2 is used
+  if (wrow) {  // only x < nx <= L/2 is used
+    warp_rows1024<1, false, true>(sm, ty + nzrows, cs, tws);
+    __syncthreads();
+  } else {
+    fft_many<1, 3, 2>(sm, logL, ty + nzrows, cs, tws);
+  }
 
   const float* m = ea.msrc ? ea.msrc : stage_m(M, G, ea.stage);
   double en = 0.0, tn = 0.0;
@@ -799,8 +815,8 @@ __global__ void __launch_bounds__(X_THREADS_MAX, 2) k_xinv(const MagnetDev* __re
     for (int e = threadIdx.x; e < ty * nx; e += blockDim.x) {
       const int yl = tile_row(e, nx, rn), x = e - yl * nx;
       const int i = rowbase + e;
-      const float2 hxy = sm[yl * cs + pidx(x)];
-      const float2 hz2 = rows_z[(yl >> 1) * cs + pidx(x)];
+      const float2 hxy = sm[yl * cs + xidx(x, sh)];
+      const float2 hz2 = rows_z[(yl >> 1) * cs + xidx(x, sh)];
       const float3 bd = f3(hxy.x, hxy.y, (yl & 1) ? hz2.y : hz2.x);
       const float3 k = stage_cell_lean(M, G, T, m, i, x, yl, y0 + yl, z, bd);
       store3(kout, N, i, k);
@@ -825,8 +841,8 @@ __global__ void __launch_bounds__(X_THREADS_MAX, 2) k_xinv(const MagnetDev* __re
     const int i = rowbase + e;
     float3 bd = f3(0, 0, 0);
     if (in_geom(M, i)) {
-      const float2 hxy = sm[yl * cs + pidx(x)];
-      const float2 hz2 = rows_z[(yl >> 1) * cs + pidx(x)];
+      const float2 hxy = sm[yl * cs + xidx(x, sh)];
+      const float2 hz2 = rows_z[(yl >> 1) * cs + xidx(x, sh)];
       bd = f3(hxy.x, hxy.y, (yl & 1) ? hz2.y : hz2.x);
     }
     double a = 0.0, b = 0.0;

@@ -397,7 +397,7 @@ mpx_status upload_vec(mpx_engine* e, Work** d, const std::vector<T>& v) {
 
 // dynamic shared memory: padded rows / columns plus the twiddle table of the length
 int x_smem(const Magnet* m) {
-  return ((m->ty + (m->ty + 1) / 2) * xstride(m->P[0]) + m->P[0]) * (int)sizeof(float2);
+  return ((m->ty + (m->ty + 1) / 2) * xrow_stride(m->P[0], m->ty) + m->P[0]) * (int)sizeof(float2);
 }
 int yz_smem(const Magnet* m) {
   return (m->nkx * 3 * m->dev.n[2] * plen(m->P[1]) + m->P[1]) * (int)sizeof(float2);
@@ -409,7 +409,8 @@ int yz_class(const Magnet* m) { return ilog2(m->P[2]) + (m->P[1] > 2048 ? 5 : 0)
 constexpr int YZ_THREADS = 384;
 
 // Tile shapes.  Row tiles: about 4096 points of the padded x transform per
-// tile (4 rows from Px = 1024 up; up to TY_MAX rows of short transforms), or
+// tile (4 rows above Px = 1024; up to TY_MAX rows of short transforms), 8 rows
+// at Px = 1024 (12 transformed rows: one per warp of the warp-row FFT), or
 // of the row itself without demag.  y/z blocks: enough consecutive kx that a
 // block holds about YZ_VPT * YZ_THREADS points of y transforms.
 // Rows per tile are even (or the single row of ny = 1): the x passes pack the
@@ -418,7 +419,7 @@ constexpr int YZ_THREADS = 384;
 // same results alone and in any batch).
 int even_rows(int t, int ny) { return ny <= 1 ? 1 : std::max(2, t & ~1); }
 int choose_ty(int ny, int len) {
-  const int t = len >= 1024 ? 4 : std::min(TY_MAX, std::max(1, 4096 / len));
+  const int t = len == 1024 ? 8 : len > 1024 ? 4 : std::min(TY_MAX, std::max(1, 4096 / len));
   return even_rows(std::max(1, std::min(t, ny)), ny);
 }
 int choose_nkx(int nz, int Py, int Fh) {

@@ -401,4 +401,15 @@ __device__ __forceinline__ void warp_rows1024(float2* buf, int nrows, int cs, co
 // else pidx.
 __device__ __forceinline__ int xidx(int i, int sh) { return i + (i >> sh); }
 
+// Row stride of the x passes for tiles of ty rows.  1024-point rows (qidx
+// layout): qlen plus 16 / (row slots of the tile, ty rounded up to a power of
+// two) complex values, so that the gather and the unpack, whose half-warps
+// touch the same few x of every row slot, hit 16 different 8-byte banks.
+__host__ __device__ inline int xrow_stride(int L, int ty) {
+  if (L != 1024) return xstride(L);
+  int slots = 1;
+  while (slots < ty) slots <<= 1;
+  return qlen(L) + (slots >= 16 ? 1 : 16 / slots);
+}
+
 }  // namespace mpx

@@ -140,7 +140,7 @@ __global__ void __launch_bounds__(X_THREADS_MAX, 2) k_xfwd(const MagnetDev* __re
   if (!load_descs(M, G, mags, groups, wk.mag, gate, stage)) return;
   const int z = wk.z, y0 = wk.y0, ty = wk.ty;
   const int nx = M.n[0], ny = M.n[1], nz = M.n[2], N = M.N;
-  const int logL = M.logP[0], L = 1 << logL, cs = xstride(L);
+  const int logL = M.logP[0], L = 1 << logL, cs = xrow_stride(L, ty);
   const int nzrows = (ty + 1) >> 1;
   const float* src = msrc_override ? msrc_override : stage_m(M, G, stage);
   float* xs = M.buf[G.map[1]];
@@ -742,7 +742,7 @@ __global__ void __launch_bounds__(X_THREADS_MAX, 2) k_xinv(const MagnetDev* __re
   if (!load_descs(M, G, mags, groups, wk.mag, ea.gate, ea.stage)) return;
   const int z = wk.z, y0 = wk.y0, ty = wk.ty;
   const int nx = M.n[0], ny = M.n[1], nz = M.n[2];
-  const int logL = M.logP[0], L = 1 << logL, cs = xstride(L);
+  const int logL = M.logP[0], L = 1 << logL, cs = xrow_stride(L, ty);
   const int nzrows = (ty + 1) >> 1;
   const int Fh = M.Fh;
   float2* rows_z = sm + ty * cs;

@@ -285,6 +285,15 @@ mpx_status mpx_solver_sensible_timestep(mpx_engine* e, int group, double* dt);
 mpx_status mpx_solver_step(mpx_engine* e, int group);
 mpx_status mpx_solver_steps(mpx_engine* e, int group, int nsteps);
 mpx_status mpx_solver_run(mpx_engine* e, int group, double duration);
+/* The loop of TimeSolver.solve (mumaxplus/timesolver.py:114-152) for average
+ * magnetizations, without a host round trip per time point: for k = 0..n-1,
+ * run(times[k] - t), then record row k of `out` (n rows of 1 + 3 * nmag doubles:
+ * the time, then <m> of every magnet of the group in the order they were added,
+ * each exactly as mpx_average of MPX_Q_MAGNETIZATION would give it).  The time
+ * points, the run() logic between them and the averages stay on the device;
+ * the table comes back once at the end.  times must be non-decreasing
+ * (MPX_ERR_INVALID otherwise).  Blocking. */
+mpx_status mpx_solver_run_sampled(mpx_engine* e, int group, const double* times, int n, double* out);
 
 /* Minimizer::exec (physics/minimizer.cu:73-160): steepest descent on the
  * damping torque with Barzilai-Borwein step sizes over the group's magnets,

@@ -182,6 +182,7 @@ SIGNATURES = {
     "mpx_solver_step": (I, [E, I]),
     "mpx_solver_steps": (I, [E, I, I]),
     "mpx_solver_run": (I, [E, I, C.c_double]),
+    "mpx_solver_run_sampled": (I, [E, I, C.POINTER(C.c_double), I, C.POINTER(C.c_double)]),
     "mpx_minimize": (I, [E, I, C.c_double, I]),
     "mpx_relax": (I, [E, I, C.c_double, C.c_double]),
     "mpx_group_start": (I, [E, I, C.c_double, C.c_double]),

@@ -228,6 +228,15 @@ class Engine:
     def run(self, g, duration):
         check(lib().mpx_solver_run(self._h, int(g), float(duration)))
 
+    def run_sampled(self, g, times, nmag):
+        """Run through the time points and return the table recorded on the
+        device: one row [t, <m> of each of the group's nmag magnets] per point."""
+        t = np.ascontiguousarray(times, dtype=np.float64)
+        out = np.zeros((t.size, 1 + 3 * int(nmag)), dtype=np.float64)
+        dp = C.POINTER(C.c_double)
+        check(lib().mpx_solver_run_sampled(self._h, int(g), t.ctypes.data_as(dp), int(t.size), out.ctypes.data_as(dp)))
+        return out
+
     def minimize(self, g, tol=1e-6, nsamples=10):
         check(lib().mpx_minimize(self._h, int(g), float(tol), int(nsamples)))
 

@@ -223,6 +223,8 @@ struct mpx_engine {
   std::vector<Pair> pairs;
   bool pairs_dirty = true;
   bool any_thermal = false;  // some started group has thermal noise: stage 0 is evaluated every attempt
+  int sampling_group = -1;   // group of the sampled run in progress (its magnets get sample kernels)
+  int samp_magnets = 0;
   // autotuned shape divisors and the launched set they belong to (mpx_autotune)
   int tune_div_x = 1, tune_div_yz = 1;
   long long tune_cells = 0;
@@ -1213,6 +1215,18 @@ mpx_status launch_attempt(mpx_engine* e, const TableauDev& T, int first_stage) {
   const int ng = (int)e->groups.size();
   k_controller<<<(ng + 127) / 128, 128, 0, e->stream>>>(e->d_groups, ng);
   e->launches++;
+  // sampled run: <m> of the group's magnets into the rows the controller marked due
+  if (e->sampling_group >= 0) {
+    Group* sg = get_group(e, e->sampling_group);
+    for (size_t j = 0; sg && j < sg->magnets.size(); ++j) {
+      const Magnet* m = get_mag(e, sg->magnets[j]);
+      if (!m) continue;
+      k_sample_partial<<<256, 256, 0, e->stream>>>(e->d_mags, e->d_groups, m->slot, e->d_red);
+      k_sample_final<<<1, 32, 0, e->stream>>>(e->d_mags, e->d_groups, m->slot, e->d_red, 256, (long long)m->ngeo,
+                                             1 + 3 * (int)j);
+      e->launches += 2;
+    }
+  }
   return check_launch(e, "attempt");
 }
 
@@ -1252,7 +1266,7 @@ int attempt_launches(const mpx_engine* e, const TableauDev& T, int first_stage) 
   int nyz = 0;
   for (int c = 0; c < YZ_CLASSES; ++c) nyz += e->n_kx_demag[c] > 0 ? 1 : 0;
   if (e->n_t_ycols > 0) nyz += 3;
-  int per = 1 + (int)e->pairs.size() * ns;  // controller, stray-field pairs
+  int per = 1 + (int)e->pairs.size() * ns + 2 * e->samp_magnets;  // controller, stray-field pairs, samples
   if (e->n_t_demag > 0) per += (2 + nyz) * ns + (T.fsal ? 0 : 1);
   if (e->n_t_local > 0) per += ns + (ns - (first_stage == 0 ? 1 : 0)) + (T.fsal ? 0 : 1);
   return per;
@@ -2074,7 +2088,7 @@ static mpx_status start_group(mpx_engine* e, Group* g, int mode, long long nstep
   G.err_bits = 0;
   G.tmax_bits = 0;
   G.finished_flag = 0;
-  if (mode == 0) {
+  if (mode == 0 || mode == 2) {
     G.t_stop = G.t + duration;
     if (!(G.t < G.t_stop - G.dt)) {  // core/timesolver.cpp:100-109
       G.phase = 1;
@@ -2113,6 +2127,87 @@ mpx_status mpx_solver_run(mpx_engine* e, int group, double duration) {
   MPX_TRY(start_group(e, g, 0, 0, duration, 0.0, &none));
   if (none) return MPX_OK;
   return drive_group(e, g);
+}
+
+mpx_status mpx_solver_run_sampled(mpx_engine* e, int group, const double* times, int n, double* out) {
+  Group* g = get_group(e, group);
+  if (!g) return fail(MPX_ERR_RANGE, "no such group");
+  if (n < 0 || (n > 0 && (!times || !out))) return fail(MPX_ERR_INVALID, "bad time points / output table");
+  for (int k = 1; k < n; ++k)
+    if (!(times[k - 1] <= times[k])) return fail(MPX_ERR_INVALID, "The list of timepoints should be increasing.");
+  if (n == 0) return MPX_OK;
+  DeviceGuard guard(e->device);
+  const int nmag = (int)g->magnets.size();
+  const int row = 1 + 3 * nmag;
+  auto record = [&](int k) -> mpx_status {  // row k from the current state, on the host
+    MPX_TRY(mpx_solver_get_time(e, group, &out[(size_t)k * row]));
+    for (int j = 0; j < nmag; ++j) MPX_TRY(mpx_average(e, g->magnets[j], MPX_Q_MAGNETIZATION, &out[(size_t)k * row + 1 + 3 * j]));
+    return MPX_OK;
+  };
+  double t;
+  MPX_TRY(mpx_solver_get_time(e, group, &t));
+  if (nmag == 0) {  // no equations: time only advances (start_group)
+    for (int k = 0; k < n; ++k) {
+      MPX_TRY(mpx_solver_run(e, group, times[k] - t));
+      MPX_TRY(record(k));
+      t = out[(size_t)k * row];
+    }
+    return MPX_OK;
+  }
+  int k0 = 0;  // points that need no step from here: run(t_k - t) would take none
+  while (k0 < n && !(times[k0] - t > 0.0)) MPX_TRY(record(k0++));
+  if (k0 == n) return MPX_OK;
+  double *d_t = nullptr, *d_out = nullptr;
+  MPX_TRY(palloc(e, (void**)&d_t, sizeof(double) * n));
+  mpx_status st = palloc(e, (void**)&d_out, sizeof(double) * (size_t)n * row);
+  if (st == MPX_OK) {
+    cudaError_t ce = cudaMemcpyAsync(d_t, times, sizeof(double) * n, cudaMemcpyHostToDevice, e->stream);
+    if (ce == cudaSuccess) ce = cudaMemsetAsync(d_out, 0, sizeof(double) * (size_t)n * row, e->stream);
+    if (ce != cudaSuccess) st = fail(MPX_ERR_CUDA, cudaGetErrorString(ce));
+  }
+  bool none = false;
+  if (st == MPX_OK) st = start_group(e, g, 2, 0, times[k0] - t, 0.0, &none);
+  if (st == MPX_OK) {
+    GroupDev G;
+    st = read_group(e, g->slot, &G);
+    if (st == MPX_OK) {
+      G.samp_t = d_t;
+      G.samp_out = d_out;
+      G.samp_n = n;
+      G.samp_k = k0;
+      G.samp_lo = G.samp_hi = 0;
+      G.samp_row = row;
+      st = write_group(e, g->slot, &G);
+    }
+  }
+  if (st == MPX_OK) {
+    e->sampling_group = group;
+    e->samp_magnets = nmag;
+    e->graph_dirty = true;
+    st = drive_group(e, g);
+    e->sampling_group = -1;
+    e->samp_magnets = 0;
+    e->graph_dirty = true;
+    GroupDev G;
+    mpx_status s2 = read_group(e, g->slot, &G);
+    if (s2 == MPX_OK) {
+      G.mode = 0;
+      G.samp_t = nullptr;
+      G.samp_out = nullptr;
+      G.samp_n = G.samp_k = G.samp_lo = G.samp_hi = 0;
+      s2 = write_group(e, g->slot, &G);
+    }
+    if (st == MPX_OK) st = s2;
+    if (st == MPX_OK) {
+      cudaError_t ce = cudaMemcpyAsync(out + (size_t)k0 * row, d_out + (size_t)k0 * row,
+                                       sizeof(double) * (size_t)(n - k0) * row, cudaMemcpyDeviceToHost, e->stream);
+      if (ce == cudaSuccess) ce = cudaStreamSynchronize(e->stream);
+      if (ce != cudaSuccess) st = fail(MPX_ERR_CUDA, cudaGetErrorString(ce));
+    }
+  }
+  pfree(e, d_t);
+  pfree(e, d_out);
+  return st;
 }
 
 // ------------------------------------------------ minimize / relax

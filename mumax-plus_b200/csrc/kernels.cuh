@@ -913,11 +913,35 @@ __global__ void __launch_bounds__(256) k_combine(const MagnetDev* __restrict__ m
 // --------------------------------------------------------------- controller
 // core/rungekutta.cpp:60-82 and core/timesolver.cpp:60-111, one thread per group,
 // in FP64.  Also runs the run()/steps() state machine on the device.
+// Sampled run: time point samp_k has been reached.  Its row (and the rows of
+// the next points that need no step, as run(t_k - t) with t_k <= t takes none)
+// become due with the time; the next point that needs steps is armed as run()
+// arms its end (core/timesolver.cpp:100-109).  Returns false when no point is
+// left.
+__device__ __forceinline__ bool sample_advance(GroupDev& G) {
+  G.samp_lo = G.samp_k;
+  do {
+    G.samp_out[(size_t)G.samp_k * G.samp_row] = G.t;
+    ++G.samp_k;
+  } while (G.samp_k < G.samp_n && !(G.samp_t[G.samp_k] - G.t > 0.0));
+  G.samp_hi = G.samp_k;
+  if (G.samp_k >= G.samp_n) return false;
+  G.phase = 0;
+  G.t_stop = G.t + (G.samp_t[G.samp_k] - G.t);
+  if (!(G.t < G.t_stop - G.dt)) {
+    G.phase = 1;
+    G.dt_saved = G.dt;
+    G.dt = G.t_stop - G.t;
+  }
+  return true;
+}
+
 __global__ void k_controller(GroupDev* __restrict__ groups, int ngroups) {
   const int g = blockIdx.x * blockDim.x + threadIdx.x;
   if (g >= ngroups) return;
   GroupDev& G = groups[g];
   if (G.status != GS_RUNNING) return;
+  G.samp_lo = G.samp_hi;  // the rows of the previous attempt have been written
   const double err = __longlong_as_double((long long)G.err_bits);
   const double tmax = __longlong_as_double((long long)G.tmax_bits);
   G.err_bits = 0ull;
@@ -963,6 +987,7 @@ __global__ void k_controller(GroupDev* __restrict__ groups, int ngroups) {
   if (G.phase == 1) {
     done = true;
     if (!G.adaptive) G.dt = G.dt_saved;
+    if (G.mode == 2) done = !sample_advance(G);
   } else if (G.mode == 1) {
     if (--G.steps_left <= 0) done = true;
   } else {
@@ -1034,6 +1059,48 @@ __global__ void k_reduce_final(const double* __restrict__ partial, int nblocks, 
       else if (v > r[c] || v != v) r[c] = v;
     }
   for (int c = 0; c < 3; ++c) out[c] = r[c];
+}
+
+// Sampled run: <m> of one magnet into the due rows of its group's table, with
+// the arithmetic of mpx_average (k_reduce_partial / k_reduce_final over the
+// same 256 x 256 grid), so the values equal a host-side average of the state.
+// Both kernels do nothing unless rows are due.
+__global__ void __launch_bounds__(256) k_sample_partial(const MagnetDev* __restrict__ mags,
+                                                        const GroupDev* __restrict__ groups, int slot,
+                                                        double* partial) {
+  __shared__ double sh[3][256];
+  const MagnetDev& M = mags[slot];
+  const GroupDev& G = groups[M.group];
+  if (G.samp_hi <= G.samp_lo) return;
+  const int N = M.N;
+  const float* __restrict__ a = M.buf[G.map[0]];
+  const unsigned char* __restrict__ geom = M.geom;
+  double acc[3] = {0, 0, 0};
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x) {
+    if (geom && !geom[i]) continue;
+    for (int c = 0; c < 3; ++c) acc[c] += (double)a[(size_t)c * N + i];
+  }
+  for (int c = 0; c < 3; ++c) sh[c][threadIdx.x] = acc[c];
+  __syncthreads();
+  for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+    if (threadIdx.x < s)
+      for (int c = 0; c < 3; ++c) sh[c][threadIdx.x] += sh[c][threadIdx.x + s];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0)
+    for (int c = 0; c < 3; ++c) partial[blockIdx.x * 3 + c] = sh[c][0];
+}
+
+__global__ void k_sample_final(const MagnetDev* __restrict__ mags, const GroupDev* __restrict__ groups, int slot,
+                               const double* __restrict__ partial, int nblocks, long long ngeo, int col) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  const GroupDev& G = groups[mags[slot].group];
+  if (G.samp_hi <= G.samp_lo) return;
+  double r[3] = {0, 0, 0};
+  for (int b = 0; b < nblocks; ++b)
+    for (int c = 0; c < 3; ++c) r[c] += partial[b * 3 + c];
+  for (int row = G.samp_lo; row < G.samp_hi; ++row)
+    for (int c = 0; c < 3; ++c) G.samp_out[(size_t)row * G.samp_row + col + c] = ngeo > 0 ? r[c] / ngeo : 0.0;
 }
 
 // Set m: normalise per cell inside the geometry (core/variable.cpp:76-87).

@@ -101,7 +101,7 @@ struct GroupDev {
   unsigned long long tmax_bits;  // max |torque| of the accepted state (double bits)
   long long steps, rejected, attempts, steps_left;
   int status;     // 0 idle, 1 running, 2 finished, 3 failed
-  int mode;       // 0 run(duration), 1 steps(n)
+  int mode;       // 0 run(duration), 1 steps(n), 2 sampled run through samp_t
   int phase;      // 0 regular steps, 1 final step of run()
   int adaptive;
   int k0_valid;
@@ -109,6 +109,12 @@ struct GroupDev {
   int map[9];     // buffer roles: [0] x0 (state), [1] xs (stage / new state), [2+s] k_s
   int torque_kind;  // right-hand side of the stages: 0 LLG torque, 1 damping torque only (relax)
   int thermal;      // some magnet of the group has thermal noise: k0 is never reused
+  // sampled run (mode 2): increasing time points samp_t[0, samp_n), the next one
+  // samp_k; rows [samp_lo, samp_hi) of the table samp_out (samp_row doubles
+  // per row: t, then <m> of every magnet of the group) are due after this attempt
+  const double* samp_t;
+  double* samp_out;
+  int samp_n, samp_k, samp_lo, samp_hi, samp_row;
 };
 
 enum { GS_IDLE = 0, GS_RUNNING = 1, GS_FINISHED = 2, GS_FAILED = 3 };

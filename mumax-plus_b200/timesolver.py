@@ -28,9 +28,12 @@ class TimeSolverOutput:
                 print("# " + "\t".join(self._keys), file=f)
 
     def write_line(self, time):
+        self._append(time, {key: func() for key, func in self._quantities.items()})
+
+    def _append(self, time, values):
         self._data["time"].append(time)
-        for key, func in self._quantities.items():
-            self._data[key].append(func())
+        for key in self._quantities.keys():
+            self._data[key].append(values[key])
         if self._file_name is not None:
             with open(self._file_name, "a") as f:
                 print(*[self._data[key][-1] for key in self._keys], sep="\t", file=f)
@@ -105,6 +108,12 @@ class TimeSolver:
         assert self.time <= timepoints[0], "The list of timepoints should lie in the future."
         self._assure_sensible_timestep()
         output = TimeSolverOutput(quantity_dict, file_name)
+        cols = self._magnetization_columns(quantity_dict)
+        if cols is not None:  # sampled on the device, one table back at the end
+            table = self._e.run_sampled(self._g, timepoints, len(self._world._magnets))
+            for row in table:
+                output._append(float(row[0]), {k: [float(v) for v in row[c:c + 3]] for k, c in cols.items()})
+            return output
         it = timepoints
         if tqdm:
             from tqdm import tqdm as _tqdm
@@ -113,6 +122,31 @@ class TimeSolver:
             self._e.run(self._g, tp - self.time)
             output.write_line(self.time)
         return output
+
+    def _magnetization_columns(self, quantity_dict):
+        """Column of each quantity in the device-sampled table when every one is
+        the average magnetization of a magnet of this world (the bound method
+        `magnet.magnetization.average`), else None (other callables are
+        evaluated on the host at every time point)."""
+        from .fieldquantity import FieldQuantity
+        from .parameter import Variable
+
+        order = {id(m): j for j, m in enumerate(self._world._magnets.values())}
+        cols = {}
+        for key, func in quantity_dict.items():
+            obj, fn = getattr(func, "__self__", None), getattr(func, "__func__", None)
+            if isinstance(obj, Variable) and fn is Variable.average:
+                magnet = obj._magnet
+            elif (isinstance(obj, FieldQuantity) and fn is FieldQuantity.average
+                  and obj._q == _abi.Q_MAGNETIZATION):
+                magnet = obj._magnet
+            else:
+                return None
+            j = order.get(id(magnet))
+            if j is None:
+                return None
+            cols[key] = 1 + 3 * j
+        return cols
 
     # -------------------------------------------------------- properties
     @property

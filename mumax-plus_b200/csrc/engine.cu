@@ -60,7 +60,7 @@ constexpr int MAX_FFT = 4096;
 constexpr int SMEM_MAX = 227 * 1024;
 // dynamic shared memory left next to the static descriptor copies of a block
 constexpr int SMEM_DYN_MAX = SMEM_MAX - 2048;
-constexpr int YZ_CLASSES = 10;  // k_yz launch classes (yz_class)
+constexpr int YZ_CLASSES = 20;  // k_yz / k_yzw / k_yzw32 launch classes (yz_class)
 
 // ------------------------------------------------------------ tableaus
 // core/butchertableau.cpp: Heun, Bogacki-Shampine, Cash-Karp, Fehlberg, Dormand-Prince
@@ -401,18 +401,29 @@ mpx_status upload_vec(mpx_engine* e, Work** d, const std::vector<T>& v) {
 int x_smem(const Magnet* m) {
   return ((m->ty + (m->ty + 1) / 2) * xrow_stride(m->P[0], m->ty) + m->P[0]) * (int)sizeof(float2);
 }
-int yz_smem(const Magnet* m) {
-  return (m->nkx * 3 * m->dev.n[2] * plen(m->P[1]) + m->P[1]) * (int)sizeof(float2);
+// y lengths of the warp-column y/z pass (k_yzw)
+bool yz_warp(int Py) { return Py >= 64 && Py <= 1024; }
+int yzw_threads_of(int Pz) { return Pz == 16 ? 384 : 256; }
+int yz_smem_of(int nz, int nkx, int Py) {
+  return (nkx * 3 * nz * (yz_warp(Py) ? qlen(Py) : plen(Py)) + Py) * (int)sizeof(float2);
 }
-// k_yz class of a magnet: log2 Pz, plus 5 for y transforms longer than 2048
-// (which need the radix-16 form).  The FFT plan of a magnet depends on its own
-// lengths only, so it computes the same alone and in any batch.
-int yz_class(const Magnet* m) { return ilog2(m->P[2]) + (m->P[1] > 2048 ? 5 : 0); }
+int yz_smem(const Magnet* m) { return yz_smem_of(m->dev.n[2], m->nkx, m->P[1]); }
+// y/z class of a magnet: 15 + log2 Pz for the warp-column pass of y length
+// 1024, 10 + log2 Pz for y lengths 64 .. 512, else log2 Pz, plus 5 for y
+// transforms longer than 2048 (which
+// need the radix-16 form).  The FFT plan of a magnet depends on its own lengths
+// only, so it computes the same alone and in any batch.
+int yz_class(const Magnet* m) {
+  if (m->P[1] == 1024) return 15 + ilog2(m->P[2]);
+  if (yz_warp(m->P[1])) return 10 + ilog2(m->P[2]);
+  return ilog2(m->P[2]) + (m->P[1] > 2048 ? 5 : 0);
+}
 constexpr int YZ_THREADS = 384;
 
 // Tile shapes.  Row tiles: about 4096 points of the padded x transform per
 // tile (4 rows above Px = 1024; up to TY_MAX rows of short transforms), 8 rows
-// at Px = 1024 (12 transformed rows: one per warp of the warp-row FFT), or
+// at Px = 1024 and 16 at Px = 512 (12 units of 1024 values for the 12 warps
+// of the warp-row FFT), or
 // of the row itself without demag.  y/z blocks: enough consecutive kx that a
 // block holds about YZ_VPT * YZ_THREADS points of y transforms.
 // Rows per tile are even (or the single row of ny = 1): the x passes pack the
@@ -421,11 +432,13 @@ constexpr int YZ_THREADS = 384;
 // same results alone and in any batch).
 int even_rows(int t, int ny) { return ny <= 1 ? 1 : std::max(2, t & ~1); }
 int choose_ty(int ny, int len) {
-  const int t = len == 1024 ? 8 : len > 1024 ? 4 : std::min(TY_MAX, std::max(1, 4096 / len));
+  const int t = len == 1024 ? 8 : len == 512 ? 16 : len > 1024 ? 4 : std::min(TY_MAX, std::max(1, 4096 / len));
   return even_rows(std::max(1, std::min(t, ny)), ny);
 }
-int choose_nkx(int nz, int Py, int Fh) {
-  return std::max(1, std::min(Fh, (YZ_VPT * YZ_THREADS) / (3 * nz * Py)));
+int choose_nkx(int nz, int Py, int Pz, int Fh) {
+  // warp columns (y lengths 64 .. 1024): 32 values per thread, one 1024-value unit per warp
+  const int pts = yz_warp(Py) ? 32 * yzw_threads_of(Pz) : YZ_VPT * YZ_THREADS;
+  return std::max(1, std::min(Fh, pts / (3 * nz * Py)));
 }
 
 int ycols_smem(const Magnet* m) { return (m->ncy * plen(m->P[1]) + m->P[1]) * (int)sizeof(float2); }
@@ -452,12 +465,16 @@ mpx_status launch_split(mpx_engine* e, const Work* ycw, int nyc, const Work* zmw
   return MPX_OK;
 }
 
-// k_yz launch for one class: the radix-8 form for z lengths up to 8 and y
-// lengths up to 2048, else the radix-16 form (with warp columns for y length
-// 1024 at z length 16)
+// y/z launch for one class: warp columns for y lengths 64 .. 1024 (k_yzw);
+// else the radix-8 form for z lengths up to 8 and y lengths up to 2048, the
+// radix-16 form otherwise (k_yz)
 mpx_status launch_yz(mpx_engine* e, int cls, const Work* work, int n, int smem, int stage, int gate) {
   if (n <= 0) return MPX_OK;
 #define MPX_YZ(PZ, LR) k_yz<PZ, LR><<<n, YZ_THREADS, smem, e->stream>>>(e->d_mags, e->d_groups, work, stage, gate, e->d_tw)
+#define MPX_YZW(PZ) \
+  k_yzw<PZ><<<n, yzw_threads<PZ>(), smem, e->stream>>>(e->d_mags, e->d_groups, work, stage, gate, e->d_tw)
+#define MPX_YZW32(PZ) \
+  k_yzw32<PZ><<<n, yzw_threads<PZ>(), smem, e->stream>>>(e->d_mags, e->d_groups, work, stage, gate, e->d_tw)
   switch (cls) {
     case 0: MPX_YZ(1, 3); break;
     case 1: MPX_YZ(2, 3); break;
@@ -467,9 +484,21 @@ mpx_status launch_yz(mpx_engine* e, int cls, const Work* work, int n, int smem, 
     case 6: MPX_YZ(2, 4); break;
     case 7: MPX_YZ(4, 4); break;
     case 8: MPX_YZ(8, 4); break;
-    default: MPX_YZ(16, 4); break;  // 4 and 9 (z length 16; y lengths up to 1024 in warp columns)
+    case 10: MPX_YZW(1); break;
+    case 11: MPX_YZW(2); break;
+    case 12: MPX_YZW(4); break;
+    case 13: MPX_YZW(8); break;
+    case 14: MPX_YZW(16); break;
+    case 15: MPX_YZW32(1); break;
+    case 16: MPX_YZW32(2); break;
+    case 17: MPX_YZW32(4); break;
+    case 18: MPX_YZW32(8); break;
+    case 19: MPX_YZW32(16); break;
+    default: MPX_YZ(16, 4); break;  // 4 and 9 (z length 16)
   }
 #undef MPX_YZ
+#undef MPX_YZW
+#undef MPX_YZW32
   e->launches++;
   return MPX_OK;
 }
@@ -1017,7 +1046,7 @@ mpx_status setup_magnet(mpx_engine* e, Magnet* m, const mpx_magnet_desc* d, bool
   D.Fh = m->P[0] / 2 + 1;
   D.kcomp = (m->P[2] == 1) ? 4 : 6;
   m->ty_def = choose_ty(D.n[1], m->demag ? m->P[0] : D.n[0]);
-  m->nkx_def = m->demag ? choose_nkx(D.n[2], m->P[1], D.Fh) : 1;
+  m->nkx_def = m->demag ? choose_nkx(D.n[2], m->P[1], m->P[2], D.Fh) : 1;
   m->ty = m->ty_def;
   m->nkx = m->nkx_def;
   plan_shapes({m}, &m->ty, &m->nkx);  // alone (plain evaluations, single solves)
@@ -1426,7 +1455,11 @@ mpx_status mpx_engine_create(int device, mpx_engine** out) {
                                (const void*)k_yz<8, 4>, (const void*)k_yz<16, 4>, (const void*)k_yz<1, 3>,
                                (const void*)k_yz<2, 3>, (const void*)k_yz<4, 3>, (const void*)k_yz<8, 3>,
                                (const void*)k_ycols<-1, 3>, (const void*)k_ycols<-1, 4>, (const void*)k_ycols<1, 3>,
-                               (const void*)k_ycols<1, 4>, (const void*)k_zmul<3>, (const void*)k_zmul<4>};
+                               (const void*)k_ycols<1, 4>, (const void*)k_zmul<3>, (const void*)k_zmul<4>,
+                               (const void*)k_yzw<1>, (const void*)k_yzw<2>, (const void*)k_yzw<4>,
+                               (const void*)k_yzw<8>, (const void*)k_yzw<16>, (const void*)k_yzw32<1>,
+                               (const void*)k_yzw32<2>, (const void*)k_yzw32<4>, (const void*)k_yzw32<8>,
+                               (const void*)k_yzw32<16>};
   for (const void* k : fft_kernels) {
     cudaFuncAttributes fa;
     CUDA_TRY(cudaFuncGetAttributes(&fa, k));
@@ -1671,9 +1704,9 @@ mpx_status mpx_magnet_bytes(const mpx_magnet_desc* d, int64_t* resident, int64_t
     const int kc = (P[2] == 1) ? 4 : 6;
     res += 8 * Fh * 3 * d->size[1] * d->size[2];                 // spectrum S[kx][c][z][y]
     res += 4 * Fh * (P[1] / 2 + 1) * (P[2] / 2 + 1) * kc;        // kernel spectrum
-    const int nkx = choose_nkx(d->size[2], P[1], (int)Fh);
+    const int nkx = choose_nkx(d->size[2], P[1], P[2], (int)Fh);
     res += (int64_t)sizeof(Work) * ((Fh + nkx - 1) / nkx);       // y/z work items
-    const int yzs = (d->size[2] * 3 * nkx * plen(P[1]) + P[1]) * (int)sizeof(float2);
+    const int yzs = yz_smem_of(d->size[2], nkx, P[1]);
     if (P[2] > 16 || yzs > SMEM_DYN_MAX) {  // split y/z path: T and its work items
       res += 8 * Fh * 3 * d->size[2] * P[1];
       const int64_t ncy = std::max<int64_t>(1, std::min<int64_t>(Fh * 3 * d->size[2], (YZ_VPT * YZ_THREADS) / P[1]));

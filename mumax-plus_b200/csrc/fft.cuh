@@ -263,16 +263,17 @@ __device__ __forceinline__ void fft_many(float2* buf, int logL, int ncols, int c
   }
 }
 
-// ------------------------------------------------ one 1024-point column per warp
-// A 1024-point transform as 32 x 32 (four-step): with n = j + 32 r and
-// k = s + 32 t,  X[s + 32 t] = sum_j W32^{j t} W1024^{j s} sum_r x[j + 32 r] W32^{r s}.
-// Lane j does the inner 32-point DFT over r and the twiddle W1024^{j s}; one
-// transpose through the warp's column in shared memory; lane s does the outer
-// 32-point DFT over j.  Only __syncwarp, no block barrier.
+// ------------------------------------------------ warp columns (four-step)
+// A transform of length L = 32 Q (Q = 2 .. 32) as Q x 32: with n = j + 32 r and
+// k = s + Q t,  X[s + Q t] = sum_j W32^{j t} W_L^{j s} sum_r x[j + 32 r] W_Q^{r s}.
+// A warp takes W = 32 / Q columns together, 32 values per lane: lane j does the
+// inner Q-point DFTs over r of every column and the twiddles W_L^{j s}; one
+// transpose through the columns in shared memory; lane c Q + s does the outer
+// 32-point DFT over j of column c.  Only __syncwarp, no block barrier.
 //
 // Column layout: element i at qidx(i) = i + i/32.  Lane j reading or writing
-// element j + 32 r, and lane s reading element j + 32 s, both touch 16
-// different 8-byte banks per half-warp.
+// element j + 32 r, and lanes (c, s) reading element j + 32 s of column c, both
+// touch 16 different 8-byte banks per half-warp.
 
 __device__ __forceinline__ int qidx(int i) { return i + (i >> 5); }
 __host__ __device__ constexpr int qlen(int L) { return L + (L >> 5); }
@@ -342,58 +343,103 @@ struct DftZ<1, DIR, ZH, LO> {
   __device__ __forceinline__ static void run(float2 (&)[1]) {}
 };
 
-// Twiddles W1024^{j s} of the four-step transform at [j * 31 + s - 1] (j in
-// [0, 32), s in [1, 32)): lanes j reading the same s hit 16 different banks.
-// 992 entries; the caller synchronises before use.
-__device__ __forceinline__ void load_tw1024(float2* dst, const float2* __restrict__ tw4096) {
-  for (int t = threadIdx.x; t < 32 * 31; t += blockDim.x) {
-    const int j = t / 31, s = t - j * 31 + 1;
-    dst[t] = __ldg(&tw4096[(j * s) << (TW_LOG - 10)]);
+// Twiddles W_L^{j s} of the four-step transform of length L = 32 Q at
+// [j * (Q - 1) + s - 1] (j in [0, 32), s in [1, Q)): lanes j reading the same s
+// hit 16 different banks (odd row stride).  32 (Q - 1) entries; the caller
+// synchronises before use.
+__device__ __forceinline__ void load_twq(float2* dst, const float2* __restrict__ tw4096, int logL) {
+  const int qm1 = (1 << (logL - 5)) - 1;
+  for (int t = threadIdx.x; t < 32 * qm1; t += blockDim.x) {
+    const int j = t / qm1, s = t - j * qm1 + 1;
+    dst[t] = __ldg(&tw4096[(j * s) << (TW_LOG - logL)]);
   }
 }
 
-// Inner step of lane j: v = the 32 values x[j + 32 r] (r = 0..31; with ZH the
-// values r >= 16 are zero and unread); on return v[s] holds
-// W1024^{j s} sum_r x[j + 32 r] W32^{r s}.
-template <int DIR, bool ZH>
-__device__ __forceinline__ void four_step_inner(float2 (&v)[32], const float2* twj, int lane) {
-  DftZ<32, DIR, ZH, false>::run(v);
-  const float2* t = twj + lane * 31 - 1;
+// Inner step of lane j for W = 32 / Q columns of length L = 32 Q held together:
+// v[c Q + r] = x_c[j + 32 r] (r < Q; with ZH the values r >= Q/2 are zero and
+// unread).  On return v[c Q + s] holds W_L^{j s} sum_r x_c[j + 32 r] W_Q^{r s}.
+template <int Q, int DIR, bool ZH>
+__device__ __forceinline__ void four_step_inner(float2 (&v)[32], const float2* twq, int lane) {
+  constexpr int W = 32 / Q;
 #pragma unroll
-  for (int s = 1; s < 32; ++s) v[s] = cmul(v[s], twiddle_raw<DIR>(t, s));
+  for (int c = 0; c < W; ++c) {
+    float2 u[Q];
+#pragma unroll
+    for (int r = 0; r < Q; ++r) u[r] = v[c * Q + r];
+    DftZ<Q, DIR, ZH, false>::run(u);
+#pragma unroll
+    for (int r = 0; r < Q; ++r) v[c * Q + r] = u[r];
+  }
+  if constexpr (Q > 1) {
+    const float2* t = twq + lane * (Q - 1) - 1;
+#pragma unroll
+    for (int s = 1; s < Q; ++s) {
+      const float2 w = twiddle_raw<DIR>(t, s);
+#pragma unroll
+      for (int c = 0; c < W; ++c) v[c * Q + s] = cmul(v[c * Q + s], w);
+    }
+  }
 }
 
-// Transpose the inner results of the warp through column C (qidx layout) and
-// do the outer step: on return lane s holds X[s + 32 t] in v[t] (t < 16 only
-// with LO).  C is free again when this returns.
-template <int DIR, bool LO>
-__device__ __forceinline__ void four_step_outer(float2 (&v)[32], float2* C, int lane) {
+// Transpose the inner results of the warp through its columns (column c at
+// base + c*cs, qidx layout; only the first nc of the W columns exist) and do the
+// outer 32-point step: on return lane l = c Q + s holds X_c[s + Q t] in v[t]
+// (t < 16 only with LO).  The columns are free again when this returns.
+// With cs = qlen(L) = 33 Q (mod 16: Q) the reads of the outer step, lanes
+// (c, s) at element j + 32 s of column c, hit 16 different banks per half-warp.
+template <int Q, int DIR, bool LO>
+__device__ __forceinline__ void four_step_outer(float2 (&v)[32], float2* base, int cs, int nc, int lane) {
+  constexpr int W = 32 / Q;
+  if constexpr (W == 1) {  // one column: no column index, no guard
 #pragma unroll
-  for (int s = 0; s < 32; ++s) C[lane + 33 * s] = v[s];  // element lane + 32 s
-  __syncwarp();
+    for (int s = 0; s < 32; ++s) base[lane + 33 * s] = v[s];  // element lane + 32 s
+    __syncwarp();
 #pragma unroll
-  for (int j = 0; j < 32; ++j) v[j] = C[j + 33 * lane];  // element j + 32 lane
+    for (int j = 0; j < 32; ++j) v[j] = base[j + 33 * lane];  // element j + 32 lane
+  } else {
+#pragma unroll
+    for (int c = 0; c < W; ++c)
+      if (c < nc)
+#pragma unroll
+        for (int s = 0; s < Q; ++s) base[c * cs + lane + 33 * s] = v[c * Q + s];  // element lane + 32 s
+    __syncwarp();
+    const int c = lane / Q, s = lane % Q;
+#pragma unroll
+    for (int j = 0; j < 32; ++j) v[j] = (c < nc) ? base[c * cs + j + 33 * s] : make_float2(0.f, 0.f);
+  }
   __syncwarp();
   DftZ<32, DIR, false, LO>::run(v);
 }
 
-// 1024-point transforms of `nrows` rows in shared memory (row r at buf + r*cs,
-// qidx layout), one row per warp at a time, in place.  ZIN: the upper half of
-// every input row is zero padding (not read).  LO: only the lower half of every
-// output row is written.  No block barrier: the caller synchronises before (rows
-// and twiddles written) and after.
-template <int DIR, bool ZIN, bool LO>
-__device__ __forceinline__ void warp_rows1024(float2* buf, int nrows, int cs, const float2* twj) {
+// Transforms of length 32 Q of `nrows` rows in shared memory (row r at
+// buf + r*cs, qidx layout), W = 32 / Q rows per warp at a time, in place.  ZIN:
+// the upper half of every input row is zero padding (not read).  LO: only the
+// lower half of every output row is written.  No block barrier: the caller
+// synchronises before (rows and twiddles written) and after.
+template <int Q, int DIR, bool ZIN, bool LO>
+__device__ __forceinline__ void warp_rows(float2* buf, int nrows, int cs, const float2* twq) {
+  constexpr int W = 32 / Q;
   const int lane = threadIdx.x & 31, nw = blockDim.x >> 5;
-  for (int row = threadIdx.x >> 5; row < nrows; row += nw) {
-    float2* R = buf + row * cs;
+  for (int r0 = (threadIdx.x >> 5) * W; r0 < nrows; r0 += nw * W) {
+    float2* R = buf + r0 * cs;
+    const int nc = W == 1 ? 1 : min(W, nrows - r0);
     float2 v[32];
 #pragma unroll
-    for (int r = 0; r < 32; ++r) v[r] = (!ZIN || r < 16) ? R[lane + 33 * r] : make_float2(0.f, 0.f);
-    four_step_inner<DIR, ZIN>(v, twj, lane);
-    four_step_outer<DIR, LO>(v, R, lane);
+    for (int c = 0; c < W; ++c)
 #pragma unroll
-    for (int t = 0; t < (LO ? 16 : 32); ++t) R[lane + 33 * t] = v[t];
+      for (int r = 0; r < Q; ++r)
+        v[c * Q + r] = (c < nc && (!ZIN || r < Q / 2)) ? R[c * cs + lane + 33 * r] : make_float2(0.f, 0.f);
+    four_step_inner<Q, DIR, ZIN>(v, twq, lane);
+    four_step_outer<Q, DIR, LO>(v, R, cs, nc, lane);
+    if constexpr (W == 1) {
+#pragma unroll
+      for (int t = 0; t < (LO ? 16 : 32); ++t) R[lane + 33 * t] = v[t];
+    } else {
+      const int c = lane / Q, s = lane % Q;
+      if (c < nc)
+#pragma unroll
+        for (int t = 0; t < (LO ? 16 : 32); ++t) R[c * cs + qidx(s + Q * t)] = v[t];
+    }
   }
 }
 
@@ -401,12 +447,13 @@ __device__ __forceinline__ void warp_rows1024(float2* buf, int nrows, int cs, co
 // else pidx.
 __device__ __forceinline__ int xidx(int i, int sh) { return i + (i >> sh); }
 
-// Row stride of the x passes for tiles of ty rows.  1024-point rows (qidx
-// layout): qlen plus 16 / (row slots of the tile, ty rounded up to a power of
-// two) complex values, so that the gather and the unpack, whose half-warps
-// touch the same few x of every row slot, hit 16 different 8-byte banks.
+// Row stride of the x passes for tiles of ty rows.  512- and 1024-point rows
+// (warp rows, qidx layout): qlen plus 16 / (row slots of the tile, ty rounded up
+// to a power of two) complex values, so that the gather and the unpack, whose
+// half-warps touch the same few x of every row slot, hit 16 different 8-byte
+// banks (the outer step of these lengths reads within one row per half-warp).
 __host__ __device__ inline int xrow_stride(int L, int ty) {
-  if (L != 1024) return xstride(L);
+  if (L != 1024 && L != 512) return xstride(L);
   int slots = 1;
   while (slots < ty) slots <<= 1;
   return qlen(L) + (slots >= 16 ? 1 : 16 / slots);

@@ -147,9 +147,9 @@ __global__ void __launch_bounds__(X_THREADS_MAX, 2) k_xfwd(const MagnetDev* __re
   const float* x0 = M.buf[G.map[0]];
   const int rowbase = nx * (y0 + ny * z);
   float2* tws = sm + (ty + nzrows) * cs;  // twiddles of length L
-  const bool wrow = logL == 10;  // 1024-point rows: one warp per row (four-step)
+  const bool wrow = logL == 10 || logL == 9;  // 1024- / 512-point rows: warp rows (four-step)
   const int sh = wrow ? 5 : 4;
-  if (wrow) load_tw1024(tws, tw);
+  if (wrow) load_twq(tws, tw, logL);
   else load_twiddles<3>(tws, tw, logL);
 
   // only the lower half of each row: the upper half (x >= L/2 >= nx) is zero
@@ -181,7 +181,8 @@ __global__ void __launch_bounds__(X_THREADS_MAX, 2) k_xfwd(const MagnetDev* __re
   }
   __syncthreads();
   if (wrow) {
-    warp_rows1024<-1, true, false>(sm, ty + nzrows, cs, tws);
+    if (logL == 10) warp_rows<32, -1, true, false>(sm, ty + nzrows, cs, tws);
+    else warp_rows<16, -1, true, false>(sm, ty + nzrows, cs, tws);
     __syncthreads();
   } else {
     fft_many<-1, 3, 1>(sm, logL, ty + nzrows, cs, tws);
@@ -322,8 +323,9 @@ __device__ __forceinline__ void zstage_pair(float2* D, int cs, const MagnetDev& 
       if (n < nz && (n & 1) == half) D[(c * nz + n) * cs + pky] = v[c][n];
 }
 
+template <bool Q5 = false>
 __device__ __forceinline__ void zstage_single(float2* D, int cs, const MagnetDev& M, int kx, int ky, int Py) {
-  const int pky = pidx(ky);
+  const int pky = Q5 ? qidx(ky) : pidx(ky);
   float2 v0 = D[pky], v1 = D[cs + pky], v2 = D[2 * cs + pky];
   const int hy = Py / 2 + 1;
   const int kyp = min(ky, Py - ky);
@@ -336,61 +338,6 @@ __device__ __forceinline__ void zstage_single(float2* D, int cs, const MagnetDev
   D[pky] = v0;
   D[cs + pky] = v1;
   D[2 * cs + pky] = v2;
-}
-
-// k_yz for y length 1024 (z length 16): every warp transforms whole columns in
-// registers (four-step 32 x 32), reading its columns of S straight into the
-// inner step and writing the y < ny outputs straight back; the block
-// synchronises only around the z stage.  Columns in the qidx layout.
-template <int PZ>
-__device__ __forceinline__ void yz_warp1024(const MagnetDev& M, int kx0, int nkx, float2* sm,
-                                            const float2* __restrict__ tw) {
-  constexpr int Py = 1024, cs = qlen(Py);
-  const int ny = M.n[1], nz = M.n[2];
-  const int ncol = nkx * 3 * nz;
-  float2* D = sm;
-  float2* twj = sm + ncol * cs;
-  load_tw1024(twj, tw);
-  __syncthreads();
-  float2* S = M.spec + (size_t)kx0 * 3 * nz * ny;
-  const int lane = threadIdx.x & 31, nw = blockDim.x >> 5;
-  for (int col = threadIdx.x >> 5; col < ncol; col += nw) {
-    const float2* __restrict__ Sc = S + (size_t)col * ny;
-    float2 v[32];
-#pragma unroll
-    for (int r = 0; r < 16; ++r) {  // y = lane + 32 r < 512; y >= ny is zero padding
-      const int y = lane + 32 * r;
-      v[r] = (y < ny) ? __ldg(Sc + y) : make_float2(0.f, 0.f);
-    }
-#pragma unroll
-    for (int r = 16; r < 32; ++r) v[r] = make_float2(0.f, 0.f);
-    four_step_inner<-1, true>(v, twj, lane);
-    float2* C = D + col * cs;
-    four_step_outer<-1, false>(v, C, lane);
-#pragma unroll
-    for (int t = 0; t < 32; ++t) C[lane + 33 * t] = v[t];  // ky = lane + 32 t
-  }
-  __syncthreads();
-  // lanes 2u and 2u+1 share one (kx, ky): the even and odd kz halves
-  for (int t = threadIdx.x; t < (2 * nkx) << 10; t += blockDim.x) {
-    const int u = t >> 1, j = u >> 10;
-    zstage_pair<PZ, true>(D + j * 3 * nz * cs, cs, M, kx0 + j, u & (Py - 1), t & 1, nz, Py);
-  }
-  __syncthreads();
-  for (int col = threadIdx.x >> 5; col < ncol; col += nw) {
-    float2* C = D + col * cs;
-    float2 v[32];
-#pragma unroll
-    for (int r = 0; r < 32; ++r) v[r] = C[lane + 33 * r];  // ky = lane + 32 r
-    four_step_inner<1, false>(v, twj, lane);
-    four_step_outer<1, true>(v, C, lane);
-    float2* __restrict__ Sc = S + (size_t)col * ny;
-#pragma unroll
-    for (int t = 0; t < 16; ++t) {  // y = lane + 32 t < 512: only y < ny is kept
-      const int y = lane + 32 * t;
-      if (y < ny) Sc[y] = v[t];
-    }
-  }
 }
 
 // MAXLR = 4: radix-16 passes, 16 values per thread (y lengths up to 4096, one
@@ -411,12 +358,6 @@ __global__ void __launch_bounds__(384, MAXLR == 3 ? 2 : 1)
   const int kx0 = wk.z, nkx = wk.y0;
   const int ny = M.n[1], nz = M.n[2];
   const int logPy = M.logP[1], Py = 1 << logPy, cs = plen(Py);
-  if constexpr (PZ == 16 && MAXLR == 4) {
-    if (logPy == 10) {
-      yz_warp1024<PZ>(M, kx0, nkx, sm, tw);
-      return;
-    }
-  }
   float2* S = M.spec + (size_t)kx0 * 3 * nz * ny;  // the nkx slabs are consecutive
   float2* D = sm;  // [nkx][3*nz] padded columns of length Py
   const int ncol = nkx * 3 * nz;
@@ -461,6 +402,143 @@ __global__ void __launch_bounds__(384, MAXLR == 3 ? 2 : 1)
     const int col = e >> logPy, y = e & (Py - 1);
     if (y < ny) S[col * ny + y] = D[col * cs + pidx(y)];
   }
+}
+
+// ---------------------------------------------------------------- k_yzw
+// The y/z pass for y lengths 64 .. 1024 (Py = 32 Q): every warp transforms
+// whole columns in registers (four-step Q x 32, 32 / Q columns at a time),
+// reading its columns of S straight into the inner step and writing the y < ny
+// outputs straight back; the block synchronises only around the z stage.
+// Columns in the qidx layout, cs = qlen(Py).
+
+// Forward y transforms of the ncol columns of S (ny rows each, zero padding
+// above) into D.
+template <int Q>
+__device__ __forceinline__ void yzw_forward(const float2* __restrict__ S, int ny, float2* D, int ncol,
+                                            const float2* twq) {
+  constexpr int W = 32 / Q, cs = qlen(32 * Q);
+  const int lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+  const int lc = lane / Q, ls = lane % Q;  // column and s of this lane in the outer step
+  for (int col0 = (threadIdx.x >> 5) * W; col0 < ncol; col0 += nw * W) {
+    const int nc = W == 1 ? 1 : min(W, ncol - col0);
+    float2 v[32];
+#pragma unroll
+    for (int c = 0; c < W; ++c)
+#pragma unroll
+      for (int r = 0; r < Q; ++r) {  // y = lane + 32 r < Py/2; y >= ny is zero padding
+        const int y = lane + 32 * r;
+        v[c * Q + r] = (c < nc && r < Q / 2 && y < ny) ? __ldg(S + (size_t)(col0 + c) * ny + y) : make_float2(0.f, 0.f);
+      }
+    four_step_inner<Q, -1, true>(v, twq, lane);
+    float2* C = D + col0 * cs;
+    four_step_outer<Q, -1, false>(v, C, cs, nc, lane);
+    if constexpr (W == 1) {
+#pragma unroll
+      for (int t = 0; t < 32; ++t) C[lane + 33 * t] = v[t];  // ky = lane + 32 t
+    } else if (lc < nc) {
+#pragma unroll
+      for (int t = 0; t < 32; ++t) C[lc * cs + qidx(ls + Q * t)] = v[t];  // ky = s + Q t
+    }
+  }
+}
+
+// Inverse y transforms of the columns of D; the y < ny outputs go to S.
+template <int Q>
+__device__ __forceinline__ void yzw_inverse(float2* __restrict__ S, int ny, float2* D, int ncol, const float2* twq) {
+  constexpr int W = 32 / Q, cs = qlen(32 * Q);
+  const int lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+  const int lc = lane / Q, ls = lane % Q;
+  for (int col0 = (threadIdx.x >> 5) * W; col0 < ncol; col0 += nw * W) {
+    const int nc = W == 1 ? 1 : min(W, ncol - col0);
+    float2* C = D + col0 * cs;
+    float2 v[32];
+#pragma unroll
+    for (int c = 0; c < W; ++c)
+#pragma unroll
+      for (int r = 0; r < Q; ++r) v[c * Q + r] = (c < nc) ? C[c * cs + lane + 33 * r] : make_float2(0.f, 0.f);
+    four_step_inner<Q, 1, false>(v, twq, lane);
+    four_step_outer<Q, 1, true>(v, C, cs, nc, lane);
+    const int cl = W == 1 ? 0 : lc, sl = W == 1 ? lane : ls;
+    if (cl < nc) {
+      float2* __restrict__ Sc = S + (size_t)(col0 + cl) * ny;
+#pragma unroll
+      for (int t = 0; t < 16; ++t) {  // y = s + Q t < Py/2: only y < ny is kept
+        const int y = sl + Q * t;
+        if (y < ny) Sc[y] = v[t];
+      }
+    }
+  }
+}
+
+// Threads per block: 384 at z length 16 (the z stage needs ~128 registers:
+// one block per SM), else 256 (128 registers, two blocks per SM).
+template <int PZ>
+constexpr int yzw_threads() { return PZ == 16 ? 384 : 256; }
+
+// The whole y/z pass of one block for y length Py = 32 Q (every length and
+// stride a compile-time constant).
+template <int PZ, int Q>
+__device__ __forceinline__ void yzw_body(const MagnetDev& M, int kx0, int nkx, float2* sm,
+                                         const float2* __restrict__ tw) {
+  constexpr int Py = 32 * Q, cs = qlen(Py);
+  constexpr int LOGPY = Q == 2 ? 6 : Q == 4 ? 7 : Q == 8 ? 8 : Q == 16 ? 9 : 10;
+  const int ny = M.n[1], nz = M.n[2];
+  const int ncol = nkx * 3 * nz;
+  float2* D = sm;
+  float2* twq = sm + ncol * cs;
+  load_twq(twq, tw, LOGPY);
+  __syncthreads();
+  float2* S = M.spec + (size_t)kx0 * 3 * nz * ny;
+  yzw_forward<Q>(S, ny, D, ncol, twq);
+  __syncthreads();
+  if constexpr (PZ == 1) {
+    for (int t = threadIdx.x; t < nkx << LOGPY; t += blockDim.x) {
+      const int j = t >> LOGPY;
+      zstage_single<true>(D + j * 3 * cs, cs, M, kx0 + j, t & (Py - 1), Py);
+    }
+  } else {
+    // lanes 2u and 2u+1 share one (kx, ky): the even and odd kz halves
+    for (int t = threadIdx.x; t < (2 * nkx) << LOGPY; t += blockDim.x) {
+      const int u = t >> 1, j = u >> LOGPY;
+      zstage_pair<PZ, true>(D + j * 3 * nz * cs, cs, M, kx0 + j, u & (Py - 1), t & 1, nz, Py);
+    }
+  }
+  __syncthreads();
+  yzw_inverse<Q>(S, ny, D, ncol, twq);
+}
+
+// Work item: magnet, first kx in z, number of consecutive kx in y0.  y lengths 64 .. 512.
+template <int PZ>
+__global__ void __launch_bounds__(yzw_threads<PZ>(), PZ == 16 ? 1 : 2)
+    k_yzw(const MagnetDev* __restrict__ mags, const GroupDev* __restrict__ groups, const Work* __restrict__ work,
+          int stage, int gate, const float2* __restrict__ tw) {
+  extern __shared__ float2 sm[];
+  __shared__ MagnetDev M;
+  __shared__ GroupDev G;
+  const Work wk = work[blockIdx.x];
+  if (!load_descs(M, G, mags, groups, wk.mag, gate, stage)) return;
+  const int kx0 = wk.z, nkx = wk.y0;
+  switch (M.logP[1]) {
+    case 6: yzw_body<PZ, 2>(M, kx0, nkx, sm, tw); break;
+    case 7: yzw_body<PZ, 4>(M, kx0, nkx, sm, tw); break;
+    case 8: yzw_body<PZ, 8>(M, kx0, nkx, sm, tw); break;
+    default: yzw_body<PZ, 16>(M, kx0, nkx, sm, tw); break;
+  }
+}
+
+// y length 1024 in a kernel of its own: the body of one length keeps the hot
+// code small (several fully unrolled bodies in one kernel stalled on
+// instruction fetch).
+template <int PZ>
+__global__ void __launch_bounds__(yzw_threads<PZ>(), PZ == 16 ? 1 : 2)
+    k_yzw32(const MagnetDev* __restrict__ mags, const GroupDev* __restrict__ groups, const Work* __restrict__ work,
+            int stage, int gate, const float2* __restrict__ tw) {
+  extern __shared__ float2 sm[];
+  __shared__ MagnetDev M;
+  __shared__ GroupDev G;
+  const Work wk = work[blockIdx.x];
+  if (!load_descs(M, G, mags, groups, wk.mag, gate, stage)) return;
+  yzw_body<PZ, 32>(M, wk.z, wk.y0, sm, tw);
 }
 
 // ------------------------------------------------------------- epilogue
@@ -747,9 +825,9 @@ __global__ void __launch_bounds__(X_THREADS_MAX, 2) k_xinv(const MagnetDev* __re
   const int Fh = M.Fh;
   float2* rows_z = sm + ty * cs;
   float2* tws = sm + (ty + nzrows) * cs;  // twiddles of length L
-  const bool wrow = logL == 10;  // 1024-point rows: one warp per row (four-step)
+  const bool wrow = logL == 10 || logL == 9;  // 1024- / 512-point rows: warp rows (four-step)
   const int sh = wrow ? 5 : 4;
-  if (wrow) load_tw1024(tws, tw);
+  if (wrow) load_twq(tws, tw, logL);
   else load_twiddles<3>(tws, tw, logL);
   __shared__ NbRows T;
   __shared__ float cf[8];  // FSAL error weights dt (b1 - b2) of the stages
@@ -797,7 +875,8 @@ __global__ void __launch_bounds__(X_THREADS_MAX, 2) k_xinv(const MagnetDev* __re
   }
   __syncthreads();
   if (wrow) {  // only x < nx <= L/2 is used
-    warp_rows1024<1, false, true>(sm, ty + nzrows, cs, tws);
+    if (logL == 10) warp_rows<32, 1, false, true>(sm, ty + nzrows, cs, tws);
+    else warp_rows<16, 1, false, true>(sm, ty + nzrows, cs, tws);
     __syncthreads();
   } else {
     fft_many<1, 3, 2>(sm, logL, ty + nzrows, cs, tws);

@@ -388,3 +388,37 @@ def test_thick_magnet_pbc_and_trajectory(mpx):
     a = np.array(magnet.magnetization.average())
     b = np.array(ow.average(q, abi.Q_MAGNETIZATION))
     assert float(np.max(np.abs(a - b))) < 1e-4
+
+
+@pytest.mark.parametrize("size", [(6, 40, 3), (5, 70, 1), (4, 200, 2), (3, 300, 6), (3, 400, 2), (200, 6, 2),
+                                  (300, 5, 1), (130, 70, 4)])
+def test_demag_warp_transform_lengths(mpx, size):
+    """y lengths 128 .. 1024 (k_yzw, k_yzw32: four-step Q x 32 with 32/Q columns per warp) at z lengths 1 .. 16,
+    and x rows of 512 and 1024 points (warp rows)."""
+    compare(MagnetSpec(size=size, cellsize=(1e-9, 2e-9, 1.5e-9), msat=8e5), mpx, [abi.Q_DEMAG_FIELD])
+
+
+def test_warp_transform_trajectory_vs_oracle(mpx):
+    """Dormand-Prince stages through the warp transforms of both axes (Px = 512, Py = 128) and the lean stage
+    epilogue (uniform parameters): <m>(t) and the field m(t) against the FP64 oracle."""
+    s = MagnetSpec(size=(132, 40, 2), cellsize=(3e-9, 3e-9, 3e-9), msat=8e5, aex=1.3e-11, alpha=0.1,
+                   dmi={"xxz": 1e-3, "yyz": 1e-3}, ku1=1e5, anisU=(0.0, 0.0, 1.0), world_bias=(0.0, 0.01, 0.0))
+    m0 = random_m(s.shape, seed=8, smooth=3)
+    ow, q = s.oracle_world(m0)
+    ow.set_method("DormandPrince")
+    world, magnet = s.product(mpx, m0)
+    world.timesolver.set_method("DormandPrince")
+    dt0 = ow.sensible_timestep()
+    ow.timestep = dt0
+    world.timesolver.timestep = dt0
+    worst = worst_cell = 0.0
+    for k in range(1, 4):
+        tp = k * 4e-12
+        ow.run(tp - ow.time)
+        world.timesolver._e.run(world._group, tp - world.timesolver.time)
+        a = np.array(magnet.magnetization.average())
+        b = np.array(ow.average(q, abi.Q_MAGNETIZATION))
+        worst = max(worst, float(np.max(np.abs(a - b))))
+        worst_cell = max(worst_cell, float(np.max(np.abs(magnet.magnetization.get() - ow.get_m(q)))))
+    assert worst < 1e-5, worst
+    assert worst_cell < 1e-3, worst_cell

@@ -180,3 +180,30 @@ def test_grid_semantics():
     assert not g.overlaps(mpx.Grid((2, 2, 2), (5, 2, 3)))
     with pytest.raises(ValueError):
         mpx.Grid((1, 2))
+
+
+def test_solve_takes_device_sampling_only_for_magnetization_averages():
+    """TimeSolver.solve uses the device-sampled table (mpx_solver_run_sampled) when every quantity is the bound
+    average of the magnetization of a magnet of this world; any other callable keeps the host loop."""
+    import mumaxplus_b200 as mpx
+    from mumaxplus_b200 import _abi
+    from mumaxplus_b200.fieldquantity import FieldQuantity
+    from mumaxplus_b200.parameter import Variable
+    from mumaxplus_b200.timesolver import TimeSolver
+
+    class _World:
+        pass
+
+    w = _World()
+    a, b, stranger = _FakeMagnet(), _FakeMagnet(), _FakeMagnet()
+    w._magnets = {"a": a, "b": b}
+    ts = TimeSolver(w)
+    cols = ts._magnetization_columns({"ma": Variable(a).average, "mb": Variable(b).average,
+                                      "fa": FieldQuantity(a, _abi.Q_MAGNETIZATION, "m", "").average})
+    assert cols == {"ma": 1, "mb": 4, "fa": 1}
+    assert ts._magnetization_columns({}) == {}
+    assert ts._magnetization_columns({"m": lambda: Variable(a).average()}) is None
+    assert ts._magnetization_columns({"m": Variable(stranger).average}) is None
+    assert ts._magnetization_columns({"h": FieldQuantity(a, _abi.Q_DEMAG_FIELD, "h", "T").average}) is None
+    assert ts._magnetization_columns({"m": Variable(a).average, "e": Variable(a).get}) is None
+    assert mpx.TimeSolver is TimeSolver

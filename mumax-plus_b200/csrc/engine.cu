@@ -136,6 +136,7 @@ struct Magnet {
   unsigned terms_base = 0;        // TERM_* / FLAG_* from the parameters, before stray fields
   bool msat_zero = false;
   bool stray_src = true, stray_dst = true;
+  bool hull = false;  // helper of an FFT stray-field pair: never stepped, not in its group's magnet list
   int pbc_rep[3] = {0, 0, 0};
   double cs_d[3] = {1, 1, 1};
   float* hstray = nullptr;        // stray field of the other magnets (3N floats), when a destination
@@ -217,8 +218,10 @@ struct mpx_engine {
   // stray-field pairs (source -> destination magnet of one group)
   struct Pair {
     int src, dst;
-    float* k;
+    float* k;         // direct-sum table (brute-force form), or NULL
     StrayTable tab;
+    int hull = -1;    // FFT form: slot of the helper magnet spanning A and B
+    int launches = 1; // kernels per evaluation
   };
   std::vector<Pair> pairs;
   bool pairs_dirty = true;
@@ -571,7 +574,7 @@ mpx_status retile(mpx_engine* e, Magnet* m, int ty, int nkx) {
 long long active_set(mpx_engine* e, std::vector<Magnet*>& act) {
   act.clear();
   for (auto& mp : e->mags) {
-    if (!mp) continue;
+    if (!mp || mp->hull) continue;
     const Group* g = (mp->group >= 0 && mp->group < (int)e->groups.size()) ? e->groups[mp->group].get() : nullptr;
     if (g && g->active) act.push_back(mp.get());
   }
@@ -599,7 +602,7 @@ mpx_status rebuild_tables(mpx_engine* e) {
   for (int c = 0; c < YZ_CLASSES; ++c) e->smem_yz[c] = 0;
   // only the magnets of started groups: finished and idle solves cost no blocks
   for (auto& mp : e->mags) {
-    if (!mp) continue;
+    if (!mp || mp->hull) continue;  // helpers of FFT stray-field pairs are launched by launch_pairs
     Magnet* m = mp.get();
     const Group* g = (m->group >= 0 && m->group < (int)e->groups.size()) ? e->groups[m->group].get() : nullptr;
     if (!g || !g->active) continue;
@@ -662,9 +665,65 @@ mpx_status rebuild_tables(mpx_engine* e) {
 // with A an enabled source (msat not zero) and B an enabled destination gets
 // the FP32 table of the Newell tensor (built in FP64, PBC images included) of
 // their displacements; B gets a stray-field buffer and FLAG_STRAY.
+mpx_status setup_magnet(mpx_engine* e, Magnet* m, const mpx_magnet_desc* d, bool keep_fields);
+void release_all(mpx_engine* e, Magnet* m);
+
+// Pairs whose direct sum would take at least this many cell interactions use
+// the FFT form (worlds without periodic boundaries).
+constexpr long long STRAY_FFT_MIN_INTERACTIONS = 1LL << 22;
+
+// Helper magnet of an FFT pair: the bounding box of A and B in world cells,
+// msat 1, demag only, no periodic images; its magnetisation buffer starts at zero.
+mpx_status create_hull(mpx_engine* e, const Magnet* A, const Magnet* B, int* out) {
+  mpx_magnet_desc d;
+  std::memset(&d, 0, sizeof d);
+  for (int ax = 0; ax < 3; ++ax) {
+    const int lo = std::min(A->dev.o[ax], B->dev.o[ax]);
+    const int hi = std::max(A->dev.o[ax] + A->dev.n[ax], B->dev.o[ax] + B->dev.n[ax]);
+    d.size[ax] = hi - lo;
+    d.origin[ax] = lo;
+    d.cellsize[ax] = A->cs_d[ax];
+  }
+  d.msat.uniform = 1.0;
+  d.scale_exchange = 1.0;
+  d.enable_demag = 1;
+  d.stray_source_off = d.stray_destination_off = 1;
+  int slot = -1;
+  for (int i = 0; i < (int)e->mags.size(); ++i)
+    if (!e->mags[i]) { slot = i; break; }
+  if (slot < 0) {
+    slot = (int)e->mags.size();
+    e->mags.emplace_back();
+  }
+  auto m = std::make_unique<Magnet>();
+  std::memset(&m->dev, 0, sizeof(MagnetDev));
+  m->slot = slot;
+  m->group = A->group;
+  m->hull = true;
+  mpx_status st = setup_magnet(e, m.get(), &d, false);
+  if (st == MPX_OK) {
+    const cudaError_t ce = cudaMemsetAsync(m->dev.buf[0], 0, sizeof(float) * 3 * (size_t)m->dev.N, e->stream);
+    if (ce != cudaSuccess) st = fail(MPX_ERR_CUDA, cudaGetErrorString(ce));
+  }
+  if (st != MPX_OK) {
+    std::string msg = g_last_error;
+    release_all(e, m.get());
+    g_last_error = msg;
+    return st;
+  }
+  e->mags[slot] = std::move(m);
+  *out = slot;
+  return MPX_OK;
+}
+
 mpx_status rebuild_pairs(mpx_engine* e) {
   for (auto& p : e->pairs) pfree(e, p.k);
   e->pairs.clear();
+  for (auto& mp : e->mags)  // helpers of the previous pairs
+    if (mp && mp->hull) {
+      release_all(e, mp.get());
+      mp.reset();
+    }
   std::vector<bool> is_dst(e->mags.size(), false);
   for (auto& gp : e->groups) {
     if (!gp) continue;
@@ -677,6 +736,17 @@ mpx_status rebuild_pairs(mpx_engine* e) {
         mpx_engine::Pair p;
         p.src = a;
         p.dst = b;
+        p.k = nullptr;
+        bool periodic = false;
+        for (int ax = 0; ax < 3; ++ax) periodic = periodic || A->dev.mg[ax] > 0 || B->dev.mg[ax] > 0;
+        if (!periodic && (long long)A->dev.N * B->dev.N >= STRAY_FFT_MIN_INTERACTIONS) {
+          MPX_TRY(create_hull(e, A, B, &p.hull));
+          const Magnet* H = e->mags[p.hull].get();
+          p.launches = 4 + (H->split ? 3 : 1);
+          e->pairs.push_back(p);
+          is_dst[b] = true;
+          continue;
+        }
         KernelGeom g;
         for (int ax = 0; ax < 3; ++ax) {
           p.tab.K[ax] = A->dev.n[ax] + B->dev.n[ax] - 1;
@@ -698,9 +768,9 @@ mpx_status rebuild_pairs(mpx_engine* e) {
   }
   for (size_t i = 0; i < e->mags.size(); ++i) {
     Magnet* m = e->mags[i].get();
-    if (!m) continue;
+    if (!m || m->hull) continue;
     unsigned terms = m->terms_base;
-    if (is_dst[i]) {
+    if (i < is_dst.size() && is_dst[i]) {
       if (!m->hstray) MPX_TRY(palloc(e, (void**)&m->hstray, sizeof(float) * 3 * (size_t)m->dev.N));
       terms |= TERM_EXT | FLAG_STRAY;
     } else if (m->hstray) {
@@ -728,6 +798,33 @@ mpx_status launch_pairs(mpx_engine* e, int dst, int stage, int gate) {
     const bool add = std::find(seen.begin(), seen.end(), p.dst) != seen.end();
     if (!add) seen.push_back(p.dst);
     Magnet* B = get_mag(e, p.dst);
+    if (p.hull >= 0) {  // FFT form through the helper magnet
+      Magnet* A = get_mag(e, p.src);
+      Magnet* H = get_mag(e, p.hull);
+      k_hull_scatter<<<(A->dev.N + 255) / 256, 256, 0, e->stream>>>(e->d_mags, e->d_groups, p.src, p.hull, stage,
+                                                                     gate);
+      const int ntile = (int)H->tiles.size(), sx = x_smem(H), nt = x_threads(H);
+      k_xfwd<false><<<ntile, nt, sx, e->stream>>>(e->d_mags, e->d_groups, H->d_tiles, stage, gate, H->dev.buf[0],
+                                                  e->d_tw);
+      if (H->split)
+        MPX_TRY(launch_split(e, H->d_ycw, (int)H->ycw.size(), H->d_zmw, (int)H->zmw.size(), ycols_smem(H),
+                             zmul_smem(H), H->P[1], H->P[2], stage, gate));
+      else
+        MPX_TRY(launch_yz(e, yz_class(H), H->d_kxw, (int)H->kxw.size(), yz_smem(H), stage, gate));
+      EpiArgs ea;
+      ea.mode = EPI_EVAL;
+      ea.stage = stage;
+      ea.quantity = MPX_Q_DEMAG_FIELD;
+      ea.fsal_err = 0;
+      ea.gate = gate;
+      ea.out = H->dev.buf[1];
+      ea.msrc = H->dev.buf[0];
+      k_xinv<<<ntile, nt, sx, e->stream>>>(e->d_mags, e->d_groups, H->d_tiles, ea, e->d_tw);
+      k_hull_gather<<<(B->dev.N + 255) / 256, 256, 0, e->stream>>>(e->d_mags, e->d_groups, p.hull, p.dst, stage, gate,
+                                                                    add ? 1 : 0, B->hstray);
+      e->launches += 4;
+      continue;
+    }
     k_stray_pair<<<(B->dev.N + 255) / 256, 256, 0, e->stream>>>(e->d_mags, e->d_groups, p.src, p.dst, p.tab, stage,
                                                                 gate, add ? 1 : 0, B->hstray);
     e->launches++;
@@ -1295,7 +1392,9 @@ int attempt_launches(const mpx_engine* e, const TableauDev& T, int first_stage) 
   int nyz = 0;
   for (int c = 0; c < YZ_CLASSES; ++c) nyz += e->n_kx_demag[c] > 0 ? 1 : 0;
   if (e->n_t_ycols > 0) nyz += 3;
-  int per = 1 + (int)e->pairs.size() * ns + 2 * e->samp_magnets;  // controller, stray-field pairs, samples
+  int npair = 0;
+  for (const auto& p : e->pairs) npair += p.launches;
+  int per = 1 + npair * ns + 2 * e->samp_magnets;  // controller, stray-field pairs, samples
   if (e->n_t_demag > 0) per += (2 + nyz) * ns + (T.fsal ? 0 : 1);
   if (e->n_t_local > 0) per += ns + (ns - (first_stage == 0 ? 1 : 0)) + (T.fsal ? 0 : 1);
   return per;
@@ -1722,7 +1821,7 @@ mpx_status mpx_magnet_bytes(const mpx_magnet_desc* d, int64_t* resident, int64_t
 
 mpx_status mpx_magnet_remove(mpx_engine* e, int magnet) {
   Magnet* m = get_mag(e, magnet);
-  if (!m) return fail(MPX_ERR_RANGE, "no such magnet");
+  if (!m || m->hull) return fail(MPX_ERR_RANGE, "no such magnet");
   DeviceGuard guard(e->device);
   // frees are stream-ordered: attempts queued before still see the buffers
   Group* g = get_group(e, m->group);
@@ -1730,6 +1829,7 @@ mpx_status mpx_magnet_remove(mpx_engine* e, int magnet) {
   release_all(e, m);
   e->mags[magnet].reset();
   e->tables_dirty = true;
+  e->pairs_dirty = true;
   return MPX_OK;
 }
 

@@ -86,3 +86,47 @@ def test_two_magnet_trajectory(mpx):
             b = np.array(ow.average(q, abi.Q_MAGNETIZATION))
             worst = max(worst, float(np.max(np.abs(a - b))))
     assert worst < 1e-4, worst
+
+
+def _large_specs(dz=0):
+    A = MagnetSpec(size=(48, 24, 2), cellsize=CS, msat=8e5, aex=1.1e-11, alpha=0.2)
+    B = MagnetSpec(size=(48, 20, 2), origin=(52, 6, dz), cellsize=CS, msat=6e5, aex=1.3e-11, alpha=0.1)
+    return A, B
+
+
+@pytest.mark.parametrize("dz", [0, 3])
+def test_large_pair_fft_form(mpx, dz):
+    """Pairs of at least 2^22 cell interactions take the FFT form (a helper magnet spanning both, its demag field
+    at the destination cells): fields of both magnets against the oracle's direct sum."""
+    specs = _large_specs(dz)
+    assert specs[0].shape[0] * specs[0].shape[1] * specs[0].shape[2] * \
+        specs[1].shape[0] * specs[1].shape[1] * specs[1].shape[2] >= 1 << 22
+    ms = [random_m(s.shape, seed=40 + k, smooth=2) for k, s in enumerate(specs)]
+    ow, qs = _oracle(specs, ms)
+    world, mags = _product(mpx, specs, ms)
+    for q, mag, s in zip(qs, mags, specs):
+        for quantity in (abi.Q_EXTERNAL_FIELD, abi.Q_EFFECTIVE_FIELD):
+            want = ow.eval(q, quantity)
+            got = mag._engine.eval(mag._id, quantity, (3, *s.shape))
+            assert max_rel(got, want) < 1e-5, (quantity, max_rel(got, want))
+
+
+def test_large_pair_fft_form_trajectory(mpx):
+    specs = _large_specs(1)
+    ms = [random_m(s.shape, seed=50 + k, smooth=3) for k, s in enumerate(specs)]
+    ow, qs = _oracle(specs, ms)
+    ow.set_method("DormandPrince")
+    world, mags = _product(mpx, specs, ms)
+    world.timesolver.set_method("DormandPrince")
+    dt0 = ow.sensible_timestep()
+    ow.timestep = dt0
+    world.timesolver.timestep = dt0
+    worst = 0.0
+    for k in range(1, 3):
+        tp = k * 1.5e-12
+        ow.run(tp - ow.time)
+        world.timesolver._e.run(world._group, tp - world.timesolver.time)
+        for q, mag in zip(qs, mags):
+            worst = max(worst, float(np.max(np.abs(np.array(mag.magnetization.average())
+                                                    - np.array(ow.average(q, abi.Q_MAGNETIZATION))))))
+    assert worst < 1e-5, worst

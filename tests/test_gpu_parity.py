@@ -422,3 +422,19 @@ def test_warp_transform_trajectory_vs_oracle(mpx):
         worst_cell = max(worst_cell, float(np.max(np.abs(magnet.magnetization.get() - ow.get_m(q)))))
     assert worst < 1e-5, worst
     assert worst_cell < 1e-3, worst_cell
+
+
+def test_warp_transforms_with_geometry_regions_frozen(mpx):
+    """A magnet with geometry, regions, per-cell parameters and frozen cells (the generic epilogue) at sizes that
+    take the warp transforms (Px = 512, Py = 256)."""
+    shape = (2, 70, 132)
+    zz, yy, xx = np.meshgrid(np.arange(2), np.arange(70), np.arange(132), indexing="ij")
+    geom = ((xx - 66) ** 2 / 66.0 ** 2 + (yy - 35) ** 2 / 35.0 ** 2) <= 1.0
+    regions = (xx >= 66).astype(np.uint32)
+    msat = np.where(yy < 20, 6e5, 8e5).astype(np.float32)
+    frozen = np.zeros(shape, np.float32)
+    frozen[1, 35, 60:70] = 1
+    s = MagnetSpec(size=(132, 70, 2), cellsize=(2e-9, 2e-9, 1.5e-9), geometry=geom, regions=regions, msat=msat,
+                   aex=1.3e-11, alpha=0.1, dmi={"xxz": 1e-3, "yyz": 1e-3}, frozen=frozen,
+                   inter_pairs={(1, 0): 5e-12}, world_bias=(0, 0, 0.05))
+    compare(s, mpx, [abi.Q_DEMAG_FIELD, abi.Q_EFFECTIVE_FIELD, abi.Q_TORQUE])

@@ -256,3 +256,18 @@ def max_rel(result, wanted):
     num = np.linalg.norm(np.asarray(result, dtype=np.float64) - np.asarray(wanted, dtype=np.float64), axis=0)
     den = np.max(np.linalg.norm(np.asarray(wanted, dtype=np.float64), axis=0))
     return float(np.max(num) / den) if den > 0 else float(np.max(num))
+
+
+_KNOWN = None
+
+
+def known(name):
+    """Known answer `name` of the reference's tests (tests/golden/known_answers.json)."""
+    global _KNOWN
+    if _KNOWN is None:
+        import json
+        import os
+
+        with open(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "known_answers.json")) as f:
+            _KNOWN = json.load(f)
+    return _KNOWN[name]

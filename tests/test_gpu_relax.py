@@ -11,7 +11,7 @@ import pytest
 
 import oracle as O
 from spec import MagnetSpec
-from test_oracle_golden import sp2_coercivity
+from test_oracle_golden import check_nanowire, nanowire_canting, sp2_coercivity
 
 pytestmark = pytest.mark.gpu
 abi = O.abi
@@ -34,6 +34,29 @@ def test_minimize_sp2_coercivity(mpx):
     rhc = sp2_coercivity(make, lambda: st["magnet"].minimize(), set_field,
                          lambda: float(np.sum(st["magnet"].magnetization.average())))
     assert abs(0.057069478 - rhc) < 1e-5, rhc
+
+
+def test_minimize_nanowire_canting_golden(mpx):
+    """test/test_boundaries.py through the mumaxplus-style API: Neumann canting vs the mumax3 value, open
+    boundaries vs the analytic and the mumax3 value (tests/golden/known_answers.json, 2e-4)."""
+    cs, D = 0.05, 0.9 * 4 / np.pi
+    st = {}
+
+    def make(openbc, m0):
+        world = mpx.World(cellsize=(cs, cs, cs))
+        magnet = mpx.Ferromagnet(world, mpx.Grid((1024, 1, 1)))
+        magnet.dmi_tensor.set_interfacial_dmi(D)
+        magnet.enable_demag = False
+        magnet.enable_openbc = openbc
+        magnet.anisU = (0, 0, 1)
+        magnet.aex = 1.0
+        magnet.ku1 = 1.0
+        magnet.msat = 1.0
+        magnet.magnetization = m0
+        st.update(magnet=magnet, world=world)
+        return lambda: magnet.magnetization.eval()
+
+    check_nanowire(*nanowire_canting(lambda: st["magnet"].minimize(1e-7), None, make))
 
 
 def _film():

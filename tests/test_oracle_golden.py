@@ -8,12 +8,15 @@ hold for this path (CPU only, no GPU).
   stray field  test/test_strayfield.py:57-84   FFT vs direct sum, with PBC
   time solver  test/test_timesolver.py:19-169  analytic macrospin precession, all 5 methods
   PBC          test/test_PBC.py:14-91          <m> after 1 ns vs the mumax3 value
+  minimize     test/test_standardproblem2_coercivity.py, test/test_boundaries.py (coercivity, wire canting)
+
+The known answers themselves are in tests/golden/known_answers.json.
 """
 import numpy as np
 import pytest
 
 import oracle as O
-from spec import MagnetSpec, max_rel, random_m
+from spec import MagnetSpec, known, max_rel, random_m
 
 abi = O.abi
 GAMMALL = 1.7595e11
@@ -213,8 +216,9 @@ def test_pbc_run_center_matches_mumax3_golden():
     w.timestep = w.sensible_timestep()
     w.run(1e-9)
     avg = w.average(q, abi.Q_MAGNETIZATION)
-    wanted = np.array([0.89947968, 0.23352228, -0.00010287])
-    assert np.linalg.norm(np.array(avg) - wanted) / np.linalg.norm(wanted) < 1e-3
+    k = known("pbc_center_m_1ns")
+    wanted = np.array(k["value"])
+    assert np.linalg.norm(np.array(avg) - wanted) / np.linalg.norm(wanted) < k["rel_tol"]
 
 
 def test_oracle_external_kernel_octant_reproduces_own(oracle):
@@ -264,8 +268,55 @@ def sp2_coercivity(make, minimize, set_field, m_sum):
     return (m0 * h1 - m1 * h0) / (m0 - m1)
 
 
+def nanowire_canting(minimize, x_of_m, make):
+    """test/test_boundaries.py: canting of the first cell of a 1024-cell wire with interfacial DMI after
+    minimize(1e-7), Neumann boundaries first, then open boundaries from that state (the reference's order).
+    make(openbc, m0) builds the magnet; returns (Neumann, open) cantings."""
+    m0 = np.zeros((3, 1, 1, 1024), np.float32)
+    m0[2] = 1.0
+    out = []
+    for openbc in (False, True):
+        get_m = make(openbc, m0)
+        minimize()
+        m = get_m()
+        out.append(float(np.arctan2(m[0, 0, 0, 0], m[2, 0, 0, 0])))
+        m0 = m.astype(np.float32)
+    return out
+
+
+NANOWIRE = dict(cs=0.05, D=0.9 * 4 / np.pi)
+
+
+def nanowire_spec(openbc):
+    cs, D = NANOWIRE["cs"], NANOWIRE["D"]
+    return MagnetSpec(size=(1024, 1, 1), cellsize=(cs, cs, cs), msat=1.0, aex=1.0, ku1=1.0, anisU=(0.0, 0.0, 1.0),
+                      dmi={"xxz": D, "yyz": D}, enable_demag=False, enable_openbc=openbc)
+
+
+def check_nanowire(neumann, open_):
+    cs, D = NANOWIRE["cs"], NANOWIRE["D"]
+    k = known("nanowire_canting_neumann")
+    assert abs(neumann - k["value"]) / k["value"] < k["rel_tol"], neumann
+    analytic = 2 * np.arctan(np.exp(-cs / 2) * np.tan(np.arcsin(D / 2) / 2))
+    k = known("nanowire_canting_open")
+    assert abs(open_ - analytic) / analytic < k["rel_tol"], open_
+    k = known("nanowire_canting_open_mumax3")
+    assert abs(open_ - k["value"]) / k["value"] < k["rel_tol"], open_
+
+
+def test_oracle_nanowire_canting_golden(oracle):
+    st = {}
+
+    def make(openbc, m0):
+        ow, q = nanowire_spec(openbc).oracle_world(m0)
+        st.update(ow=ow)
+        return lambda: ow.get_m(q)
+
+    check_nanowire(*nanowire_canting(lambda: st["ow"].minimize(1e-7, 10), None, make))
+
+
 def test_oracle_minimize_sp2_coercivity_golden(oracle):
-    """Known answer of the reference test: H_c / Msat = 0.057069478 (1e-5)."""
+    """Known answer of the reference test: H_c / Msat (tests/golden/known_answers.json)."""
     st = {}
 
     def make(cs, msat, aex):
@@ -276,7 +327,8 @@ def test_oracle_minimize_sp2_coercivity_golden(oracle):
     rhc = sp2_coercivity(make, lambda: st["ow"].minimize(1e-6, 10),
                          lambda b: st["ow"].set_world_bias(tuple(b)),
                          lambda: float(np.sum(st["ow"].average(st["q"], oracle.abi.Q_MAGNETIZATION))))
-    assert abs(0.057069478 - rhc) < 1e-5, rhc
+    k = known("sp2_coercivity")
+    assert abs(k["value"] - rhc) < k["abs_tol"], rhc
 
 
 def test_oracle_relax_reaches_the_minimum_of_a_uniaxial_film(oracle):

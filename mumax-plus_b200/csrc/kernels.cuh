@@ -306,21 +306,23 @@ __device__ __forceinline__ void zstage_pair(float2* D, int cs, const MagnetDev& 
         }
       }
   }
+  // reduce-scatter over the lane pair: lane `half` keeps the outputs n with
+  // n % 2 == half (own value + the partner's), so each lane sends only the half
+  // its partner keeps
   const unsigned mask = __activemask();
 #pragma unroll
   for (int c = 0; c < 3; ++c)
 #pragma unroll
-    for (int n = 0; n < H; ++n) {
-      const float ox = __shfl_xor_sync(mask, v[c][n].x, 1);
-      const float oy = __shfl_xor_sync(mask, v[c][n].y, 1);
-      v[c][n] = make_float2(v[c][n].x + ox, v[c][n].y + oy);
+    for (int k = 0; 2 * k < H; ++k) {
+      const float2 ev = v[c][2 * k];
+      const float2 od = (2 * k + 1 < H) ? v[c][2 * k + 1] : make_float2(0.f, 0.f);
+      const float2 send = half ? ev : od;
+      const float2 mine = half ? od : ev;
+      const float ox = __shfl_xor_sync(mask, send.x, 1);
+      const float oy = __shfl_xor_sync(mask, send.y, 1);
+      const int n = 2 * k + half;
+      if (n < H && n < nz) D[(c * nz + n) * cs + pky] = make_float2(mine.x + ox, mine.y + oy);
     }
-  // both lanes hold the sum; lane `half` writes the outputs n with n % 2 == half
-#pragma unroll
-  for (int c = 0; c < 3; ++c)
-#pragma unroll
-    for (int n = 0; n < H; ++n)
-      if (n < nz && (n & 1) == half) D[(c * nz + n) * cs + pky] = v[c][n];
 }
 
 template <bool Q5 = false>

@@ -732,6 +732,37 @@ __device__ __forceinline__ bool lean_ok(const MagnetDev& M) {
   return M.fast && !M.geom && (M.mg[0] == 0 || (off >= 0 && off + M.n[0] <= M.mg[0]));
 }
 
+// Exchange and DMI sums over the six neighbours nb[] (-1: none) of the lean
+// path, in the order of local_terms_fast.  INNER: every neighbour is present
+// (the ghost-cell code of the Neumann boundary is left out).
+template <bool INNER>
+__device__ __forceinline__ void neighbour_sums(const MagnetDev& M, const float* __restrict__ m, int N, const int (&nb)[6],
+                                               float3 mc, bool neumann, bool dmi_open, bool do_exch, bool do_dmi,
+                                               float3& he, float3& hd) {
+  float3 mn[6];
+#pragma unroll
+  for (int r = 0; r < 6; ++r) mn[r] = (INNER || nb[r] >= 0) ? ldg3(m, N, nb[r]) : mc;
+#pragma unroll
+  for (int r = 0; r < 6; ++r) {
+    const int axis = r >> 1;
+    const int d = (r & 1) ? 1 : -1;
+    const bool nin = INNER || nb[r] >= 0;
+    float3 m_ = mn[r];
+    if (!INNER && !nin && neumann) {  // ghost cell m + Gamma/(2A) delta
+      const float3 Gm = gamma_uniform(M.fd, axis, mc);
+      m_ = mc + (d * M.cs[axis]) * (M.finv_2a * Gm);
+    }
+    if (do_exch && (nin || neumann)) he = he + M.fe[axis] * (m_ - mc);
+    if (do_dmi && (nin || !dmi_open)) {
+      const float Dxy = M.fd[3 * axis], Dxz = M.fd[3 * axis + 1], Dyz = M.fd[3 * axis + 2];
+      const float inv_delta = d * M.inv_cs[axis];
+      hd.x += (Dxy * m_.y + Dxz * m_.z) * inv_delta;
+      hd.y += (-Dxy * m_.x + Dyz * m_.z) * inv_delta;
+      hd.z += (-Dxz * m_.x - Dyz * m_.y) * inv_delta;
+    }
+  }
+}
+
 // Right-hand side of one cell of a stage on the lean path: the arithmetic of
 // local_terms_fast and of the torque in epilogue_cell, in the same order,
 // with the neighbours taken from the block's row table.
@@ -759,28 +790,12 @@ __device__ __forceinline__ float3 stage_cell_lean(const MagnetDev& M, const Grou
       const int b = T.r[yl][q];
       nb[2 + q] = b >= 0 ? b + x : -1;
     }
-    float3 mn[6];
-#pragma unroll
-    for (int r = 0; r < 6; ++r) mn[r] = nb[r] >= 0 ? ldg3(m, N, nb[r]) : mc;
     float3 he = f3(0, 0, 0), hd = f3(0, 0, 0);
-#pragma unroll
-    for (int r = 0; r < 6; ++r) {
-      const int axis = r >> 1;
-      const int d = (r & 1) ? 1 : -1;
-      const bool nin = nb[r] >= 0;
-      float3 m_ = mn[r];
-      if (!nin && neumann) {  // ghost cell m + Gamma/(2A) delta
-        const float3 Gm = gamma_uniform(M.fd, axis, mc);
-        m_ = mc + (d * M.cs[axis]) * (M.finv_2a * Gm);
-      }
-      if (do_exch && (nin || neumann)) he = he + M.fe[axis] * (m_ - mc);
-      if (do_dmi && (nin || !dmi_open)) {
-        const float Dxy = M.fd[3 * axis], Dxz = M.fd[3 * axis + 1], Dyz = M.fd[3 * axis + 2];
-        const float inv_delta = d * M.inv_cs[axis];
-        hd.x += (Dxy * m_.y + Dxz * m_.z) * inv_delta;
-        hd.y += (-Dxy * m_.x + Dyz * m_.z) * inv_delta;
-        hd.z += (-Dxz * m_.x - Dyz * m_.y) * inv_delta;
-      }
+    const bool inner = nb[0] >= 0 && nb[1] >= 0 && nb[2] >= 0 && nb[3] >= 0 && nb[4] >= 0 && nb[5] >= 0;
+    if (__all_sync(__activemask(), inner)) {  // every neighbour present: no ghost cells
+      neighbour_sums<true>(M, m, N, nb, mc, neumann, dmi_open, do_exch, do_dmi, he, hd);
+    } else {
+      neighbour_sums<false>(M, m, N, nb, mc, neumann, dmi_open, do_exch, do_dmi, he, hd);
     }
     if (do_exch) exch = M.finv_ms * he;
     if (do_dmi) dmi = M.finv_ms * hd;

@@ -112,6 +112,27 @@ __device__ __forceinline__ float3 combine_cell(const MagnetDev& M, const GroupDe
   return f3(v.x * inv, v.y * inv, v.z * inv);
 }
 
+// combine_cell for a stage (not the final b1 sum) with the coefficients
+// (float)(dt a_sj) and the k_j pointers of the block taken from shared memory:
+// the same sums, without an FP64 product and a double indirection per cell.
+__device__ __forceinline__ float3 combine_cell_pre(const float* __restrict__ x0, int N, int stage, int i,
+                                                   const float* cf, const float* const* kp) {
+  float3 v = ldg3(x0, N, i);
+  float3 k[7];
+#pragma unroll
+  for (int j = 0; j < 7; ++j)
+    if (j < stage) k[j] = ldg3(kp[j], N, i);
+#pragma unroll
+  for (int j = 0; j < 7; ++j) {
+    if (j < stage) {
+      const float c = cf[j];
+      v = f3(v.x + c * k[j].x, v.y + c * k[j].y, v.z + c * k[j].z);
+    }
+  }
+  const float inv = rsqrtf(v.x * v.x + v.y * v.y + v.z * v.z);
+  return f3(v.x * inv, v.y * inv, v.z * inv);
+}
+
 // Row index e / n within a tile of at most TY_MAX rows of length n, without
 // an integer division: a float estimate of (e + 1/2) / n (exact unless n is
 // very large) corrected by one step either way.
@@ -151,6 +172,16 @@ __global__ void __launch_bounds__(X_THREADS_MAX, 2) k_xfwd(const MagnetDev* __re
   const int sh = wrow ? 5 : 4;
   if (wrow) load_twq(tws, tw, logL);
   else load_twiddles<3>(tws, tw, logL);
+  __shared__ float s_cf[8];
+  __shared__ const float* s_kp[8];
+  if (COMBINE) {  // the stage's coefficients and k_j buffers, once per block
+    if (threadIdx.x < 7) {
+      const int j = threadIdx.x;
+      s_cf[j] = (j < stage) ? (float)(G.dt * c_tab.a[stage][j]) : 0.f;
+      s_kp[j] = M.buf[G.map[2 + j]];
+    }
+    __syncthreads();
+  }
 
   // only the lower half of each row: the upper half (x >= L/2 >= nx) is zero
   // padding that the pruned first FFT pass does not read
@@ -164,7 +195,7 @@ __global__ void __launch_bounds__(X_THREADS_MAX, 2) k_xfwd(const MagnetDev* __re
       if (in_geom(M, i)) {
         float3 m;
         if (COMBINE) {
-          m = combine_cell(M, G, stage, i, false);
+          m = combine_cell_pre(x0, N, stage, i, s_cf, s_kp);
           store3(xs, N, i, m);
         } else {
           m = ldg3(src, N, i);

@@ -211,6 +211,17 @@ mpx_status mpx_engine_launch_count(mpx_engine* e, int64_t* count);
 mpx_status mpx_group_create(mpx_engine* e, int* group);
 mpx_status mpx_group_destroy(mpx_engine* e, int group);   /* removes its magnets */
 mpx_status mpx_group_info_get(mpx_engine* e, int group, mpx_group_info* out);
+/* Checkpoint / resume of a group (no counterpart in the reference, whose state
+ * is reachable only through magnetization.get/set and time/timestep).  The
+ * snapshot holds the time, time step, accepted-step count (the counter of the
+ * thermal noise generator), whether the FSAL derivative k0 is valid, and per
+ * magnet of the group (in the order added) its state m and k0, 3 * ncells floats
+ * each, copied without normalisation.  Loading a snapshot into a group of
+ * magnets of the same sizes continues exactly as the saved run would have.
+ * mpx_group_state_bytes gives the size of the host buffer. */
+mpx_status mpx_group_state_bytes(mpx_engine* e, int group, int64_t* bytes);
+mpx_status mpx_group_save(mpx_engine* e, int group, void* buf, int64_t bytes);
+mpx_status mpx_group_load(mpx_engine* e, int group, const void* buf, int64_t bytes);
 
 /* ---- magnets ------------------------------------------------------------ */
 /* Adds a ferromagnet to `group`; builds its FP64 Newell kernel spectrum when

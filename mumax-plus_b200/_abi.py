@@ -156,6 +156,9 @@ SIGNATURES = {
     "mpx_group_create": (I, [E, P_I]),
     "mpx_group_destroy": (I, [E, I]),
     "mpx_group_info_get": (I, [E, I, C.POINTER(GroupInfo)]),
+    "mpx_group_state_bytes": (I, [E, I, C.POINTER(C.c_int64)]),
+    "mpx_group_save": (I, [E, I, C.c_void_p, C.c_int64]),
+    "mpx_group_load": (I, [E, I, C.c_void_p, C.c_int64]),
     # descriptions are passed by address so that an identical struct layout
     # declared elsewhere (e.g. by a test harness) is accepted as well
     "mpx_magnet_add": (I, [E, I, C.c_void_p, P_I]),

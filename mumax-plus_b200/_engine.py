@@ -104,6 +104,19 @@ class Engine:
         check(lib().mpx_group_info_get(self._h, int(g), C.byref(info)))
         return info
 
+    def group_save(self, g):
+        """Snapshot of group g (time, time step, step count, m and FSAL k0 of its
+        magnets) as a uint8 array."""
+        n = C.c_int64()
+        check(lib().mpx_group_state_bytes(self._h, int(g), C.byref(n)))
+        buf = np.empty(n.value, dtype=np.uint8)
+        check(lib().mpx_group_save(self._h, int(g), buf.ctypes.data, int(n.value)))
+        return buf
+
+    def group_load(self, g, state):
+        buf = np.ascontiguousarray(state, dtype=np.uint8)
+        check(lib().mpx_group_load(self._h, int(g), buf.ctypes.data, int(buf.size)))
+
     # -- magnets
     def magnet_add(self, group, desc):
         m = C.c_int()

@@ -35,7 +35,7 @@ GS_FAILED = 3
 class Solve:
     """One solve of a batch: its workload, device ids and outcome."""
 
-    __slots__ = ("key", "w", "group", "magnet", "shape", "cells", "resident", "transient", "duration",
+    __slots__ = ("key", "w", "group", "magnet", "shape", "cells", "resident", "transient", "duration", "t_start",
                  "torque_stop", "arrival", "t_admit", "t_done", "steps", "rejected", "sim_time", "failed", "m")
 
     def __init__(self, key, w):
@@ -45,7 +45,7 @@ class Solve:
         self.shape = (3, nz, ny, nx)
         self.cells = nx * ny * nz
         self.group = self.magnet = None
-        self.duration = self.torque_stop = 0.0
+        self.duration = self.torque_stop = self.t_start = 0.0
         self.arrival = self.t_admit = self.t_done = None
         self.steps = self.rejected = 0
         self.sim_time = 0.0
@@ -109,6 +109,7 @@ class Batch:
         max|torque|/gamma_LL < torque_stop tesla."""
         s.duration = float(duration)
         s.torque_stop = float(torque_stop)
+        s.t_start = float(self.engine.group_info(s.group).time)
         self.engine.group_start(s.group, s.duration, s.torque_stop)
 
     def advance(self, attempts):
@@ -132,6 +133,42 @@ class Batch:
         del self.solves[s.group]
         self.resident -= s.resident
         return s
+
+
+class Checkpoint:
+    """A solve taken off the device mid-run: its workload, its group state
+    (Engine.group_save) and the simulated time left."""
+
+    __slots__ = ("key", "w", "state", "t_stop", "torque_stop")
+
+    def __init__(self, key, w, state, t_stop, torque_stop):
+        self.key, self.w, self.state, self.t_stop, self.torque_stop = key, w, state, t_stop, torque_stop
+
+
+def checkpoint(batch, s):
+    """Save running solve `s` to host memory and free it (preemption).  The
+    queued attempts must have been polled."""
+    info = batch.engine.group_info(s.group)
+    ck = Checkpoint(s.key, s.w, batch.engine.group_save(s.group), s.t_start + s.duration, s.torque_stop)
+    s.sim_time = float(info.time)
+    batch.engine.group_destroy(s.group)
+    del batch.solves[s.group]
+    batch.resident -= s.resident
+    return ck
+
+
+def resume(batch, ck):
+    """Re-admit a checkpointed solve: a new group with the same magnet, the
+    saved state loaded, started for the simulated time it had left.  It then
+    continues bit for bit as it would have without the interruption."""
+    s = batch.add(ck.w, key=ck.key)
+    batch.engine.group_load(s.group, ck.state)
+    t = float(batch.engine.group_info(s.group).time)
+    s.duration = ck.t_stop - t
+    s.t_start = t
+    s.torque_stop = ck.torque_stop
+    batch.engine.group_start(s.group, s.duration, s.torque_stop)
+    return s
 
 
 class _Pacer:

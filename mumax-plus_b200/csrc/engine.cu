@@ -7,6 +7,7 @@
 // kernel launches with a status read every few attempts; no per-kernel host
 // synchronisation as in the reference (cudautil/cudalaunch.hpp:10-19).
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
 
 #include <algorithm>
 #include <cmath>
@@ -27,6 +28,15 @@
 using namespace mpx;
 
 namespace {
+
+// NVTX range over a host entry point or phase (shown by Nsight tools, no cost
+// without one attached).
+struct NvtxRange {
+  explicit NvtxRange(const char* name) { nvtxRangePushA(name); }
+  ~NvtxRange() { nvtxRangePop(); }
+  NvtxRange(const NvtxRange&) = delete;
+  NvtxRange& operator=(const NvtxRange&) = delete;
+};
 
 thread_local std::string g_last_error;
 
@@ -584,6 +594,7 @@ long long active_set(mpx_engine* e, std::vector<Magnet*>& act) {
 }
 
 mpx_status rebuild_tables(mpx_engine* e) {
+  NvtxRange nvtx_range("rebuild_tables");
   {  // shapes for the set of magnets launched together
     std::vector<Magnet*> act;
     const long long cells = active_set(e, act);
@@ -717,6 +728,7 @@ mpx_status create_hull(mpx_engine* e, const Magnet* A, const Magnet* B, int* out
 }
 
 mpx_status rebuild_pairs(mpx_engine* e) {
+  NvtxRange nvtx_range("rebuild_pairs");
   for (auto& p : e->pairs) pfree(e, p.k);
   e->pairs.clear();
   for (auto& mp : e->mags)  // helpers of the previous pairs
@@ -1462,6 +1474,7 @@ void fill_group_params(GroupDev& G, const mpx_solver_params& sp) {
 
 // Blocks until the group leaves the running state.
 mpx_status drive_group(mpx_engine* e, Group* g) {
+  NvtxRange nvtx_range("drive_group");
   int chunk = 1;
   for (;;) {
     MPX_TRY(run_attempts(e, g->sp.method, chunk));
@@ -1688,6 +1701,96 @@ mpx_status mpx_group_destroy(mpx_engine* e, int group) {
   return MPX_OK;
 }
 
+// Snapshot layout: header, then per magnet m and k0 (3N floats each).
+struct GroupStateHeader {
+  char magic[8];  // "MPXSTAT1"
+  double t, dt;
+  int64_t steps;
+  int32_t k0_valid, nmag;
+};
+
+static int64_t group_state_bytes(mpx_engine* e, Group* g) {
+  int64_t b = sizeof(GroupStateHeader) + sizeof(int64_t) * (int64_t)g->magnets.size();
+  for (int id : g->magnets) b += 2 * (int64_t)sizeof(float) * 3 * get_mag(e, id)->dev.N;
+  return b;
+}
+
+mpx_status mpx_group_state_bytes(mpx_engine* e, int group, int64_t* bytes) {
+  Group* g = get_group(e, group);
+  if (!g || !bytes) return fail(MPX_ERR_RANGE, "no such group / null output");
+  *bytes = group_state_bytes(e, g);
+  return MPX_OK;
+}
+
+mpx_status mpx_group_save(mpx_engine* e, int group, void* buf, int64_t bytes) {
+  Group* g = get_group(e, group);
+  if (!g || !buf) return fail(MPX_ERR_RANGE, "no such group / null buffer");
+  if (bytes < group_state_bytes(e, g)) return fail(MPX_ERR_INVALID, "state buffer too small");
+  DeviceGuard guard(e->device);
+  GroupDev G;
+  MPX_TRY(read_group(e, g->slot, &G));
+  GroupStateHeader h;
+  std::memcpy(h.magic, "MPXSTAT1", 8);
+  h.t = G.t;
+  h.dt = G.dt;
+  h.steps = G.steps;
+  h.k0_valid = G.k0_valid;
+  h.nmag = (int32_t)g->magnets.size();
+  char* p = static_cast<char*>(buf);
+  std::memcpy(p, &h, sizeof h);
+  p += sizeof h;
+  for (int id : g->magnets) {
+    const int64_t n = get_mag(e, id)->dev.N;
+    std::memcpy(p, &n, sizeof n);
+    p += sizeof n;
+  }
+  for (int id : g->magnets) {
+    Magnet* m = get_mag(e, id);
+    const size_t b = sizeof(float) * 3 * (size_t)m->dev.N;
+    CUDA_TRY(cudaMemcpyAsync(p, m->dev.buf[G.map[0]], b, cudaMemcpyDeviceToHost, e->stream));
+    CUDA_TRY(cudaMemcpyAsync(p + b, m->dev.buf[G.map[2]], b, cudaMemcpyDeviceToHost, e->stream));
+    p += 2 * b;
+  }
+  CUDA_TRY(cudaStreamSynchronize(e->stream));
+  return MPX_OK;
+}
+
+mpx_status mpx_group_load(mpx_engine* e, int group, const void* buf, int64_t bytes) {
+  Group* g = get_group(e, group);
+  if (!g || !buf) return fail(MPX_ERR_RANGE, "no such group / null buffer");
+  if (bytes < (int64_t)sizeof(GroupStateHeader)) return fail(MPX_ERR_INVALID, "state buffer too small");
+  GroupStateHeader h;
+  const char* p = static_cast<const char*>(buf);
+  std::memcpy(&h, p, sizeof h);
+  if (std::memcmp(h.magic, "MPXSTAT1", 8) != 0) return fail(MPX_ERR_INVALID, "not a group state");
+  if (h.nmag != (int32_t)g->magnets.size() || bytes < group_state_bytes(e, g))
+    return fail(MPX_ERR_INVALID, "the state does not match the magnets of the group");
+  p += sizeof h;
+  for (int id : g->magnets) {
+    int64_t n;
+    std::memcpy(&n, p, sizeof n);
+    p += sizeof n;
+    if (n != get_mag(e, id)->dev.N) return fail(MPX_ERR_INVALID, "the state does not match the magnets of the group");
+  }
+  DeviceGuard guard(e->device);
+  GroupDev G;
+  MPX_TRY(read_group(e, g->slot, &G));
+  for (int id : g->magnets) {
+    Magnet* m = get_mag(e, id);
+    const size_t b = sizeof(float) * 3 * (size_t)m->dev.N;
+    CUDA_TRY(cudaMemcpyAsync(m->dev.buf[G.map[0]], p, b, cudaMemcpyHostToDevice, e->stream));
+    CUDA_TRY(cudaMemcpyAsync(m->dev.buf[G.map[2]], p + b, b, cudaMemcpyHostToDevice, e->stream));
+    p += 2 * b;
+  }
+  G.t = h.t;
+  G.dt = h.dt;
+  G.steps = h.steps;
+  G.k0_valid = h.k0_valid;
+  MPX_TRY(write_group(e, g->slot, &G));
+  CUDA_TRY(cudaStreamSynchronize(e->stream));
+  return MPX_OK;
+}
+
 mpx_status mpx_group_info_get(mpx_engine* e, int group, mpx_group_info* out) {
   Group* g = get_group(e, group);
   if (!g || !out) return fail(MPX_ERR_RANGE, "no such group");
@@ -1706,6 +1809,7 @@ mpx_status mpx_group_info_get(mpx_engine* e, int group, mpx_group_info* out) {
 }
 
 mpx_status mpx_magnet_add(mpx_engine* e, int group, const mpx_magnet_desc* d, int* magnet) {
+  NvtxRange nvtx_range("mpx_magnet_add");
   if (!e || !magnet) return fail(MPX_ERR_INVALID, "null argument");
   Group* g = get_group(e, group);
   if (!g) return fail(MPX_ERR_RANGE, "no such group");
@@ -1861,6 +1965,7 @@ mpx_status mpx_magnet_get_m(mpx_engine* e, int magnet, float* out, int on_device
 }
 
 mpx_status mpx_eval(mpx_engine* e, int magnet, int quantity, float* out, int on_device) {
+  NvtxRange nvtx_range("mpx_eval");
   Magnet* m = get_mag(e, magnet);
   if (!m || (!out && on_device != 2)) return fail(MPX_ERR_INVALID, "no such magnet / null output");
   if (quantity < 0 || quantity >= MPX_Q_COUNT) return fail(MPX_ERR_INVALID, "unknown quantity");
@@ -1986,6 +2091,7 @@ mpx_status mpx_profile_attempt(mpx_engine* e, int method, int reps, double ms[4]
 }
 
 mpx_status mpx_autotune(mpx_engine* e, int method, int* div_x, int* div_yz) {
+  NvtxRange nvtx_range("mpx_autotune");
   if (!e) return fail(MPX_ERR_INVALID, "null engine");
   DeviceGuard guard(e->device);
   std::vector<Magnet*> act;
@@ -2239,6 +2345,7 @@ static mpx_status start_group(mpx_engine* e, Group* g, int mode, long long nstep
 }
 
 mpx_status mpx_solver_steps(mpx_engine* e, int group, int nsteps) {
+  NvtxRange nvtx_range("mpx_solver_steps");
   Group* g = get_group(e, group);
   if (!g) return fail(MPX_ERR_RANGE, "no such group");
   if (nsteps <= 0) return MPX_OK;
@@ -2252,6 +2359,7 @@ mpx_status mpx_solver_steps(mpx_engine* e, int group, int nsteps) {
 mpx_status mpx_solver_step(mpx_engine* e, int group) { return mpx_solver_steps(e, group, 1); }
 
 mpx_status mpx_solver_run(mpx_engine* e, int group, double duration) {
+  NvtxRange nvtx_range("mpx_solver_run");
   Group* g = get_group(e, group);
   if (!g) return fail(MPX_ERR_RANGE, "no such group");
   if (duration <= 0) return MPX_OK;
@@ -2263,6 +2371,7 @@ mpx_status mpx_solver_run(mpx_engine* e, int group, double duration) {
 }
 
 mpx_status mpx_solver_run_sampled(mpx_engine* e, int group, const double* times, int n, double* out) {
+  NvtxRange nvtx_range("mpx_solver_run_sampled");
   Group* g = get_group(e, group);
   if (!g) return fail(MPX_ERR_RANGE, "no such group");
   if (n < 0 || (n > 0 && (!times || !out))) return fail(MPX_ERR_INVALID, "bad time points / output table");
@@ -2381,6 +2490,7 @@ static mpx_status group_torque_sq(mpx_engine* e, Group* g, double* out) {
 constexpr long long RELAX_MAX_STEPS = 10000000;
 
 mpx_status mpx_minimize(mpx_engine* e, int group, double tol, int nsamples) {
+  NvtxRange nvtx_range("mpx_minimize");
   Group* g = get_group(e, group);
   if (!g) return fail(MPX_ERR_RANGE, "no such group");
   if (nsamples <= 0) return fail(MPX_ERR_INVALID, "nsamples must be positive");
@@ -2435,6 +2545,7 @@ mpx_status mpx_minimize(mpx_engine* e, int group, double tol, int nsamples) {
 }
 
 mpx_status mpx_relax(mpx_engine* e, int group, double tol, double threshold) {
+  NvtxRange nvtx_range("mpx_relax");
   Group* g = get_group(e, group);
   if (!g) return fail(MPX_ERR_RANGE, "no such group");
   if (threshold == 0.0) return fail(MPX_ERR_INVALID, "The relax threshold should not be zero.");
@@ -2569,6 +2680,7 @@ mpx_status mpx_group_start(mpx_engine* e, int group, double duration, double tor
 }
 
 mpx_status mpx_advance(mpx_engine* e, int attempts) {
+  NvtxRange nvtx_range("mpx_advance");
   if (!e) return fail(MPX_ERR_INVALID, "null engine");
   if (attempts <= 0) return MPX_OK;
   DeviceGuard guard(e->device);

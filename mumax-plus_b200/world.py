@@ -186,6 +186,16 @@ class World:
         """Minimize the total energy of the world (mumaxplus/world.py:95-115)."""
         self._engine.minimize(self._group, tol, nsamples)
 
+    def save_state(self):
+        """Checkpoint of the time integration (no counterpart in mumax+): time,
+        time step, step count and, for every magnet, m and the Dormand-Prince
+        FSAL derivative, as a uint8 array.  load_state() into a world with
+        magnets of the same sizes continues exactly as this one would."""
+        return self._engine.group_save(self._group)
+
+    def load_state(self, state):
+        self._engine.group_load(self._group, state)
+
     @property
     def RelaxTorqueThreshold(self):
         """Threshold torque for relax (default -1, see Ferromagnet.RelaxTorqueThreshold)."""

@@ -273,10 +273,12 @@ __device__ __forceinline__ void apply3(float2* v0, float2* v1, float2* v2, float
 
 // z stage of one ky, half = 0 / 1 computing the even / odd kz of the PZ-point
 // transform of nz <= PZ/2 inputs as a PZ/2-point transform (of x, or of
-// x[n] W_PZ^n); the partner lane holds the other half and the two inverse
-// halves are summed with one shuffle.  Q5: columns in the qidx layout of the
-// warp transforms (else pidx).
-template <int PZ, bool Q5 = false>
+// x[n] W_PZ^n); the partner lane (lane ^ PARTNER) holds the other half and the
+// two inverse halves are summed with one shuffle.  Q5: columns in the qidx
+// layout of the warp transforms (else pidx).  PARTNER 16: the two halves of a
+// warp take the even / odd kz of the same 16 ky, so that every store of a
+// half-warp goes to one column at 16 consecutive ky (no bank conflicts).
+template <int PZ, bool Q5 = false, int PARTNER = 1>
 __device__ __forceinline__ void zstage_pair(float2* D, int cs, const MagnetDev& M, int kx, int ky, int half, int nz,
                                             int Py) {
   constexpr int H = PZ / 2;
@@ -349,8 +351,8 @@ __device__ __forceinline__ void zstage_pair(float2* D, int cs, const MagnetDev& 
       const float2 od = (2 * k + 1 < H) ? v[c][2 * k + 1] : make_float2(0.f, 0.f);
       const float2 send = half ? ev : od;
       const float2 mine = half ? od : ev;
-      const float ox = __shfl_xor_sync(mask, send.x, 1);
-      const float oy = __shfl_xor_sync(mask, send.y, 1);
+      const float ox = __shfl_xor_sync(mask, send.x, PARTNER);
+      const float oy = __shfl_xor_sync(mask, send.y, PARTNER);
       const int n = 2 * k + half;
       if (n < H && n < nz) D[(c * nz + n) * cs + pky] = make_float2(mine.x + ox, mine.y + oy);
     }
@@ -530,10 +532,11 @@ __device__ __forceinline__ void yzw_body(const MagnetDev& M, int kx0, int nkx, f
       zstage_single<true>(D + j * 3 * cs, cs, M, kx0 + j, t & (Py - 1), Py);
     }
   } else {
-    // lanes 2u and 2u+1 share one (kx, ky): the even and odd kz halves
+    // lanes l and l + 16 of a warp share one (kx, ky): the even and odd kz
+    // halves (the item count is a multiple of 32 and so is the block)
     for (int t = threadIdx.x; t < (2 * nkx) << LOGPY; t += blockDim.x) {
-      const int u = t >> 1, j = u >> LOGPY;
-      zstage_pair<PZ, true>(D + j * 3 * nz * cs, cs, M, kx0 + j, u & (Py - 1), t & 1, nz, Py);
+      const int u = ((t >> 5) << 4) | (t & 15), j = u >> LOGPY;
+      zstage_pair<PZ, true, 16>(D + j * 3 * nz * cs, cs, M, kx0 + j, u & (Py - 1), (t >> 4) & 1, nz, Py);
     }
   }
   __syncthreads();

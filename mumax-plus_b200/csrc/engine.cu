@@ -478,16 +478,37 @@ mpx_status launch_split(mpx_engine* e, const Work* ycw, int nyc, const Work* zmw
   return MPX_OK;
 }
 
+// Launch with programmatic dependent launch allowed: the kernel may start its
+// prologue while the previous kernel of the stream finishes (the kernel calls
+// pdl_wait before it reads anything the earlier kernels write).
+template <typename... KArgs, typename... Args>
+cudaError_t launch_pdl(void (*kernel)(KArgs...), int grid, int block, int smem, cudaStream_t st, Args&&... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(grid);
+  cfg.blockDim = dim3(block);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = st;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...);
+}
+
 // y/z launch for one class: warp columns for y lengths 64 .. 1024 (k_yzw);
 // else the radix-8 form for z lengths up to 8 and y lengths up to 2048, the
 // radix-16 form otherwise (k_yz)
 mpx_status launch_yz(mpx_engine* e, int cls, const Work* work, int n, int smem, int stage, int gate) {
   if (n <= 0) return MPX_OK;
-#define MPX_YZ(PZ, LR) k_yz<PZ, LR><<<n, YZ_THREADS, smem, e->stream>>>(e->d_mags, e->d_groups, work, stage, gate, e->d_tw)
+#define MPX_YZ(PZ, LR) \
+  CUDA_TRY(launch_pdl(k_yz<PZ, LR>, n, YZ_THREADS, smem, e->stream, e->d_mags, e->d_groups, work, stage, gate, e->d_tw))
 #define MPX_YZW(PZ) \
-  k_yzw<PZ><<<n, yzw_threads<PZ>(), smem, e->stream>>>(e->d_mags, e->d_groups, work, stage, gate, e->d_tw)
+  CUDA_TRY(launch_pdl(k_yzw<PZ>, n, yzw_threads<PZ>(), smem, e->stream, e->d_mags, e->d_groups, work, stage, gate, \
+                      e->d_tw))
 #define MPX_YZW32(PZ) \
-  k_yzw32<PZ><<<n, yzw_threads<PZ>(), smem, e->stream>>>(e->d_mags, e->d_groups, work, stage, gate, e->d_tw)
+  CUDA_TRY(launch_pdl(k_yzw32<PZ>, n, yzw_threads<PZ>(), smem, e->stream, e->d_mags, e->d_groups, work, stage, gate, \
+                      e->d_tw))
   switch (cls) {
     case 0: MPX_YZ(1, 3); break;
     case 1: MPX_YZ(2, 3); break;
@@ -831,7 +852,7 @@ mpx_status launch_pairs(mpx_engine* e, int dst, int stage, int gate) {
       ea.gate = gate;
       ea.out = H->dev.buf[1];
       ea.msrc = H->dev.buf[0];
-      k_xinv<<<ntile, nt, sx, e->stream>>>(e->d_mags, e->d_groups, H->d_tiles, ea, e->d_tw);
+      CUDA_TRY(launch_pdl(k_xinv, ntile, nt, sx, e->stream, e->d_mags, e->d_groups, H->d_tiles, ea, e->d_tw));
       k_hull_gather<<<(B->dev.N + 255) / 256, 256, 0, e->stream>>>(e->d_mags, e->d_groups, p.hull, p.dst, stage, gate,
                                                                     add ? 1 : 0, B->hstray);
       e->launches += 4;
@@ -1290,7 +1311,7 @@ mpx_status eval_into(mpx_engine* e, Magnet* m, int q, float* out) {
                            zmul_smem(m), m->P[1], m->P[2], 0, 0));
     else
       MPX_TRY(launch_yz(e, yz_class(m), m->d_kxw, (int)m->kxw.size(), syz, 0, 0));
-    k_xinv<<<ntile, nt, sx, e->stream>>>(e->d_mags, e->d_groups, m->d_tiles, ea, e->d_tw);
+    CUDA_TRY(launch_pdl(k_xinv, ntile, nt, sx, e->stream, e->d_mags, e->d_groups, m->d_tiles, ea, e->d_tw));
     e->launches += 2;
   } else {
     k_local<<<ntile, 256, 0, e->stream>>>(e->d_mags, e->d_groups, m->d_tiles, ea);
@@ -1332,7 +1353,8 @@ mpx_status launch_attempt(mpx_engine* e, const TableauDev& T, int first_stage) {
         MPX_TRY(launch_yz(e, c, e->d_kx_demag[c], e->n_kx_demag[c], e->smem_yz[c], s, 1));
       MPX_TRY(launch_split(e, e->d_t_ycols, e->n_t_ycols, e->d_t_zmul, e->n_t_zmul, e->smem_ycols, e->smem_zmul,
                            e->maxpy_split, e->maxpz_split, s, 1));
-      k_xinv<<<e->n_t_demag, e->nt_x, e->smem_x, e->stream>>>(e->d_mags, e->d_groups, e->d_t_demag, ea, e->d_tw);
+      CUDA_TRY(launch_pdl(k_xinv, e->n_t_demag, e->nt_x, e->smem_x, e->stream, e->d_mags, e->d_groups, e->d_t_demag, ea,
+                          e->d_tw));
       e->launches++;
     }
     if (e->n_t_local > 0) {
@@ -2073,7 +2095,8 @@ mpx_status mpx_profile_attempt(mpx_engine* e, int method, int reps, double ms[4]
     }
     CUDA_TRY(cudaEventRecord(ev[3], e->stream));
     if (e->n_t_demag > 0)
-      k_xinv<<<e->n_t_demag, e->nt_x, e->smem_x, e->stream>>>(e->d_mags, e->d_groups, e->d_t_demag, ea, e->d_tw);
+      CUDA_TRY(launch_pdl(k_xinv, e->n_t_demag, e->nt_x, e->smem_x, e->stream, e->d_mags, e->d_groups, e->d_t_demag, ea,
+                          e->d_tw));
     if (e->n_t_local > 0) k_local<<<e->n_t_local, 256, 0, e->stream>>>(e->d_mags, e->d_groups, e->d_t_local, ea);
     CUDA_TRY(cudaEventRecord(ev[4], e->stream));
     CUDA_TRY(cudaEventSynchronize(ev[4]));
@@ -2156,7 +2179,7 @@ mpx_status mpx_profile_eval(mpx_engine* e, int magnet, int reps, double ms[4]) {
       else
         MPX_TRY(launch_yz(e, yz_class(m), m->d_kxw, (int)m->kxw.size(), syz, 0, 0));
       CUDA_TRY(cudaEventRecord(ev[2], e->stream));
-      k_xinv<<<ntile, nt, sx, e->stream>>>(e->d_mags, e->d_groups, m->d_tiles, ea, e->d_tw);
+      CUDA_TRY(launch_pdl(k_xinv, ntile, nt, sx, e->stream, e->d_mags, e->d_groups, m->d_tiles, ea, e->d_tw));
       CUDA_TRY(cudaEventRecord(ev[3], e->stream));
       e->launches += 2;
       CUDA_TRY(cudaEventSynchronize(ev[3]));

@@ -82,6 +82,16 @@ __device__ __forceinline__ bool load_descs(MagnetDev& sM, GroupDev& sG, const Ma
   return true;
 }
 
+// Programmatic dependent launch.  A kernel launched with the programmatic
+// serialisation attribute may start while the previous kernel of the stream is
+// still running (after every block of that kernel has passed pdl_trigger or
+// exited): before pdl_wait it reads only data that no kernel of the current
+// attempt writes (magnet and group descriptors, twiddle tables); pdl_wait
+// returns once the previous kernel has completed and its writes are visible.
+// Both are no-ops for a kernel launched without the attribute.
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+
 // Current magnetisation used by stage `stage`: x0 for stage 0, the stage state otherwise.
 __device__ __forceinline__ const float* stage_m(const MagnetDev& M, const GroupDev& G, int stage) {
   return stage == 0 ? M.buf[G.map[0]] : M.buf[G.map[1]];
@@ -157,6 +167,7 @@ __global__ void __launch_bounds__(X_THREADS_MAX, 2) k_xfwd(const MagnetDev* __re
   extern __shared__ float2 sm[];
   __shared__ MagnetDev M;
   __shared__ GroupDev G;
+  pdl_trigger();  // the y/z pass may start its prologue during this kernel's last wave
   const Work wk = work[blockIdx.x];
   if (!load_descs(M, G, mags, groups, wk.mag, gate, stage)) return;
   const int z = wk.z, y0 = wk.y0, ty = wk.ty;
@@ -388,6 +399,7 @@ __global__ void __launch_bounds__(384, MAXLR == 3 ? 2 : 1)
   extern __shared__ float2 sm[];
   __shared__ MagnetDev M;
   __shared__ GroupDev G;
+  pdl_trigger();
   const Work wk = work[blockIdx.x];
   if (!load_descs(M, G, mags, groups, wk.mag, gate, stage)) return;
   const int kx0 = wk.z, nkx = wk.y0;
@@ -398,6 +410,7 @@ __global__ void __launch_bounds__(384, MAXLR == 3 ? 2 : 1)
   const int ncol = nkx * 3 * nz;
   float2* tws = sm + ncol * cs;  // twiddles of length Py
   load_twiddles<MAXLR>(tws, tw, logPy);
+  pdl_wait();  // the spectrum is written by the x pass
   // slab load: 8 independent read-only loads in flight per thread; only the
   // lower half of each column (y < Py/2, of which y >= ny is zero padding),
   // which is all the pruned first FFT pass reads
@@ -523,6 +536,7 @@ __device__ __forceinline__ void yzw_body(const MagnetDev& M, int kx0, int nkx, f
   float2* twq = sm + ncol * cs;
   load_twq(twq, tw, LOGPY);
   __syncthreads();
+  pdl_wait();  // the spectrum is written by the x pass
   float2* S = M.spec + (size_t)kx0 * 3 * nz * ny;
   yzw_forward<Q>(S, ny, D, ncol, twq);
   __syncthreads();
@@ -551,6 +565,7 @@ __global__ void __launch_bounds__(yzw_threads<PZ>(), PZ == 16 ? 1 : 2)
   extern __shared__ float2 sm[];
   __shared__ MagnetDev M;
   __shared__ GroupDev G;
+  pdl_trigger();  // the x-inverse pass may start its prologue during the last wave
   const Work wk = work[blockIdx.x];
   if (!load_descs(M, G, mags, groups, wk.mag, gate, stage)) return;
   const int kx0 = wk.z, nkx = wk.y0;
@@ -572,6 +587,7 @@ __global__ void __launch_bounds__(yzw_threads<PZ>(), PZ == 16 ? 1 : 2)
   extern __shared__ float2 sm[];
   __shared__ MagnetDev M;
   __shared__ GroupDev G;
+  pdl_trigger();  // the x-inverse pass may start its prologue during the last wave
   const Work wk = work[blockIdx.x];
   if (!load_descs(M, G, mags, groups, wk.mag, gate, stage)) return;
   yzw_body<PZ, 32>(M, wk.z, wk.y0, sm, tw);
@@ -887,6 +903,7 @@ __global__ void __launch_bounds__(X_THREADS_MAX, 2) k_xinv(const MagnetDev* __re
     nb_rows_fill(T, M, y0, ty, z);
     if (threadIdx.x < c_tab.S) cf[threadIdx.x] = (float)(G.dt * (c_tab.b1[threadIdx.x] - c_tab.b2[threadIdx.x]));
   }
+  pdl_wait();  // the spectrum and the stage state are written by the earlier passes
   const float2* __restrict__ S = M.spec;
   const size_t cstride = (size_t)nz * ny;
   // rebuild full-length Hermitian rows: Z = A + iB.  Lanes e (kx = e >> tyl,

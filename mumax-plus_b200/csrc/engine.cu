@@ -1337,9 +1337,12 @@ mpx_status launch_attempt(mpx_engine* e, const TableauDev& T, int first_stage) {
       if (s == 0)
         k_xfwd<false><<<e->n_t_demag, e->nt_x, e->smem_x, e->stream>>>(e->d_mags, e->d_groups, e->d_t_demag, 0, 1,
                                                                        nullptr, e->d_tw);
-      else
+      else if (s == first_stage)  // after the step controller: fully serialised
         k_xfwd<true><<<e->n_t_demag, e->nt_x, e->smem_x, e->stream>>>(e->d_mags, e->d_groups, e->d_t_demag, s, 1,
                                                                       nullptr, e->d_tw);
+      else  // after the previous stage (the group state is constant within an attempt)
+        CUDA_TRY(launch_pdl(k_xfwd<true>, e->n_t_demag, e->nt_x, e->smem_x, e->stream, e->d_mags, e->d_groups,
+                            e->d_t_demag, s, 1, (const float*)nullptr, e->d_tw));
       e->launches++;
     }
     if (e->n_t_local > 0 && s > 0) {

@@ -193,6 +193,7 @@ __global__ void __launch_bounds__(X_THREADS_MAX, 2) k_xfwd(const MagnetDev* __re
     }
     __syncthreads();
   }
+  pdl_wait();  // the stage state and derivatives are written by the earlier passes
 
   // only the lower half of each row: the upper half (x >= L/2 >= nx) is zero
   // padding that the pruned first FFT pass does not read
@@ -883,6 +884,7 @@ __global__ void __launch_bounds__(X_THREADS_MAX, 2) k_xinv(const MagnetDev* __re
   extern __shared__ float2 sm[];
   __shared__ MagnetDev M;
   __shared__ GroupDev G;
+  pdl_trigger();  // the next stage's x pass may start its prologue during the last wave
   const Work wk = work[blockIdx.x];
   if (!load_descs(M, G, mags, groups, wk.mag, ea.gate, ea.stage)) return;
   const int z = wk.z, y0 = wk.y0, ty = wk.ty;

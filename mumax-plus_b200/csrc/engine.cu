@@ -1548,7 +1548,17 @@ mpx_status drive_group(mpx_engine* e, Group* g) {
       MPX_TRY(write_group(e, g->slot, &G));
       return MPX_OK;
     }
-    chunk = std::min(chunk * 2, 16);
+    // attempts queued after the group has finished launch their kernels for
+    // nothing: no more than the steps left of steps(n), or of run() at the
+    // current time step (the final shortened step included)
+    int left = 16;
+    if (G.mode == 1) {
+      left = (int)std::min<long long>(16, std::max<long long>(1, G.steps_left));
+    } else if (G.mode == 0 && G.dt > 0) {
+      const double r = (G.t_stop - G.t) / G.dt;
+      left = (G.phase == 1 || r < 1.0) ? 1 : (r < 15.0 ? (int)r + 1 : 16);
+    }
+    chunk = std::max(1, std::min(std::min(chunk * 2, 16), left));
   }
 }
 

@@ -913,34 +913,69 @@ __global__ void __launch_bounds__(X_THREADS_MAX, 2) k_xinv(const MagnetDev* __re
   // the z value of the odd row comes from the next lane by a shuffle, so every
   // lane issues its three loads together and all lanes run the same trip count.
   const int tyl = tile_log(ty);
-  const int total = Fh << tyl;
+  if ((ny & 1) == 0) {
+    // even ny: tiles have an even number of rows starting on even rows, and every
+    // spectrum offset of a row pair is even, so each lane loads rows 2p, 2p + 1
+    // of its kx with 16-byte loads (the same values, half the load instructions)
+    const int pl = tyl - 1;
+    const int totalp = Fh << pl;
 #pragma unroll 2
-  for (int e0 = 0; e0 < total; e0 += blockDim.x) {
-    const int e = e0 + threadIdx.x;
-    const int yl = e & ((1 << tyl) - 1), kx = e >> tyl;
-    const bool act = e < total && yl < ty;
-    const size_t base = (size_t)kx * 3 * cstride + (size_t)z * ny + y0 + yl;
-    float2 A = make_float2(0.f, 0.f), B = A, Cz = A;
-    if (act) {
-      A = __ldg(S + base);
-      B = __ldg(S + base + cstride);
-      Cz = __ldg(S + base + 2 * cstride);
+    for (int e0 = 0; e0 < totalp; e0 += blockDim.x) {
+      const int e = e0 + threadIdx.x;
+      const int yp = e & ((1 << pl) - 1), kx = e >> pl;
+      if (e >= totalp || 2 * yp >= ty) continue;
+      const size_t base = (size_t)kx * 3 * cstride + (size_t)z * ny + y0 + 2 * yp;
+      const float4 a2 = __ldg(reinterpret_cast<const float4*>(S + base));
+      const float4 b2 = __ldg(reinterpret_cast<const float4*>(S + base + cstride));
+      const float4 c2 = __ldg(reinterpret_cast<const float4*>(S + base + 2 * cstride));
+      float2 A0 = make_float2(a2.x, a2.y), A1 = make_float2(a2.z, a2.w);
+      float2 B0 = make_float2(b2.x, b2.y), B1 = make_float2(b2.z, b2.w);
+      float2 C0 = make_float2(c2.x, c2.y), C1 = make_float2(c2.z, c2.w);
+      const bool edge = (kx == 0) || (2 * kx == L);
+      if (edge) {
+        A0.y = A1.y = B0.y = B1.y = C0.y = C1.y = 0.f;
+      }
+      const bool mirror = kx > 0 && 2 * kx < L;
+      const int y = 2 * yp;
+      sm[y * cs + xidx(kx, sh)] = make_float2(A0.x - B0.y, A0.y + B0.x);
+      sm[(y + 1) * cs + xidx(kx, sh)] = make_float2(A1.x - B1.y, A1.y + B1.x);
+      rows_z[yp * cs + xidx(kx, sh)] = make_float2(C0.x - C1.y, C0.y + C1.x);
+      if (mirror) {
+        sm[y * cs + xidx(L - kx, sh)] = make_float2(A0.x + B0.y, -A0.y + B0.x);
+        sm[(y + 1) * cs + xidx(L - kx, sh)] = make_float2(A1.x + B1.y, -A1.y + B1.x);
+        rows_z[yp * cs + xidx(L - kx, sh)] = make_float2(C0.x + C1.y, -C0.y + C1.x);
+      }
     }
-    const float dx = __shfl_down_sync(0xffffffffu, Cz.x, 1), dy = __shfl_down_sync(0xffffffffu, Cz.y, 1);
-    if (!act) continue;
-    const bool edge = (kx == 0) || (2 * kx == L);
-    if (edge) {
-      A.y = 0.f;
-      B.y = 0.f;
-      Cz.y = 0.f;
-    }
-    sm[yl * cs + xidx(kx, sh)] = make_float2(A.x - B.y, A.y + B.x);
-    if (kx > 0 && 2 * kx < L) sm[yl * cs + xidx(L - kx, sh)] = make_float2(A.x + B.y, -A.y + B.x);
-    if ((yl & 1) == 0) {
-      float2 Dv = (yl + 1 < ty) ? make_float2(dx, dy) : make_float2(0.f, 0.f);
-      if (edge) Dv.y = 0.f;
-      rows_z[(yl >> 1) * cs + xidx(kx, sh)] = make_float2(Cz.x - Dv.y, Cz.y + Dv.x);
-      if (kx > 0 && 2 * kx < L) rows_z[(yl >> 1) * cs + xidx(L - kx, sh)] = make_float2(Cz.x + Dv.y, -Cz.y + Dv.x);
+  } else {
+    const int total = Fh << tyl;
+#pragma unroll 2
+    for (int e0 = 0; e0 < total; e0 += blockDim.x) {
+      const int e = e0 + threadIdx.x;
+      const int yl = e & ((1 << tyl) - 1), kx = e >> tyl;
+      const bool act = e < total && yl < ty;
+      const size_t base = (size_t)kx * 3 * cstride + (size_t)z * ny + y0 + yl;
+      float2 A = make_float2(0.f, 0.f), B = A, Cz = A;
+      if (act) {
+        A = __ldg(S + base);
+        B = __ldg(S + base + cstride);
+        Cz = __ldg(S + base + 2 * cstride);
+      }
+      const float dx = __shfl_down_sync(0xffffffffu, Cz.x, 1), dy = __shfl_down_sync(0xffffffffu, Cz.y, 1);
+      if (!act) continue;
+      const bool edge = (kx == 0) || (2 * kx == L);
+      if (edge) {
+        A.y = 0.f;
+        B.y = 0.f;
+        Cz.y = 0.f;
+      }
+      sm[yl * cs + xidx(kx, sh)] = make_float2(A.x - B.y, A.y + B.x);
+      if (kx > 0 && 2 * kx < L) sm[yl * cs + xidx(L - kx, sh)] = make_float2(A.x + B.y, -A.y + B.x);
+      if ((yl & 1) == 0) {
+        float2 Dv = (yl + 1 < ty) ? make_float2(dx, dy) : make_float2(0.f, 0.f);
+        if (edge) Dv.y = 0.f;
+        rows_z[(yl >> 1) * cs + xidx(kx, sh)] = make_float2(Cz.x - Dv.y, Cz.y + Dv.x);
+        if (kx > 0 && 2 * kx < L) rows_z[(yl >> 1) * cs + xidx(L - kx, sh)] = make_float2(Cz.x + Dv.y, -Cz.y + Dv.x);
+      }
     }
   }
   __syncthreads();

@@ -235,6 +235,39 @@ __global__ void __launch_bounds__(X_THREADS_MAX, 2) k_xfwd(const MagnetDev* __re
   const int Fh = M.Fh;
   float2* S = M.spec;
   const int tyl = tile_log(ty);
+  if ((ny & 1) == 0) {
+    // even ny: rows 2p, 2p + 1 of one (kx, c) with one 16-byte store (every
+    // offset is even); the z values of the pair come from one packed row
+    const int pl = tyl - 1;
+    for (int e = threadIdx.x; e < (Fh * 3) << pl; e += blockDim.x) {
+      const int yp = e & ((1 << pl) - 1);
+      if (2 * yp >= ty) continue;
+      const int rest = e >> pl;
+      const int c = rest % 3, kx = rest / 3;
+      float2 v0, v1;
+      if (c < 2) {
+        const float2* Z0 = sm + (2 * yp) * cs;
+        const float2* Z1 = Z0 + cs;
+        const float2 zk0 = Z0[xidx(kx, sh)], zc0 = cconj(Z0[xidx((L - kx) & (L - 1), sh)]);
+        const float2 zk1 = Z1[xidx(kx, sh)], zc1 = cconj(Z1[xidx((L - kx) & (L - 1), sh)]);
+        if (c == 0) {
+          v0 = make_float2(0.5f * (zk0.x + zc0.x), 0.5f * (zk0.y + zc0.y));
+          v1 = make_float2(0.5f * (zk1.x + zc1.x), 0.5f * (zk1.y + zc1.y));
+        } else {  // -i/2 (zk - zc)
+          v0 = make_float2(0.5f * (zk0.y - zc0.y), -0.5f * (zk0.x - zc0.x));
+          v1 = make_float2(0.5f * (zk1.y - zc1.y), -0.5f * (zk1.x - zc1.x));
+        }
+      } else {
+        const float2* Z = sm + (ty + yp) * cs;
+        const float2 zk = Z[xidx(kx, sh)], zc = cconj(Z[xidx((L - kx) & (L - 1), sh)]);
+        v0 = make_float2(0.5f * (zk.x + zc.x), 0.5f * (zk.y + zc.y));
+        v1 = make_float2(0.5f * (zk.y - zc.y), -0.5f * (zk.x - zc.x));
+      }
+      *reinterpret_cast<float4*>(S + ((size_t)(kx * 3 + c) * nz + z) * ny + y0 + 2 * yp) =
+          make_float4(v0.x, v0.y, v1.x, v1.y);
+    }
+    return;
+  }
   for (int e = threadIdx.x; e < (Fh * 3) << tyl; e += blockDim.x) {
     const int yl = e & ((1 << tyl) - 1);
     if (yl >= ty) continue;

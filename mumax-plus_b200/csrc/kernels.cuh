@@ -97,6 +97,12 @@ __device__ __forceinline__ const float* stage_m(const MagnetDev& M, const GroupD
   return stage == 0 ? M.buf[G.map[0]] : M.buf[G.map[1]];
 }
 
+// x^2 + y^2 + z^2 with its roundings spelled out, so that every form of the
+// stage combination below rounds alike
+__device__ __forceinline__ float norm2_rn(float x, float y, float z) {
+  return __fmaf_rn(z, z, __fmaf_rn(y, y, __fmul_rn(x, x)));
+}
+
 // Stage combination x_s = normalize(x0 + sum_j dt a_sj k_j) of one cell
 // (core/rungekutta.cpp:108-134, core/fieldops.cu:232-258).
 __device__ __forceinline__ float3 combine_cell(const MagnetDev& M, const GroupDev& G, int stage, int i,
@@ -115,11 +121,11 @@ __device__ __forceinline__ float3 combine_cell(const MagnetDev& M, const GroupDe
     if (j < nj) {
       const double co = final_b1 ? c_tab.b1[j] : c_tab.a[stage][j];
       const float cf = (float)(G.dt * co);
-      v = f3(v.x + cf * k[j].x, v.y + cf * k[j].y, v.z + cf * k[j].z);
+      v = f3(__fmaf_rn(cf, k[j].x, v.x), __fmaf_rn(cf, k[j].y, v.y), __fmaf_rn(cf, k[j].z, v.z));
     }
   }
-  const float inv = rsqrtf(v.x * v.x + v.y * v.y + v.z * v.z);
-  return f3(v.x * inv, v.y * inv, v.z * inv);
+  const float inv = rsqrtf(norm2_rn(v.x, v.y, v.z));
+  return f3(__fmul_rn(v.x, inv), __fmul_rn(v.y, inv), __fmul_rn(v.z, inv));
 }
 
 // combine_cell for a stage (not the final b1 sum) with the coefficients
@@ -136,11 +142,47 @@ __device__ __forceinline__ float3 combine_cell_pre(const float* __restrict__ x0,
   for (int j = 0; j < 7; ++j) {
     if (j < stage) {
       const float c = cf[j];
-      v = f3(v.x + c * k[j].x, v.y + c * k[j].y, v.z + c * k[j].z);
+      v = f3(__fmaf_rn(c, k[j].x, v.x), __fmaf_rn(c, k[j].y, v.y), __fmaf_rn(c, k[j].z, v.z));
     }
   }
-  const float inv = rsqrtf(v.x * v.x + v.y * v.y + v.z * v.z);
-  return f3(v.x * inv, v.y * inv, v.z * inv);
+  const float inv = rsqrtf(norm2_rn(v.x, v.y, v.z));
+  return f3(__fmul_rn(v.x, inv), __fmul_rn(v.y, inv), __fmul_rn(v.z, inv));
+}
+
+__device__ __forceinline__ float f4c(const float4& a, int q) { return q == 0 ? a.x : q == 1 ? a.y : q == 2 ? a.z : a.w; }
+__device__ __forceinline__ void f4set(float4& a, int q, float v) {
+  if (q == 0) a.x = v; else if (q == 1) a.y = v; else if (q == 2) a.z = v; else a.w = v;
+}
+
+// combine_cell_pre for the four consecutive cells i .. i + 3 (i a multiple of
+// 4, every buffer 16-byte aligned): 16-byte loads and stores, the same sums in
+// the same order per cell. The stage state goes to xs; returns it in r.
+__device__ __forceinline__ void combine_quad_pre(const float* __restrict__ x0, float* xs, int N, int stage, int i,
+                                                 const float* cf, const float* const* kp, float4 r[3]) {
+#pragma unroll
+  for (int c = 0; c < 3; ++c) r[c] = __ldg(reinterpret_cast<const float4*>(x0 + c * N + i));
+#pragma unroll
+  for (int j = 0; j < 7; ++j) {
+    if (j < stage) {
+      const float cj = cf[j];
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        const float4 k = __ldg(reinterpret_cast<const float4*>(kp[j] + c * N + i));
+        r[c] = make_float4(__fmaf_rn(cj, k.x, r[c].x), __fmaf_rn(cj, k.y, r[c].y), __fmaf_rn(cj, k.z, r[c].z),
+                           __fmaf_rn(cj, k.w, r[c].w));
+      }
+    }
+  }
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    const float vx = f4c(r[0], q), vy = f4c(r[1], q), vz = f4c(r[2], q);
+    const float inv = rsqrtf(norm2_rn(vx, vy, vz));
+    f4set(r[0], q, __fmul_rn(vx, inv));
+    f4set(r[1], q, __fmul_rn(vy, inv));
+    f4set(r[2], q, __fmul_rn(vz, inv));
+  }
+#pragma unroll
+  for (int c = 0; c < 3; ++c) *reinterpret_cast<float4*>(xs + c * N + i) = r[c];
 }
 
 // Row index e / n within a tile of at most TY_MAX rows of length n, without
@@ -185,19 +227,60 @@ __global__ void __launch_bounds__(X_THREADS_MAX, 2) k_xfwd(const MagnetDev* __re
   else load_twiddles<3>(tws, tw, logL);
   __shared__ float s_cf[8];
   __shared__ const float* s_kp[8];
+  __shared__ int s_al;  // every buffer the block reads or writes is 16-byte aligned
+  if (threadIdx.x == 0) {
+    uintptr_t a = (uintptr_t)src | (uintptr_t)xs | (uintptr_t)x0;
+    if (COMBINE)
+      for (int j = 0; j < stage; ++j) a |= (uintptr_t)M.buf[G.map[2 + j]];
+    s_al = (a & 15) == 0;
+  }
   if (COMBINE) {  // the stage's coefficients and k_j buffers, once per block
     if (threadIdx.x < 7) {
       const int j = threadIdx.x;
       s_cf[j] = (j < stage) ? (float)(G.dt * c_tab.a[stage][j]) : 0.f;
       s_kp[j] = M.buf[G.map[2 + j]];
     }
-    __syncthreads();
   }
+  __syncthreads();
   pdl_wait();  // the stage state and derivatives are written by the earlier passes
 
   // only the lower half of each row: the upper half (x >= L/2 >= nx) is zero
   // padding that the pruned first FFT pass does not read
   const int logLh = logL > 0 ? logL - 1 : 0;
+  if ((nx & 3) == 0 && logLh >= 2 && !M.geom && !M.msat.p && s_al) {
+    // four consecutive cells per thread with 16-byte loads and stores (no
+    // geometry, uniform Ms; nx and so N a multiple of 4)
+    const int lq = logLh - 2;
+    const float ms = M.msat.u;
+    for (int e = threadIdx.x; e < (ty << lq); e += blockDim.x) {
+      const int yl = e >> lq, x = (e & ((1 << lq) - 1)) << 2;
+      float4 r[3];
+      if (x < nx) {
+        const int i = rowbase + yl * nx + x;
+        if (COMBINE) {
+          combine_quad_pre(x0, xs, N, stage, i, s_cf, s_kp, r);
+        } else {
+#pragma unroll
+          for (int c = 0; c < 3; ++c) r[c] = __ldg(reinterpret_cast<const float4*>(src + c * N + i));
+        }
+#pragma unroll
+        for (int c = 0; c < 3; ++c)
+          r[c] = make_float4(__fmul_rn(ms, r[c].x), __fmul_rn(ms, r[c].y), __fmul_rn(ms, r[c].z), __fmul_rn(ms, r[c].w));
+      } else {
+#pragma unroll
+        for (int c = 0; c < 3; ++c) r[c] = make_float4(0.f, 0.f, 0.f, 0.f);
+      }
+      float2* row = sm + yl * cs;
+      float* zr = reinterpret_cast<float*>(sm + (ty + (yl >> 1)) * cs);
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const int xi = xidx(x + q, sh);
+        row[xi] = make_float2(f4c(r[0], q), f4c(r[1], q));
+        zr[2 * xi + (yl & 1)] = f4c(r[2], q);
+        if ((ty & 1) && yl == ty - 1) zr[2 * xi + 1] = 0.0f;
+      }
+    }
+  } else {
 #pragma unroll 2
   for (int e = threadIdx.x; e < (ty << logLh); e += blockDim.x) {
     const int yl = e >> logLh, x = e & ((1 << logLh) - 1);
@@ -221,6 +304,7 @@ __global__ void __launch_bounds__(X_THREADS_MAX, 2) k_xfwd(const MagnetDev* __re
     float* zr = reinterpret_cast<float*>(sm + (ty + (yl >> 1)) * cs + xidx(x, sh));
     zr[yl & 1] = Mv.z;
     if ((ty & 1) && yl == ty - 1) zr[1] = 0.0f;
+  }
   }
   __syncthreads();
   if (wrow) {

@@ -354,6 +354,18 @@ mpx_status mpx_poll(mpx_engine* e, int* done, int cap, int* n_done, int* n_runni
 mpx_status mpx_reduce_noalloc(const float* field, int ncells, int ncomp, const unsigned char* geometry, int op,
                               void* stream, double out[3]);
 
+/* No counterpart in the reference (it has no sanitizer or checked build):
+ * index checking for the checked library libmpx_checked.so, built from the
+ * same sources with -DMPX_BOUNDS_CHECK.  There every per-cell access of a
+ * field buffer (stencil neighbours, stage states and derivatives, stray-field
+ * buffers) verifies 0 <= i < N; a bad access is skipped (loads give 0) and the
+ * first one recorded, without trapping.  Synchronises the current device,
+ * writes the record to *first_bad (0 = none; else bit 63 set, N in bits
+ * 32..62, i in bits 0..31) and clears it.  The vectorised four-cell loads of
+ * the forward x pass and the spectrum passes are not checked.  In libmpx.so
+ * the checks are compiled out and this returns MPX_ERR_UNSUPPORTED. */
+mpx_status mpx_bounds_check(unsigned long long* first_bad);
+
 #ifdef __cplusplus
 }
 #endif

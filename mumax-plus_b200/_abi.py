@@ -7,7 +7,9 @@ import ctypes as C
 import os
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "libmpx.so")
+# MPX_LIBRARY selects another build of the same ABI (the checked build,
+# libmpx_checked.so); the default is the in-tree libmpx.so.
+LIB_PATH = os.environ.get("MPX_LIBRARY") or os.path.join(HERE, "libmpx.so")
 
 # status codes
 MPX_OK = 0
@@ -192,6 +194,7 @@ SIGNATURES = {
     "mpx_advance": (I, [E, I]),
     "mpx_poll": (I, [E, P_I, I, P_I, P_I]),
     "mpx_reduce_noalloc": (I, [C.c_void_p, I, I, C.c_void_p, I, C.c_void_p, P_D]),
+    "mpx_bounds_check": (I, [C.POINTER(C.c_ulonglong)]),
 }
 
 

@@ -2785,6 +2785,20 @@ mpx_status mpx_poll(mpx_engine* e, int* done, int cap, int* n_done, int* n_runni
   return MPX_OK;
 }
 
+mpx_status mpx_bounds_check(unsigned long long* first_bad) {
+  if (!first_bad) return fail(MPX_ERR_INVALID, "mpx_bounds_check: null output");
+  *first_bad = 0;
+#ifdef MPX_BOUNDS_CHECK
+  CUDA_TRY(cudaDeviceSynchronize());
+  CUDA_TRY(cudaMemcpyFromSymbol(first_bad, g_bounds_first_bad, sizeof(unsigned long long)));
+  const unsigned long long zero = 0;
+  CUDA_TRY(cudaMemcpyToSymbol(g_bounds_first_bad, &zero, sizeof zero));
+  return MPX_OK;
+#else
+  return fail(MPX_ERR_UNSUPPORTED, "mpx_bounds_check: library built without MPX_BOUNDS_CHECK (use libmpx_checked.so)");
+#endif
+}
+
 }  // extern "C"
 
 // ============================================ allocation-free reduction

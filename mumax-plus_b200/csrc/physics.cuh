@@ -137,14 +137,33 @@ __device__ __forceinline__ float3 cross3(float3 a, float3 b) {
 
 __device__ __forceinline__ bool in_geom(const MagnetDev& M, int i) { return !M.geom || M.geom[i]; }
 
+#ifdef MPX_BOUNDS_CHECK
+// Checked build (libmpx_checked.so): every per-cell access of a SoA field
+// buffer through load3 / ldg3 / store3 verifies 0 <= i < N.  The first bad
+// access is recorded (bit 63 set, N in bits 32..62, i in the low word) and
+// skipped -- a load gives 0 -- so the kernel runs to its end and the host reads
+// the record with mpx_bounds_check.  Nothing traps.
+__device__ unsigned long long g_bounds_first_bad;
+__device__ __forceinline__ bool cell_ok(int N, int i) {
+  if ((unsigned)i < (unsigned)N) return true;
+  atomicCAS(&g_bounds_first_bad, 0ull, (1ull << 63) | ((unsigned long long)(unsigned)N << 32) | (unsigned)i);
+  return false;
+}
+#else
+__device__ __forceinline__ bool cell_ok(int, int) { return true; }
+#endif
+
 __device__ __forceinline__ float3 load3(const float* __restrict__ a, int N, int i) {
+  if (!cell_ok(N, i)) return f3(0.f, 0.f, 0.f);
   return f3(a[i], a[N + i], a[2 * N + i]);
 }
 // read-only path: for buffers a kernel never writes
 __device__ __forceinline__ float3 ldg3(const float* __restrict__ a, int N, int i) {
+  if (!cell_ok(N, i)) return f3(0.f, 0.f, 0.f);
   return f3(__ldg(a + i), __ldg(a + N + i), __ldg(a + 2 * N + i));
 }
 __device__ __forceinline__ void store3(float* a, int N, int i, float3 v) {
+  if (!cell_ok(N, i)) return;
   a[i] = v.x;
   a[N + i] = v.y;
   a[2 * N + i] = v.z;

@@ -42,3 +42,23 @@ def mpx():
     import mumaxplus_b200
 
     return mumaxplus_b200
+
+
+@pytest.fixture(scope="session", autouse=True)
+def bounds_record():
+    """With MPX_BOUNDS_CHECK_RUN=1 (set by tests/test_gpu_bounds.py together
+    with MPX_LIBRARY=libmpx_checked.so): after the session, the checked
+    library must report that no per-cell field access was out of range."""
+    yield
+    if os.environ.get("MPX_BOUNDS_CHECK_RUN") != "1":
+        return
+    import ctypes
+
+    import mumaxplus_b200
+
+    lib = mumaxplus_b200._abi.load()
+    bad = ctypes.c_ulonglong(0)
+    st = lib.mpx_bounds_check(ctypes.byref(bad))
+    assert st == 0, f"mpx_bounds_check: status {st} ({lib.mpx_last_error()}); not the checked build?"
+    v = bad.value
+    assert v == 0, f"out-of-range field access: index {v & 0xFFFFFFFF} with N = {(v >> 32) & 0x7FFFFFFF}"

@@ -31,6 +31,10 @@ def test_library_exports_every_header_symbol(built_lib):
     assert not missing, missing
     # the ctypes signature table covers the whole header
     assert sorted(mpx._abi.SIGNATURES) == names
+    # the checked build (-DMPX_BOUNDS_CHECK) exports the same ABI
+    checked = C.CDLL(os.path.join(ROOT, "mumax-plus_b200", "libmpx_checked.so"))
+    missing = [n for n in names if not hasattr(checked, n)]
+    assert not missing, missing
 
 
 def test_device_count_without_gpu_is_safe(built_lib):

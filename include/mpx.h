@@ -361,9 +361,10 @@ mpx_status mpx_reduce_noalloc(const float* field, int ncells, int ncomp, const u
  * buffers) verifies 0 <= i < N; a bad access is skipped (loads give 0) and the
  * first one recorded, without trapping.  Synchronises the current device,
  * writes the record to *first_bad (0 = none; else bit 63 set, N in bits
- * 32..62, i in bits 0..31) and clears it.  The vectorised four-cell loads of
- * the forward x pass and the spectrum passes are not checked.  In libmpx.so
- * the checks are compiled out and this returns MPX_ERR_UNSUPPORTED. */
+ * 32..62, i in bits 0..31) and clears it.  The four-cell vector accesses of
+ * the forward x pass and the spectrum stores / gathers of the x passes are
+ * checked the same way; the y/z pass is not.  In libmpx.so the checks are
+ * compiled out and this returns MPX_ERR_UNSUPPORTED. */
 mpx_status mpx_bounds_check(unsigned long long* first_bad);
 
 #ifdef __cplusplus

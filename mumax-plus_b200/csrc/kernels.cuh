@@ -255,8 +255,8 @@ __global__ void __launch_bounds__(X_THREADS_MAX, 2) k_xfwd(const MagnetDev* __re
     for (int e = threadIdx.x; e < (ty << lq); e += blockDim.x) {
       const int yl = e >> lq, x = (e & ((1 << lq) - 1)) << 2;
       float4 r[3];
-      if (x < nx) {
-        const int i = rowbase + yl * nx + x;
+      const int i = rowbase + yl * nx + x;
+      if (x < nx && cell_ok(N, i) && cell_ok(N, i + 3)) {
         if (COMBINE) {
           combine_quad_pre(x0, xs, N, stage, i, s_cf, s_kp, r);
         } else {
@@ -347,8 +347,9 @@ __global__ void __launch_bounds__(X_THREADS_MAX, 2) k_xfwd(const MagnetDev* __re
         v0 = make_float2(0.5f * (zk.x + zc.x), 0.5f * (zk.y + zc.y));
         v1 = make_float2(0.5f * (zk.y - zc.y), -0.5f * (zk.x - zc.x));
       }
-      *reinterpret_cast<float4*>(S + ((size_t)(kx * 3 + c) * nz + z) * ny + y0 + 2 * yp) =
-          make_float4(v0.x, v0.y, v1.x, v1.y);
+      const size_t si = ((size_t)(kx * 3 + c) * nz + z) * ny + y0 + 2 * yp;
+      if (span_ok(si + 1, (size_t)Fh * 3 * nz * ny))
+        *reinterpret_cast<float4*>(S + si) = make_float4(v0.x, v0.y, v1.x, v1.y);
     }
     return;
   }
@@ -367,7 +368,8 @@ __global__ void __launch_bounds__(X_THREADS_MAX, 2) k_xfwd(const MagnetDev* __re
     } else {  // -i/2 (zk - zc)
       val = make_float2(0.5f * (zk.y - zc.y), -0.5f * (zk.x - zc.x));
     }
-    S[((size_t)(kx * 3 + c) * nz + z) * ny + y0 + yl] = val;
+    const size_t si = ((size_t)(kx * 3 + c) * nz + z) * ny + y0 + yl;
+    if (span_ok(si, (size_t)Fh * 3 * nz * ny)) S[si] = val;
   }
 }
 
@@ -1042,6 +1044,7 @@ __global__ void __launch_bounds__(X_THREADS_MAX, 2) k_xinv(const MagnetDev* __re
       const int yp = e & ((1 << pl) - 1), kx = e >> pl;
       if (e >= totalp || 2 * yp >= ty) continue;
       const size_t base = (size_t)kx * 3 * cstride + (size_t)z * ny + y0 + 2 * yp;
+      if (!span_ok(base + 2 * cstride + 1, (size_t)Fh * 3 * cstride)) continue;
       const float4 a2 = __ldg(reinterpret_cast<const float4*>(S + base));
       const float4 b2 = __ldg(reinterpret_cast<const float4*>(S + base + cstride));
       const float4 c2 = __ldg(reinterpret_cast<const float4*>(S + base + 2 * cstride));
@@ -1069,8 +1072,8 @@ __global__ void __launch_bounds__(X_THREADS_MAX, 2) k_xinv(const MagnetDev* __re
     for (int e0 = 0; e0 < total; e0 += blockDim.x) {
       const int e = e0 + threadIdx.x;
       const int yl = e & ((1 << tyl) - 1), kx = e >> tyl;
-      const bool act = e < total && yl < ty;
       const size_t base = (size_t)kx * 3 * cstride + (size_t)z * ny + y0 + yl;
+      const bool act = e < total && yl < ty && span_ok(base + 2 * cstride, (size_t)Fh * 3 * cstride);
       float2 A = make_float2(0.f, 0.f), B = A, Cz = A;
       if (act) {
         A = __ldg(S + base);

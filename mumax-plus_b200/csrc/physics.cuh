@@ -149,8 +149,17 @@ __device__ __forceinline__ bool cell_ok(int N, int i) {
   atomicCAS(&g_bounds_first_bad, 0ull, (1ull << 63) | ((unsigned long long)(unsigned)N << 32) | (unsigned)i);
   return false;
 }
+// the same for an element index i of an array of n elements (spectra, vector
+// accesses); n above 2^31 - 1 is recorded as 2^31 - 1, i by its low 32 bits
+__device__ __forceinline__ bool span_ok(size_t i, size_t n) {
+  if (i < n) return true;
+  const unsigned long long nn = n < 0x7fffffffull ? n : 0x7fffffffull;
+  atomicCAS(&g_bounds_first_bad, 0ull, (1ull << 63) | (nn << 32) | (i & 0xffffffffull));
+  return false;
+}
 #else
 __device__ __forceinline__ bool cell_ok(int, int) { return true; }
+__device__ __forceinline__ bool span_ok(size_t, size_t) { return true; }
 #endif
 
 __device__ __forceinline__ float3 load3(const float* __restrict__ a, int N, int i) {

@@ -211,3 +211,16 @@ def test_solve_takes_device_sampling_only_for_magnetization_averages():
     assert ts._magnetization_columns({"h": FieldQuantity(a, _abi.Q_DEMAG_FIELD, "h", "T").average}) is None
     assert ts._magnetization_columns({"m": Variable(a).average, "e": Variable(a).get}) is None
     assert mpx.TimeSolver is TimeSolver
+
+
+def test_checked_build_command_defines_the_check():
+    import importlib.util
+
+    spec = importlib.util.spec_from_file_location("_mpx_build", os.path.join(ROOT, "mumax-plus_b200", "build.py"))
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    plain, checked = mod._command(mod.OUT, ()), mod._command(mod.OUT_CHECKED, ())
+    assert "-DMPX_BOUNDS_CHECK" in checked and "-DMPX_BOUNDS_CHECK" not in plain
+    for cmd in (plain, checked):
+        assert "arch=compute_100a,code=sm_100a" in cmd
+    assert [a for a in plain if a != mod.OUT] == [a for a in checked if a not in (mod.OUT_CHECKED, "-DMPX_BOUNDS_CHECK")]

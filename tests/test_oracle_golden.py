@@ -2,6 +2,7 @@
 hold for this path (CPU only, no GPU).
 
   exchange     test/test_exchange.py:6-46     numpy Laplacian, Neumann edges
+               test/test_exchange.py:48-85    spiral energy vs A k^2 up to 20 degrees
   DMI          test/test_interfacialdmi.py     numpy, open boundaries
   anisotropy   test/test_anisotropy.py:15-57   numpy uniaxial field / energy
   demag        test/test_demag.py:6-45         numpy FFT of the real-space kernel
@@ -62,6 +63,34 @@ def test_exchange_neumann_vs_numpy():
     wanted = _exchange_numpy(m, s.cellsize, s.aex, s.msat)
     got = w.eval(q, abi.Q_EXCHANGE_FIELD)
     assert np.max(np.abs(got - wanted) / np.abs(wanted)) < 1e-9
+
+
+def test_exchange_energy_of_spirals_vs_analytic():
+    """test/test_exchange.py:48-85 (figure 5 of the MuMax3 verification paper): the exchange energy of the
+    spiral m = (cos kx, sin kx, 0) on a 100 um x 1 nm x 1 nm wire, in units of Km V (Km = mu0 Msat^2 / 2),
+    against the continuum value A k^2 / Km, for k = 1e7, 2e7, ... 1/m until the angle between neighbouring
+    cells reaches 20 degrees; relative error < 1e-2 (the discrete energy is 2A(1 - cos k dx)/dx^2 per volume,
+    plus the two free ends)."""
+    msat, aex, dx = 800e3, 5e-12, 1e-9
+    nx = 100_000
+    mu0 = 4 * np.pi * 1e-7
+    km = 0.5 * mu0 * msat**2
+    volume = nx * dx * dx * dx
+    s = MagnetSpec(size=(nx, 1, 1), cellsize=(dx, dx, dx), aex=aex, msat=msat, enable_demag=False)
+    X = np.arange(nx, dtype=np.float64) * dx
+    w, q = s.oracle_world(np.stack([np.ones(nx), np.zeros(nx), np.zeros(nx)]).reshape(3, 1, 1, nx))
+    assert w.energy(q, abi.Q_EXCHANGE_ENERGY_DENSITY) == pytest.approx(0.0, abs=1e-30)
+    errors = []
+    k = 1e7
+    while k * dx < 20 * np.pi / 180:
+        m = np.stack([np.cos(k * X), np.sin(k * X), np.zeros(nx)]).reshape(3, 1, 1, nx)
+        w.set_m(q, m)
+        e_num = w.energy(q, abi.Q_EXCHANGE_ENERGY_DENSITY) / (km * volume)
+        e_ana = aex * k**2 / km
+        errors.append(abs(e_ana - e_num) / e_ana)
+        k += 1e7
+    assert len(errors) >= 30
+    assert max(errors) < 1e-2
 
 
 def _idmi_numpy(m, cs, Dxxz, Dyyz, msat):

@@ -10,6 +10,7 @@ hold for this path (CPU only, no GPU).
   time solver  test/test_timesolver.py:19-169  analytic macrospin precession, all 5 methods
   PBC          test/test_PBC.py:14-91          <m> after 1 ns vs the mumax3 value
   minimize     test/test_standardproblem2_coercivity.py, test/test_boundaries.py (coercivity, wire canting)
+  frozen spins test/test_frozenspins.py:28-56   <m> after minimize and a 1 ns reversal, half the film frozen
 
 The known answers themselves are in tests/golden/known_answers.json.
 """
@@ -342,6 +343,33 @@ def test_oracle_nanowire_canting_golden(oracle):
         return lambda: ow.get_m(q)
 
     check_nanowire(*nanowire_canting(lambda: st["ow"].minimize(1e-7, 10), None, make))
+
+
+def test_oracle_frozen_half_film_golden(oracle):
+    """test/test_frozenspins.py:28-56: a standard-problem-4 film (128 x 32 x 2) with the cells right of the centre
+    frozen (the centre is the midpoint of the first and last cell positions, so cells x >= 64), minimized from
+    (1, 0.1, 0), then run for 1 ns with the bias field (-24.6, 4.3, 0) mT on, Fehlberg (the reference's default
+    method) from the sensible time step; <m> after each against the reference's vectors (1e-4 per component).
+    The bias is applied as the world bias, which enters the Zeeman term like the magnet's own."""
+    nx, ny, nz = 128, 32, 2
+    frozen = np.zeros((nz, ny, nx), np.float32)
+    frozen[:, :, 64:] = 1
+    s = MagnetSpec(size=(nx, ny, nz), cellsize=(500e-9 / 128, 125e-9 / 32, 3e-9 / 2), msat=800e3, aex=13e-12,
+                   alpha=0.02, frozen=frozen)
+    m0 = np.zeros((3, nz, ny, nx))
+    m0[0], m0[1] = 1.0, 0.1
+    w, q = s.oracle_world(m0)
+    w.set_method("Fehlberg")
+    w.minimize()
+    k = known("frozen_half_minimized_m")
+    assert np.max(np.abs(np.array(w.average(q, abi.Q_MAGNETIZATION)) - k["value"])) < k["abs_tol"]
+    frozen_m = w.get_m(q)[:, :, :, 64:].copy()
+    w.set_world_bias((-24.6e-3, 4.3e-3, 0.0))
+    w.timestep = w.sensible_timestep()
+    w.run(1e-9)
+    k = known("frozen_half_reversal_m_1ns")
+    assert np.max(np.abs(np.array(w.average(q, abi.Q_MAGNETIZATION)) - k["value"])) < k["abs_tol"]
+    assert np.array_equal(w.get_m(q)[:, :, :, 64:], frozen_m)  # frozen cells never move
 
 
 def test_oracle_minimize_sp2_coercivity_golden(oracle):

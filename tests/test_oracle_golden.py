@@ -11,6 +11,7 @@ hold for this path (CPU only, no GPU).
   PBC          test/test_PBC.py:14-91          <m> after 1 ns vs the mumax3 value
   minimize     test/test_standardproblem2_coercivity.py, test/test_boundaries.py (coercivity, wire canting)
   frozen spins test/test_frozenspins.py:28-56   <m> after minimize and a 1 ns reversal, half the film frozen
+  STT          test/test_free_layer_thickness.py  Slonczewski torque unchanged by empty layers
 
 The known answers themselves are in tests/golden/known_answers.json.
 """
@@ -589,3 +590,28 @@ def test_oracle_thermal_noise_langevin(oracle):
 
     got, want = thermal_macrospins(run_steps, lambda: st["ow"].average(st["q"], oracle.abi.Q_MAGNETIZATION)[2])
     assert abs(got - want) < 0.02, (got, want)
+
+
+def test_oracle_slonczewski_torque_unchanged_by_empty_layers(oracle):
+    """test/test_free_layer_thickness.py:27-61: with the free-layer thickness given explicitly, the Slonczewski
+    torque of a 1 x 1 x 2 stack equals that of the same two cells in a 1 x 1 x 4 stack whose top two cells are
+    outside the geometry (the empty layers change nothing), within 1e-5 per cell.  The reference test leaves
+    Lambda at its default 0, which with epsilon' = 0 makes the Slonczewski term assuredly zero
+    (src/physics/stt.cu:18-26, src/physics/ferromagnet.cpp:36), so it compares rounding noise of the Zhang-Li
+    term; Lambda = 1 here makes the Slonczewski torque the one compared."""
+    rng = np.random.default_rng(21)
+    mdir = rng.uniform(size=3)
+    mdir /= np.linalg.norm(mdir)
+    common = dict(cellsize=(1e-9, 1e-9, 1e-9), msat=4.3, jcur=(0.0, 0.0, 5.4), pol=0.6, fixed_layer=(1.0, 0.0, 1.0),
+                  free_layer_thickness=1e-9, Lambda=1.0, enable_demag=False)
+    wanted_spec = MagnetSpec(size=(1, 1, 2), **common)
+    w1, q1 = wanted_spec.oracle_world(np.broadcast_to(mdir[:, None, None, None], (3, 2, 1, 1)).copy())
+    wanted = w1.eval(q1, abi.Q_SPIN_TRANSFER_TORQUE)[:, :, 0, 0]
+    geom = np.array([1, 1, 0, 0], dtype=np.uint8).reshape(4, 1, 1)
+    result_spec = MagnetSpec(size=(1, 1, 4), geometry=geom, **common)
+    w2, q2 = result_spec.oracle_world(np.broadcast_to(mdir[:, None, None, None], (3, 4, 1, 1)).copy())
+    got = w2.eval(q2, abi.Q_SPIN_TRANSFER_TORQUE)[:, :, 0, 0]
+    assert np.all(np.linalg.norm(wanted, axis=0) > 1e-3)  # a real torque, not rounding noise
+    err = np.linalg.norm(got[:, :2] - wanted, axis=0) / np.linalg.norm(wanted, axis=0)
+    assert np.max(err) < 1e-5
+    assert np.all(got[:, 2:] == 0)  # outside the geometry

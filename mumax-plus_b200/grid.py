@@ -1,4 +1,5 @@
 """Grid (mirror of mumaxplus/grid.py and core/grid.hpp:7-89)."""
+import numbers
 
 
 class Grid:
@@ -9,6 +10,13 @@ class Grid:
             raise ValueError("'size' should have three dimensions.")
         if len(origin) != 3:
             raise ValueError("'origin' should have three dimensions.")
+        # the reference converts to int3 (non-integers are a TypeError) and
+        # rejects negative sizes (core/grid.cu:11-17); 0 marks a non-periodic
+        # mastergrid axis
+        if not all(isinstance(v, numbers.Integral) for v in (*size, *origin)):
+            raise TypeError("grid size and origin must be integers")
+        if any(s < 0 for s in size):
+            raise ValueError("The grid size should be larger than or equal to 0")
         self._size = tuple(int(s) for s in size)
         self._origin = tuple(int(o) for o in origin)
 

@@ -224,3 +224,24 @@ def test_checked_build_command_defines_the_check():
     for cmd in (plain, checked):
         assert "arch=compute_100a,code=sm_100a" in cmd
     assert [a for a in plain if a != mod.OUT] == [a for a in checked if a not in (mod.OUT_CHECKED, "-DMPX_BOUNDS_CHECK")]
+
+
+def test_grid_argument_validation():
+    """test/test_grid.py:7-56: integer sizes >= 0 and integer origins of three components; anything else is a
+    ValueError or TypeError."""
+    import mumaxplus_b200 as mpx
+
+    for size in [(1, 1, 1), [12, 5, 1], (3, 1, 64), (0, 0, 0)]:
+        for origin in [(-2, 7, 0), (0, 0, 0)]:
+            g = mpx.Grid(size, origin)
+            assert g.size == tuple(size) and g.origin == tuple(origin)
+        assert mpx.Grid(size).origin == (0, 0, 0)
+    assert mpx.Grid(tuple(np.array([4, 2, 1]))).size == (4, 2, 1)  # numpy integers are integers
+    for size in [(2, -1, 1), [-3, 4, 4], (2.5, 3.0, 1.0), (4, 4), 7, (1, 2, 3, 4), "xy"]:
+        with pytest.raises((ValueError, TypeError)):
+            mpx.Grid(size)
+        with pytest.raises((ValueError, TypeError)):
+            mpx.Grid(size, (1, 1, 1))
+    for origin in [(0, 1.5, 0), (3, 3), 1]:
+        with pytest.raises((ValueError, TypeError)):
+            mpx.Grid((2, 2, 2), origin)

@@ -245,3 +245,32 @@ def test_grid_argument_validation():
     for origin in [(0, 1.5, 0), (3, 3), 1]:
         with pytest.raises((ValueError, TypeError)):
             mpx.Grid((2, 2, 2), origin)
+
+
+def test_geometry_and_region_masks():
+    """test/test_geometry.py:8-56 on the host-side mask conversion of Ferromagnet (no device): an array of the
+    grid shape or a function of (x, y, z) at the cell positions origin + index * cellsize; a wrong shape is a
+    ValueError, a function of the wrong arity a TypeError, negative region indices a ValueError."""
+    import mumaxplus_b200 as mpx
+    from mumaxplus_b200.ferromagnet import Ferromagnet
+
+    class _World:
+        cellsize = (3e-9, 4e-9, 5e-9)
+
+    fm = Ferromagnet.__new__(Ferromagnet)
+    fm._world, fm._grid = _World(), mpx.Grid((32, 16, 3), (2, -1, 0))
+    nx, ny, nz = fm._grid.size
+    geom = np.random.default_rng(4).uniform(size=(nz, ny, nx)) > 0.3
+    assert np.array_equal(fm._mask(geom, "geometry").astype(bool), geom)
+    f = lambda x, y, z: x**2 + y**2 < (40e-9) ** 2  # noqa: E731
+    X, Y, Z = fm.meshgrid
+    assert X[0, 0, 1] == pytest.approx(3 * 3e-9) and Y[0, 0, 0] == pytest.approx(-4e-9)
+    assert np.array_equal(fm._mask(f, "geometry").astype(bool), X**2 + Y**2 < (40e-9) ** 2)
+    with pytest.raises(ValueError):
+        fm._mask(np.ones((nz, ny, nx + 1), bool), "geometry")
+    with pytest.raises(TypeError):
+        fm._mask(lambda x, y: True, "geometry")
+    regions = np.arange(nx * ny * nz).reshape(nz, ny, nx) % 5
+    assert np.array_equal(fm._mask(regions, "regions"), regions)
+    with pytest.raises(ValueError):
+        fm._mask(-regions - 1, "regions")

@@ -200,6 +200,21 @@ mpx_status mpx_engine_destroy(mpx_engine* e);
 /* Launch subsequent work on this cudaStream_t (NULL = the engine's own stream). */
 mpx_status mpx_engine_set_stream(mpx_engine* e, void* stream);
 mpx_status mpx_engine_synchronize(mpx_engine* e);
+/* Arithmetic of the y transforms of the demag convolution (the cuFFT y
+ * stages of physics/strayfieldfft.cu:216-218, 238-240).  MPX_DFT_FP32
+ * (default): shared-memory FFTs in FP32 on the CUDA cores.  MPX_DFT_TF32X3:
+ * for y lengths 1024 and 2048, the 32-point DFT stages as TF32 tensor-core
+ * GEMMs (tcgen05) with 3xTF32 split products accumulated in FP32, in the
+ * three-pass y / z / y form; other lengths keep the FP32 FFTs.  Applies to
+ * the magnets added afterwards: set it before the first mpx_magnet_add
+ * (MPX_ERR_INVALID otherwise). */
+enum { MPX_DFT_FP32 = 0, MPX_DFT_TF32X3 = 1 };
+mpx_status mpx_engine_set_dft(mpx_engine* e, int mode);
+/* Number of waits of the tensor-core kernels on their MMA completion that
+ * gave up (each bounded at about 0.3 s; the kernel then stops its work and
+ * releases its tensor memory instead of hanging), since the last call, on the
+ * current device; synchronises the device and clears the count. */
+mpx_status mpx_tc_status(unsigned int* timeouts);
 /* Uniform field over the whole world, T (physics/mumaxworld.hpp biasMagneticField). */
 mpx_status mpx_engine_set_world_bias(mpx_engine* e, const double b[3]);
 /* Device bytes currently held by the engine (buffers, spectra, kernels). */
@@ -218,7 +233,9 @@ mpx_status mpx_group_info_get(mpx_engine* e, int group, mpx_group_info* out);
  * magnet of the group (in the order added) its state m and k0, 3 * ncells floats
  * each, copied without normalisation.  Loading a snapshot into a group of
  * magnets of the same sizes continues exactly as the saved run would have.
- * mpx_group_state_bytes gives the size of the host buffer. */
+ * A group that is running (started by mpx_group_start and not yet finished)
+ * is refused with MPX_ERR_INVALID; loading clears the final-step state of an
+ * earlier run.  mpx_group_state_bytes gives the size of the host buffer. */
 mpx_status mpx_group_state_bytes(mpx_engine* e, int group, int64_t* bytes);
 mpx_status mpx_group_save(mpx_engine* e, int group, void* buf, int64_t bytes);
 mpx_status mpx_group_load(mpx_engine* e, int group, const void* buf, int64_t bytes);
@@ -282,6 +299,22 @@ mpx_status mpx_autotune(mpx_engine* e, int method, int* div_x, int* div_yz);
  * (physics/strayfieldkernel.cu:80-99; bindings/wrap_magnet.cpp:56-59).
  * dims receives the kernel grid size (Kx, Ky, Kz). Pass out=NULL to query dims. */
 mpx_status mpx_demag_kernel(mpx_engine* e, int magnet, float* out, int dims[3]);
+/* Stray field (T) of magnet `src`'s current state on a destination grid:
+ * StrayField(magnet, grid).eval() (physics/strayfield.cpp:45-82,
+ * bindings/wrap_strayfield.cpp:12-24) when dst_magnet < 0 -- the grid of
+ * `size` cells at `origin` (cell units, the source's cell size), every cell --
+ * or Magnet.stray_field_from_magnet(source).eval() (bindings/wrap_magnet.cpp:
+ * 45-52) when dst_magnet >= 0 -- that magnet's grid, zero outside its
+ * geometry; both magnets must belong to one group (world), else
+ * MPX_ERR_RUNTIME.  method MPX_STRAY_FFT (the reference's default: FFT
+ * convolution through a helper grid spanning source and destination) or
+ * MPX_STRAY_BRUTE (direct sum over the source cells,
+ * physics/strayfieldbrute.cu:15-57); both include the world's periodic images
+ * (the source's mastergrid and repetitions).  out: 3 x ncells floats (SoA),
+ * host memory unless on_device. */
+enum { MPX_STRAY_FFT = 0, MPX_STRAY_BRUTE = 1 };
+mpx_status mpx_stray_field(mpx_engine* e, int src, int dst_magnet, const int size[3], const int origin[3], int method,
+                           float* out, int on_device);
 
 /* ---- time solver of a group (core/timesolver.cpp) ----------------------- */
 mpx_status mpx_solver_set_params(mpx_engine* e, int group, const mpx_solver_params* p);
@@ -348,9 +381,12 @@ mpx_status mpx_poll(mpx_engine* e, int* done, int cap, int* n_done, int* n_runni
  * every GPU loading the library holds until exit.  ncells must be in
  * [1, 715827882] and ncomp in [1, 3]; larger sizes are rejected with
  * MPX_ERR_INVALID.  The first call on a device looks up the array's device
- * address (set-up); make that first call before any stream capture.  All calls
- * share the array: calls that overlap on the GPU race.  Blocks until `out` is
- * written; `stream` NULL = the legacy default stream. */
+ * address (set-up); make that first call before any stream capture.  The
+ * address stays cached for the life of the process: do not use the library
+ * across a cudaDeviceReset of that device.  All calls share the array: calls
+ * that overlap on the GPU race.  A CUDA error already pending on the calling
+ * thread is returned as MPX_ERR_CUDA and left pending (not cleared).  Blocks
+ * until `out` is written; `stream` NULL = the legacy default stream. */
 mpx_status mpx_reduce_noalloc(const float* field, int ncells, int ncomp, const unsigned char* geometry, int op,
                               void* stream, double out[3]);
 
@@ -362,9 +398,11 @@ mpx_status mpx_reduce_noalloc(const float* field, int ncells, int ncomp, const u
  * first one recorded, without trapping.  Synchronises the current device,
  * writes the record to *first_bad (0 = none; else bit 63 set, N in bits
  * 32..62, i in bits 0..31) and clears it.  The four-cell vector accesses of
- * the forward x pass and the spectrum stores / gathers of the x passes are
- * checked the same way; the y/z pass is not.  In libmpx.so the checks are
- * compiled out and this returns MPX_ERR_UNSUPPORTED. */
+ * the forward x pass, the spectrum stores / gathers of the x passes, and in
+ * the y/z passes the spectrum column gathers and scatters, the kernel-spectrum
+ * reads and the split path's y-transformed spectrum (FFT and tensor-core
+ * forms) are checked the same way.  In libmpx.so the checks are compiled out
+ * and this returns MPX_ERR_UNSUPPORTED. */
 mpx_status mpx_bounds_check(unsigned long long* first_bad);
 
 #ifdef __cplusplus

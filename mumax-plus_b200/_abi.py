@@ -23,6 +23,11 @@ MPX_ERR_TIMEOUT = 7
 MPX_ERR_NODEVICE = 8
 
 # quantities
+MPX_STRAY_FFT = 0
+MPX_STRAY_BRUTE = 1
+MPX_DFT_FP32 = 0
+MPX_DFT_TF32X3 = 1
+
 Q_MAGNETIZATION = 0
 Q_EFFECTIVE_FIELD = 1
 Q_EXCHANGE_FIELD = 2
@@ -152,6 +157,8 @@ SIGNATURES = {
     "mpx_engine_destroy": (I, [E]),
     "mpx_engine_set_stream": (I, [E, C.c_void_p]),
     "mpx_engine_synchronize": (I, [E]),
+    "mpx_engine_set_dft": (I, [E, I]),
+    "mpx_tc_status": (I, [C.POINTER(C.c_uint)]),
     "mpx_engine_set_world_bias": (I, [E, P_D]),
     "mpx_engine_memory": (I, [E, P_I64]),
     "mpx_engine_launch_count": (I, [E, P_I64]),
@@ -174,6 +181,7 @@ SIGNATURES = {
     "mpx_max_norm": (I, [E, I, I, P_D]),
     "mpx_energy": (I, [E, I, I, P_D]),
     "mpx_demag_kernel": (I, [E, I, C.c_void_p, P_I]),
+    "mpx_stray_field": (I, [E, I, I, P_I, P_I, I, C.c_void_p, I]),
     "mpx_profile_eval": (I, [E, I, I, P_D]),
     "mpx_profile_attempt": (I, [E, I, I, P_D]),
     "mpx_autotune": (I, [E, I, P_I, P_I]),

@@ -76,6 +76,17 @@ class Engine:
     def synchronize(self):
         check(lib().mpx_engine_synchronize(self._h))
 
+    def set_dft(self, mode):
+        """_abi.MPX_DFT_FP32 or _abi.MPX_DFT_TF32X3 (before the first magnet)."""
+        check(lib().mpx_engine_set_dft(self._h, int(mode)))
+
+    @staticmethod
+    def tc_timeouts():
+        """Tensor-core waits that gave up since the last call (device synchronised, count cleared)."""
+        n = C.c_uint(0)
+        check(lib().mpx_tc_status(C.byref(n)))
+        return n.value
+
     def set_world_bias(self, b):
         arr = (C.c_double * 3)(*[float(v) for v in b])
         check(lib().mpx_engine_set_world_bias(self._h, arr))

@@ -24,6 +24,7 @@
 #include "newell.cuh"
 #include "stray.cuh"
 #include "yzsplit.cuh"
+#include "dft_tc.cuh"
 
 using namespace mpx;
 
@@ -162,6 +163,9 @@ struct Magnet {
   int64_t tspec_bytes = 0;
   std::vector<Work> ycw, zmw;            // k_ycols / k_zmul work items
   Work *d_ycw = nullptr, *d_zmw = nullptr;
+  bool tc = false;                       // split path with the tensor-core y transforms (k_ydft_tc)
+  std::vector<Work> tcw;                 // k_ydft_tc work items (tiles of 4 / R columns)
+  Work* d_tcw = nullptr;
   int P[3] = {1, 1, 1};
   // kernel-defining geometry (rebuild the spectrum when it changes)
   int kkey_n[3], kkey_mg[3], kkey_pbc[3];
@@ -221,6 +225,13 @@ struct mpx_engine {
   // split y/z path over all split magnets
   Work *d_t_ycols = nullptr, *d_t_zmul = nullptr;
   int n_t_ycols = 0, n_t_zmul = 0, smem_ycols = 0, smem_zmul = 0, maxpy_split = 0, maxpz_split = 0;
+  Work* d_t_tc = nullptr;  // k_ydft_tc items over all started tensor-core magnets
+  int n_t_tc = 0;
+  // y transforms of the demag convolution: MPX_DFT_FP32 (shared-memory FFT) or
+  // MPX_DFT_TF32X3 (tcgen05 GEMMs, for y lengths 1024 and 2048); the DFT32
+  // matrix (hi, lo) of the tensor-core form
+  int dft_mode = MPX_DFT_FP32;
+  float* d_dftB = nullptr;
   int smem_x = 0, nt_x = 256;
   bool any_nodemag = false;
   int64_t bytes = 0;
@@ -316,7 +327,9 @@ void release_all(mpx_engine* e, Magnet* m) {
   m->tspec_bytes = 0;
   pfree(e, m->d_ycw);
   pfree(e, m->d_zmw);
+  pfree(e, m->d_tcw);
   m->d_ycw = m->d_zmw = nullptr;
+  m->d_tcw = nullptr;
   pfree(e, m->fields);
   pfree(e, m->spec);
   pfree(e, m->kspec);
@@ -459,24 +472,49 @@ int choose_nkx(int nz, int Py, int Pz, int Fh) {
 int ycols_smem(const Magnet* m) { return (m->ncy * plen(m->P[1]) + m->P[1]) * (int)sizeof(float2); }
 int zmul_smem(const Magnet* m) { return (3 * m->nkz * plen(m->P[2]) + m->P[2]) * (int)sizeof(float2); }
 
-// The three passes of the split y/z path (radix-8 forms when the lengths allow).
+// The three passes of the split y/z path (radix-8 forms when the lengths allow);
+// magnets with the tensor-core y transforms take k_ydft_tc (work list tcw)
+// instead of k_ycols.
+constexpr int TC_GRID_PER_SM = 1;
 mpx_status launch_split(mpx_engine* e, const Work* ycw, int nyc, const Work* zmw, int nzm, int smem_y, int smem_z,
-                        int max_py, int max_pz, int stage, int gate) {
-  if (nyc <= 0) return MPX_OK;
+                        int max_py, int max_pz, int stage, int gate, const Work* tcw = nullptr, int ntc = 0) {
+  if (nyc <= 0 && ntc <= 0) return MPX_OK;
   const bool ry = max_py <= 2048, rz = max_pz <= 2048;
-  if (ry)
-    k_ycols<-1, 3><<<nyc, YZ_THREADS, smem_y, e->stream>>>(e->d_mags, e->d_groups, ycw, stage, gate, e->d_tw);
-  else
-    k_ycols<-1, 4><<<nyc, YZ_THREADS, smem_y, e->stream>>>(e->d_mags, e->d_groups, ycw, stage, gate, e->d_tw);
+  static int n_sm = 0;
+  if (!n_sm) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev);
+    if (n_sm <= 0) n_sm = 148;
+  }
+  const int gtc = std::min(ntc, TC_GRID_PER_SM * n_sm);
+  if (ntc > 0) {
+    k_ydft_tc<-1><<<gtc, 128, TC_SMEM, e->stream>>>(e->d_mags, e->d_groups, tcw, ntc, stage, gate, e->d_dftB);
+    e->launches++;
+  }
+  if (nyc > 0) {
+    if (ry)
+      k_ycols<-1, 3><<<nyc, YZ_THREADS, smem_y, e->stream>>>(e->d_mags, e->d_groups, ycw, stage, gate, e->d_tw);
+    else
+      k_ycols<-1, 4><<<nyc, YZ_THREADS, smem_y, e->stream>>>(e->d_mags, e->d_groups, ycw, stage, gate, e->d_tw);
+    e->launches++;
+  }
   if (rz)
     k_zmul<3><<<nzm, YZ_THREADS, smem_z, e->stream>>>(e->d_mags, e->d_groups, zmw, stage, gate, e->d_tw);
   else
     k_zmul<4><<<nzm, YZ_THREADS, smem_z, e->stream>>>(e->d_mags, e->d_groups, zmw, stage, gate, e->d_tw);
-  if (ry)
-    k_ycols<1, 3><<<nyc, YZ_THREADS, smem_y, e->stream>>>(e->d_mags, e->d_groups, ycw, stage, gate, e->d_tw);
-  else
-    k_ycols<1, 4><<<nyc, YZ_THREADS, smem_y, e->stream>>>(e->d_mags, e->d_groups, ycw, stage, gate, e->d_tw);
-  e->launches += 3;
+  e->launches++;
+  if (nyc > 0) {
+    if (ry)
+      k_ycols<1, 3><<<nyc, YZ_THREADS, smem_y, e->stream>>>(e->d_mags, e->d_groups, ycw, stage, gate, e->d_tw);
+    else
+      k_ycols<1, 4><<<nyc, YZ_THREADS, smem_y, e->stream>>>(e->d_mags, e->d_groups, ycw, stage, gate, e->d_tw);
+    e->launches++;
+  }
+  if (ntc > 0) {
+    k_ydft_tc<1><<<gtc, 128, TC_SMEM, e->stream>>>(e->d_mags, e->d_groups, tcw, ntc, stage, gate, e->d_dftB);
+    e->launches++;
+  }
   return MPX_OK;
 }
 
@@ -629,7 +667,7 @@ mpx_status rebuild_tables(mpx_engine* e) {
     for (size_t i = 0; i < act.size(); ++i)
       if (ty[i] != act[i]->ty || nkx[i] != act[i]->nkx) MPX_TRY(retile(e, act[i], ty[i], nkx[i]));
   }
-  std::vector<Work> td, tl, kd[YZ_CLASSES], yc, zm;
+  std::vector<Work> td, tl, kd[YZ_CLASSES], yc, zm, tcl;
   e->smem_ycols = e->smem_zmul = e->maxpy_split = e->maxpz_split = 0;
   e->smem_x = 0;
   e->nt_x = 256;
@@ -645,6 +683,7 @@ mpx_status rebuild_tables(mpx_engine* e) {
       e->smem_x = std::max(e->smem_x, x_smem(m));
       if (m->split) {
         yc.insert(yc.end(), m->ycw.begin(), m->ycw.end());
+        tcl.insert(tcl.end(), m->tcw.begin(), m->tcw.end());
         zm.insert(zm.end(), m->zmw.begin(), m->zmw.end());
         e->smem_ycols = std::max(e->smem_ycols, ycols_smem(m));
         e->smem_zmul = std::max(e->smem_zmul, zmul_smem(m));
@@ -691,6 +730,7 @@ mpx_status rebuild_tables(mpx_engine* e) {
   put(tl);
   put(yc);
   put(zm);
+  put(tcl);
   for (int c = 0; c < YZ_CLASSES; ++c) {
     put(kd[c]);
     sig.push_back(e->smem_yz[c]);
@@ -704,6 +744,8 @@ mpx_status rebuild_tables(mpx_engine* e) {
   MPX_TRY(upload_vec(e, &e->d_t_local, tl));
   MPX_TRY(upload_vec(e, &e->d_t_ycols, yc));
   MPX_TRY(upload_vec(e, &e->d_t_zmul, zm));
+  MPX_TRY(upload_vec(e, &e->d_t_tc, tcl));
+  e->n_t_tc = (int)tcl.size();
   e->n_t_ycols = (int)yc.size();
   e->n_t_zmul = (int)zm.size();
   for (int c = 0; c < YZ_CLASSES; ++c) {
@@ -732,7 +774,13 @@ constexpr long long STRAY_FFT_MIN_INTERACTIONS = 1LL << 22;
 
 // Helper magnet of an FFT pair: the bounding box of A and B in world cells,
 // msat 1, demag only, no periodic images; its magnetisation buffer starts at zero.
-mpx_status create_hull(mpx_engine* e, const Magnet* A, const Magnet* B, int* out) {
+// A helper magnet spanning the bounding box of A and B (msat 1, demag only).
+// With `periodic` its demag kernel carries the periodic images of A's world
+// (image period = the world's mastergrid size, A's repetitions): the Newell
+// tensor summed over the images depends on the displacement only, so the
+// helper may be larger than the mastergrid (its exchange, which would wrap, is
+// zero).
+mpx_status create_hull(mpx_engine* e, const Magnet* A, const Magnet* B, int* out, bool periodic = false) {
   mpx_magnet_desc d;
   std::memset(&d, 0, sizeof d);
   for (int ax = 0; ax < 3; ++ax) {
@@ -741,6 +789,11 @@ mpx_status create_hull(mpx_engine* e, const Magnet* A, const Magnet* B, int* out
     d.size[ax] = hi - lo;
     d.origin[ax] = lo;
     d.cellsize[ax] = A->cs_d[ax];
+    if (periodic && A->dev.mg[ax] > 0) {
+      d.mastergrid_size[ax] = A->dev.mg[ax];
+      d.mastergrid_origin[ax] = lo;
+      d.pbc_repetitions[ax] = A->pbc_rep[ax];
+    }
   }
   d.msat.uniform = 1.0;
   d.scale_exchange = 1.0;
@@ -1211,8 +1264,10 @@ mpx_status setup_magnet(mpx_engine* e, Magnet* m, const mpx_magnet_desc* d, bool
     if (m->P[0] > X_VPT * X_THREADS_MAX || m->P[1] > std::min(MAX_FFT, YZ_VPT * YZ_THREADS))
       return fail(MPX_ERR_UNSUPPORTED, "demag: padded FFT length above 2048 along x or 4096 along y "
                                        "(grid side above 1024 along x or 2048 along y)");
-    // thick magnets (nz > 8) and long y transforms of many columns take the split y/z path
-    m->split = m->P[2] > 16 || yz_smem(m) > SMEM_DYN_MAX;
+    // thick magnets (nz > 8) and long y transforms of many columns take the split y/z path;
+    // so do y lengths 1024 and 2048 when the engine runs the tensor-core y transforms
+    m->tc = e->dft_mode == MPX_DFT_TF32X3 && (m->P[1] == 1024 || m->P[1] == 2048) && !m->hull;
+    m->split = m->tc || m->P[2] > 16 || yz_smem(m) > SMEM_DYN_MAX;
     if (m->split) {
       if (m->P[2] > MAX_FFT) return fail(MPX_ERR_UNSUPPORTED, "demag: padded FFT length above 4096 along z");
       m->ncy = std::max(1, std::min(D.Fh * 3 * D.n[2], (YZ_VPT * YZ_THREADS) / m->P[1]));
@@ -1272,15 +1327,22 @@ mpx_status setup_magnet(mpx_engine* e, Magnet* m, const mpx_magnet_desc* d, bool
   MPX_TRY(retile(e, m, m->ty, m->nkx));
   m->ycw.clear();
   m->zmw.clear();
+  m->tcw.clear();
   if (m->demag && m->split) {
     const int ncols = D.Fh * 3 * D.n[2];
-    for (int c0 = 0; c0 < ncols; c0 += m->ncy) m->ycw.push_back(Work{m->slot, c0, std::min(m->ncy, ncols - c0), 0});
+    if (m->tc) {
+      const int cpt = 4096 / m->P[1];  // columns per 128-sequence tile: 4 at Py = 1024, 2 at 2048
+      for (int c0 = 0; c0 < ncols; c0 += cpt) m->tcw.push_back(Work{m->slot, c0, std::min(cpt, ncols - c0), 0});
+    } else {
+      for (int c0 = 0; c0 < ncols; c0 += m->ncy) m->ycw.push_back(Work{m->slot, c0, std::min(m->ncy, ncols - c0), 0});
+    }
     for (int kx = 0; kx < D.Fh; ++kx)
       for (int ky0 = 0; ky0 < m->P[1]; ky0 += m->nkz)
         m->zmw.push_back(Work{m->slot, kx, ky0, std::min(m->nkz, m->P[1] - ky0)});
   }
   MPX_TRY(upload_vec(e, &m->d_ycw, m->ycw));
   MPX_TRY(upload_vec(e, &m->d_zmw, m->zmw));
+  MPX_TRY(upload_vec(e, &m->d_tcw, m->tcw));
   MPX_TRY(upload_magnet_desc(e, m));
   e->tables_dirty = true;
   return MPX_OK;
@@ -1335,7 +1397,8 @@ mpx_status eval_into(mpx_engine* e, Magnet* m, int q, float* out) {
     k_xfwd<false><<<ntile, nt, sx, e->stream>>>(e->d_mags, e->d_groups, m->d_tiles, 0, 0, nullptr, e->d_tw);
     if (m->split)
       MPX_TRY(launch_split(e, m->d_ycw, (int)m->ycw.size(), m->d_zmw, (int)m->zmw.size(), ycols_smem(m),
-                           zmul_smem(m), m->P[1], m->P[2], 0, 0));
+                           zmul_smem(m), m->P[1], m->P[2], 0, 0, m->d_tcw,
+                           (int)m->tcw.size()));
     else
       MPX_TRY(launch_yz(e, yz_class(m), m->d_kxw, (int)m->kxw.size(), syz, 0, 0));
     CUDA_TRY(launch_pdl(k_xinv, ntile, nt, sx, e->stream, e->d_mags, e->d_groups, m->d_tiles, ea, e->d_tw));
@@ -1382,7 +1445,7 @@ mpx_status launch_attempt(mpx_engine* e, const TableauDev& T, int first_stage) {
       for (int c = 0; c < YZ_CLASSES; ++c)
         MPX_TRY(launch_yz(e, c, e->d_kx_demag[c], e->n_kx_demag[c], e->smem_yz[c], s, 1));
       MPX_TRY(launch_split(e, e->d_t_ycols, e->n_t_ycols, e->d_t_zmul, e->n_t_zmul, e->smem_ycols, e->smem_zmul,
-                           e->maxpy_split, e->maxpz_split, s, 1));
+                           e->maxpy_split, e->maxpz_split, s, 1, e->d_t_tc, e->n_t_tc));
       CUDA_TRY(launch_pdl(k_xinv, e->n_t_demag, e->nt_x, e->smem_x, e->stream, e->d_mags, e->d_groups, e->d_t_demag, ea,
                           e->d_tw));
       e->launches++;
@@ -1634,6 +1697,39 @@ mpx_status mpx_engine_create(int device, mpx_engine** out) {
                                (const void*)k_yzw<8>, (const void*)k_yzw<16>, (const void*)k_yzw32<1>,
                                (const void*)k_yzw32<2>, (const void*)k_yzw32<4>, (const void*)k_yzw32<8>,
                                (const void*)k_yzw32<16>};
+  // the DFT32 matrix of the tensor-core y transforms in its real 64 x 64 form
+  // B[2 k + r][2 n + s] (output k, part r; input n, part s; forward, angle
+  // 2 pi k n / 32): re <- cos re + sin im, im <- -sin re + cos im; split into
+  // TF32 hi and lo (round to nearest, ties away, as cvt.rna.tf32.f32)
+  {
+    auto tf32 = [](double v) {
+      float f = (float)v;
+      uint32_t u;
+      std::memcpy(&u, &f, 4);
+      u = (u + 0x1000u) & 0xFFFFE000u;
+      std::memcpy(&f, &u, 4);
+      return f;
+    };
+    std::vector<float> B(2 * 64 * 64);
+    for (int k = 0; k < 32; ++k)
+      for (int n = 0; n < 32; ++n) {
+        const double a = 2.0 * M_PI * ((k * n) % 32) / 32.0, c = std::cos(a), sn = std::sin(a);
+        const double v[2][2] = {{c, sn}, {-sn, c}};
+        for (int r = 0; r < 2; ++r)
+          for (int q = 0; q < 2; ++q) {
+            const int i = (2 * k + r) * 64 + 2 * n + q;
+            const float hi = tf32(v[r][q]);
+            B[i] = hi;
+            B[4096 + i] = tf32(v[r][q] - (double)hi);
+          }
+      }
+    CUDA_TRY(cudaMalloc(&e->d_dftB, sizeof(float) * B.size()));
+    CUDA_TRY(cudaMemcpy(e->d_dftB, B.data(), sizeof(float) * B.size(), cudaMemcpyHostToDevice));
+  }
+  {
+    const void* tck[] = {(const void*)k_ydft_tc<-1>, (const void*)k_ydft_tc<1>};
+    for (const void* k : tck) CUDA_TRY(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, TC_SMEM));
+  }
   for (const void* k : fft_kernels) {
     cudaFuncAttributes fa;
     CUDA_TRY(cudaFuncGetAttributes(&fa, k));
@@ -1656,6 +1752,7 @@ mpx_status mpx_engine_destroy(mpx_engine* e) {
   cudaFree(e->d_mags);
   cudaFree(e->d_groups);
   cudaFree(e->d_tw);
+  cudaFree(e->d_dftB);
   cudaFree(e->d_red);
   cudaFree(e->d_redout);
   pfree(e, e->d_scratch);
@@ -1675,6 +1772,24 @@ mpx_status mpx_engine_set_stream(mpx_engine* e, void* stream) {
   // pool allocations and frees are ordered on the old stream: let them finish
   CUDA_TRY(cudaStreamSynchronize(e->stream));
   e->stream = stream ? (cudaStream_t)stream : e->own;
+  return MPX_OK;
+}
+
+mpx_status mpx_engine_set_dft(mpx_engine* e, int mode) {
+  if (!e) return fail(MPX_ERR_INVALID, "null engine");
+  if (mode != MPX_DFT_FP32 && mode != MPX_DFT_TF32X3) return fail(MPX_ERR_INVALID, "unknown DFT mode");
+  for (auto& m : e->mags)
+    if (m && !m->hull) return fail(MPX_ERR_INVALID, "set the DFT mode before adding magnets");
+  e->dft_mode = mode;
+  return MPX_OK;
+}
+
+mpx_status mpx_tc_status(unsigned int* timeouts) {
+  if (!timeouts) return fail(MPX_ERR_INVALID, "null output");
+  CUDA_TRY(cudaDeviceSynchronize());
+  CUDA_TRY(cudaMemcpyFromSymbol(timeouts, g_tc_timeouts, sizeof(unsigned int)));
+  const unsigned int zero = 0;
+  CUDA_TRY(cudaMemcpyToSymbol(g_tc_timeouts, &zero, sizeof zero));
   return MPX_OK;
 }
 
@@ -1837,6 +1952,10 @@ mpx_status mpx_group_load(mpx_engine* e, int group, const void* buf, int64_t byt
   DeviceGuard guard(e->device);
   GroupDev G;
   MPX_TRY(read_group(e, g->slot, &G));
+  // a run in progress keeps controller state (the final-step phase, the time
+  // step saved before it) that belongs to its own time line: loading another
+  // time into it would mix the two
+  if (G.status == GS_RUNNING) return fail(MPX_ERR_INVALID, "mpx_group_load: the group is running");
   for (int id : g->magnets) {
     Magnet* m = get_mag(e, id);
     const size_t b = sizeof(float) * 3 * (size_t)m->dev.N;
@@ -1848,6 +1967,8 @@ mpx_status mpx_group_load(mpx_engine* e, int group, const void* buf, int64_t byt
   G.dt = h.dt;
   G.steps = h.steps;
   G.k0_valid = h.k0_valid;
+  G.phase = 0;  // controller state of an earlier, finished run does not carry over
+  G.dt_saved = 0.0;
   MPX_TRY(write_group(e, g->slot, &G));
   CUDA_TRY(cudaStreamSynchronize(e->stream));
   return MPX_OK;
@@ -2100,6 +2221,151 @@ mpx_status mpx_energy(mpx_engine* e, int magnet, int quantity, double* out) {
   return MPX_OK;
 }
 
+// StrayField(magnet, grid).eval() (physics/strayfield.cpp:45-82) and
+// Magnet.stray_field_from_magnet(source).eval() (bindings/wrap_magnet.cpp:45-52):
+// the field of `src`'s current state on a destination grid, by direct sum over
+// the source cells (METHOD_BRUTE, physics/strayfieldbrute.cu:15-57: the FP64
+// Newell tensor of the displacements with the world's periodic images,
+// tabulated in FP32) or by FFT convolution (METHOD_FFT, the default of the
+// reference, physics/strayfieldfft.cu): the demag passes of a helper magnet
+// spanning both grids, holding Ms m of the source and zero elsewhere.
+mpx_status mpx_stray_field(mpx_engine* e, int src, int dst_magnet, const int size[3], const int origin[3], int method,
+                           float* out, int on_device) {
+  if (!e || !out) return fail(MPX_ERR_INVALID, "null engine / output");
+  if (method != MPX_STRAY_FFT && method != MPX_STRAY_BRUTE)
+    return fail(MPX_ERR_INVALID, "Method should be \"fft\" or \"brute\"");
+  Magnet* A = get_mag(e, src);
+  if (!A || A->hull) return fail(MPX_ERR_RANGE, "no such source magnet");
+  DeviceGuard guard(e->device);
+  int dst = dst_magnet, tmp = -1;
+  if (dst_magnet >= 0) {
+    Magnet* B0 = get_mag(e, dst_magnet);
+    if (!B0 || B0->hull) return fail(MPX_ERR_RANGE, "no such destination magnet");
+    if (B0->group != A->group) return fail(MPX_ERR_RUNTIME, "Can not compute the magnetic field of the magnet");
+  } else {
+    if (!size || !origin) return fail(MPX_ERR_INVALID, "null grid");
+    mpx_magnet_desc d;
+    std::memset(&d, 0, sizeof d);
+    for (int a = 0; a < 3; ++a) {
+      if (size[a] <= 0) return fail(MPX_ERR_INVALID, "grid size must be positive");
+      d.size[a] = size[a];
+      d.origin[a] = origin[a];
+      d.cellsize[a] = A->cs_d[a];
+    }
+    if ((long long)size[0] * size[1] * size[2] >= (1LL << 31) / 3)
+      return fail(MPX_ERR_UNSUPPORTED, "grid too large for 32-bit cell indices");
+    d.msat.uniform = 1.0;
+    d.scale_exchange = 1.0;
+    d.stray_source_off = d.stray_destination_off = 1;
+    for (int i = 0; i < (int)e->mags.size(); ++i)
+      if (!e->mags[i]) { tmp = i; break; }
+    if (tmp < 0) {
+      tmp = (int)e->mags.size();
+      e->mags.emplace_back();
+    }
+    auto m = std::make_unique<Magnet>();
+    std::memset(&m->dev, 0, sizeof(MagnetDev));
+    m->slot = tmp;
+    m->group = A->group;
+    m->hull = true;  // a probe of the destination grid: in no group's tables
+    const mpx_status st = setup_magnet(e, m.get(), &d, false);
+    if (st != MPX_OK) {
+      std::string msg = g_last_error;
+      release_all(e, m.get());
+      g_last_error = msg;
+      return st;
+    }
+    e->mags[tmp] = std::move(m);
+    dst = tmp;
+  }
+  Magnet* B = get_mag(e, dst);
+  const int NB = B->dev.N;
+  float* dout = out;
+  mpx_status st = MPX_OK;
+  auto cleanup = [&]() {
+    if (dout != out) pfree(e, dout);
+    if (tmp >= 0) {
+      release_all(e, e->mags[tmp].get());
+      e->mags[tmp].reset();
+    }
+  };
+  if (!on_device && (st = palloc(e, (void**)&dout, sizeof(float) * 3 * (size_t)NB)) != MPX_OK) {
+    dout = out;
+    cleanup();
+    return st;
+  }
+  if (A->msat_zero) {  // physics/strayfield.cpp:77-80: assuredly zero
+    const cudaError_t ce = cudaMemsetAsync(dout, 0, sizeof(float) * 3 * (size_t)NB, e->stream);
+    if (ce != cudaSuccess) st = fail(MPX_ERR_CUDA, cudaGetErrorString(ce));
+  } else if (method == MPX_STRAY_BRUTE) {
+    StrayTable tab;
+    KernelGeom g;
+    for (int ax = 0; ax < 3; ++ax) {
+      tab.K[ax] = A->dev.n[ax] + B->dev.n[ax] - 1;
+      tab.O[ax] = B->dev.o[ax] - A->dev.o[ax] - (A->dev.n[ax] - 1);
+      g.n[ax] = B->dev.n[ax];
+      g.mg[ax] = A->dev.mg[ax];
+      g.pbc[ax] = A->pbc_rep[ax];
+      g.cs[ax] = A->cs_d[ax];
+    }
+    const size_t KK = (size_t)tab.K[0] * tab.K[1] * tab.K[2];
+    float* k = nullptr;
+    st = palloc(e, (void**)&k, sizeof(float) * 6 * KK);
+    if (st == MPX_OK) {
+      k_newell_reflayout<<<148 * 8, 128, 0, e->stream>>>(k, g, tab.K[0], tab.K[1], tab.K[2], tab.O[0], tab.O[1],
+                                                         tab.O[2]);
+      tab.k = k;
+      k_stray_pair<<<(NB + 255) / 256, 256, 0, e->stream>>>(e->d_mags, e->d_groups, src, dst, tab, 0, 0, 0, dout);
+      e->launches += 2;
+      pfree(e, k);
+    }
+  } else {
+    bool periodic = false;
+    for (int ax = 0; ax < 3; ++ax) periodic = periodic || A->dev.mg[ax] > 0;
+    int hull = -1;
+    st = create_hull(e, A, B, &hull, periodic);
+    if (st == MPX_OK) {
+      Magnet* H = get_mag(e, hull);
+      k_hull_scatter<<<(A->dev.N + 255) / 256, 256, 0, e->stream>>>(e->d_mags, e->d_groups, src, hull, 0, 0);
+      const int ntile = (int)H->tiles.size(), sx = x_smem(H), nt = x_threads(H);
+      k_xfwd<false><<<ntile, nt, sx, e->stream>>>(e->d_mags, e->d_groups, H->d_tiles, 0, 0, H->dev.buf[0], e->d_tw);
+      if (H->split)
+        st = launch_split(e, H->d_ycw, (int)H->ycw.size(), H->d_zmw, (int)H->zmw.size(), ycols_smem(H), zmul_smem(H),
+                          H->P[1], H->P[2], 0, 0);
+      else
+        st = launch_yz(e, yz_class(H), H->d_kxw, (int)H->kxw.size(), yz_smem(H), 0, 0);
+      if (st == MPX_OK) {
+        EpiArgs ea;
+        ea.mode = EPI_EVAL;
+        ea.stage = 0;
+        ea.quantity = MPX_Q_DEMAG_FIELD;
+        ea.fsal_err = 0;
+        ea.gate = 0;
+        ea.out = H->dev.buf[1];
+        ea.msrc = H->dev.buf[0];
+        const cudaError_t ce =
+            launch_pdl(k_xinv, ntile, nt, sx, e->stream, e->d_mags, e->d_groups, H->d_tiles, ea, e->d_tw);
+        if (ce != cudaSuccess) st = fail(MPX_ERR_CUDA, cudaGetErrorString(ce));
+        k_hull_gather<<<(NB + 255) / 256, 256, 0, e->stream>>>(e->d_mags, e->d_groups, hull, dst, 0, 0, 0, dout);
+        e->launches += 4;
+      }
+      release_all(e, H);
+      e->mags[hull].reset();
+    }
+  }
+  if (st == MPX_OK) {
+    const cudaError_t ce = cudaGetLastError();
+    if (ce != cudaSuccess) st = fail(MPX_ERR_CUDA, std::string("stray field: ") + cudaGetErrorString(ce));
+  }
+  if (st == MPX_OK && !on_device) {
+    cudaError_t ce = cudaMemcpyAsync(out, dout, sizeof(float) * 3 * (size_t)NB, cudaMemcpyDeviceToHost, e->stream);
+    if (ce == cudaSuccess) ce = cudaStreamSynchronize(e->stream);
+    if (ce != cudaSuccess) st = fail(MPX_ERR_CUDA, cudaGetErrorString(ce));
+  }
+  cleanup();
+  return st;
+}
+
 mpx_status mpx_profile_attempt(mpx_engine* e, int method, int reps, double ms[4]) {
   if (!e || !ms || reps <= 0) return fail(MPX_ERR_INVALID, "bad arguments");
   if (method < 0 || method > MPX_RK_DORMAND_PRINCE) return fail(MPX_ERR_INVALID, "unknown method");
@@ -2131,7 +2397,7 @@ mpx_status mpx_profile_attempt(mpx_engine* e, int method, int reps, double ms[4]
       for (int c = 0; c < YZ_CLASSES; ++c)
         MPX_TRY(launch_yz(e, c, e->d_kx_demag[c], e->n_kx_demag[c], e->smem_yz[c], s, 1));
       MPX_TRY(launch_split(e, e->d_t_ycols, e->n_t_ycols, e->d_t_zmul, e->n_t_zmul, e->smem_ycols, e->smem_zmul,
-                           e->maxpy_split, e->maxpz_split, s, 1));
+                           e->maxpy_split, e->maxpz_split, s, 1, e->d_t_tc, e->n_t_tc));
     }
     CUDA_TRY(cudaEventRecord(ev[3], e->stream));
     if (e->n_t_demag > 0)
@@ -2215,7 +2481,8 @@ mpx_status mpx_profile_eval(mpx_engine* e, int magnet, int reps, double ms[4]) {
       CUDA_TRY(cudaEventRecord(ev[1], e->stream));
       if (m->split)
         MPX_TRY(launch_split(e, m->d_ycw, (int)m->ycw.size(), m->d_zmw, (int)m->zmw.size(), ycols_smem(m),
-                             zmul_smem(m), m->P[1], m->P[2], 0, 0));
+                             zmul_smem(m), m->P[1], m->P[2], 0, 0, m->d_tcw,
+                           (int)m->tcw.size()));
       else
         MPX_TRY(launch_yz(e, yz_class(m), m->d_kxw, (int)m->kxw.size(), syz, 0, 0));
       CUDA_TRY(cudaEventRecord(ev[2], e->stream));
@@ -2822,7 +3089,11 @@ constexpr long long NOALLOC_MAX_CELLS = 0x7fffffffLL / 3;  // 32-bit cell indice
 static __device__ __align__(256) double g_noalloc_scratch[NOALLOC_RESULT + 3];
 
 std::mutex g_noalloc_mutex;
-double* g_noalloc_ptr[128] = {nullptr};  // device address of the array, per device
+// Device address of the array, per device, looked up by the first call on that
+// device.  A cudaDeviceReset (or any re-creation of the device's primary
+// context) by the host application unloads the module and would leave the
+// cached address stale: the library must not be used across a device reset.
+double* g_noalloc_ptr[128] = {nullptr};
 
 }  // namespace
 
@@ -2851,6 +3122,14 @@ extern "C" mpx_status mpx_reduce_noalloc(const float* field, int ncells, int nco
     scratch = g_noalloc_ptr[dev];
   }
   cudaStream_t s = (cudaStream_t)stream;
+  // an error left pending by the caller's own earlier work is reported as it
+  // is and not cleared, so that the caller still sees it
+  {
+    const cudaError_t pending = cudaPeekAtLastError();
+    if (pending != cudaSuccess)
+      return fail(MPX_ERR_CUDA, std::string("mpx_reduce_noalloc: CUDA error pending before the call: ") +
+                                    cudaGetErrorString(pending));
+  }
   // every partial slot the final pass reads is written by this call's partial
   // pass, and the final pass overwrites the results: nothing needs clearing
   k_reduce_partial<<<NOALLOC_BLOCKS, 256, 0, s>>>(field, ncells, ncomp, geometry, op, scratch);

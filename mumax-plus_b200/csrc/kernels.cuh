@@ -376,11 +376,17 @@ __global__ void __launch_bounds__(X_THREADS_MAX, 2) k_xfwd(const MagnetDev* __re
 // --------------------------------------------------------------------- k_yz
 // Kernel spectrum entry (comp cc of the xx,yy,zz,xy,xz,yz order) at (kx, ky, kz)
 // from the symmetry-reduced storage [kx][kz'][kcomp][ky'].
+// `left`: elements of the kernel spectrum from Kx to its end (checked build).
 template <int PZ>
 __device__ __forceinline__ void kernel_at(const float* __restrict__ Kx, int kc, int hy, int kyp, float sy, int kz,
-                                          float& kxx, float& kyy, float& kzz, float& kxy, float& kxz, float& kyz) {
+                                          float& kxx, float& kyy, float& kzz, float& kxy, float& kxz, float& kyz,
+                                          size_t left) {
   const int kzp = min(kz, PZ - kz);
   const float sz = (kz > PZ / 2) ? -1.f : 1.f;
+  if (!span_ok((size_t)kzp * kc * hy + kyp + (size_t)(kc - 1) * hy, left)) {
+    kxx = kyy = kzz = kxy = kxz = kyz = 0.f;
+    return;
+  }
   const float* Kk = Kx + (size_t)kzp * kc * hy + kyp;
   kxx = __ldg(Kk);
   kyy = __ldg(Kk + hy);
@@ -421,10 +427,12 @@ __device__ __forceinline__ void zstage_pair(float2* D, int cs, const MagnetDev& 
   const float sy = (ky > Py / 2) ? -1.f : 1.f;
   const int kc = M.kcomp;
   const float* __restrict__ Kx = M.kspec + (size_t)kx * (PZ / 2 + 1) * kc * hy;
+  const size_t kleft = (size_t)(M.Fh - kx) * (PZ / 2 + 1) * kc * hy;
   float kk[H][6];
 #pragma unroll
   for (int q = 0; q < H; ++q)
-    kernel_at<PZ>(Kx, kc, hy, kyp, sy, 2 * q + half, kk[q][0], kk[q][1], kk[q][2], kk[q][3], kk[q][4], kk[q][5]);
+    kernel_at<PZ>(Kx, kc, hy, kyp, sy, 2 * q + half, kk[q][0], kk[q][1], kk[q][2], kk[q][3], kk[q][4], kk[q][5],
+                  kleft);
 #pragma unroll
   for (int c = 0; c < 3; ++c)
 #pragma unroll
@@ -499,7 +507,7 @@ __device__ __forceinline__ void zstage_single(float2* D, int cs, const MagnetDev
   const int kc = M.kcomp;
   const float* __restrict__ Kx = M.kspec + (size_t)kx * kc * hy;
   float kxx, kyy, kzz, kxy, kxz, kyz;
-  kernel_at<1>(Kx, kc, hy, kyp, sy, 0, kxx, kyy, kzz, kxy, kxz, kyz);
+  kernel_at<1>(Kx, kc, hy, kyp, sy, 0, kxx, kyy, kzz, kxy, kxz, kyz, (size_t)(M.Fh - kx) * kc * hy);
   apply3(&v0, &v1, &v2, kxx, kyy, kzz, kxy, kxz, kyz);
   D[pky] = v0;
   D[cs + pky] = v1;
@@ -526,6 +534,7 @@ __global__ void __launch_bounds__(384, MAXLR == 3 ? 2 : 1)
   const int ny = M.n[1], nz = M.n[2];
   const int logPy = M.logP[1], Py = 1 << logPy, cs = plen(Py);
   float2* S = M.spec + (size_t)kx0 * 3 * nz * ny;  // the nkx slabs are consecutive
+  const size_t sleft = (size_t)(M.Fh - kx0) * 3 * nz * ny;  // elements of the spectrum from S on (checked build)
   float2* D = sm;  // [nkx][3*nz] padded columns of length Py
   const int ncol = nkx * 3 * nz;
   float2* tws = sm + ncol * cs;  // twiddles of length Py
@@ -542,7 +551,8 @@ __global__ void __launch_bounds__(384, MAXLR == 3 ? 2 : 1)
     for (int u = 0; u < 8; ++u) {
       const int e = e0 + u * blockDim.x;
       const int col = e >> logPyh, y = e & ((1 << logPyh) - 1);
-      r[u] = (e < total && y < ny) ? __ldg(S + col * ny + y) : make_float2(0.f, 0.f);
+      r[u] = (e < total && y < ny && span_ok((size_t)col * ny + y, sleft)) ? __ldg(S + col * ny + y)
+                                                                           : make_float2(0.f, 0.f);
     }
 #pragma unroll
     for (int u = 0; u < 8; ++u) {
@@ -568,7 +578,7 @@ __global__ void __launch_bounds__(384, MAXLR == 3 ? 2 : 1)
   fft_many<1, MAXLR, 2>(D, logPy, ncol, cs, tws);  // only y < ny <= Py/2 is written back
   for (int e = threadIdx.x; e < (ncol << logPy); e += blockDim.x) {
     const int col = e >> logPy, y = e & (Py - 1);
-    if (y < ny) S[col * ny + y] = D[col * cs + pidx(y)];
+    if (y < ny && span_ok((size_t)col * ny + y, sleft)) S[col * ny + y] = D[col * cs + pidx(y)];
   }
 }
 
@@ -583,7 +593,7 @@ __global__ void __launch_bounds__(384, MAXLR == 3 ? 2 : 1)
 // above) into D.
 template <int Q>
 __device__ __forceinline__ void yzw_forward(const float2* __restrict__ S, int ny, float2* D, int ncol,
-                                            const float2* twq) {
+                                            const float2* twq, size_t sleft) {
   constexpr int W = 32 / Q, cs = qlen(32 * Q);
   const int lane = threadIdx.x & 31, nw = blockDim.x >> 5;
   const int lc = lane / Q, ls = lane % Q;  // column and s of this lane in the outer step
@@ -595,7 +605,9 @@ __device__ __forceinline__ void yzw_forward(const float2* __restrict__ S, int ny
 #pragma unroll
       for (int r = 0; r < Q; ++r) {  // y = lane + 32 r < Py/2; y >= ny is zero padding
         const int y = lane + 32 * r;
-        v[c * Q + r] = (c < nc && r < Q / 2 && y < ny) ? __ldg(S + (size_t)(col0 + c) * ny + y) : make_float2(0.f, 0.f);
+        v[c * Q + r] = (c < nc && r < Q / 2 && y < ny && span_ok((size_t)(col0 + c) * ny + y, sleft))
+                           ? __ldg(S + (size_t)(col0 + c) * ny + y)
+                           : make_float2(0.f, 0.f);
       }
     four_step_inner<Q, -1, true>(v, twq, lane);
     float2* C = D + col0 * cs;
@@ -612,7 +624,8 @@ __device__ __forceinline__ void yzw_forward(const float2* __restrict__ S, int ny
 
 // Inverse y transforms of the columns of D; the y < ny outputs go to S.
 template <int Q>
-__device__ __forceinline__ void yzw_inverse(float2* __restrict__ S, int ny, float2* D, int ncol, const float2* twq) {
+__device__ __forceinline__ void yzw_inverse(float2* __restrict__ S, int ny, float2* D, int ncol, const float2* twq,
+                                            size_t sleft) {
   constexpr int W = 32 / Q, cs = qlen(32 * Q);
   const int lane = threadIdx.x & 31, nw = blockDim.x >> 5;
   const int lc = lane / Q, ls = lane % Q;
@@ -632,7 +645,7 @@ __device__ __forceinline__ void yzw_inverse(float2* __restrict__ S, int ny, floa
 #pragma unroll
       for (int t = 0; t < 16; ++t) {  // y = s + Q t < Py/2: only y < ny is kept
         const int y = sl + Q * t;
-        if (y < ny) Sc[y] = v[t];
+        if (y < ny && span_ok((size_t)(col0 + cl) * ny + y, sleft)) Sc[y] = v[t];
       }
     }
   }
@@ -658,7 +671,8 @@ __device__ __forceinline__ void yzw_body(const MagnetDev& M, int kx0, int nkx, f
   __syncthreads();
   pdl_wait();  // the spectrum is written by the x pass
   float2* S = M.spec + (size_t)kx0 * 3 * nz * ny;
-  yzw_forward<Q>(S, ny, D, ncol, twq);
+  const size_t sleft = (size_t)(M.Fh - kx0) * 3 * nz * ny;  // elements from S on (checked build)
+  yzw_forward<Q>(S, ny, D, ncol, twq, sleft);
   __syncthreads();
   if constexpr (PZ == 1) {
     for (int t = threadIdx.x; t < nkx << LOGPY; t += blockDim.x) {
@@ -674,7 +688,7 @@ __device__ __forceinline__ void yzw_body(const MagnetDev& M, int kx0, int nkx, f
     }
   }
   __syncthreads();
-  yzw_inverse<Q>(S, ny, D, ncol, twq);
+  yzw_inverse<Q>(S, ny, D, ncol, twq, sleft);
 }
 
 // Work item: magnet, first kx in z, number of consecutive kx in y0.  y lengths 64 .. 512.

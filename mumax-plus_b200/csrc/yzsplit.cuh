@@ -23,9 +23,13 @@ namespace mpx {
 // symmetry-reduced storage [kx][kz'][kcomp][ky'] (as kernel_at).
 __device__ __forceinline__ void kernel_at_rt(const float* __restrict__ Kx, int kc, int hy, int kyp, float sy, int kz,
                                              int Pz, float& kxx, float& kyy, float& kzz, float& kxy, float& kxz,
-                                             float& kyz) {
+                                             float& kyz, size_t left) {
   const int kzp = min(kz, Pz - kz);
   const float sz = (kz > Pz / 2) ? -1.f : 1.f;
+  if (!span_ok((size_t)kzp * kc * hy + kyp + (size_t)(kc - 1) * hy, left)) {
+    kxx = kyy = kzz = kxy = kxz = kyz = 0.f;
+    return;
+  }
   const float* Kk = Kx + (size_t)kzp * kc * hy + kyp;
   kxx = __ldg(Kk);
   kyy = __ldg(Kk + hy);
@@ -57,29 +61,33 @@ __global__ void __launch_bounds__(384, MAXLR == 3 ? 2 : 1)
   load_twiddles<MAXLR>(tws, tw, logPy);
   float2* __restrict__ T = M.tspec + (size_t)col0 * Py;
   float2* __restrict__ S = M.spec + (size_t)col0 * ny;
+  const size_t ncols_all = (size_t)M.Fh * 3 * M.n[2];  // columns of S and T (checked build)
+  const size_t sleft = (ncols_all - col0) * ny, tleft = (ncols_all - col0) * Py;
   if (DIR < 0) {  // S (ny rows, zero above) -> lower half of each column
     const int logh = logPy > 0 ? logPy - 1 : 0;
     const int total = ncol << logh;
     for (int e = threadIdx.x; e < total; e += blockDim.x) {
       const int col = e >> logh, y = e & ((1 << logh) - 1);
-      D[col * cs + pidx(y)] = (y < ny) ? __ldg(S + (size_t)col * ny + y) : make_float2(0.f, 0.f);
+      D[col * cs + pidx(y)] =
+          (y < ny && span_ok((size_t)col * ny + y, sleft)) ? __ldg(S + (size_t)col * ny + y) : make_float2(0.f, 0.f);
     }
     __syncthreads();
     fft_many<-1, MAXLR, 1>(D, logPy, ncol, cs, tws);
     for (int e = threadIdx.x; e < (ncol << logPy); e += blockDim.x) {
       const int col = e >> logPy, y = e & (Py - 1);
-      T[(size_t)col * Py + y] = D[col * cs + pidx(y)];
+      if (span_ok((size_t)col * Py + y, tleft)) T[(size_t)col * Py + y] = D[col * cs + pidx(y)];
     }
   } else {  // T (Py rows) -> S (the ny rows that are not padding)
     for (int e = threadIdx.x; e < (ncol << logPy); e += blockDim.x) {
       const int col = e >> logPy, y = e & (Py - 1);
-      D[col * cs + pidx(y)] = __ldg(T + (size_t)col * Py + y);
+      D[col * cs + pidx(y)] = span_ok((size_t)col * Py + y, tleft) ? __ldg(T + (size_t)col * Py + y)
+                                                                    : make_float2(0.f, 0.f);
     }
     __syncthreads();
     fft_many<1, MAXLR, 2>(D, logPy, ncol, cs, tws);
     for (int e = threadIdx.x; e < ncol * ny; e += blockDim.x) {
       const int col = e / ny, y = e - col * ny;
-      S[(size_t)col * ny + y] = D[col * cs + pidx(y)];
+      if (span_ok((size_t)col * ny + y, sleft)) S[(size_t)col * ny + y] = D[col * cs + pidx(y)];
     }
   }
 }
@@ -103,13 +111,15 @@ __global__ void __launch_bounds__(384, MAXLR == 3 ? 2 : 1)
   float2* tws = sm + ncol * cs;
   load_twiddles<MAXLR>(tws, tw, logPz);
   const float2* __restrict__ Tk = M.tspec + (size_t)kx * 3 * nz * Py;
+  const size_t tleft = (size_t)(M.Fh - kx) * 3 * nz * Py;  // elements of T from Tk on (checked build)
   // gather: consecutive threads take consecutive ky (coalesced rows of T)
   const int logh = logPz > 0 ? logPz - 1 : 0;
   for (int e = threadIdx.x; e < (ncol << logh); e += blockDim.x) {
     const int kyl = e % nky, rest = e / nky;
     const int c = rest % 3, z = rest / 3;
-    D[(c * nky + kyl) * cs + pidx(z)] =
-        (z < nz) ? __ldg(Tk + ((size_t)c * nz + z) * Py + ky0 + kyl) : make_float2(0.f, 0.f);
+    D[(c * nky + kyl) * cs + pidx(z)] = (z < nz && span_ok(((size_t)c * nz + z) * Py + ky0 + kyl, tleft))
+                                            ? __ldg(Tk + ((size_t)c * nz + z) * Py + ky0 + kyl)
+                                            : make_float2(0.f, 0.f);
   }
   __syncthreads();
   fft_many<-1, MAXLR, 1>(D, logPz, ncol, cs, tws);
@@ -122,7 +132,7 @@ __global__ void __launch_bounds__(384, MAXLR == 3 ? 2 : 1)
     const int kyp = min(ky, Py - ky);
     const float sy = (ky > Py / 2) ? -1.f : 1.f;
     float kxx, kyy, kzz, kxy, kxz, kyz;
-    kernel_at_rt(Kx, kc, hy, kyp, sy, kz, Pz, kxx, kyy, kzz, kxy, kxz, kyz);
+    kernel_at_rt(Kx, kc, hy, kyp, sy, kz, Pz, kxx, kyy, kzz, kxy, kxz, kyz, (size_t)(M.Fh - kx) * (Pz / 2 + 1) * kc * hy);
     apply3(&D[(0 * nky + kyl) * cs + pidx(kz)], &D[(1 * nky + kyl) * cs + pidx(kz)],
            &D[(2 * nky + kyl) * cs + pidx(kz)], kxx, kyy, kzz, kxy, kxz, kyz);
   }
@@ -132,7 +142,8 @@ __global__ void __launch_bounds__(384, MAXLR == 3 ? 2 : 1)
   for (int e = threadIdx.x; e < ncol * nz; e += blockDim.x) {
     const int kyl = e % nky, rest = e / nky;
     const int c = rest % 3, z = rest / 3;
-    Tw[((size_t)c * nz + z) * Py + ky0 + kyl] = D[(c * nky + kyl) * cs + pidx(z)];
+    if (span_ok(((size_t)c * nz + z) * Py + ky0 + kyl, tleft))
+      Tw[((size_t)c * nz + z) * Py + ky0 + kyl] = D[(c * nky + kyl) * cs + pidx(z)];
   }
 }
 

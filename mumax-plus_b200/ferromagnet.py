@@ -351,10 +351,15 @@ class Ferromagnet:
         return StrayField(self, self.grid)
 
     def stray_field_from_magnet(self, source_magnet):
+        """The field created by `source_magnet`, felt by this magnet: a
+        StrayField on this magnet's grid, zero outside its geometry
+        (mumaxplus/magnet.py:532-552).  The source must be in the same world."""
         from .strayfield import StrayField
-        if source_magnet is not self:
-            raise NotImplementedError("stray fields between different magnets are not implemented yet")
-        return StrayField(self, self.grid)
+        if source_magnet is self:
+            return StrayField(self, self.grid)
+        if getattr(source_magnet, "_world", None) is not self._world:
+            raise RuntimeError("Can not compute the magnetic field of the magnet")
+        return StrayField._between(source_magnet, self)
 
     @property
     def torque(self):

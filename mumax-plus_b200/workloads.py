@@ -163,11 +163,11 @@ def desc(w, keep):
     return d
 
 
-def build(mpx, w, device=None):
+def build(mpx, w, device=None, demag_dft="fp32"):
     """World + Ferromagnet for workload `w` through the mumaxplus-style API."""
     mg = w.get("mastergrid", (0, 0, 0))
     world = mpx.World(w["cellsize"], pbc_repetitions=tuple(w.get("pbc", (0, 0, 0))), mastergrid=mpx.Grid(mg),
-                      device=device)
+                      device=device, demag_dft=demag_dft)
     magnet = mpx.Ferromagnet(world, mpx.Grid(w["size"]))
     magnet._suspend = True
     magnet.msat = w.get("msat", 1.0)

@@ -14,7 +14,17 @@ class World:
     """A world with a given cell size, optional periodic box (mastergrid) and
     demag image repetitions (pbc_repetitions)."""
 
-    def __init__(self, cellsize, pbc_repetitions=(0, 0, 0), mastergrid=Grid((0, 0, 0)), device=None):
+    _DFT_MODES = {"fp32": 0, "tf32x3": 1}
+
+    def __init__(self, cellsize, pbc_repetitions=(0, 0, 0), mastergrid=Grid((0, 0, 0)), device=None,
+                 demag_dft="fp32"):
+        """demag_dft (no counterpart in the reference, which calls cuFFT): the
+        arithmetic of the y transforms of the demag convolution, "fp32"
+        (shared-memory FFTs on the CUDA cores, the default) or "tf32x3"
+        (tensor-core DFT GEMMs with 3xTF32 split products for y lengths 1024
+        and 2048 of the padded grid)."""
+        if demag_dft not in self._DFT_MODES:
+            raise ValueError(f"demag_dft must be one of {sorted(self._DFT_MODES)}")
         if len(cellsize) != 3:
             raise ValueError("'cellsize' should have three dimensions.")
         if len(pbc_repetitions) != 3:
@@ -28,6 +38,8 @@ class World:
         self._pbc = tuple(int(p) for p in pbc_repetitions)
         self._mastergrid = Grid(mastergrid.size, mastergrid.origin)
         self._engine = Engine(device)
+        self._engine.set_dft(self._DFT_MODES[demag_dft])
+        self._demag_dft = demag_dft
         self._group = self._engine.group_create()
         self._relax_threshold = -1.0
         self._magnets = {}
@@ -37,6 +49,11 @@ class World:
 
     def __repr__(self):
         return f"World(cellsize={self.cellsize})"
+
+    @property
+    def demag_dft(self):
+        """Arithmetic of the demag y transforms ("fp32" or "tf32x3"), fixed at construction."""
+        return self._demag_dft
 
     # ------------------------------------------------------------- internals
     @staticmethod

@@ -1,8 +1,10 @@
-"""Checked build: the parity, random-magnet and stray-field suites run again
-against libmpx_checked.so (the same sources compiled with -DMPX_BOUNDS_CHECK),
-where every per-cell access of a field buffer -- stencil neighbours under every
-boundary condition, stage states and derivatives, stray-field buffers --
-verifies its index.  A bad access is skipped and recorded, never trapped; the
+"""Checked build: the parity, random-magnet, stray-field and tensor-core suites
+run again against libmpx_checked.so (the same sources compiled with
+-DMPX_BOUNDS_CHECK), where every per-cell access of a field buffer -- stencil
+neighbours under every boundary condition, stage states and derivatives,
+stray-field buffers -- and every spectrum access of the x passes and of the
+y/z passes (column gathers and scatters, kernel-spectrum reads, the split
+path's y-transformed spectrum) verifies its index.  A bad access is skipped and recorded, never trapped; the
 session hook in conftest.py then requires mpx_bounds_check to report none.
 This stands in for compute-sanitizer's memcheck, which is not available on
 these GPUs.
@@ -22,7 +24,7 @@ CHECKED = os.path.join(ROOT, "mumax-plus_b200", "libmpx_checked.so")
 def test_checked_build_suites_stay_in_bounds():
     assert os.path.exists(CHECKED), "libmpx_checked.so is missing: run __graft_entry__.build()"
     env = dict(os.environ, MPX_LIBRARY=CHECKED, MPX_BOUNDS_CHECK_RUN="1")
-    suites = ["tests/test_gpu_parity.py", "tests/test_gpu_fuzz.py", "tests/test_gpu_stray.py"]
+    suites = ["tests/test_gpu_parity.py", "tests/test_gpu_fuzz.py", "tests/test_gpu_stray.py", "tests/test_gpu_tc.py"]
     res = subprocess.run([sys.executable, "-m", "pytest", "-q", "-x", "-m", "gpu", "-p", "no:cacheprovider"] + suites,
                          cwd=ROOT, env=env, capture_output=True, text=True, timeout=900)
     assert res.returncode == 0, res.stdout[-4000:] + res.stderr[-2000:]

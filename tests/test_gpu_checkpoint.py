@@ -86,3 +86,34 @@ def test_batch_solve_preempted_and_resumed(mpx):
     b.poll()
     np.testing.assert_array_equal(b.engine.get_m(s0.magnet, s0.shape), want)
     assert b.engine.group_info(s0.group).time == ref.engine.group_info(rs[0].group).time
+
+
+def test_load_refused_while_running_and_clean_after_a_run(mpx):
+    """A group in the middle of a started run refuses a state (its controller
+    state belongs to that run); after run() has finished, a loaded state
+    continues exactly like the uninterrupted run (the final-step phase of the
+    earlier run does not carry over)."""
+    from mumaxplus_b200 import batch as B
+
+    sols = _mix()[:1]
+    b = B.Batch()
+    s = b.add(sols[0], key=0)
+    state0 = b.engine.group_save(s.group)
+    b.start(s, 1e-6)
+    b.advance(3)
+    b.poll()
+    with pytest.raises(ValueError):
+        b.engine.group_load(s.group, state0)
+
+    world, magnet = _film(mpx)
+    world.timesolver.steps(4)
+    state = world.save_state()
+    world.timesolver.steps(6)
+    want = magnet.magnetization.get()
+    t_want = world.timesolver.time
+    world.load_state(state)
+    world.timesolver.run(3.7e-12)  # ends with a shortened final step
+    world.load_state(state)
+    world.timesolver.steps(6)
+    np.testing.assert_array_equal(magnet.magnetization.get(), want)
+    assert world.timesolver.time == t_want

@@ -130,3 +130,125 @@ def test_large_pair_fft_form_trajectory(mpx):
             worst = max(worst, float(np.max(np.abs(np.array(mag.magnetization.average())
                                                     - np.array(ow.average(q, abi.Q_MAGNETIZATION))))))
     assert worst < 1e-5, worst
+
+
+# ------------------------------------------------ StrayField on other grids
+# test/test_strayfield.py:29-136: a magnet on mgrid, its field on hgrid, by the
+# FFT method against the brute-force method (with and without periodic
+# images), and against the demag field of one magnet spanning both grids whose
+# msat is zero outside mgrid; here also against the FP64 oracle's demag of
+# that union magnet.
+STRAY_CASES = [
+    ((17, 4, 1), (3, 6, 0), (17, 4, 1), (3, 6, 0)),
+    ((8, 10, 1), (2, 15, 0), (6, 7, 2), (-5, 0, 2)),
+    ((8, 10, 1), (2, 15, 0), (32, 32, 1), (-5, 0, 0)),
+    ((8, 10, 1), (2, 15, -1), (32, 32, 1), (-5, 0, 0)),
+    ((8, 10, 2), (2, 15, -1), (32, 32, 1), (-5, 0, 1)),
+    ((8, 10, 2), (2, 15, 2), (32, 32, 5), (0, 0, 1)),
+]
+STRAY_CS = (1e-9, 2e-9, 3.1e-9)
+
+
+def _rel_err_cellwise(result, wanted):
+    """test/test_strayfield.py:7-10: max over cells of |dH| / |H_wanted|."""
+    err = np.linalg.norm(np.asarray(result, np.float64) - np.asarray(wanted, np.float64), axis=0)
+    return float(np.max(err / np.linalg.norm(np.asarray(wanted, np.float64), axis=0)))
+
+
+def _extended(g1, g2):
+    lo = [min(g1[1][c], g2[1][c]) for c in range(3)]
+    hi = [max(g1[1][c] + g1[0][c], g2[1][c] + g2[0][c]) for c in range(3)]
+    return tuple(hi[c] - lo[c] for c in range(3)), tuple(lo)
+
+
+@pytest.mark.parametrize("pbc", [None, (1, 2, 0)])
+@pytest.mark.parametrize("case", STRAY_CASES)
+def test_stray_field_fft_against_brute(mpx, case, pbc):
+    msize, morig, hsize, horig = case
+    world = mpx.World(STRAY_CS)
+    magnet = mpx.Ferromagnet(world, mpx.Grid(msize, morig))
+    magnet.msat = 800e3
+    magnet.magnetization = (1, 0, 0)
+    if pbc is not None:
+        world.set_pbc(pbc)
+    sf = mpx.StrayField(magnet, mpx.Grid(hsize, horig))
+    sf.set_method("fft")
+    result = sf.eval()
+    sf.set_method("brute")
+    wanted = sf.eval()
+    assert result.shape == (3, hsize[2], hsize[1], hsize[0])
+    assert _rel_err_cellwise(result, wanted) < 1e-4
+
+
+@pytest.mark.parametrize("pbc", [None, (1, 2, 1)])
+@pytest.mark.parametrize("case", STRAY_CASES)
+def test_stray_field_equals_union_demag(mpx, case, pbc):
+    msize, morig, hsize, horig = case
+    bsize, borig = _extended((msize, morig), (hsize, horig))
+    box = mpx.Grid(bsize, borig)
+    world = mpx.World(STRAY_CS, (0, 0, 0) if pbc is None else pbc, mpx.Grid((0, 0, 0)) if pbc is None else box)
+    magnet = mpx.Ferromagnet(world, mpx.Grid(msize, morig))
+    magnet.msat = 800e3
+    magnet.magnetization = (1, -1, 2)
+    hfield = mpx.StrayField(magnet, mpx.Grid(hsize, horig)).eval()
+    hbrute = mpx.StrayField(magnet, mpx.Grid(hsize, horig))
+    hbrute.set_method("brute")
+    hbrute = hbrute.eval()
+
+    world2 = mpx.World(STRAY_CS, (0, 0, 0) if pbc is None else pbc, mpx.Grid((0, 0, 0)) if pbc is None else box)
+    magnet2 = mpx.Ferromagnet(world2, box)
+    mi = [morig[c] - borig[c] for c in range(3)]
+    mf = [mi[c] + msize[c] for c in range(3)]
+    hi = [horig[c] - borig[c] for c in range(3)]
+    hf = [hi[c] + hsize[c] for c in range(3)]
+    ms = np.zeros((bsize[2], bsize[1], bsize[0]), np.float32)
+    ms[mi[2]:mf[2], mi[1]:mf[1], mi[0]:mf[0]] = 800e3
+    magnet2.msat = ms
+    m = np.ones((3, bsize[2], bsize[1], bsize[0]), np.float32)
+    m[:, mi[2]:mf[2], mi[1]:mf[1], mi[0]:mf[0]] = magnet.magnetization.eval()
+    magnet2.magnetization = m
+    wanted = magnet2.demag_field.eval()[:, hi[2]:hf[2], hi[1]:hf[1], hi[0]:hf[0]]
+    assert _rel_err_cellwise(hfield, wanted) < 1e-4
+    assert _rel_err_cellwise(hbrute, wanted) < 1e-4
+
+    # the FP64 oracle's demag field of the same union magnet
+    s = MagnetSpec(size=bsize, origin=borig, cellsize=STRAY_CS, msat=ms,
+                   mastergrid_size=(0, 0, 0) if pbc is None else bsize,
+                   mastergrid_origin=(0, 0, 0) if pbc is None else borig,
+                   pbc=(0, 0, 0) if pbc is None else pbc)
+    ow, q = s.oracle_world(magnet2.magnetization.eval())
+    want64 = ow.eval(q, abi.Q_DEMAG_FIELD)[:, hi[2]:hf[2], hi[1]:hf[1], hi[0]:hf[0]]
+    assert max_rel(hfield, want64) < 1e-5
+    assert max_rel(hbrute, want64) < 1e-5
+
+
+def test_stray_field_from_magnet(mpx):
+    """Magnet.stray_field_from_magnet(source) (mumaxplus/magnet.py:532-552):
+    the source's field on this magnet's grid, zero outside its geometry, the
+    same as the StrayField of the source on that grid; both methods; the
+    magnet's own stray field is its demag field; a magnet of another world
+    has none."""
+    A, B = _specs()
+    geomB = np.ones(B.shape, bool)
+    geomB[:, 4:8, 2:9] = False
+    B.geometry = geomB
+    ms = [random_m(A.shape, seed=3, smooth=1), random_m(B.shape, seed=4, smooth=1)]
+    world = mpx.World(CS)
+    ma = mpx.Ferromagnet(world, mpx.Grid(A.size, A.origin))
+    mb = mpx.Ferromagnet(world, mpx.Grid(B.size, B.origin), geometry=geomB)
+    for mag, s, m in ((ma, A, ms[0]), (mb, B, ms[1])):
+        mag.msat, mag.aex, mag.alpha = s.msat, s.aex, s.alpha
+        mag.magnetization = m
+    sf = mb.stray_field_from_magnet(ma)
+    got = sf.eval()
+    plain = mpx.StrayField(ma, mb.grid).eval()
+    np.testing.assert_array_equal(got[:, ~geomB], 0.0)
+    assert max_rel(got[:, geomB], plain[:, geomB]) < 1e-6
+    sf.set_method("brute")
+    assert max_rel(sf.eval(), got) < 1e-5
+    own = ma.stray_field_from_magnet(ma).eval()
+    np.testing.assert_array_equal(own, ma.demag_field.eval())
+    other = mpx.World(CS)
+    mc = mpx.Ferromagnet(other, mpx.Grid((4, 4, 1)))
+    with pytest.raises(RuntimeError):
+        mc.stray_field_from_magnet(ma)

@@ -27,9 +27,6 @@ sys.path.insert(0, os.path.join(ROOT, "oracle"))
 
 import numpy as np  # noqa: E402
 
-GAMMA_EVALS_REFERENCE_DP = 7  # the reference's Dormand-Prince evaluates the torque 7 times per step (no FSAL)
-
-
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -40,6 +37,10 @@ def parse():
                     default="multilayer")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=8)
+    ap.add_argument("--no-batched", action="store_true",
+                    help="default workload: leave out the batched-form sub-record (configuration 4)")
+    ap.add_argument("--batched-duration", type=float, default=2e-9,
+                    help="default workload: simulated seconds per relaxation of the batched sub-record")
     # batched / served forms
     ap.add_argument("--duration", type=float, default=0.2e-9,
                     help="batched: simulated seconds per relaxation (the full problem runs 2 ns)")
@@ -48,6 +49,8 @@ def parse():
     ap.add_argument("--rate", type=float, default=1.0, help="serving: Poisson arrival rate (requests/s)")
     ap.add_argument("--seconds", type=float, default=30.0, help="serving: length of the arrival window (s)")
     ap.add_argument("--budget-gb", type=float, default=150.0, help="serving: device-memory budget")
+    ap.add_argument("--time-limit", type=float, default=None,
+                    help="serving: wall-clock limit of each served run (s); unfinished requests are reported")
     return ap.parse_args()
 
 
@@ -67,16 +70,48 @@ def measured_peaks():
         return 6650.0, "fallback"
 
 
-def profile_traffic(wname):
-    """dram bytes per k_yz launch from the committed ncu summary, or None."""
-    path = os.path.join(ROOT, "profiles", f"k_yz_{wname}.md")
+# CUDA sources each profiled kernel is compiled from (the hash in its
+# committed ncu summary covers these files)
+PROFILE_SOURCES = {
+    "k_yz": ("kernels.cuh", "fft.cuh", "physics.cuh"),
+    "k_xinv": ("kernels.cuh", "fft.cuh", "physics.cuh"),
+    "k_xfwd": ("kernels.cuh", "fft.cuh", "physics.cuh"),
+}
+
+
+def kernel_sources_sha(files):
+    """Hash of the given CUDA sources of the product library (csrc/)."""
+    import hashlib
+
+    d = os.path.join(ROOT, "mumax-plus_b200", "csrc")
+    h = hashlib.sha256()
+    for name in sorted(files):
+        with open(os.path.join(d, name), "rb") as f:
+            h.update(name.encode() + b"\0" + f.read())
+    return h.hexdigest()[:16]
+
+
+def profile_traffic(kernel, wname):
+    """DRAM bytes per launch of `kernel` from the committed ncu summary
+    profiles/<kernel>_<workload>.md, with the hash of the CUDA sources it was
+    captured from.  The bytes are reported only while that hash equals the
+    hash of the sources this run was built from (else the capture is stale
+    and traffic is null)."""
+    rel = os.path.join("profiles", f"{kernel}_{wname}.md")
+    files = PROFILE_SOURCES.get(kernel, ())
+    src = {"file": rel, "sources": list(files), "sources_sha": None,
+           "build_sources_sha": kernel_sources_sha(files) if files else None, "matches_build": False}
+    val = None
     try:
-        for line in open(path):
+        for line in open(os.path.join(ROOT, rel)):
             if line.startswith("traffic_bytes_per_launch:"):
-                return float(line.split(":")[1])
+                val = float(line.split(":")[1])
+            elif line.startswith("sources_sha:"):
+                src["sources_sha"] = line.split(":")[1].strip()
     except OSError:
-        pass
-    return None
+        return None, src
+    src["matches_build"] = src["sources_sha"] is not None and src["sources_sha"] == src["build_sources_sha"]
+    return (val if src["matches_build"] else None), src
 
 
 class ClockSampler:
@@ -126,9 +161,10 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(rows)}
 
 
-def cpu_baseline(w, n_evals=1):
-    """FP64 oracle on the host cores: one effective-field evaluation of the
-    full workload (a bounded sample), scaled to a reference Dormand-Prince step."""
+def _oracle_world(w):
+    """FP64 oracle world of workload `w` with its initial state, the kernel
+    spectrum already built (setup, outside every timed region), Dormand-Prince
+    from the sensible time step."""
     import oracle as O
     from mumaxplus_b200 import workloads as Wl
 
@@ -138,31 +174,48 @@ def cpu_baseline(w, n_evals=1):
     q = ow.add_magnet(Wl.desc(w, keep))
     ow.set_m(q, w["m0"]())
     t0 = time.time()
-    ow.eval(q, O.abi.Q_DEMAG_FIELD)  # builds the FP64 kernel spectrum (setup, untimed below)
+    ow.eval(q, O.abi.Q_DEMAG_FIELD)  # builds the FP64 kernel spectrum
     t_setup = time.time() - t0
-    times = []
-    for _ in range(n_evals):
-        t0 = time.time()
-        ow.eval(q, O.abi.Q_EFFECTIVE_FIELD)
-        times.append(time.time() - t0)
-    t_eval = statistics.median(times)
+    ow.set_method("DormandPrince")
+    ow.timestep = ow.sensible_timestep()
+    return ow, q, keep, t_setup
+
+
+def _oracle_steps(ow, n):
+    """n Dormand-Prince step attempts of the oracle (the reference's
+    TimeSolver::step: 7 torque evaluations each, rejected attempts retried on
+    the next call); returns (seconds, accepted steps, attempts)."""
+    c0 = ow.counters()
+    t0 = time.time()
+    ow.steps(n)
+    t = time.time() - t0
+    c1 = ow.counters()
+    return t, c1["steps"] - c0["steps"], n
+
+
+def cpu_baseline(w, n_steps=2):
+    """FP64 oracle on the host cores: a bounded sample of real Dormand-Prince
+    steps of the full workload (stage combinations, normalisation, torque,
+    error norm and controller included)."""
+    from mumaxplus_b200 import workloads as Wl
+
+    ow, q, keep, t_setup = _oracle_world(w)
+    t, acc, att = _oracle_steps(ow, n_steps)
     N = Wl.ncells(w)
     return {
-        "value": N / (GAMMA_EVALS_REFERENCE_DP * t_eval),
+        "value": N * acc / t,
         "unit": "cell-updates/s",
         "cores": os.cpu_count(),
         "kind": "port",
-        "sample": (f"{n_evals} FP64 effective-field evaluation(s) of the full {w['name']} grid "
-                   f"({t_eval:.2f} s each, kernel build {t_setup:.1f} s untimed), scaled by the "
-                   f"{GAMMA_EVALS_REFERENCE_DP} evaluations of one reference Dormand-Prince step"),
+        "sample": (f"{att} FP64 Dormand-Prince step attempts ({acc} accepted, 7 torque evaluations each) of the "
+                   f"full {w['name']} grid from its initial state, {t:.1f} s; FP64 kernel build {t_setup:.1f} s "
+                   f"untimed"),
     }
 
 
 def run_reference_many(args):
-    """CPU FP64 oracle on a bounded sample of the batched / served solves: one
-    effective-field evaluation per sampled solve, scaled by the 7 evaluations of
-    one reference Dormand-Prince step."""
-    import oracle as O
+    """CPU FP64 oracle on a bounded sample of the batched / served solves: per
+    sampled solve, real Dormand-Prince steps from its initial state."""
     from mumaxplus_b200 import batch as B
     from mumaxplus_b200 import workloads as Wl
 
@@ -170,26 +223,31 @@ def run_reference_many(args):
         ws = Wl.batch_instances(256)[::32]
     else:
         ws = Wl.serving_requests(rate=2.0, seconds=4.0)[:6]
-    t_tot, cells = 0.0, 0
+    t_tot, upd, att_tot = 0.0, 0, 0
     for k in range(args.warmup + args.steps):
-        w = ws[k % len(ws)]
+        w = dict(ws[k % len(ws)])
+        w.setdefault("name", f"solve_{k}")
+        import oracle as O
+
         keep = []
-        ow = O.OracleWorld()
+        ow = O.OracleWorld()  # the applied field is the solve's own bias field (solve_desc)
         q = ow.add_magnet(B.solve_desc(w, keep))
         ow.set_m(q, w["m0"]())
         ow.eval(q, O.abi.Q_DEMAG_FIELD)  # kernel construction, untimed
-        t0 = time.time()
-        ow.eval(q, O.abi.Q_EFFECTIVE_FIELD)
+        ow.set_method("DormandPrince")
+        ow.timestep = ow.sensible_timestep()
+        t, acc, att = _oracle_steps(ow, 4)
         if k >= args.warmup:
-            t_tot += time.time() - t0
-            cells += Wl.ncells(w)
-    value = cells / (GAMMA_EVALS_REFERENCE_DP * t_tot)
-    sample = (f"{args.steps} FP64 effective-field evaluations of {args.workload} solves ({cells} cells), "
-              f"scaled by {GAMMA_EVALS_REFERENCE_DP} evaluations per reference Dormand-Prince step")
+            t_tot += t
+            upd += Wl.ncells(w) * acc
+            att_tot += att
+    value = upd / t_tot
+    sample = (f"{args.steps} {args.workload} solves (every 32nd of the pool), 4 FP64 Dormand-Prince step "
+              f"attempts each ({att_tot} in all) from the initial state")
     line = {
         "impl": "reference", "metric": "cell-updates/s", "value": value, "unit": "cell-updates/s",
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": 1e3 * GAMMA_EVALS_REFERENCE_DP * t_tot / args.steps, "higher_is_better": True,
+        "ms_per_step": 1e3 * t_tot / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": args.workload, "method": "DormandPrince", "parallelism": "host cores (OpenMP)"},
         "cpu_baseline": {"value": value, "unit": "cell-updates/s", "cores": os.cpu_count(), "kind": "port",
@@ -200,6 +258,9 @@ def run_reference_many(args):
 
 
 def run_reference(args):
+    """The reference arm: the CPU FP64 restatement of the reference's path
+    (oracle/, all host cores) taking real Dormand-Prince steps of the same
+    workload; each timed step is one step attempt of the full grid."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
@@ -207,31 +268,23 @@ def run_reference(args):
         return run_reference_many(args)
     w = workload(args.workload)
     from mumaxplus_b200 import workloads as Wl
-    import oracle as O
 
-    keep = []
-    ow = O.OracleWorld()
-    ow.set_world_bias(w.get("world_bias", (0, 0, 0)))
-    q = ow.add_magnet(Wl.desc(w, keep))
-    ow.set_m(q, w["m0"]())
-    ow.eval(q, O.abi.Q_DEMAG_FIELD)  # kernel build, untimed
-    for _ in range(args.warmup):
-        ow.eval(q, O.abi.Q_EFFECTIVE_FIELD)
-    t0 = time.time()
-    for _ in range(args.steps):
-        ow.eval(q, O.abi.Q_EFFECTIVE_FIELD)
-    t = (time.time() - t0) / args.steps
+    ow, q, keep, t_setup = _oracle_world(w)
+    _oracle_steps(ow, args.warmup)
+    t, acc, att = _oracle_steps(ow, args.steps)
     N = Wl.ncells(w)
-    value = N / (GAMMA_EVALS_REFERENCE_DP * t)
+    value = N * acc / t
+    sample = (f"{att} FP64 Dormand-Prince step attempts of the full grid ({acc} accepted, 7 torque evaluations "
+              f"each) after {args.warmup} warm-up attempts; FP64 kernel build {t_setup:.1f} s untimed")
     line = {
         "impl": "reference", "metric": "cell-updates/s", "value": value, "unit": "cell-updates/s",
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": GAMMA_EVALS_REFERENCE_DP * t * 1e3, "higher_is_better": True, "scaling": "weak",
+        "ms_per_step": 1e3 * t / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": w["name"], "method": "DormandPrince", "parallelism": "host cores (OpenMP)"},
+        "config": {"workload": w["name"], "method": "DormandPrince (adaptive, max_error 1e-5)",
+                   "accepted_steps": int(acc), "parallelism": "host cores (OpenMP)"},
         "cpu_baseline": {"value": value, "unit": "cell-updates/s", "cores": os.cpu_count(), "kind": "port",
-                         "sample": f"each step = one FP64 effective-field evaluation of the full grid, scaled by "
-                                   f"{GAMMA_EVALS_REFERENCE_DP} evaluations per reference Dormand-Prince step"},
+                         "sample": sample},
         "e2e": {"value": value, "unit": "cell-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -362,7 +415,15 @@ def run_ours(args):
     }[names[dom]]
     peak, peak_kind = measured_peaks()
     achieved = alg_bytes / (kms[dom] / 1e3) / 1e9
-    traffic = profile_traffic(w["name"]) if names[dom] == "k_yz" else None
+    traffic, traffic_src = profile_traffic(names[dom], w["name"])
+
+    # configuration 4 as a sub-record of the default line (one GPU): the 256
+    # relaxations batched vs the plain one-at-a-time form
+    batched = None
+    if world_size == 1 and args.workload == "multilayer" and not args.no_batched:
+        insts = Wl.batch_instances(256)
+        r = _batched_measure(insts, args.batched_duration, args.plain_every, 1, local)
+        batched = {"workload": "batch_256_relax", **r}
 
     cpu = None
     if rank == 0 and world_size == 1 and not args.no_cpu_baseline:
@@ -387,7 +448,8 @@ def run_ours(args):
                        "fft_padding": f"{P[0]}x{P[1]}x{P[2]}"},
             "roofline": {"bound": "hbm", "kernel": names[dom], "achieved": achieved, "peak": peak,
                          "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_kind,
-                         "traffic": traffic, "algorithmic_bytes_per_launch": alg_bytes,
+                         "traffic": traffic, "traffic_source": traffic_src,
+                         "algorithmic_bytes_per_launch": alg_bytes,
                          "kernel_ms": {n: round(t, 4) for n, t in zip(names, kms)}},
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_value, "unit": "cell-updates/s", "h2d_bytes_per_step": 12 * N,
@@ -397,6 +459,8 @@ def run_ours(args):
         }
         if solve_info is not None:
             line["solve"] = solve_info
+        if batched is not None:
+            line["batched_form"] = batched
         print(json.dumps(line), flush=True)
     if dist is not None:
         dist.barrier()
@@ -431,6 +495,66 @@ def _max_over_ranks(dist, value, device):
     return float(t.item())
 
 
+def _batched_measure(insts, duration, plain_every, warmup, local):
+    """Configuration 4 on this GPU: `insts` relaxed together in one batch
+    (torque stop 1e-4 T or `duration`), then every `plain_every`-th of them
+    one at a time (the plain form); per-kernel times of one stage over the
+    started batch.  Returns a dict of the measurements."""
+    from mumaxplus_b200 import batch as B
+
+    wb = B.Batch(device=local)  # warm-up: first graph captures, pool growth
+    B.relax_batch(wb, insts[: max(1, warmup)], duration=2e-12, torque_stop=1e-4)
+    del wb
+    b = B.Batch(device=local)
+    l0 = b.engine.launch_count()
+    t0 = time.perf_counter()
+    solves, t_run, t_setup = B.relax_batch(b, insts, duration=duration, torque_stop=1e-4)
+    t_e2e = time.perf_counter() - t0
+    launches = b.engine.launch_count() - l0
+    tuned = b.tuned
+    del b
+    upd = sum(s.cells * s.steps for s in solves)
+    k = max(1, plain_every)
+    sub = insts[::k]
+    psol, p_run, p_setup = B.run_plain(B.Batch(device=local), sub, duration=duration, torque_stop=1e-4)
+    p_upd = sum(s.cells * s.steps for s in psol)
+    same = {s.key: s for s in solves}
+    worst = max(float(np.max(np.abs(same[k * i].m - p.m))) for i, p in enumerate(psol))
+    # per-kernel time of one attempt stage over the whole started batch
+    kb = B.Batch(device=local)
+    started = [kb.add(w, key=i) for i, w in enumerate(insts)]
+    for s in started:
+        kb.start(s, 1e-9, 0.0)
+    kb.advance(2)
+    kb.poll()
+    kms = kb.engine.profile_attempt("DormandPrince", reps=5)
+    del kb, started
+    steps = [s.steps for s in solves]
+    sub_set = set(range(0, len(insts), k))
+    b_sub_upd = sum(s.cells * s.steps for s in solves if s.key in sub_set)
+    return {
+        "instances": len(insts), "cells": int(sum(s.cells for s in solves)), "duration_s": duration,
+        "torque_stop_T": 1e-4,
+        "batched": {"cell_updates": int(upd), "seconds": t_run, "setup_seconds": t_setup,
+                    "value": upd / t_run, "unit": "cell-updates/s", "solves_per_s": len(solves) / t_run,
+                    "steps_min_median_max": [int(min(steps)), float(np.median(steps)), int(max(steps))],
+                    "stopped_on_torque": int(sum(1 for s in solves if s.sim_time < 0.999 * duration)),
+                    "failed": int(sum(s.failed for s in solves)),
+                    "autotuned_shape_divisors": {"x": tuned[0], "y_z": tuned[1]}},
+        "plain": {"instances": len(sub), "every": k, "cell_updates": int(p_upd), "seconds": p_run,
+                  "setup_seconds": p_setup, "value": p_upd / p_run, "unit": "cell-updates/s",
+                  "solves_per_s": len(sub) / p_run,
+                  "same_solves_cell_updates_in_batch": int(b_sub_upd)},
+        "batched_over_plain": (upd / t_run) / (p_upd / p_run),
+        "stage_kernel_ms": {"combine+x_forward": kms[0], "stray_pairs": kms[1], "y_z": kms[2],
+                            "x_inverse+epilogue": kms[3],
+                            "note": "one stage (of 6 per accepted step) over all started solves"},
+        "max_abs_dm_batched_vs_plain": worst,
+        "e2e_seconds": t_e2e, "e2e_bytes_each_way": int(sum(12 * s.cells for s in solves)),
+        "gpu_launches": int(launches),
+    }
+
+
 def run_batched(args):
     """Relaxation batch: 256 solves of side 32-256 (nz 1 or 2) advanced together
     vs the same solves one at a time (the plain form, on every k-th instance).
@@ -447,71 +571,33 @@ def run_batched(args):
     # 256 solves per GPU: a pool of 256 x N spread over the ranks by cells
     pool = Wl.batch_instances(256 * world_size)
     insts = [pool[i] for i in B.shard(pool, rank, world_size)]
-    wb = B.Batch(device=local)  # warm-up: first graph captures, pool growth
-    B.relax_batch(wb, insts[: max(1, args.warmup)], duration=2e-12, torque_stop=1e-4)
-    del wb
     sampler = ClockSampler(local)
     sampler.start()
     if dist is not None:
         dist.barrier()
     torch.cuda.synchronize(dev)
-    b = B.Batch(device=local)
-    l0 = b.engine.launch_count()
-    t0 = time.perf_counter()
-    solves, t_run, t_setup = B.relax_batch(b, insts, duration=args.duration, torque_stop=1e-4)
-    t_e2e = time.perf_counter() - t0
-    launches = b.engine.launch_count() - l0
+    r = _batched_measure(insts, args.duration, args.plain_every, args.warmup, local)
     clocks = sampler.stop()
-    upd = sum(s.cells * s.steps for s in solves)
-    t_run_max = _max_over_ranks(dist, t_run, dev)
-    t_e2e_max = _max_over_ranks(dist, t_e2e, dev)
-    # the plain form: the same solves one at a time (one solve resident)
-    k = max(1, args.plain_every)
-    sub = insts[::k]
-    psol, p_run, p_setup = B.run_plain(B.Batch(device=local), sub, duration=args.duration, torque_stop=1e-4)
-    p_upd = sum(s.cells * s.steps for s in psol)
-    same = {s.key: s for s in solves}
-    worst = max(float(np.max(np.abs(same[k * i].m - p.m))) for i, p in enumerate(psol))
-    # per-kernel time of one attempt stage over the whole started batch
-    kb = B.Batch(device=local)
-    started = [kb.add(w, key=i) for i, w in enumerate(insts)]
-    for s in started:
-        kb.start(s, 1e-9, 0.0)
-    kb.advance(2)
-    kb.poll()
-    kms = kb.engine.profile_attempt("DormandPrince", reps=5)
-    del kb, started
+    t_run_max = _max_over_ranks(dist, r["batched"]["seconds"], dev)
+    t_e2e_max = _max_over_ranks(dist, r["e2e_seconds"], dev)
     if rank == 0:
+        upd = r["batched"]["cell_updates"]
         value = world_size * upd / t_run_max
-        plain = p_upd / p_run
-        steps = [s.steps for s in solves]
         line = {
             "metric": "cell-updates/s", "value": value, "unit": "cell-updates/s", "n_gpus": world_size,
-            "steps": int(sum(steps)), "warmup": args.warmup, "ms_per_step": 1e3 * t_run_max / max(1, max(steps)),
+            "steps": None, "warmup": args.warmup, "ms_per_step": None,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": "batch_256_relax", "instances": len(insts),
-                       "cells": int(sum(s.cells for s in solves)), "duration_s": args.duration,
-                       "torque_stop_T": 1e-4, "method": "DormandPrince 1e-5",
+            "config": {"workload": "batch_256_relax", "instances": r["instances"], "cells": r["cells"],
+                       "duration_s": args.duration, "torque_stop_T": 1e-4, "method": "DormandPrince 1e-5",
                        "parallelism": f"solves sharded over {world_size} ranks" if world_size > 1 else "single GPU",
                        "l2": "state + spectra of the batch ~ 2 GB, larger than L2"},
-            "batched": {"cell_updates": upd, "seconds": t_run, "setup_seconds": t_setup,
-                        "solves_per_s": len(solves) / t_run,
-                        "steps_min_median_max": [int(min(steps)), float(np.median(steps)), int(max(steps))],
-                        "stopped_on_torque": int(sum(1 for s in solves if s.sim_time < 0.999 * args.duration)),
-                        "failed": int(sum(s.failed for s in solves)),
-                        "autotuned_shape_divisors": {"x": b.tuned[0], "y_z": b.tuned[1]}},
-            "plain": {"instances": len(sub), "cell_updates": p_upd, "seconds": p_run, "setup_seconds": p_setup,
-                      "value": plain, "unit": "cell-updates/s"},
-            "batched_over_plain": value / world_size / plain,
-            "stage_kernel_ms": {"combine+x_forward": kms[0], "stray_pairs": kms[1], "y_z": kms[2],
-                                "x_inverse+epilogue": kms[3], "note": "one stage (of 6 per accepted step) over all "
-                                                                      "256 started solves"},
-            "max_abs_dm_batched_vs_plain": worst,
+            "batched": r["batched"], "plain": r["plain"], "batched_over_plain": r["batched_over_plain"],
+            "stage_kernel_ms": r["stage_kernel_ms"],
+            "max_abs_dm_batched_vs_plain": r["max_abs_dm_batched_vs_plain"],
             "e2e": {"value": world_size * upd / t_e2e_max, "unit": "cell-updates/s",
-                    "h2d_bytes_per_step": int(sum(12 * s.cells for s in solves)),
-                    "d2h_bytes_per_step": int(sum(12 * s.cells for s in solves)),
+                    "h2d_bytes_per_step": r["e2e_bytes_each_way"], "d2h_bytes_per_step": r["e2e_bytes_each_way"],
                     "note": "one step = the whole batch: host m0 in, kernel construction, integration, host m out"},
-            "gpu_launches": int(launches),
+            "gpu_launches": r["gpu_launches"],
             "clocks": clocks,
         }
         print(json.dumps(line), flush=True)
@@ -542,13 +628,16 @@ def run_serving(args):
     b = B.Batch(device=local)
     l0 = b.engine.launch_count()
     t0 = time.perf_counter()
-    served = B.Server(b, budget).run(reqs)
+    st_served, st_plain = {}, {}
+    served = B.Server(b, budget).run(reqs, time_limit=args.time_limit, stats=st_served)
     span = time.perf_counter() - t0
     launches = b.engine.launch_count() - l0
     clocks = sampler.stop()
+    del b
     span_max = _max_over_ranks(dist, span, dev)
     t0 = time.perf_counter()
-    plain = B.Server(B.Batch(device=local), budget, max_active=1).run(reqs)
+    plain = B.Server(B.Batch(device=local), budget, max_active=1).run(reqs, time_limit=args.time_limit,
+                                                                      stats=st_plain)
     p_span = time.perf_counter() - t0
     p50, p99 = B.latency_stats(served)
     q50, q99 = B.latency_stats(plain)
@@ -564,10 +653,12 @@ def run_serving(args):
             "ms_per_step": None, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic",
             "config": {"workload": "serving_poisson", "rate_per_s": args.rate, "window_s": args.seconds,
-                       "requests": len(reqs), "budget_gb": args.budget_gb, "method": "DormandPrince 1e-5"},
-            "served": {"p50_s": p50, "p99_s": p99, "makespan_s": span, "cell_updates_per_s": upd / span},
+                       "requests": len(reqs), "budget_gb": args.budget_gb, "method": "DormandPrince 1e-5",
+                       "time_limit_s": args.time_limit},
+            "served": {"p50_s": p50, "p99_s": p99, "makespan_s": span, "cell_updates_per_s": upd / span,
+                       **_serving_summary(st_served)},
             "plain": {"p50_s": q50, "p99_s": q99, "makespan_s": p_span, "solves_per_s": len(plain) / p_span,
-                      "cell_updates_per_s": p_upd / p_span},
+                      "cell_updates_per_s": p_upd / p_span, **_serving_summary(st_plain)},
             "max_abs_dm_served_vs_plain": worst,
             "e2e": {"value": world_size * len(served) / span_max, "unit": "solves/s",
                     "h2d_bytes_per_step": per_req, "d2h_bytes_per_step": per_req,
@@ -581,11 +672,28 @@ def run_serving(args):
         dist.destroy_process_group()
 
 
+def _serving_summary(st):
+    """Counts and queue history of one served run (Server.run stats)."""
+    smp = st.get("samples", [])
+    step = max(1, len(smp) // 40)
+    return {"arrived": st.get("arrived"), "admitted": st.get("admitted"), "finished": st.get("finished"),
+            "still_queued": st.get("still_queued"), "still_running": st.get("still_running"),
+            "max_queued": max((q for _, q, _ in smp), default=0),
+            "max_running": max((r for _, _, r in smp), default=0),
+            "host_admit_s": st.get("host_admit_s"), "host_advance_s": st.get("host_advance_s"),
+            "queue_samples_t_queued_running": smp[::step]}
+
+
 def run_precision(args):
     """Precision form: demag-only field of 1024x1024x4 random unit vectors
-    (padded FFT 2048x2048x8) against the FP64 oracle, per cell
-    |dB| / |B_ref| over cells with |B_ref| > 1e-6 max|B_ref|, and the
-    evaluation rate of the field on the GPU."""
+    (padded FFT 2048x2048x8) against the FP64 oracle, for both arithmetics of
+    the y transforms: the FP32 shared-memory FFT and the TF32 tensor-core DFT
+    GEMMs with 3xTF32 split products.  Per cell |dB| / |B_ref| over cells
+    with |B_ref| > 1e-6 max|B_ref| (max and RMS), and max|dB| / max|B_ref|,
+    against (i) the oracle's own FP64 kernel and (ii) the oracle convolving
+    the GPU's kernel values in FP64 (which isolates the transform arithmetic
+    from the FP64 rounding noise of the two Newell constructions); and the
+    evaluation rate of each form."""
     import torch
 
     import mumaxplus_b200 as mpx
@@ -595,25 +703,37 @@ def run_precision(args):
     world_size, rank, local, dist = _dist_setup()
     w = Wl.precision()
     N = Wl.ncells(w)
-    world, magnet = Wl.build(mpx, w, device=local)
-    eng = magnet._engine
     q = mpx._abi.Q_DEMAG_FIELD
-    shape = (3, *magnet.grid.shape)
-    got = eng.eval(magnet._id, q, shape).astype(np.float64)
-    stream = torch.cuda.Stream(device=local)
-    eng.set_stream(stream.cuda_stream)
-    for _ in range(max(3, args.warmup)):
-        eng.eval_only(magnet._id, q)
-    e0 = torch.cuda.Event(enable_timing=True)
-    e1 = torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    for _ in range(args.steps):
-        eng.eval_only(magnet._id, q)
-    e1.record(stream)
-    torch.cuda.synchronize(local)
-    ms = e0.elapsed_time(e1) / args.steps
-    ms = _max_over_ranks(dist, ms, torch.device("cuda", local))
-    kms = eng.profile_eval(magnet._id, reps=5)
+    forms = {}
+    kernel_oct = None
+    for dft in ("fp32", "tf32x3"):
+        world, magnet = Wl.build(mpx, w, device=local, demag_dft=dft)
+        eng = magnet._engine
+        shape = (3, *magnet.grid.shape)
+        got = eng.eval(magnet._id, q, shape).astype(np.float64)
+        stream = torch.cuda.Stream(device=local)
+        eng.set_stream(stream.cuda_stream)
+        for _ in range(max(3, args.warmup)):
+            eng.eval_only(magnet._id, q)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(args.steps):
+            eng.eval_only(magnet._id, q)
+        e1.record(stream)
+        torch.cuda.synchronize(local)
+        ms = _max_over_ranks(dist, e0.elapsed_time(e1) / args.steps, torch.device("cuda", local))
+        kms = eng.profile_eval(magnet._id, reps=5)
+        if kernel_oct is None and rank == 0:
+            K = eng.demag_kernel(magnet._id)
+            nx, ny, nz = w["size"]
+            o = [K.shape[3] - nx, K.shape[2] - ny, K.shape[1] - nz]
+            kernel_oct = K[:, o[2]:, o[1]:, o[0]:].astype(np.float64)
+            del K
+        forms[dft] = {"field": got, "ms": ms, "kernel_ms": {"x_forward": kms[0], "y_z": kms[1], "x_inverse": kms[2]},
+                      "timeouts": mpx._engine.Engine.tc_timeouts()}
+        eng.synchronize()
+        del world, magnet, eng
     if rank == 0:
         keep = []
         ow = O.OracleWorld()
@@ -622,44 +742,44 @@ def run_precision(args):
         t0 = time.time()
         want = ow.eval(oq, O.abi.Q_DEMAG_FIELD)
         t_oracle = time.time() - t0
-        nref = np.linalg.norm(want, axis=0)
-        mask = nref > 1e-6 * nref.max()
-        rel = np.linalg.norm(got - want, axis=0)[mask] / nref[mask]
-        # the same FP64 convolution with the GPU's own kernel values: separates the
-        # FP32 FFT arithmetic from the FP64 rounding noise of the two kernel
-        # constructions, which dominates far from the source (newell.cu's
-        # 27-point differences of O(r^3) terms cancel to O(r^-3) values)
-        K = eng.demag_kernel(magnet._id)
-        nx, ny, nz = w["size"]
-        o = [K.shape[3] - nx, K.shape[2] - ny, K.shape[1] - nz]
-        oct = K[:, o[2]:, o[1]:, o[0]:].astype(np.float64)
-        del K
+        del ow
         ow2 = O.OracleWorld()
         oq2 = ow2.add_magnet(Wl.desc(w, keep))
         ow2.set_m(oq2, w["m0"]())
-        ow2.set_kernel_octant(oq2, oct)
+        ow2.set_kernel_octant(oq2, kernel_oct)
         want2 = ow2.eval(oq2, O.abi.Q_DEMAG_FIELD)
-        nref2 = np.linalg.norm(want2, axis=0)
-        mask2 = nref2 > 1e-6 * nref2.max()
-        rel2 = np.linalg.norm(got - want2, axis=0)[mask2] / nref2[mask2]
+        del ow2, kernel_oct
+
+        def errs(got, ref):
+            nref = np.linalg.norm(ref, axis=0)
+            mask = nref > 1e-6 * nref.max()
+            rel = np.linalg.norm(got - ref, axis=0)[mask] / nref[mask]
+            return {"max_relative_error": float(rel.max()), "rms_relative_error": float(np.sqrt(np.mean(rel * rel))),
+                    "max_abs_error_over_max_field": float(np.abs(got - ref).max() / np.abs(ref).max()),
+                    "cells_compared": int(mask.sum())}
+
+        report = {}
+        for dft, f in forms.items():
+            report[dft] = {"vs_fp64_own_kernel": errs(f["field"], want),
+                           "vs_fp64_same_kernel": errs(f["field"], want2),
+                           "ms_per_eval": f["ms"], "evals_per_s": world_size * 1e3 / f["ms"],
+                           "cell_evals_per_s": world_size * N * 1e3 / f["ms"], "kernel_ms": f["kernel_ms"],
+                           "tensor_core_wait_timeouts": f["timeouts"]}
+        report["tf32x3_vs_fp32_gpu"] = errs(forms["tf32x3"]["field"], forms["fp32"]["field"])
+        tc = report["tf32x3"]
         line = {
-            "metric": "B_demag max relative error vs FP64", "value": float(rel.max()), "unit": "relative",
-            "n_gpus": world_size, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
-            "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": w["name"], "fft_padding": "2048x2048x8", "dft": "FP32 shared-memory Stockham",
-                       "cells_compared": int(mask.sum())},
-            "rms_relative_error": float(np.sqrt(np.mean(rel * rel))),
-            "max_abs_error_over_max_field": float(np.abs(got - want).max() / np.abs(want).max()),
-            "same_kernel": {"max_relative_error": float(rel2.max()),
-                            "rms_relative_error": float(np.sqrt(np.mean(rel2 * rel2))),
-                            "max_abs_error_over_max_field": float(np.abs(got - want2).max() / np.abs(want2).max()),
-                            "note": "FP64 oracle convolution with the GPU's FP64 kernel values (rounded to FP32)"},
-            "evals_per_s": world_size * 1e3 / ms, "cell_evals_per_s": world_size * N * 1e3 / ms,
-            "kernel_ms": {"k_xfwd": kms[0], "k_yz": kms[1], "k_xinv": kms[2]},
+            "metric": "B_demag max relative error vs FP64", "value": tc["vs_fp64_same_kernel"]["max_relative_error"],
+            "unit": "relative", "n_gpus": world_size, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": tc["ms_per_eval"], "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+            "dtype": "tf32x3 (y DFT) / f32", "data": "synthetic",
+            "config": {"workload": w["name"], "fft_padding": "2048x2048x8",
+                       "dft": "y stages: TF32 tensor-core GEMMs with 3xTF32 split (tcgen05); x stages FP32 FFT",
+                       "value_is": "TF32x3 form vs the FP64 oracle convolving the same kernel values"},
+            "forms": report,
             "oracle_seconds": t_oracle,
-            "e2e": {"value": float(rel.max()), "unit": "relative", "h2d_bytes_per_step": 12 * N,
-                    "d2h_bytes_per_step": 12 * N},
-            "gpu_launches": 3 * args.steps,
+            "e2e": {"value": tc["vs_fp64_same_kernel"]["max_relative_error"], "unit": "relative",
+                    "h2d_bytes_per_step": 12 * N, "d2h_bytes_per_step": 12 * N},
+            "gpu_launches": 5 * args.steps,
         }
         print(json.dumps(line), flush=True)
     if dist is not None:

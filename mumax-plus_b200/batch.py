@@ -277,9 +277,14 @@ class Server:
         self.prefetch = prefetch
         self.pool = concurrent.futures.ThreadPoolExecutor(max_workers=workers)
 
-    def run(self, requests, torque_stop=0.0, fetch=True, time_limit=None):
+    def run(self, requests, torque_stop=0.0, fetch=True, time_limit=None, stats=None):
         """Serve `requests` (sorted by arrival) and return the finished solves,
-        each with arrival, t_admit and t_done (seconds since the stream start)."""
+        each with arrival, t_admit and t_done (seconds since the stream start).
+        With `time_limit` (seconds) the loop stops there, requests still queued
+        or running unfinished.  `stats`, a dict, receives the counts of
+        arrived, admitted and finished requests, the host seconds spent
+        admitting (add + start) and advancing (advance + poll), and samples
+        (seconds, queued, running) about every 0.5 s."""
         reqs = sorted(enumerate(requests), key=lambda kv: kv[1]["arrival"])
         m0 = {}
         nxt_gen = 0
@@ -297,9 +302,16 @@ class Server:
         nxt = 0
         pacer = _Pacer()
         b = self.batch
+        admitted = 0
+        t_admit = t_adv = 0.0
+        samples = []
+        t_sample = 0.0
         t0 = time.perf_counter()
         while nxt < len(reqs) or queue or b.solves:
             now = time.perf_counter() - t0
+            if now >= t_sample:
+                samples.append((round(now, 3), len(queue), len(b.solves)))
+                t_sample = now + 0.5
             if time_limit is not None and now > time_limit:
                 break
             while nxt < len(reqs) and reqs[nxt][1]["arrival"] <= now:
@@ -315,10 +327,14 @@ class Server:
                 if self.max_active is not None and len(b.solves) >= self.max_active:
                     break
                 queue.popleft()
-                s = b.add(w, key=k, m0=m0.pop(k).result())
+                m0k = m0.pop(k).result()
+                ta = time.perf_counter()
+                s = b.add(w, key=k, m0=m0k)
                 s.arrival = w["arrival"]
                 s.t_admit = time.perf_counter() - t0
                 b.start(s, w["duration"], torque_stop)
+                t_admit += time.perf_counter() - ta
+                admitted += 1
             if not b.solves:
                 if nxt < len(reqs):  # idle until the next arrival
                     time.sleep(max(0.0, reqs[nxt][1]["arrival"] - (time.perf_counter() - t0)))
@@ -328,10 +344,15 @@ class Server:
             b.advance(n)
             done, _ = b.poll()
             pacer.update(n, time.perf_counter() - ta)
+            t_adv += time.perf_counter() - ta
             for s in done:
                 b.finish(s, fetch=fetch)
                 s.t_done = time.perf_counter() - t0
                 finished.append(s)
+        if stats is not None:
+            stats.update(arrived=nxt, admitted=admitted, finished=len(finished), still_queued=len(queue),
+                         still_running=len(b.solves), host_admit_s=t_admit, host_advance_s=t_adv,
+                         wall_s=time.perf_counter() - t0, samples=samples)
         return finished
 
 

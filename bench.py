@@ -51,6 +51,8 @@ def parse():
     ap.add_argument("--budget-gb", type=float, default=150.0, help="serving: device-memory budget")
     ap.add_argument("--time-limit", type=float, default=None,
                     help="serving: wall-clock limit of each served run (s); unfinished requests are reported")
+    ap.add_argument("--max-cells", type=float, default=None,
+                    help="serving: also run the served form with admission capped at this many resident cells")
     return ap.parse_args()
 
 
@@ -635,6 +637,18 @@ def run_serving(args):
     clocks = sampler.stop()
     del b
     span_max = _max_over_ranks(dist, span, dev)
+    capped = None
+    if args.max_cells:
+        st_cap = {}
+        t0 = time.perf_counter()
+        served_cap = B.Server(B.Batch(device=local), budget, max_cells=args.max_cells).run(
+            reqs, time_limit=args.time_limit, stats=st_cap)
+        c_span = time.perf_counter() - t0
+        c50, c99 = B.latency_stats(served_cap)
+        c_upd = sum(s.cells * s.steps for s in served_cap)
+        capped = {"max_cells": args.max_cells, "p50_s": c50, "p99_s": c99, "makespan_s": c_span,
+                  "solves_per_s": len(served_cap) / c_span, "cell_updates_per_s": c_upd / c_span,
+                  **_serving_summary(st_cap)}
     t0 = time.perf_counter()
     plain = B.Server(B.Batch(device=local), budget, max_active=1).run(reqs, time_limit=args.time_limit,
                                                                       stats=st_plain)
@@ -659,6 +673,7 @@ def run_serving(args):
                        **_serving_summary(st_served)},
             "plain": {"p50_s": q50, "p99_s": q99, "makespan_s": p_span, "solves_per_s": len(plain) / p_span,
                       "cell_updates_per_s": p_upd / p_span, **_serving_summary(st_plain)},
+            "served_cell_capped": capped,
             "max_abs_dm_served_vs_plain": worst,
             "e2e": {"value": world_size * len(served) / span_max, "unit": "solves/s",
                     "h2d_bytes_per_step": per_req, "d2h_bytes_per_step": per_req,

@@ -221,6 +221,11 @@ mpx_status mpx_engine_set_world_bias(mpx_engine* e, const double b[3]);
 mpx_status mpx_engine_memory(mpx_engine* e, int64_t* bytes);
 /* Number of kernels this engine has launched since creation. */
 mpx_status mpx_engine_launch_count(mpx_engine* e, int64_t* count);
+/* No counterpart in the reference.  How often the CUDA graphs of one attempt
+ * were instantiated anew and how often an existing one was updated in place
+ * (a solve that starts or finishes changes only the launch sizes and tables,
+ * so the graph is updated rather than rebuilt). */
+mpx_status mpx_engine_graph_stats(mpx_engine* e, int64_t* instantiations, int64_t* updates);
 
 /* ---- solve groups: magnets that share one time and time step ----------- */
 mpx_status mpx_group_create(mpx_engine* e, int* group);

@@ -162,6 +162,7 @@ SIGNATURES = {
     "mpx_engine_set_world_bias": (I, [E, P_D]),
     "mpx_engine_memory": (I, [E, P_I64]),
     "mpx_engine_launch_count": (I, [E, P_I64]),
+    "mpx_engine_graph_stats": (I, [E, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]),
     "mpx_group_create": (I, [E, P_I]),
     "mpx_group_destroy": (I, [E, I]),
     "mpx_group_info_get": (I, [E, I, C.POINTER(GroupInfo)]),

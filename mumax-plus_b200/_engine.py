@@ -96,6 +96,12 @@ class Engine:
         check(lib().mpx_engine_memory(self._h, C.byref(v)))
         return v.value
 
+    def graph_stats(self):
+        """(instantiations, in-place updates) of the attempt graphs."""
+        a, b = C.c_int64(), C.c_int64()
+        check(lib().mpx_engine_graph_stats(self._h, C.byref(a), C.byref(b)))
+        return a.value, b.value
+
     def launch_count(self):
         v = C.c_int64()
         check(lib().mpx_engine_launch_count(self._h, C.byref(v)))

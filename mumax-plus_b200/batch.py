@@ -270,10 +270,16 @@ class Server:
     magnetization to the host and free their memory.  Initial magnetizations
     are generated ahead of arrival on host threads (client-side data)."""
 
-    def __init__(self, batch, budget_bytes, max_active=None, prefetch=32, workers=4):
+    def __init__(self, batch, budget_bytes, max_active=None, prefetch=32, workers=4, max_cells=None):
+        """`max_cells` (optional): admit only while the resident solves hold
+        at most this many cells, i.e. bound the device work of one attempt,
+        so that under overload the admitted solves keep finishing instead of
+        all sharing the device (the memory budget alone admits everything
+        that fits)."""
         self.batch = batch
         self.budget = int(budget_bytes)
         self.max_active = max_active
+        self.max_cells = max_cells
         self.prefetch = prefetch
         self.pool = concurrent.futures.ThreadPoolExecutor(max_workers=workers)
 
@@ -325,6 +331,9 @@ class Server:
                 if b.resident + res + tr > self.budget and b.solves:
                     break
                 if self.max_active is not None and len(b.solves) >= self.max_active:
+                    break
+                if (self.max_cells is not None and b.solves
+                        and sum(x.cells for x in b.solves.values()) + workloads.ncells(w) > self.max_cells):
                     break
                 queue.popleft()
                 m0k = m0.pop(k).result()

@@ -119,19 +119,25 @@ __device__ __forceinline__ void split_tf32(float a, float& hi, float& lo) {
   lo = __uint_as_float(l);
 }
 
+__device__ __forceinline__ float2 cmul(float2 a, float2 b) {
+  return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+
 }  // namespace tc
 
 // Shared-memory plan of k_ydft_tc (bytes).  B: the 64 x 64 DFT32 real form,
 // hi and lo (K-major, LBO 1024).  A: the operand of one stage, hi and lo, 128
 // rows x 64 K (16 chunks, LBO padded to 2064).  Twiddles: W1024^{ab} as
-// [b][a] (1024) and W2048^k (1024, R = 2 only).
+// [b][a] (1024), and for R = 2 the factors of W2048^(c + 32 d) =
+// W2048^c W64^d (32 + 32).  107,840 bytes: two blocks per SM.
 constexpr int TC_ROWS = 128;
 constexpr int TC_B_BYTES = 64 * 64 * 4;                 // one of hi / lo
 constexpr int TC_B_LBO = 8 * 128;                       // 64 rows / 8 x 128 B
 constexpr int TC_A_LBO = (TC_ROWS / 8) * 128 + 16;      // 2064
 constexpr int TC_A_BYTES = 16 * TC_A_LBO;               // 64 K = 16 chunks (33,024 B)
-constexpr int TC_SMEM = 2 * TC_B_BYTES + 2 * TC_A_BYTES + 2 * 1024 * 8 + 64;
+constexpr int TC_SMEM = 2 * TC_B_BYTES + 2 * TC_A_BYTES + (1024 + 64) * 8 + 64;
 constexpr int TC_TMEM_COLS = 128;
+constexpr int TC_BLOCKS_PER_SM = 2;
 
 // Byte offset of element (row, k) in a K-major no-swizzle tile with LBO `lbo`.
 __host__ __device__ constexpr int tc_off(int row, int k, int lbo) {
@@ -160,7 +166,7 @@ __device__ __forceinline__ void tc_stage(uint32_t d, uint32_t a_hi, uint32_t a_l
 // dftB: the DFT32 real form, hi then lo, each 64 x 64 floats row-major [n][k].
 // Grid: persistent, blocks loop over the work items.
 template <int DIR>
-__global__ void __launch_bounds__(128, 1)
+__global__ void __launch_bounds__(128, TC_BLOCKS_PER_SM)
     k_ydft_tc(const MagnetDev* __restrict__ mags, const GroupDev* __restrict__ groups, const Work* __restrict__ work,
               int nwork, int stage, int gate, const float* __restrict__ dftB) {
   extern __shared__ __align__(1024) unsigned char tsm[];
@@ -169,8 +175,9 @@ __global__ void __launch_bounds__(128, 1)
   unsigned char* sAh = sBl + TC_B_BYTES;
   unsigned char* sAl = sAh + TC_A_BYTES;
   float2* tw1 = reinterpret_cast<float2*>(sAl + TC_A_BYTES);  // W1024^{ab} at [b * 32 + a]
-  float2* tw2 = tw1 + 1024;                                    // W2048^k
-  unsigned long long* mbar = reinterpret_cast<unsigned long long*>(tw2 + 1024);
+  float2* twc = tw1 + 1024;                                    // W2048^c, c < 32
+  float2* twd = twc + 32;                                      // W64^d, d < 32
+  unsigned long long* mbar = reinterpret_cast<unsigned long long*>(twd + 32);
   uint32_t* tbase = reinterpret_cast<uint32_t*>(mbar + 1);
   __shared__ MagnetDev M;
   __shared__ GroupDev G;
@@ -187,8 +194,11 @@ __global__ void __launch_bounds__(128, 1)
     double sd, cd;
     sincospi(-2.0 * (double)(a * b) / 1024.0, &sd, &cd);
     tw1[e] = make_float2((float)cd, (float)sd);
-    sincospi(-2.0 * (double)e / 2048.0, &sd, &cd);
-    tw2[e] = make_float2((float)cd, (float)sd);
+  }
+  if (tid < 64) {
+    double sd, cd;
+    sincospi(tid < 32 ? -2.0 * tid / 2048.0 : -2.0 * (tid - 32) / 64.0, &sd, &cd);
+    twc[tid] = make_float2((float)cd, (float)sd);  // twd follows twc
   }
   if (tid == 0) tc::mbar_init(mbar);
   if (warp == 0) {
@@ -251,28 +261,34 @@ __global__ void __launch_bounds__(128, 1)
       // inverse: with Y = conj(T), z[k] = Y[k] + Y[k+1024] (p = 0) or
       // (Y[k] - Y[k+1024]) W2048^k (p = 1) for R = 2, Y[k] for R = 1, at
       // k = a + 32 b, b < 32
-#pragma unroll 2
-      for (int j = 0; j < 16; ++j) {
+      const float2 wa = twc[a];  // W2048^(a + 32 b) = W2048^a W64^b
+#pragma unroll
+      for (int half = 0; half < 2; ++half) {
+        // the 32 loads of 16 inputs (both halves of the transform) issued together
+        float2 t0[16], t1[16];
+#pragma unroll
+        for (int jj = 0; jj < 16; ++jj) {
+          const int k = a + 32 * (16 * half + jj);
+          const bool ok = live && span_ok(k + (size_t)(R - 1) * 1024, tleft);
+          t0[jj] = ok ? __ldg(T + k) : make_float2(0.f, 0.f);
+          t1[jj] = (ok && R == 2) ? __ldg(T + k + 1024) : make_float2(0.f, 0.f);
+        }
+#pragma unroll
+        for (int j8 = 0; j8 < 8; ++j8) {
+        const int j = 8 * half + j8;
         float v[4];
 #pragma unroll
         for (int h = 0; h < 2; ++h) {
-          const int k = a + 32 * (2 * j + h);
-          float2 z = make_float2(0.f, 0.f);
-          if (live && span_ok(k + (size_t)(R - 1) * 1024, tleft)) {
-            const float2 t0 = __ldg(T + k);
-            const float2 y0 = make_float2(t0.x, -t0.y);
-            if (R == 1) {
-              z = y0;
-            } else {
-              const float2 t1 = __ldg(T + k + 1024);
-              if (p == 0) {
-                z = make_float2(y0.x + t1.x, y0.y - t1.y);
-              } else {
-                const float2 d = make_float2(y0.x - t1.x, y0.y + t1.y);
-                const float2 w = tw2[k];
-                z = make_float2(d.x * w.x - d.y * w.y, d.x * w.y + d.y * w.x);
-              }
-            }
+          const int jj = 2 * j8 + h;
+          const float2 y0 = make_float2(t0[jj].x, -t0[jj].y);
+          float2 z;
+          if (R == 1) {
+            z = y0;
+          } else if (p == 0) {
+            z = make_float2(y0.x + t1[jj].x, y0.y - t1[jj].y);
+          } else {
+            const float2 d = make_float2(y0.x - t1[jj].x, y0.y + t1[jj].y);
+            z = tc::cmul(d, tc::cmul(wa, twd[2 * j + h]));
           }
           v[2 * h] = z.x;
           v[2 * h + 1] = z.y;
@@ -284,6 +300,7 @@ __global__ void __launch_bounds__(128, 1)
         tc::split_tf32(v[3], hi.w, lo.w);
         *reinterpret_cast<float4*>(sAh + tc_off(row, 4 * j, TC_A_LBO)) = hi;
         *reinterpret_cast<float4*>(sAl + tc_off(row, 4 * j, TC_A_LBO)) = lo;
+        }
       }
     }
     tc::fence_async_smem();
@@ -352,10 +369,7 @@ __global__ void __launch_bounds__(128, 1)
           const int k = c + 32 * dd;
           float2 x = make_float2(v[2 * h], v[2 * h + 1]);
           if (R == 2) {
-            if (p == 1) {
-              const float2 w = tw2[k];
-              x = make_float2(x.x * w.x - x.y * w.y, x.x * w.y + x.y * w.x);
-            }
+            if (p == 1) x = tc::cmul(x, tc::cmul(twc[c], twd[dd]));  // W2048^(c + 32 dd)
             const float ox = __shfl_xor_sync(0xffffffffu, x.x, 1);
             const float oy = __shfl_xor_sync(0xffffffffu, x.y, 1);
             x = p == 0 ? make_float2(x.x + ox, x.y + oy) : make_float2(ox - x.x, oy - x.y);

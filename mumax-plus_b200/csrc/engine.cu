@@ -259,6 +259,7 @@ struct mpx_engine {
   cudaGraphExec_t graph = nullptr, graph_nok0 = nullptr;
   int graph_method = -1;
   bool graph_dirty = true;
+  int64_t graph_instantiations = 0, graph_updates = 0;  // attempt graphs built anew / updated in place
   bool need_stage0 = true;  // some started group may lack a valid k0
 };
 
@@ -475,7 +476,7 @@ int zmul_smem(const Magnet* m) { return (3 * m->nkz * plen(m->P[2]) + m->P[2]) *
 // The three passes of the split y/z path (radix-8 forms when the lengths allow);
 // magnets with the tensor-core y transforms take k_ydft_tc (work list tcw)
 // instead of k_ycols.
-constexpr int TC_GRID_PER_SM = 1;
+constexpr int TC_GRID_PER_SM = TC_BLOCKS_PER_SM;
 mpx_status launch_split(mpx_engine* e, const Work* ycw, int nyc, const Work* zmw, int nzm, int smem_y, int smem_z,
                         int max_py, int max_pz, int stage, int gate, const Work* tcw = nullptr, int ntc = 0) {
   if (nyc <= 0 && ntc <= 0) return MPX_OK;
@@ -1491,11 +1492,12 @@ mpx_status prepare_run(mpx_engine* e, int method) {
 }
 
 // Captures one attempt (from `first_stage` on) as an executable graph.
+// Captures one attempt into *out.  When *out already holds an attempt graph of
+// the same shape (the same kernels in the same order; a solve that arrives or
+// finishes changes only grid sizes and table pointers), the executable graph
+// is updated in place (cudaGraphExecUpdate) instead of being instantiated
+// again.
 mpx_status capture_attempt(mpx_engine* e, const TableauDev& T, int first_stage, cudaGraphExec_t* out) {
-  if (*out) {
-    cudaGraphExecDestroy(*out);
-    *out = nullptr;
-  }
   cudaGraph_t g = nullptr;
   CUDA_TRY(cudaStreamBeginCapture(e->stream, cudaStreamCaptureModeThreadLocal));
   const int64_t before = e->launches;
@@ -1507,7 +1509,19 @@ mpx_status capture_attempt(mpx_engine* e, const TableauDev& T, int first_stage, 
     return st;
   }
   if (ce != cudaSuccess) return fail(MPX_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(ce));
+  if (*out) {
+    cudaGraphExecUpdateResultInfo info;
+    if (cudaGraphExecUpdate(*out, g, &info) == cudaSuccess) {
+      cudaGraphDestroy(g);
+      e->graph_updates++;
+      return MPX_OK;
+    }
+    (void)cudaGetLastError();  // the update was refused: instantiate anew
+    cudaGraphExecDestroy(*out);
+    *out = nullptr;
+  }
   ce = cudaGraphInstantiate(out, g, 0);
+  e->graph_instantiations++;
   cudaGraphDestroy(g);
   if (ce != cudaSuccess) return fail(MPX_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(ce));
   return MPX_OK;
@@ -1830,6 +1844,13 @@ mpx_status mpx_engine_set_world_bias(mpx_engine* e, const double b[3]) {
 mpx_status mpx_engine_memory(mpx_engine* e, int64_t* bytes) {
   if (!e || !bytes) return fail(MPX_ERR_INVALID, "null argument");
   *bytes = e->bytes;
+  return MPX_OK;
+}
+
+mpx_status mpx_engine_graph_stats(mpx_engine* e, int64_t* instantiations, int64_t* updates) {
+  if (!e || !instantiations || !updates) return fail(MPX_ERR_INVALID, "null engine / output");
+  *instantiations = e->graph_instantiations;
+  *updates = e->graph_updates;
   return MPX_OK;
 }
 

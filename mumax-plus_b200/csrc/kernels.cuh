@@ -916,9 +916,34 @@ __device__ __forceinline__ bool lean_ok(const MagnetDev& M) {
   return M.fast && !M.geom && (M.mg[0] == 0 || (off >= 0 && off + M.n[0] <= M.mg[0]));
 }
 
+// Contribution of neighbour r (0..5: x-, x+, y-, y+, z-, z+) of a cell with
+// state mc to its exchange (he) and DMI (hd) sums on the lean path; `present`:
+// the neighbour exists (its state mn), else the Neumann ghost or nothing.
+// INNER: every neighbour is present (the ghost-cell code is left out).
+template <bool INNER>
+__device__ __forceinline__ void neighbour_term(const MagnetDev& M, int r, bool present, float3 mn, float3 mc,
+                                               bool neumann, bool dmi_open, bool do_exch, bool do_dmi, float3& he,
+                                               float3& hd) {
+  const int axis = r >> 1;
+  const int d = (r & 1) ? 1 : -1;
+  const bool nin = INNER || present;
+  float3 m_ = nin ? mn : mc;
+  if (!INNER && !nin && neumann) {  // ghost cell m + Gamma/(2A) delta
+    const float3 Gm = gamma_uniform(M.fd, axis, mc);
+    m_ = mc + (d * M.cs[axis]) * (M.finv_2a * Gm);
+  }
+  if (do_exch && (nin || neumann)) he = he + M.fe[axis] * (m_ - mc);
+  if (do_dmi && (nin || !dmi_open)) {
+    const float Dxy = M.fd[3 * axis], Dxz = M.fd[3 * axis + 1], Dyz = M.fd[3 * axis + 2];
+    const float inv_delta = d * M.inv_cs[axis];
+    hd.x += (Dxy * m_.y + Dxz * m_.z) * inv_delta;
+    hd.y += (-Dxy * m_.x + Dyz * m_.z) * inv_delta;
+    hd.z += (-Dxz * m_.x - Dyz * m_.y) * inv_delta;
+  }
+}
+
 // Exchange and DMI sums over the six neighbours nb[] (-1: none) of the lean
-// path, in the order of local_terms_fast.  INNER: every neighbour is present
-// (the ghost-cell code of the Neumann boundary is left out).
+// path, in the order of local_terms_fast.
 template <bool INNER>
 __device__ __forceinline__ void neighbour_sums(const MagnetDev& M, const float* __restrict__ m, int N, const int (&nb)[6],
                                                float3 mc, bool neumann, bool dmi_open, bool do_exch, bool do_dmi,
@@ -927,24 +952,33 @@ __device__ __forceinline__ void neighbour_sums(const MagnetDev& M, const float* 
 #pragma unroll
   for (int r = 0; r < 6; ++r) mn[r] = (INNER || nb[r] >= 0) ? ldg3(m, N, nb[r]) : mc;
 #pragma unroll
-  for (int r = 0; r < 6; ++r) {
-    const int axis = r >> 1;
-    const int d = (r & 1) ? 1 : -1;
-    const bool nin = INNER || nb[r] >= 0;
-    float3 m_ = mn[r];
-    if (!INNER && !nin && neumann) {  // ghost cell m + Gamma/(2A) delta
-      const float3 Gm = gamma_uniform(M.fd, axis, mc);
-      m_ = mc + (d * M.cs[axis]) * (M.finv_2a * Gm);
-    }
-    if (do_exch && (nin || neumann)) he = he + M.fe[axis] * (m_ - mc);
-    if (do_dmi && (nin || !dmi_open)) {
-      const float Dxy = M.fd[3 * axis], Dxz = M.fd[3 * axis + 1], Dyz = M.fd[3 * axis + 2];
-      const float inv_delta = d * M.inv_cs[axis];
-      hd.x += (Dxy * m_.y + Dxz * m_.z) * inv_delta;
-      hd.y += (-Dxy * m_.x + Dyz * m_.z) * inv_delta;
-      hd.z += (-Dxz * m_.x - Dyz * m_.y) * inv_delta;
-    }
+  for (int r = 0; r < 6; ++r)
+    neighbour_term<INNER>(M, r, nb[r] >= 0, mn[r], mc, neumann, dmi_open, do_exch, do_dmi, he, hd);
+}
+
+// The rest of a lean-path cell once its exchange / DMI sums are known:
+// anisotropy, applied field, demag, the sum in local_terms_fast's order and the
+// torque of epilogue_cell.  `ext` is the applied field of the cell.
+__device__ __forceinline__ float3 finish_cell_lean(const MagnetDev& M, const GroupDev& G, float3 mc, float3 he,
+                                                   float3 hd, float3 ext, float3 bdemag) {
+  const unsigned terms = M.terms;
+  float3 exch = f3(0, 0, 0), dmi = f3(0, 0, 0), anis = f3(0, 0, 0);
+  if (terms & TERM_EXCH) exch = M.finv_ms * he;
+  if (terms & TERM_DMI) dmi = M.finv_ms * hd;
+  if ((terms & TERM_ANIS) && (terms & FLAG_CUBIC)) {
+    anis = cubic_field(mc, f3(M.fc[0][0], M.fc[0][1], M.fc[0][2]), f3(M.fc[1][0], M.fc[1][1], M.fc[1][2]),
+                       f3(M.fc[2][0], M.fc[2][1], M.fc[2][2]), M.fkc[0], M.fkc[1], M.fkc[2], M.finv_ms);
+  } else if (terms & TERM_ANIS) {
+    const float3 u = f3(M.fu[0], M.fu[1], M.fu[2]);
+    const float mu = dot3(mc, u);
+    anis = M.finv_ms * ((2 * M.fk1 * mu + 4 * M.fk2 * mu * mu * mu) * u);
   }
+  float3 h = exch;
+  h = h + anis;
+  h = h + ext;
+  h = h + dmi;
+  h = h + bdemag;
+  return G.torque_kind ? damping_torque(mc, h) : llg_torque(mc, h, M.alpha.u);
 }
 
 // Right-hand side of one cell of a stage on the lean path: the arithmetic of
@@ -957,7 +991,7 @@ __device__ __forceinline__ float3 stage_cell_lean(const MagnetDev& M, const Grou
   if (M.frozen.u != 0.0f) return f3(0.f, 0.f, 0.f);
   const unsigned terms = M.terms;
   const float3 mc = ldg3(m, N, i);
-  float3 exch = f3(0, 0, 0), dmi = f3(0, 0, 0), anis = f3(0, 0, 0), ext = f3(0, 0, 0);
+  float3 he = f3(0, 0, 0), hd = f3(0, 0, 0);
   const bool openbc = (terms & FLAG_OPENBC) != 0;
   const bool do_exch = (terms & TERM_EXCH) != 0;
   const bool do_dmi = (terms & TERM_DMI) != 0;
@@ -974,24 +1008,14 @@ __device__ __forceinline__ float3 stage_cell_lean(const MagnetDev& M, const Grou
       const int b = T.r[yl][q];
       nb[2 + q] = b >= 0 ? b + x : -1;
     }
-    float3 he = f3(0, 0, 0), hd = f3(0, 0, 0);
     const bool inner = nb[0] >= 0 && nb[1] >= 0 && nb[2] >= 0 && nb[3] >= 0 && nb[4] >= 0 && nb[5] >= 0;
     if (__all_sync(__activemask(), inner)) {  // every neighbour present: no ghost cells
       neighbour_sums<true>(M, m, N, nb, mc, neumann, dmi_open, do_exch, do_dmi, he, hd);
     } else {
       neighbour_sums<false>(M, m, N, nb, mc, neumann, dmi_open, do_exch, do_dmi, he, hd);
     }
-    if (do_exch) exch = M.finv_ms * he;
-    if (do_dmi) dmi = M.finv_ms * hd;
   }
-  if ((terms & TERM_ANIS) && (terms & FLAG_CUBIC)) {
-    anis = cubic_field(mc, f3(M.fc[0][0], M.fc[0][1], M.fc[0][2]), f3(M.fc[1][0], M.fc[1][1], M.fc[1][2]),
-                       f3(M.fc[2][0], M.fc[2][1], M.fc[2][2]), M.fkc[0], M.fkc[1], M.fkc[2], M.finv_ms);
-  } else if (terms & TERM_ANIS) {
-    const float3 u = f3(M.fu[0], M.fu[1], M.fu[2]);
-    const float mu = dot3(mc, u);
-    anis = M.finv_ms * ((2 * M.fk1 * mu + 4 * M.fk2 * mu * mu * mu) * u);
-  }
+  float3 ext = f3(0, 0, 0);
   if (terms & TERM_EXT) {
     ext = f3(M.fb[0], M.fb[1], M.fb[2]);
     if (terms & FLAG_STRAY) {
@@ -999,15 +1023,135 @@ __device__ __forceinline__ float3 stage_cell_lean(const MagnetDev& M, const Grou
       ext = f3(ext.x + s.x, ext.y + s.y, ext.z + s.z);
     }
   }
-  float3 h = exch;
-  h = h + anis;
-  h = h + ext;
-  h = h + dmi;
-  h = h + bdemag;
-  float3 k = G.torque_kind ? damping_torque(mc, h) : llg_torque(mc, h, M.alpha.u);
+  float3 k = finish_cell_lean(M, G, mc, he, hd, ext, bdemag);
   if (!G.torque_kind && (terms & (FLAG_STT_ZL | FLAG_STT_SL))) k = k + stt_torque(M, m, x, y, z, i, mc);
   if (terms & FLAG_THERMAL) k = k + thermal_term(M, i, G.steps, G.dt);
   return k;
+}
+
+// Four consecutive cells i0 .. i0 + 3 (i0 a multiple of 4, buffers 16-byte
+// aligned) of a SoA field: three 16-byte loads.
+__device__ __forceinline__ void ld4x3(const float* __restrict__ a, int N, int i0, float3 (&v)[4]) {
+  if (!cell_ok(N, i0) || !cell_ok(N, i0 + 3)) {
+#pragma unroll
+    for (int q = 0; q < 4; ++q) v[q] = f3(0.f, 0.f, 0.f);
+    return;
+  }
+  const float4 x = *reinterpret_cast<const float4*>(a + i0);
+  const float4 y = *reinterpret_cast<const float4*>(a + N + i0);
+  const float4 z = *reinterpret_cast<const float4*>(a + 2 * N + i0);
+  v[0] = f3(x.x, y.x, z.x);
+  v[1] = f3(x.y, y.y, z.y);
+  v[2] = f3(x.z, y.z, z.z);
+  v[3] = f3(x.w, y.w, z.w);
+}
+__device__ __forceinline__ void ldg4x3(const float* __restrict__ a, int N, int i0, float3 (&v)[4]) {
+  if (!cell_ok(N, i0) || !cell_ok(N, i0 + 3)) {
+#pragma unroll
+    for (int q = 0; q < 4; ++q) v[q] = f3(0.f, 0.f, 0.f);
+    return;
+  }
+  const float4 x = __ldg(reinterpret_cast<const float4*>(a + i0));
+  const float4 y = __ldg(reinterpret_cast<const float4*>(a + N + i0));
+  const float4 z = __ldg(reinterpret_cast<const float4*>(a + 2 * N + i0));
+  v[0] = f3(x.x, y.x, z.x);
+  v[1] = f3(x.y, y.y, z.y);
+  v[2] = f3(x.z, y.z, z.z);
+  v[3] = f3(x.w, y.w, z.w);
+}
+__device__ __forceinline__ void st4x3(float* a, int N, int i0, const float3 (&v)[4]) {
+  if (!cell_ok(N, i0) || !cell_ok(N, i0 + 3)) return;
+  *reinterpret_cast<float4*>(a + i0) = make_float4(v[0].x, v[1].x, v[2].x, v[3].x);
+  *reinterpret_cast<float4*>(a + N + i0) = make_float4(v[0].y, v[1].y, v[2].y, v[3].y);
+  *reinterpret_cast<float4*>(a + 2 * N + i0) = make_float4(v[0].z, v[1].z, v[2].z, v[3].z);
+}
+
+// The exchange / DMI sums of four consecutive cells x0 .. x0 + 3 of tile row
+// yl: the y and z neighbour rows with 16-byte loads, the x neighbours inside
+// the quad from its own values, per cell the terms in the order r = 0 .. 5
+// of neighbour_sums (so each cell gets the same arithmetic as there).
+template <bool INNER>
+__device__ __forceinline__ void quad_sums(const MagnetDev& M, const float* __restrict__ m, int N, int i0, int x0,
+                                          int il, int ir, const int (&rb)[4], const float3 (&mc)[4], bool neumann,
+                                          bool dmi_open, bool do_exch, bool do_dmi, float3 (&he)[4],
+                                          float3 (&hd)[4]) {
+  {  // x-
+    const float3 xl = (INNER || il >= 0) ? ldg3(m, N, il) : mc[0];
+    neighbour_term<INNER>(M, 0, il >= 0, xl, mc[0], neumann, dmi_open, do_exch, do_dmi, he[0], hd[0]);
+#pragma unroll
+    for (int q = 1; q < 4; ++q)
+      neighbour_term<INNER>(M, 0, true, mc[q - 1], mc[q], neumann, dmi_open, do_exch, do_dmi, he[q], hd[q]);
+  }
+  {  // x+
+#pragma unroll
+    for (int q = 0; q < 3; ++q)
+      neighbour_term<INNER>(M, 1, true, mc[q + 1], mc[q], neumann, dmi_open, do_exch, do_dmi, he[q], hd[q]);
+    const float3 xr = (INNER || ir >= 0) ? ldg3(m, N, ir) : mc[3];
+    neighbour_term<INNER>(M, 1, ir >= 0, xr, mc[3], neumann, dmi_open, do_exch, do_dmi, he[3], hd[3]);
+  }
+#pragma unroll
+  for (int r = 2; r < 6; ++r) {  // y-, y+, z-, z+: whole neighbour rows
+    const int b = rb[r - 2];
+    if (INNER || b >= 0) {
+      float3 nn[4];
+      ldg4x3(m, N, b + x0, nn);
+#pragma unroll
+      for (int q = 0; q < 4; ++q)
+        neighbour_term<INNER>(M, r, true, nn[q], mc[q], neumann, dmi_open, do_exch, do_dmi, he[q], hd[q]);
+    } else {
+#pragma unroll
+      for (int q = 0; q < 4; ++q)
+        neighbour_term<INNER>(M, r, false, mc[q], mc[q], neumann, dmi_open, do_exch, do_dmi, he[q], hd[q]);
+    }
+  }
+}
+
+// stage_cell_lean for four consecutive cells (no stray field, spin-transfer
+// torque or thermal noise on the magnet): the same arithmetic per cell.  The
+// demag field of cell q comes from bdemag(q); the torques go to kx / ky / kz
+// (component-wise, cell q in lane q of the float4).
+template <typename BD>
+__device__ __forceinline__ void stage_quad_lean(const MagnetDev& M, const GroupDev& G, const NbRows& T,
+                                                const float* __restrict__ m, int i0, int x0, int yl, BD bdemag,
+                                                float4& kx, float4& ky, float4& kz) {
+  const int N = M.N;
+  if (M.frozen.u != 0.0f) {
+    kx = ky = kz = make_float4(0.f, 0.f, 0.f, 0.f);
+    return;
+  }
+  const unsigned terms = M.terms;
+  float3 mc[4];
+  ldg4x3(m, N, i0, mc);
+  float3 he[4], hd[4];
+#pragma unroll
+  for (int q = 0; q < 4; ++q) he[q] = hd[q] = f3(0.f, 0.f, 0.f);
+  const bool openbc = (terms & FLAG_OPENBC) != 0;
+  const bool do_exch = (terms & TERM_EXCH) != 0;
+  const bool do_dmi = (terms & TERM_DMI) != 0;
+  if (do_exch || do_dmi) {
+    const float a = M.fa;
+    const bool dmi_open = (a == 0.0f) || openbc;
+    const bool neumann = !openbc && a != 0.0f;
+    const int r0 = i0 - x0;
+    const int il = x0 > 0 ? i0 - 1 : (T.xl >= 0 ? r0 + T.xl : -1);
+    const int ir = x0 + 4 < M.n[0] ? i0 + 4 : (T.xr >= 0 ? r0 + T.xr : -1);
+    int rb[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) rb[q] = T.r[yl][q];
+    const bool inner = il >= 0 && ir >= 0 && rb[0] >= 0 && rb[1] >= 0 && rb[2] >= 0 && rb[3] >= 0;
+    if (__all_sync(__activemask(), inner))
+      quad_sums<true>(M, m, N, i0, x0, il, ir, rb, mc, neumann, dmi_open, do_exch, do_dmi, he, hd);
+    else
+      quad_sums<false>(M, m, N, i0, x0, il, ir, rb, mc, neumann, dmi_open, do_exch, do_dmi, he, hd);
+  }
+  const float3 ext = (terms & TERM_EXT) ? f3(M.fb[0], M.fb[1], M.fb[2]) : f3(0.f, 0.f, 0.f);
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    const float3 k = finish_cell_lean(M, G, mc[q], he[q], hd[q], ext, bdemag(q));
+    f4set(kx, q, k.x);
+    f4set(ky, q, k.y);
+    f4set(kz, q, k.z);
+  }
 }
 
 // ------------------------------------------------------------------ k_xinv
@@ -1033,10 +1177,20 @@ __global__ void __launch_bounds__(X_THREADS_MAX, 2) k_xinv(const MagnetDev* __re
   else load_twiddles<3>(tws, tw, logL);
   __shared__ NbRows T;
   __shared__ float cf[8];  // FSAL error weights dt (b1 - b2) of the stages
+  __shared__ int s_quad;   // lean epilogue four cells at a time (16-byte loads and stores)
   const bool lean = ea.mode == EPI_STAGE && lean_ok(M);
   if (lean) {
     nb_rows_fill(T, M, y0, ty, z);
     if (threadIdx.x < c_tab.S) cf[threadIdx.x] = (float)(G.dt * (c_tab.b1[threadIdx.x] - c_tab.b2[threadIdx.x]));
+    if (threadIdx.x == 0) {
+      // every buffer the epilogue touches 16-byte aligned (N, nx multiples of
+      // 4); no per-cell stray field, spin-transfer torque or thermal noise
+      uintptr_t a = (uintptr_t)stage_m(M, G, ea.stage) | (uintptr_t)M.buf[G.map[2 + ea.stage]];
+      if (ea.fsal_err)
+        for (int j = 0; j < c_tab.S; ++j) a |= (uintptr_t)M.buf[G.map[2 + j]];
+      s_quad = (a & 15) == 0 && (nx & 3) == 0 && (M.N & 3) == 0 &&
+               !(M.terms & (FLAG_STRAY | FLAG_STT_ZL | FLAG_STT_SL | FLAG_THERMAL));
+    }
   }
   pdl_wait();  // the spectrum and the stage state are written by the earlier passes
   const float2* __restrict__ S = M.spec;
@@ -1130,6 +1284,59 @@ __global__ void __launch_bounds__(X_THREADS_MAX, 2) k_xinv(const MagnetDev* __re
     // maximum norm after one square root per thread
     const int N = M.N;
     float* __restrict__ kout = M.buf[G.map[2 + ea.stage]];
+    if (s_quad) {
+      const int nq = nx >> 2;
+      const float rq = 1.0f / (float)nq;
+      for (int e = threadIdx.x; e < ty * nq; e += blockDim.x) {
+        const int yl = tile_row(e, nq, rq), x0 = (e - yl * nq) << 2;
+        const int i0 = rowbase + yl * nx + x0;
+        const float2* __restrict__ hrow = sm + yl * cs;
+        const float2* __restrict__ zrow = rows_z + (yl >> 1) * cs;
+        const bool odd = yl & 1;
+        auto bdemag = [&](int q) {
+          const float2 hxy = hrow[xidx(x0 + q, sh)];
+          const float2 hz2 = zrow[xidx(x0 + q, sh)];
+          return f3(hxy.x, hxy.y, odd ? hz2.y : hz2.x);
+        };
+        float4 kx, ky, kz;
+        stage_quad_lean(M, G, T, m, i0, x0, yl, bdemag, kx, ky, kz);
+        if (cell_ok(N, i0) && cell_ok(N, i0 + 3)) {
+          *reinterpret_cast<float4*>(kout + i0) = kx;
+          *reinterpret_cast<float4*>(kout + N + i0) = ky;
+          *reinterpret_cast<float4*>(kout + 2 * N + i0) = kz;
+        }
+        if (ea.fsal_err) {
+          float4 ex = make_float4(0.f, 0.f, 0.f, 0.f), ey = ex, ez = ex;
+          for (int j = 0; j < c_tab.S; ++j) {
+            const float c = cf[j];
+            float4 jx = kx, jy = ky, jz = kz;
+            if (j != ea.stage && cell_ok(N, i0) && cell_ok(N, i0 + 3)) {
+              const float* __restrict__ kb = M.buf[G.map[2 + j]];
+              jx = *reinterpret_cast<const float4*>(kb + i0);
+              jy = *reinterpret_cast<const float4*>(kb + N + i0);
+              jz = *reinterpret_cast<const float4*>(kb + 2 * N + i0);
+            }
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+              f4set(ex, q, f4c(ex, q) + c * f4c(jx, q));
+              f4set(ey, q, f4c(ey, q) + c * f4c(jy, q));
+              f4set(ez, q, f4c(ez, q) + c * f4c(jz, q));
+            }
+          }
+#pragma unroll
+          for (int q = 0; q < 4; ++q) {
+            const double erx = f4c(ex, q), ery = f4c(ey, q), erz = f4c(ez, q);
+            const double es = erx * erx + ery * ery + erz * erz;
+            const double kxq = f4c(kx, q), kyq = f4c(ky, q), kzq = f4c(kz, q);
+            const double ts = kxq * kxq + kyq * kyq + kzq * kzq;
+            en = (es > en || es != es) ? es : en;
+            tn = fmax(tn, ts);
+          }
+        }
+      }
+      if (ea.fsal_err) block_max2(sqrt(en), sqrt(tn), &groups[M.group].err_bits, &groups[M.group].tmax_bits);
+      return;
+    }
     for (int e = threadIdx.x; e < ty * nx; e += blockDim.x) {
       const int yl = tile_row(e, nx, rn), x = e - yl * nx;
       const int i = rowbase + e;

@@ -131,3 +131,34 @@ def test_same_result_with_small_and_large_tiles(mpx):
     mixed, _, _ = B.relax_batch(B.Batch(), [w] + fill, duration=15e-12, torque_stop=0.0)
     assert alone.steps == mixed[0].steps
     assert np.array_equal(alone.m, mixed[0].m)
+
+
+def test_membership_changes_update_the_attempt_graph(mpx):
+    """A solve that starts or finishes while others run changes only the launch
+    sizes and tables of the attempt: the captured graphs are updated in place
+    (no new instantiation), and the solves give the same results as without
+    the change."""
+    from mumaxplus_b200 import batch as B
+
+    sols = [_solve(10 + k, (40, 32, 1), 3e-9, 8e5, 1.3e-11, 0.1, (0.02, 0.0, 0.05), duration=1e-6) for k in range(3)]
+    ref = B.Batch()
+    rs = [ref.add(w, key=i) for i, w in enumerate(sols)]
+    for s in rs:
+        ref.start(s, 1e-6)
+    ref.advance(20)
+    ref.poll()
+    want = ref.engine.get_m(rs[0].magnet, rs[0].shape)
+
+    b = B.Batch()
+    ss = [b.add(w, key=i) for i, w in enumerate(sols)]
+    b.start(ss[0], 1e-6)
+    b.start(ss[1], 1e-6)
+    b.advance(8)
+    b.poll()
+    inst0, upd0 = b.engine.graph_stats()
+    b.start(ss[2], 1e-6)  # a new solve of the same shape class joins
+    b.advance(12)
+    b.poll()
+    inst1, upd1 = b.engine.graph_stats()
+    assert inst1 == inst0 and upd1 > upd0, (inst0, upd0, inst1, upd1)
+    np.testing.assert_array_equal(b.engine.get_m(ss[0].magnet, ss[0].shape), want)

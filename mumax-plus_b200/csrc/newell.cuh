@@ -152,6 +152,9 @@ __global__ void k_kernel_expand(double2* __restrict__ full, const double* __rest
 }
 
 // One radix-2 Stockham pass (FP64) along `axis` of a P0 x P1 x P2 array.
+// Consecutive threads take consecutive butterflies of a line along x and
+// consecutive lines (adjacent x) along y and z, so that every load and store
+// of a warp is contiguous.
 __global__ void k_fft64_pass(const double2* __restrict__ in, double2* __restrict__ out, int P0, int P1, int P2,
                              int axis, int Ns) {
   const int L = axis == 0 ? P0 : axis == 1 ? P1 : P2;
@@ -160,8 +163,8 @@ __global__ void k_fft64_pass(const double2* __restrict__ in, double2* __restrict
   const long long total = nlines * (L / 2);
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
        t += (long long)gridDim.x * blockDim.x) {
-    const int j = (int)(t % (L / 2));
-    const long long line = t / (L / 2);
+    const int j = axis == 0 ? (int)(t % (L / 2)) : (int)(t / nlines);
+    const long long line = axis == 0 ? t / (L / 2) : t % nlines;
     long long base;
     if (axis == 0) base = line * P0;
     else if (axis == 1) base = (line / P0) * ((long long)P0 * P1) + (line % P0);

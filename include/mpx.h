@@ -252,6 +252,13 @@ mpx_status mpx_group_load(mpx_engine* e, int group, const void* buf, int64_t byt
  * an adaptive group's time step becomes the sensible one for that state
  * (core/timesolver.cpp:49-52). */
 mpx_status mpx_magnet_add(mpx_engine* e, int group, const mpx_magnet_desc* d, int* magnet);
+/* mpx_magnet_add with the initial magnetization given (3 * ncells floats, SoA,
+ * host memory unless on_device; normalised as by mpx_magnet_set_m) instead of
+ * the random one: one field evaluation (the sensible time step of an adaptive
+ * group, for this state) instead of two, no separate set_m.  No counterpart in
+ * the reference, where a new magnet starts random and is then set. */
+mpx_status mpx_magnet_add_state(mpx_engine* e, int group, const mpx_magnet_desc* d, const float* m0, int on_device,
+                                int* magnet);
 /* Device bytes mpx_magnet_add would take for `d`: *resident stays allocated
  * until the magnet is removed (state buffers, spectra, per-cell parameters,
  * work tables); *transient is the extra peak while it is added (the FP64

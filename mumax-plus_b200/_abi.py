@@ -172,6 +172,7 @@ SIGNATURES = {
     # descriptions are passed by address so that an identical struct layout
     # declared elsewhere (e.g. by a test harness) is accepted as well
     "mpx_magnet_add": (I, [E, I, C.c_void_p, P_I]),
+    "mpx_magnet_add_state": (I, [E, I, C.c_void_p, C.c_void_p, I, P_I]),
     "mpx_magnet_update": (I, [E, I, C.c_void_p]),
     "mpx_magnet_remove": (I, [E, I]),
     "mpx_magnet_bytes": (I, [C.c_void_p, P_I64, P_I64]),

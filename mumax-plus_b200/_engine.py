@@ -140,6 +140,13 @@ class Engine:
         check(lib().mpx_magnet_add(self._h, int(group), C.byref(desc), C.byref(m)))
         return m.value
 
+    def magnet_add_state(self, group, desc, m0):
+        """Add a magnet with its initial magnetization (float32 (3, nz, ny, nx))."""
+        a = np.ascontiguousarray(m0, dtype=np.float32)
+        m = C.c_int()
+        check(lib().mpx_magnet_add_state(self._h, int(group), C.byref(desc), a.ctypes.data, 0, C.byref(m)))
+        return m.value
+
     def magnet_update(self, magnet, desc):
         check(lib().mpx_magnet_update(self._h, int(magnet), C.byref(desc)))
 

@@ -93,9 +93,9 @@ class Batch:
             keep = []
             d = solve_desc(w, keep)
             s.resident, s.transient = magnet_bytes(d)
-            s.magnet = eng.magnet_add(g, d)
-            eng.set_m(s.magnet, w["m0"]() if m0 is None else m0)
-            eng.set_timestep(g, eng.sensible_timestep(g))
+            # the magnet with its initial state: the group's time step is then
+            # the sensible one for that state
+            s.magnet = eng.magnet_add_state(g, d, w["m0"]() if m0 is None else m0)
         except Exception:
             eng.group_destroy(g)
             raise

@@ -232,6 +232,7 @@ struct mpx_engine {
   // matrix (hi, lo) of the tensor-core form
   int dft_mode = MPX_DFT_FP32;
   float* d_dftB = nullptr;
+  int n_sm = 148;  // multiprocessors of the engine's device
   int smem_x = 0, nt_x = 256;
   bool any_nodemag = false;
   int64_t bytes = 0;
@@ -481,14 +482,7 @@ mpx_status launch_split(mpx_engine* e, const Work* ycw, int nyc, const Work* zmw
                         int max_py, int max_pz, int stage, int gate, const Work* tcw = nullptr, int ntc = 0) {
   if (nyc <= 0 && ntc <= 0) return MPX_OK;
   const bool ry = max_py <= 2048, rz = max_pz <= 2048;
-  static int n_sm = 0;
-  if (!n_sm) {
-    int dev = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev);
-    if (n_sm <= 0) n_sm = 148;
-  }
-  const int gtc = std::min(ntc, TC_GRID_PER_SM * n_sm);
+  const int gtc = std::min(ntc, TC_GRID_PER_SM * e->n_sm);
   if (ntc > 0) {
     k_ydft_tc<-1><<<gtc, 128, TC_SMEM, e->stream>>>(e->d_mags, e->d_groups, tcw, ntc, stage, gate, e->d_dftB);
     e->launches++;
@@ -1677,6 +1671,7 @@ mpx_status mpx_engine_create(int device, mpx_engine** out) {
   DeviceGuard guard(device);
   auto e = std::make_unique<mpx_engine>();
   e->device = device;
+  CUDA_TRY(cudaDeviceGetAttribute(&e->n_sm, cudaDevAttrMultiProcessorCount, device));
   CUDA_TRY(cudaStreamCreateWithFlags(&e->own, cudaStreamNonBlocking));
   e->stream = e->own;
   {
@@ -2012,7 +2007,10 @@ mpx_status mpx_group_info_get(mpx_engine* e, int group, mpx_group_info* out) {
   return MPX_OK;
 }
 
-mpx_status mpx_magnet_add(mpx_engine* e, int group, const mpx_magnet_desc* d, int* magnet) {
+// mpx_magnet_add / mpx_magnet_add_state: `m0` (3N floats, host unless
+// on_device) is the initial magnetisation, or NULL for the random one.
+static mpx_status magnet_add_impl(mpx_engine* e, int group, const mpx_magnet_desc* d, const float* m0, int on_device,
+                                  int* magnet) {
   NvtxRange nvtx_range("mpx_magnet_add");
   if (!e || !magnet) return fail(MPX_ERR_INVALID, "null argument");
   Group* g = get_group(e, group);
@@ -2038,19 +2036,27 @@ mpx_status mpx_magnet_add(mpx_engine* e, int group, const mpx_magnet_desc* d, in
     g_last_error = msg;
     return st;
   }
-  // initial magnetisation: normalised random vectors, generated on the device
-  // (the reference seeds its generator with the clock, ferromagnet.cpp:62-76;
-  // here the seed is the magnet slot)
+  // initial magnetisation: the given one, or normalised random vectors
+  // generated on the device (the reference seeds its generator with the clock,
+  // ferromagnet.cpp:62-76; here the seed is the magnet slot)
   const int n3 = 3 * m->dev.N;
-  MPX_TRY(ensure_scratch(e, sizeof(float) * (size_t)n3));
-  k_random_normal<<<std::min((n3 + 255) / 256, 148 * 16), 256, 0, e->stream>>>(
-      e->d_scratch, n3, 0x5DEECE66Dull * (unsigned long long)(slot + 1));
-  e->launches++;
+  const float* src = m0;
+  if (!m0 || !on_device) {
+    MPX_TRY(ensure_scratch(e, sizeof(float) * (size_t)n3));
+    if (m0) {
+      CUDA_TRY(cudaMemcpyAsync(e->d_scratch, m0, sizeof(float) * (size_t)n3, cudaMemcpyHostToDevice, e->stream));
+    } else {
+      k_random_normal<<<std::min((n3 + 255) / 256, 148 * 16), 256, 0, e->stream>>>(
+          e->d_scratch, n3, 0x5DEECE66Dull * (unsigned long long)(slot + 1));
+      e->launches++;
+    }
+    src = e->d_scratch;
+  }
   Magnet* mp = m.get();
   e->mags[slot] = std::move(m);
   g->magnets.push_back(slot);
   e->tables_dirty = true;
-  MPX_TRY(set_m_device(e, mp, e->d_scratch));
+  MPX_TRY(set_m_device(e, mp, src));
   // core/timesolver.cpp:49-52: new equations -> sensible time step (adaptive solvers)
   if (g->sp.adaptive) {
     double dt;
@@ -2062,6 +2068,16 @@ mpx_status mpx_magnet_add(mpx_engine* e, int group, const mpx_magnet_desc* d, in
   }
   *magnet = slot;
   return MPX_OK;
+}
+
+mpx_status mpx_magnet_add(mpx_engine* e, int group, const mpx_magnet_desc* d, int* magnet) {
+  return magnet_add_impl(e, group, d, nullptr, 0, magnet);
+}
+
+mpx_status mpx_magnet_add_state(mpx_engine* e, int group, const mpx_magnet_desc* d, const float* m0, int on_device,
+                                int* magnet) {
+  if (!m0) return fail(MPX_ERR_INVALID, "null initial magnetization");
+  return magnet_add_impl(e, group, d, m0, on_device, magnet);
 }
 
 mpx_status mpx_magnet_update(mpx_engine* e, int magnet, const mpx_magnet_desc* d) {

@@ -17,6 +17,7 @@
 #include <memory>
 #include <mutex>
 #include <string>
+#include <unordered_map>
 #include <vector>
 
 #include "../../include/mpx.h"
@@ -143,6 +144,8 @@ TableauDev make_tableau(int method) {
 // ---------------------------------------------------------------- objects
 struct Magnet {
   int slot = -1, group = -1;
+  uint64_t uid = 0;  // unique per magnet object of the engine (slots are reused)
+  uint64_t ver = 0;  // bumped whenever its work lists (tiles, y/z blocks) change
   MagnetDev dev;
   unsigned terms_base = 0;        // TERM_* / FLAG_* from the parameters, before stray fields
   bool msat_zero = false;
@@ -192,6 +195,52 @@ struct Group {
   int thermal = 0;      // mirrors GroupDev::thermal
 };
 
+// A launch table whose entries keep their place while solves come and go.
+// Each magnet occupies one contiguous range (its work items, in order); a
+// magnet that is no longer launched leaves a hole (entries with mag = -1,
+// which every kernel skips in load_descs).  New magnets are appended, and
+// the table is compacted when the holes outnumber the live entries.  Only
+// the changed range is uploaded: a solve that arrives or finishes costs a
+// copy of its own items, not a rebuild of every table.
+struct SlotTable {
+  struct Place {
+    int off, len;
+    uint64_t ver;
+  };
+  std::vector<Work> items;                     // host copy of the used entries
+  std::unordered_map<uint64_t, Place> place;   // by magnet uid
+  Work* dev = nullptr;                         // device copy, capacity cap
+  int cap = 0, live = 0;
+  int dlo = 1 << 30, dhi = -1;                 // entries to upload
+  void dirty(int lo, int hi) {
+    dlo = std::min(dlo, lo);
+    dhi = std::max(dhi, hi);
+  }
+  void remove(uint64_t uid) {
+    auto it = place.find(uid);
+    if (it == place.end()) return;
+    const Place p = it->second;
+    for (int i = p.off; i < p.off + p.len; ++i) items[i].mag = -1;
+    dirty(p.off, p.off + p.len);
+    live -= p.len;
+    place.erase(it);
+  }
+  void add(uint64_t uid, uint64_t ver, const std::vector<Work>& w) {
+    const int off = (int)items.size();
+    items.insert(items.end(), w.begin(), w.end());
+    dirty(off, off + (int)w.size());
+    live += (int)w.size();
+    place[uid] = Place{off, (int)w.size(), ver};
+  }
+  void clear() {
+    items.clear();
+    place.clear();
+    live = 0;
+    dlo = 0;
+    dhi = 0;
+  }
+};
+
 }  // namespace
 
 struct mpx_engine {
@@ -212,10 +261,14 @@ struct mpx_engine {
   double* d_redout = nullptr;
   float* d_scratch = nullptr;
   size_t scratch_bytes = 0;
-  // run tables over all magnets
+  // run tables over all magnets: x tiles (demag / local), y/z blocks per
+  // class, split path (k_ycols, k_zmul, k_ydft_tc)
+  enum { TT_DEMAG = 0, TT_LOCAL, TT_YCOLS, TT_ZMUL, TT_TC, TT_YZ0 };
+  SlotTable tt[TT_YZ0 + YZ_CLASSES];
+  uint64_t next_uid = 1;
   bool tables_dirty = true;
   bool tables_valid = false;     // the device tables below hold tables_sig
-  std::vector<int> tables_sig;
+  std::vector<long long> tables_sig;
   Work *d_t_demag = nullptr, *d_t_local = nullptr;
   int n_t_demag = 0, n_t_local = 0;
   // k_yz work per class (yz_class: the z length and whether Py > 2048)
@@ -625,6 +678,7 @@ mpx_status retile(mpx_engine* e, Magnet* m, int ty, int nkx) {
   const MagnetDev& D = m->dev;
   m->ty = ty;
   m->nkx = nkx;
+  m->ver++;  // the launch tables place this magnet's items again
   m->tiles.clear();
   m->kxw.clear();
   for (int z = 0; z < D.n[2]; ++z)
@@ -662,37 +716,83 @@ mpx_status rebuild_tables(mpx_engine* e) {
     for (size_t i = 0; i < act.size(); ++i)
       if (ty[i] != act[i]->ty || nkx[i] != act[i]->nkx) MPX_TRY(retile(e, act[i], ty[i], nkx[i]));
   }
-  std::vector<Work> td, tl, kd[YZ_CLASSES], yc, zm, tcl;
+  // the work lists each table should hold: the magnets of started groups
+  // (finished and idle solves cost no blocks), in slot order
+  const int NT = mpx_engine::TT_YZ0 + YZ_CLASSES;
+  std::vector<std::pair<Magnet*, const std::vector<Work>*>> want[mpx_engine::TT_YZ0 + YZ_CLASSES];
   e->smem_ycols = e->smem_zmul = e->maxpy_split = e->maxpz_split = 0;
   e->smem_x = 0;
   e->nt_x = 256;
   for (int c = 0; c < YZ_CLASSES; ++c) e->smem_yz[c] = 0;
-  // only the magnets of started groups: finished and idle solves cost no blocks
   for (auto& mp : e->mags) {
     if (!mp || mp->hull) continue;  // helpers of FFT stray-field pairs are launched by launch_pairs
     Magnet* m = mp.get();
     const Group* g = (m->group >= 0 && m->group < (int)e->groups.size()) ? e->groups[m->group].get() : nullptr;
     if (!g || !g->active) continue;
     if (m->demag) {
-      td.insert(td.end(), m->tiles.begin(), m->tiles.end());
+      want[mpx_engine::TT_DEMAG].push_back({m, &m->tiles});
       e->smem_x = std::max(e->smem_x, x_smem(m));
       if (m->split) {
-        yc.insert(yc.end(), m->ycw.begin(), m->ycw.end());
-        tcl.insert(tcl.end(), m->tcw.begin(), m->tcw.end());
-        zm.insert(zm.end(), m->zmw.begin(), m->zmw.end());
+        want[mpx_engine::TT_YCOLS].push_back({m, &m->ycw});
+        want[mpx_engine::TT_TC].push_back({m, &m->tcw});
+        want[mpx_engine::TT_ZMUL].push_back({m, &m->zmw});
         e->smem_ycols = std::max(e->smem_ycols, ycols_smem(m));
         e->smem_zmul = std::max(e->smem_zmul, zmul_smem(m));
         e->maxpy_split = std::max(e->maxpy_split, m->P[1]);
         e->maxpz_split = std::max(e->maxpz_split, m->P[2]);
       } else {
         const int cls = yz_class(m);
-        kd[cls].insert(kd[cls].end(), m->kxw.begin(), m->kxw.end());
+        want[mpx_engine::TT_YZ0 + cls].push_back({m, &m->kxw});
         e->smem_yz[cls] = std::max(e->smem_yz[cls], yz_smem(m));
       }
       e->nt_x = std::max(e->nt_x, x_threads(m));
     } else {
-      tl.insert(tl.end(), m->tiles.begin(), m->tiles.end());
+      want[mpx_engine::TT_LOCAL].push_back({m, &m->tiles});
     }
+  }
+  // each table: holes for the magnets that left (or whose lists changed), the
+  // newcomers appended, compaction when the holes outnumber the live entries,
+  // and an upload of the changed entries only
+  for (int t = 0; t < NT; ++t) {
+    SlotTable& T = e->tt[t];
+    std::unordered_map<uint64_t, std::pair<Magnet*, const std::vector<Work>*>> w;
+    for (auto& pr : want[t])
+      if (!pr.second->empty()) w[pr.first->uid] = pr;
+    std::vector<uint64_t> gone;
+    for (auto& kv : T.place) {
+      auto it = w.find(kv.first);
+      if (it == w.end() || it->second.first->ver != kv.second.ver) gone.push_back(kv.first);
+    }
+    for (uint64_t uid : gone) T.remove(uid);
+    int add_len = 0;
+    for (auto& pr : want[t])
+      if (!pr.second->empty() && !T.place.count(pr.first->uid)) add_len += (int)pr.second->size();
+    const int used_after = (int)T.items.size() + add_len, live_after = T.live + add_len;
+    if (used_after > 64 && used_after - live_after > live_after) {  // compact, in slot order
+      T.clear();
+      for (auto& pr : want[t])
+        if (!pr.second->empty()) T.add(pr.first->uid, pr.first->ver, *pr.second);
+    } else {
+      for (auto& pr : want[t])
+        if (!pr.second->empty() && !T.place.count(pr.first->uid)) T.add(pr.first->uid, pr.first->ver, *pr.second);
+    }
+    while (!T.items.empty() && T.items.back().mag < 0) T.items.pop_back();  // trailing holes
+    const int used = (int)T.items.size();
+    if (used > T.cap) {  // grow: a new device array, everything uploaded
+      const int nc = std::max({used, 2 * T.cap, 64});
+      Work* nd = nullptr;
+      MPX_TRY(palloc(e, (void**)&nd, sizeof(Work) * (size_t)nc));
+      pfree(e, T.dev);  // stream-ordered after the attempts already queued
+      T.dev = nd;
+      T.cap = nc;
+      T.dirty(0, used);
+    }
+    const int lo = std::max(0, T.dlo), hi = std::min(used, T.dhi);
+    if (hi > lo)
+      CUDA_TRY(cudaMemcpyAsync(T.dev + lo, T.items.data() + lo, sizeof(Work) * (size_t)(hi - lo),
+                               cudaMemcpyHostToDevice, e->stream));
+    T.dlo = 1 << 30;
+    T.dhi = -1;
   }
   // groups with thermal noise never reuse k0 (GroupDev::thermal, read by the controller)
   e->any_thermal = false;
@@ -712,46 +812,32 @@ mpx_status rebuild_tables(mpx_engine* e) {
       gp->thermal = th;
     }
   }
-  // Everything the attempt graphs take from the tables.  A run that finishes
-  // takes its group out of the tables and the next run puts it back: when the
-  // result is the same as last time, the device tables and the captured graphs
-  // stay as they are (no upload, no recapture per step() / run() call).
-  std::vector<int> sig;
-  auto put = [&sig](const std::vector<Work>& v) {
-    sig.push_back((int)v.size());
-    for (const Work& w : v) sig.insert(sig.end(), {w.mag, w.z, w.y0, w.ty});
-  };
-  put(td);
-  put(tl);
-  put(yc);
-  put(zm);
-  put(tcl);
+  e->d_t_demag = e->tt[mpx_engine::TT_DEMAG].dev;
+  e->n_t_demag = (int)e->tt[mpx_engine::TT_DEMAG].items.size();
+  e->d_t_local = e->tt[mpx_engine::TT_LOCAL].dev;
+  e->n_t_local = (int)e->tt[mpx_engine::TT_LOCAL].items.size();
+  e->d_t_ycols = e->tt[mpx_engine::TT_YCOLS].dev;
+  e->n_t_ycols = (int)e->tt[mpx_engine::TT_YCOLS].items.size();
+  e->d_t_zmul = e->tt[mpx_engine::TT_ZMUL].dev;
+  e->n_t_zmul = (int)e->tt[mpx_engine::TT_ZMUL].items.size();
+  e->d_t_tc = e->tt[mpx_engine::TT_TC].dev;
+  e->n_t_tc = (int)e->tt[mpx_engine::TT_TC].items.size();
   for (int c = 0; c < YZ_CLASSES; ++c) {
-    put(kd[c]);
-    sig.push_back(e->smem_yz[c]);
+    e->d_kx_demag[c] = e->tt[mpx_engine::TT_YZ0 + c].dev;
+    e->n_kx_demag[c] = (int)e->tt[mpx_engine::TT_YZ0 + c].items.size();
   }
+  // Everything the attempt graphs take from the tables: their device arrays,
+  // launch sizes and the launch shapes.  A solve that arrives or finishes in
+  // an unchanged range of the tables leaves them as they are (no capture); a
+  // changed launch size updates the captured graphs in place.
+  std::vector<long long> sig;
+  for (int t = 0; t < NT; ++t) sig.insert(sig.end(), {(long long)(uintptr_t)e->tt[t].dev, (long long)e->tt[t].items.size()});
+  for (int c = 0; c < YZ_CLASSES; ++c) sig.push_back(e->smem_yz[c]);
   sig.insert(sig.end(), {e->smem_x, e->nt_x, e->smem_ycols, e->smem_zmul, e->maxpy_split, e->maxpz_split});
-  if (e->tables_valid && sig == e->tables_sig) {
-    e->tables_dirty = false;
-    return MPX_OK;
-  }
-  MPX_TRY(upload_vec(e, &e->d_t_demag, td));
-  MPX_TRY(upload_vec(e, &e->d_t_local, tl));
-  MPX_TRY(upload_vec(e, &e->d_t_ycols, yc));
-  MPX_TRY(upload_vec(e, &e->d_t_zmul, zm));
-  MPX_TRY(upload_vec(e, &e->d_t_tc, tcl));
-  e->n_t_tc = (int)tcl.size();
-  e->n_t_ycols = (int)yc.size();
-  e->n_t_zmul = (int)zm.size();
-  for (int c = 0; c < YZ_CLASSES; ++c) {
-    MPX_TRY(upload_vec(e, &e->d_kx_demag[c], kd[c]));
-    e->n_kx_demag[c] = (int)kd[c].size();
-  }
-  e->n_t_demag = (int)td.size();
-  e->n_t_local = (int)tl.size();
+  e->tables_dirty = false;
+  if (e->tables_valid && sig == e->tables_sig) return MPX_OK;
   e->tables_sig = std::move(sig);
   e->tables_valid = true;
-  e->tables_dirty = false;
   e->graph_dirty = true;
   return MPX_OK;
 }
@@ -806,6 +892,7 @@ mpx_status create_hull(mpx_engine* e, const Magnet* A, const Magnet* B, int* out
   m->slot = slot;
   m->group = A->group;
   m->hull = true;
+  m->uid = e->next_uid++;
   mpx_status st = setup_magnet(e, m.get(), &d, false);
   if (st == MPX_OK) {
     const cudaError_t ce = cudaMemsetAsync(m->dev.buf[0], 0, sizeof(float) * 3 * (size_t)m->dev.N, e->stream);
@@ -1338,6 +1425,7 @@ mpx_status setup_magnet(mpx_engine* e, Magnet* m, const mpx_magnet_desc* d, bool
   MPX_TRY(upload_vec(e, &m->d_ycw, m->ycw));
   MPX_TRY(upload_vec(e, &m->d_zmw, m->zmw));
   MPX_TRY(upload_vec(e, &m->d_tcw, m->tcw));
+  m->ver++;
   MPX_TRY(upload_magnet_desc(e, m));
   e->tables_dirty = true;
   return MPX_OK;
@@ -1765,9 +1853,7 @@ mpx_status mpx_engine_destroy(mpx_engine* e) {
   cudaFree(e->d_red);
   cudaFree(e->d_redout);
   pfree(e, e->d_scratch);
-  pfree(e, e->d_t_demag);
-  for (int c = 0; c < YZ_CLASSES; ++c) pfree(e, e->d_kx_demag[c]);
-  pfree(e, e->d_t_local);
+  for (auto& t : e->tt) pfree(e, t.dev);  // the launch tables (d_t_* and d_kx_demag alias them)
   cudaStreamSynchronize(e->stream);
   if (e->pool) cudaMemPoolDestroy(e->pool);
   if (e->own) cudaStreamDestroy(e->own);
@@ -2028,6 +2114,7 @@ static mpx_status magnet_add_impl(mpx_engine* e, int group, const mpx_magnet_des
   std::memset(&m->dev, 0, sizeof(MagnetDev));
   m->slot = slot;
   m->group = group;
+  m->uid = e->next_uid++;
   mpx_status st = setup_magnet(e, m.get(), d, false);
   if (st != MPX_OK) {
     std::string msg = g_last_error;
@@ -2305,6 +2392,7 @@ mpx_status mpx_stray_field(mpx_engine* e, int src, int dst_magnet, const int siz
     m->slot = tmp;
     m->group = A->group;
     m->hull = true;  // a probe of the destination grid: in no group's tables
+    m->uid = e->next_uid++;
     const mpx_status st = setup_magnet(e, m.get(), &d, false);
     if (st != MPX_OK) {
       std::string msg = g_last_error;

@@ -70,8 +70,11 @@ __device__ __forceinline__ void copy_to_smem(T* dst, const T* __restrict__ src) 
 
 // Loads the magnet and group descriptors of this block; returns false when the
 // block has nothing to do (group not running, or k0 already valid for stage 0).
+// A negative magnet slot marks a hole of a launch table (a solve that is no
+// longer launched): the block has nothing to do.
 __device__ __forceinline__ bool load_descs(MagnetDev& sM, GroupDev& sG, const MagnetDev* __restrict__ mags,
                                            const GroupDev* __restrict__ groups, int mag, int gate, int stage) {
+  if (mag < 0) return false;
   copy_to_smem(&sM, mags + mag);
   __syncthreads();
   copy_to_smem(&sG, groups + sM.group);

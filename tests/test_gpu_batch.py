@@ -162,3 +162,43 @@ def test_membership_changes_update_the_attempt_graph(mpx):
     inst1, upd1 = b.engine.graph_stats()
     assert inst1 == inst0 and upd1 > upd0, (inst0, upd0, inst1, upd1)
     np.testing.assert_array_equal(b.engine.get_m(ss[0].magnet, ss[0].shape), want)
+
+
+def test_launch_tables_keep_places_through_churn(mpx):
+    """Many short solves finishing while others arrive: the launch tables
+    leave holes for the finished ones, append the newcomers and compact when
+    the holes outnumber the live entries; every solve still ends as it does
+    alone (bit for bit)."""
+    from mumaxplus_b200 import batch as B
+
+    sols = [_solve(20 + k, (48 + 16 * (k % 3), 32, 1 + (k % 2)), 3e-9, 8e5, 1.3e-11, 0.2, (0.01, 0.02, 0.03),
+                   duration=(2 + (k % 5)) * 1e-12) for k in range(24)]
+    alone = {}
+    for k in (0, 7, 13, 23):
+        b1 = B.Batch()
+        s = b1.add(sols[k], key=k)
+        b1.start(s, sols[k]["duration"])
+        while True:
+            b1.advance(4)
+            done, running = b1.poll()
+            if running == 0:
+                break
+        alone[k] = b1.engine.get_m(s.magnet, s.shape)
+    b = B.Batch()
+    live, got = {}, {}
+    nxt = 0
+    while nxt < len(sols) or live:
+        while nxt < len(sols) and len(live) < 6:  # a few resident at a time: arrivals and completions interleave
+            s = b.add(sols[nxt], key=nxt)
+            b.start(s, sols[nxt]["duration"])
+            live[s.group] = s
+            nxt += 1
+        b.advance(3)
+        done, _ = b.poll()
+        for s in done:
+            if s.key in alone:
+                got[s.key] = b.engine.get_m(s.magnet, s.shape)
+            b.finish(s, fetch=False)
+            live.pop(s.group)
+    for k, want in alone.items():
+        np.testing.assert_array_equal(got[k], want)

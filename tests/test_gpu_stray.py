@@ -252,3 +252,27 @@ def test_stray_field_from_magnet(mpx):
     mc = mpx.Ferromagnet(other, mpx.Grid((4, 4, 1)))
     with pytest.raises(RuntimeError):
         mc.stray_field_from_magnet(ma)
+
+
+def test_stray_field_argument_errors(mpx):
+    """bindings/wrap_strayfield.cpp:16-24: an unknown method is a ValueError;
+    a destination grid of no cells is refused by the C ABI."""
+    import ctypes as C
+
+    world = mpx.World(STRAY_CS)
+    magnet = mpx.Ferromagnet(world, mpx.Grid((8, 4, 1)))
+    magnet.msat = 8e5
+    sf = mpx.StrayField(magnet, mpx.Grid((4, 4, 1), (10, 0, 0)))
+    with pytest.raises(ValueError):
+        sf.set_method("direct")
+    lib = mpx._abi.load()
+    out = np.zeros(12, np.float32)
+    st = lib.mpx_stray_field(magnet._engine.handle, magnet._id, -1, (C.c_int * 3)(0, 4, 1), (C.c_int * 3)(0, 0, 0),
+                             mpx._abi.MPX_STRAY_FFT, out.ctypes.data, 0)
+    assert st == mpx._abi.MPX_ERR_INVALID
+    st = lib.mpx_stray_field(magnet._engine.handle, magnet._id, -1, (C.c_int * 3)(4, 4, 1), (C.c_int * 3)(0, 0, 0), 7,
+                             out.ctypes.data, 0)
+    assert st == mpx._abi.MPX_ERR_INVALID
+    # a source with msat 0 gives no field
+    magnet.msat = 0.0
+    np.testing.assert_array_equal(sf.eval(), 0.0)

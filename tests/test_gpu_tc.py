@@ -135,3 +135,15 @@ def test_tc_multilayer_full_size(mpx):
     assert errs[abi.Q_EFFECTIVE_FIELD] < FIELD_TOL, errs
     assert errs[abi.Q_DEMAG_FIELD] < 5 * FIELD_TOL, errs
     assert mpx._engine.Engine.tc_timeouts() == 0
+
+
+def test_tc_mode_leaves_other_lengths_on_the_fp32_path(mpx):
+    """In the tensor-core mode a magnet whose padded y length is neither 1024
+    nor 2048 keeps the FP32 y transforms: the same field, bit for bit."""
+    s = MagnetSpec(size=(24, 100, 2), cellsize=(2e-9, 2e-9, 1e-9), msat=8e5, aex=1.3e-11)  # Py = 256
+    m0 = random_m(s.shape, seed=3, smooth=1)
+    _, a = _product(s, mpx, m0, "tf32x3")
+    _, b = _product(s, mpx, m0, "fp32")
+    fa = a._engine.eval(a._id, abi.Q_DEMAG_FIELD, (3, *s.shape))
+    fb = b._engine.eval(b._id, abi.Q_DEMAG_FIELD, (3, *s.shape))
+    np.testing.assert_array_equal(fa, fb)

@@ -215,6 +215,12 @@ mpx_status mpx_engine_set_dft(mpx_engine* e, int mode);
  * releases its tensor memory instead of hanging), since the last call, on the
  * current device; synchronises the device and clears the count. */
 mpx_status mpx_tc_status(unsigned int* timeouts);
+/* No counterpart in the reference.  Exercises the timeout path of the
+ * tensor-core kernels without a fault: one block on the current device takes
+ * tensor memory and waits (at most about 1 ms) on an mbarrier that nothing
+ * arrives at, then counts the timeout, releases its tensor memory and returns.
+ * *timeouts: the count read back (1 expected); the device stays usable. */
+mpx_status mpx_tc_timeout_selftest(unsigned int* timeouts);
 /* Uniform field over the whole world, T (physics/mumaxworld.hpp biasMagneticField). */
 mpx_status mpx_engine_set_world_bias(mpx_engine* e, const double b[3]);
 /* Device bytes currently held by the engine (buffers, spectra, kernels). */

@@ -159,6 +159,7 @@ SIGNATURES = {
     "mpx_engine_synchronize": (I, [E]),
     "mpx_engine_set_dft": (I, [E, I]),
     "mpx_tc_status": (I, [C.POINTER(C.c_uint)]),
+    "mpx_tc_timeout_selftest": (I, [C.POINTER(C.c_uint)]),
     "mpx_engine_set_world_bias": (I, [E, P_D]),
     "mpx_engine_memory": (I, [E, P_I64]),
     "mpx_engine_launch_count": (I, [E, P_I64]),

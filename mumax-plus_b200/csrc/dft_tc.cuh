@@ -404,4 +404,33 @@ __global__ void __launch_bounds__(128, TC_BLOCKS_PER_SM)
   if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tm), "r"(TC_TMEM_COLS));
 }
 
+// The timeout path of the tensor-core kernels, without a fault: one block
+// takes tensor memory and an mbarrier as k_ydft_tc does, but nothing arrives
+// on the barrier, so its bounded wait (`polls` polls) runs out.  The block then
+// counts the timeout, waits once more (bounded), releases its tensor memory and
+// returns; the context stays usable.
+__global__ void __launch_bounds__(128, 1) k_tc_timeout_probe(int polls) {
+  __shared__ __align__(8) unsigned long long mbar;
+  __shared__ uint32_t tbase;
+  const int tid = threadIdx.x, warp = tid >> 5;
+  if (tid == 0) tc::mbar_init(&mbar);
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(tc::smem_u32(&tbase)),
+                 "r"(TC_TMEM_COLS));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n");
+  }
+  tc::fence_before();
+  __syncthreads();
+  tc::fence_after();
+  const uint32_t tm = tbase;
+  const bool gave_up = __syncthreads_or(!tc::mbar_wait(&mbar, 0, polls));
+  if (gave_up) {
+    if (tid == 0) atomicAdd(&g_tc_timeouts, 1u);
+    tc::mbar_wait(&mbar, 0, polls);
+  }
+  tc::fence_before();
+  __syncthreads();
+  if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tm), "r"(TC_TMEM_COLS));
+}
+
 }  // namespace mpx

@@ -1879,6 +1879,16 @@ mpx_status mpx_engine_set_dft(mpx_engine* e, int mode) {
   return MPX_OK;
 }
 
+mpx_status mpx_tc_timeout_selftest(unsigned int* timeouts) {
+  if (!timeouts) return fail(MPX_ERR_INVALID, "null output");
+  unsigned int before = 0;
+  MPX_TRY(mpx_tc_status(&before));  // synchronises and clears
+  k_tc_timeout_probe<<<1, 128>>>(1 << 14);
+  CUDA_TRY(cudaGetLastError());
+  MPX_TRY(mpx_tc_status(timeouts));
+  return MPX_OK;
+}
+
 mpx_status mpx_tc_status(unsigned int* timeouts) {
   if (!timeouts) return fail(MPX_ERR_INVALID, "null output");
   CUDA_TRY(cudaDeviceSynchronize());

@@ -147,3 +147,24 @@ def test_tc_mode_leaves_other_lengths_on_the_fp32_path(mpx):
     fa = a._engine.eval(a._id, abi.Q_DEMAG_FIELD, (3, *s.shape))
     fb = b._engine.eval(b._id, abi.Q_DEMAG_FIELD, (3, *s.shape))
     np.testing.assert_array_equal(fa, fb)
+
+
+def test_tc_wait_timeout_path_leaves_the_device_usable(mpx):
+    """Failure detection without a fault: a block of the tensor-core kind waits
+    on an mbarrier that nothing arrives at; its bounded wait runs out, the
+    timeout is counted and its tensor memory released, and the next
+    tensor-core evaluation runs normally (no timeout, same field)."""
+    import ctypes as C
+
+    lib = mpx._abi.load()
+    n = C.c_uint(0)
+    assert lib.mpx_tc_timeout_selftest(C.byref(n)) == 0
+    assert n.value == 1
+    s = MagnetSpec(size=(16, 512, 2), cellsize=(2e-9, 2e-9, 1e-9), msat=8e5, aex=1.3e-11)
+    m0 = random_m(s.shape, seed=2, smooth=1)
+    world, magnet = _product(s, mpx, m0, "tf32x3")
+    eng = magnet._engine
+    got = eng.eval(magnet._id, abi.Q_DEMAG_FIELD, (3, *s.shape))
+    ow, q = _same_kernel_oracle(s, eng, magnet, m0)
+    assert max_rel(got, ow.eval(q, abi.Q_DEMAG_FIELD)) < FIELD_TOL
+    assert mpx._engine.Engine.tc_timeouts() == 0

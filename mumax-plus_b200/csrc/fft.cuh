@@ -31,6 +31,39 @@ __device__ __forceinline__ float2 cmul(float2 a, float2 b) {
 }
 __device__ __forceinline__ float2 cconj(float2 a) { return make_float2(a.x, -a.y); }
 
+// Packed FP32 pair arithmetic (add/sub.rn.f32x2 of sm_100): one instruction for
+// both components, each rounded like the scalar add/sub.  Used in the
+// butterflies whose twiddle is 1 or a general rotation; a quarter turn swaps and
+// negates components, which the scalar adds absorb for free.
+__device__ __forceinline__ float2 padd(float2 a, float2 b) {
+  float2 r;
+  asm("{\n\t.reg .b64 pa, pb, pd;\n\tmov.b64 pa, {%2, %3};\n\tmov.b64 pb, {%4, %5};\n\t"
+      "add.rn.f32x2 pd, pa, pb;\n\tmov.b64 {%0, %1}, pd;\n\t}"
+      : "=f"(r.x), "=f"(r.y)
+      : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
+  return r;
+}
+__device__ __forceinline__ float2 psub(float2 a, float2 b) {
+  float2 r;
+  asm("{\n\t.reg .b64 pa, pb, pd;\n\tmov.b64 pa, {%2, %3};\n\tmov.b64 pb, {%4, %5};\n\t"
+      "sub.rn.f32x2 pd, pa, pb;\n\tmov.b64 {%0, %1}, pd;\n\t}"
+      : "=f"(r.x), "=f"(r.y)
+      : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
+  return r;
+}
+// Butterfly e +- t where t = o rotated by exp(DIR 2 pi i M / P) (M < P/2):
+// packed unless the rotation is a quarter turn.
+template <int M, int P>
+__device__ __forceinline__ void bfly(float2 e, float2 t, float2& lo, float2& hi) {
+  if constexpr (M != 0 && 4 * M == P) {
+    lo = cadd(e, t);
+    hi = csub(e, t);
+  } else {
+    lo = padd(e, t);
+    hi = psub(e, t);
+  }
+}
+
 // padded shared-memory index and padded column length
 __device__ __forceinline__ int pidx(int i) { return i + (i >> 4); }
 __host__ __device__ constexpr int plen(int L) { return L + (L >> 4); }
@@ -111,8 +144,7 @@ struct Dft {
   __device__ __forceinline__ static void combine(float2 (&v)[N], const float2 (&e)[N / 2], const float2 (&o)[N / 2]) {
     if constexpr (K < N / 2) {
       const float2 t = rotN<DIR, N, K>(o[K]);
-      v[K] = cadd(e[K], t);
-      v[K + N / 2] = csub(e[K], t);
+      bfly<(K * (16 / N)) % 16, 16>(e[K], t, v[K], v[K + N / 2]);
       combine<K + 1>(v, e, o);
     }
   }
@@ -309,8 +341,12 @@ struct DftZ {
   __device__ __forceinline__ static void combine(float2 (&v)[N], const float2 (&e)[N / 2], const float2 (&o)[N / 2]) {
     if constexpr (K < N / 2) {
       const float2 t = rot32<DIR, (K * (32 / N)) % 32>(o[K]);
-      v[K] = cadd(e[K], t);
-      if constexpr (!LO) v[K + N / 2] = csub(e[K], t);
+      constexpr int M = (K * (32 / N)) % 32;
+      if constexpr (LO) {
+        v[K] = (M != 0 && 4 * M == 32) ? cadd(e[K], t) : padd(e[K], t);
+      } else {
+        bfly<M, 32>(e[K], t, v[K], v[K + N / 2]);
+      }
       combine<K + 1>(v, e, o);
     }
   }
@@ -333,8 +369,8 @@ struct DftZ<2, DIR, ZH, LO> {
       v[1] = v[0];
     } else {
       const float2 a = v[0], b = v[1];
-      v[0] = cadd(a, b);
-      if constexpr (!LO) v[1] = csub(a, b);
+      v[0] = padd(a, b);
+      if constexpr (!LO) v[1] = psub(a, b);
     }
   }
 };

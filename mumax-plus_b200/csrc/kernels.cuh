@@ -95,6 +95,22 @@ __device__ __forceinline__ bool load_descs(MagnetDev& sM, GroupDev& sG, const Ma
 __device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
 __device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
 
+// Bulk L2 prefetch (cp.async.bulk.prefetch.L2) of the 16-byte-aligned interior
+// of [p, p + bytes), in pieces of at most 64 KB: a hint with no completion to
+// wait for, issued by one thread for data that the block reads later (the
+// Newell spectrum slab of its kx), so that those loads find the lines in L2
+// instead of DRAM.  The range never leaves the given buffer.  (The tile rows of
+// the x passes are L2 hits already: prefetching them measured slower.)
+__device__ __forceinline__ void prefetch_l2(const void* p, size_t bytes) {
+  uintptr_t a = ((uintptr_t)p + 15) & ~(uintptr_t)15;
+  const uintptr_t e = ((uintptr_t)p + bytes) & ~(uintptr_t)15;
+  while (a < e) {
+    const uint32_t n = (uint32_t)min((uintptr_t)65536, e - a);
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(a), "r"(n) : "memory");
+    a += n;
+  }
+}
+
 // Current magnetisation used by stage `stage`: x0 for stage 0, the stage state otherwise.
 __device__ __forceinline__ const float* stage_m(const MagnetDev& M, const GroupDev& G, int stage) {
   return stage == 0 ? M.buf[G.map[0]] : M.buf[G.map[1]];
@@ -517,6 +533,17 @@ __device__ __forceinline__ void zstage_single(float2* D, int cs, const MagnetDev
   D[2 * cs + pky] = v2;
 }
 
+// L2 prefetch (thread 0) of the Newell spectrum slabs [kx][kz'][kcomp][ky'] of
+// kx0 .. kx0 + nkx - 1 that a y/z block reads in its z stage: constant data, so
+// it is issued before pdl_wait and lands while the y transforms run.
+__device__ __forceinline__ void prefetch_kslab(const MagnetDev& M, int kx0, int nkx, int Pz) {
+  if (threadIdx.x != 0) return;
+  const int n = min(nkx, M.Fh - kx0);
+  if (n <= 0) return;
+  const size_t slab = (size_t)(Pz / 2 + 1) * M.kcomp * ((1 << M.logP[1]) / 2 + 1);
+  prefetch_l2(M.kspec + (size_t)kx0 * slab, (size_t)n * slab * sizeof(float));
+}
+
 // MAXLR = 4: radix-16 passes, 16 values per thread (y lengths up to 4096, one
 // 384-thread block per SM by registers); MAXLR = 3: radix-8 passes, 8 values
 // per thread, two blocks per SM (y lengths up to 2048, z length up to 8).  At
@@ -542,6 +569,7 @@ __global__ void __launch_bounds__(384, MAXLR == 3 ? 2 : 1)
   const int ncol = nkx * 3 * nz;
   float2* tws = sm + ncol * cs;  // twiddles of length Py
   load_twiddles<MAXLR>(tws, tw, logPy);
+  prefetch_kslab(M, kx0, nkx, PZ);
   pdl_wait();  // the spectrum is written by the x pass
   // slab load: 8 independent read-only loads in flight per thread; only the
   // lower half of each column (y < Py/2, of which y >= ny is zero padding),
@@ -671,6 +699,7 @@ __device__ __forceinline__ void yzw_body(const MagnetDev& M, int kx0, int nkx, f
   float2* D = sm;
   float2* twq = sm + ncol * cs;
   load_twq(twq, tw, LOGPY);
+  prefetch_kslab(M, kx0, nkx, PZ);
   __syncthreads();
   pdl_wait();  // the spectrum is written by the x pass
   float2* S = M.spec + (size_t)kx0 * 3 * nz * ny;

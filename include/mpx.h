@@ -325,7 +325,9 @@ mpx_status mpx_demag_kernel(mpx_engine* e, int magnet, float* out, int dims[3]);
  * 45-52) when dst_magnet >= 0 -- that magnet's grid, zero outside its
  * geometry; both magnets must belong to one group (world), else
  * MPX_ERR_RUNTIME.  method MPX_STRAY_FFT (the reference's default: FFT
- * convolution through a helper grid spanning source and destination) or
+ * convolution on the pair's kernel grid, n_src + n_dst - 1 cells per axis,
+ * physics/strayfieldkernel.cu:80-99; the direct sum where a padded length
+ * would exceed 4096 along x or y or 2048 along z) or
  * MPX_STRAY_BRUTE (direct sum over the source cells,
  * physics/strayfieldbrute.cu:15-57); both include the world's periodic images
  * (the source's mastergrid and repetitions).  out: 3 x ncells floats (SoA),

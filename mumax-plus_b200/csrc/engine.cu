@@ -24,6 +24,7 @@
 #include "kernels.cuh"
 #include "newell.cuh"
 #include "stray.cuh"
+#include "pairfft.cuh"
 #include "yzsplit.cuh"
 #include "dft_tc.cuh"
 
@@ -150,7 +151,7 @@ struct Magnet {
   unsigned terms_base = 0;        // TERM_* / FLAG_* from the parameters, before stray fields
   bool msat_zero = false;
   bool stray_src = true, stray_dst = true;
-  bool hull = false;  // helper of an FFT stray-field pair: never stepped, not in its group's magnet list
+  bool probe = false;  // probe grid of a stray-field evaluation: never stepped, in no group's tables
   int pbc_rep[3] = {0, 0, 0};
   double cs_d[3] = {1, 1, 1};
   float* hstray = nullptr;        // stray field of the other magnets (3N floats), when a destination
@@ -243,6 +244,19 @@ struct SlotTable {
 
 }  // namespace
 
+// FFT form of a stray-field pair on its own kernel grid (pairfft.cuh): the
+// lengths, buffers and launch shapes of its five passes.
+struct PairPlan {
+  PairFft pf{};
+  float2* t = nullptr;   // work spectrum, 3 components
+  float2* ks = nullptr;  // kernel spectrum, 6 components
+  int ry_f = 1, zc_f = 1, tky = 1, zc_i = 1, ry_i = 1;  // rows / columns per block of each pass
+  int g_xf = 0, g_yf = 0, g_z = 0, g_yi = 0, g_xi = 0;  // grids
+  int s_xf = 0, s_yf = 0, s_z = 0, s_yi = 0, s_xi = 0;  // dynamic shared memory (bytes)
+  int s_yz = 0;  // > 0: the fused y / z pass k_pair_yz (one block per kx) with this shared memory
+  int launches() const { return s_yz > 0 ? 3 : 5; }
+};
+
 struct mpx_engine {
   int device = 0;
   cudaStream_t own = nullptr, stream = nullptr;
@@ -297,8 +311,9 @@ struct mpx_engine {
     int src, dst;
     float* k;         // direct-sum table (brute-force form), or NULL
     StrayTable tab;
-    int hull = -1;    // FFT form: slot of the helper magnet spanning A and B
-    int launches = 1; // kernels per evaluation
+    bool fft = false;  // FFT form on the pair's kernel grid (plan), else the direct sum (k, tab)
+    PairPlan plan;
+    int launches = 1;  // kernels per evaluation
   };
   std::vector<Pair> pairs;
   bool pairs_dirty = true;
@@ -694,7 +709,7 @@ mpx_status retile(mpx_engine* e, Magnet* m, int ty, int nkx) {
 long long active_set(mpx_engine* e, std::vector<Magnet*>& act) {
   act.clear();
   for (auto& mp : e->mags) {
-    if (!mp || mp->hull) continue;
+    if (!mp || mp->probe) continue;
     const Group* g = (mp->group >= 0 && mp->group < (int)e->groups.size()) ? e->groups[mp->group].get() : nullptr;
     if (g && g->active) act.push_back(mp.get());
   }
@@ -725,7 +740,7 @@ mpx_status rebuild_tables(mpx_engine* e) {
   e->nt_x = 256;
   for (int c = 0; c < YZ_CLASSES; ++c) e->smem_yz[c] = 0;
   for (auto& mp : e->mags) {
-    if (!mp || mp->hull) continue;  // helpers of FFT stray-field pairs are launched by launch_pairs
+    if (!mp || mp->probe) continue;  // probe grids of stray-field evaluations
     Magnet* m = mp.get();
     const Group* g = (m->group >= 0 && m->group < (int)e->groups.size()) ? e->groups[m->group].get() : nullptr;
     if (!g || !g->active) continue;
@@ -850,74 +865,146 @@ mpx_status setup_magnet(mpx_engine* e, Magnet* m, const mpx_magnet_desc* d, bool
 void release_all(mpx_engine* e, Magnet* m);
 
 // Pairs whose direct sum would take at least this many cell interactions use
-// the FFT form (worlds without periodic boundaries).
+// the FFT form on the pair's kernel grid (periodic images included).
 constexpr long long STRAY_FFT_MIN_INTERACTIONS = 1LL << 22;
 
-// Helper magnet of an FFT pair: the bounding box of A and B in world cells,
-// msat 1, demag only, no periodic images; its magnetisation buffer starts at zero.
-// A helper magnet spanning the bounding box of A and B (msat 1, demag only).
-// With `periodic` its demag kernel carries the periodic images of A's world
-// (image period = the world's mastergrid size, A's repetitions): the Newell
-// tensor summed over the images depends on the displacement only, so the
-// helper may be larger than the mastergrid (its exchange, which would wrap, is
-// zero).
-mpx_status create_hull(mpx_engine* e, const Magnet* A, const Magnet* B, int* out, bool periodic = false) {
-  mpx_magnet_desc d;
-  std::memset(&d, 0, sizeof d);
-  for (int ax = 0; ax < 3; ++ax) {
-    const int lo = std::min(A->dev.o[ax], B->dev.o[ax]);
-    const int hi = std::max(A->dev.o[ax] + A->dev.n[ax], B->dev.o[ax] + B->dev.n[ax]);
-    d.size[ax] = hi - lo;
-    d.origin[ax] = lo;
-    d.cellsize[ax] = A->cs_d[ax];
-    if (periodic && A->dev.mg[ax] > 0) {
-      d.mastergrid_size[ax] = A->dev.mg[ax];
-      d.mastergrid_origin[ax] = lo;
-      d.pbc_repetitions[ax] = A->pbc_rep[ax];
-    }
+// log2 of the FFT lengths of the pair grid n_A + n_B - 1 per axis; false when
+// a length exceeds what the pair passes transform (4096 along x and y, 2048
+// along z, where six kernel components share one block's shared memory).
+bool pair_fft_lengths(const int nA[3], const int nB[3], int logP[3]) {
+  for (int a = 0; a < 3; ++a) {
+    const long long K = (long long)nA[a] + nB[a] - 1;
+    int l = 0;
+    while ((1LL << l) < K) ++l;
+    if (l > (a == 2 ? 11 : 12)) return false;
+    logP[a] = l;
   }
-  d.msat.uniform = 1.0;
-  d.scale_exchange = 1.0;
-  d.enable_demag = 1;
-  d.stray_source_off = d.stray_destination_off = 1;
-  int slot = -1;
-  for (int i = 0; i < (int)e->mags.size(); ++i)
-    if (!e->mags[i]) { slot = i; break; }
-  if (slot < 0) {
-    slot = (int)e->mags.size();
-    e->mags.emplace_back();
+  return true;
+}
+
+// Launch shapes of the passes for `ncomp` components with input rows nin and
+// output window rows nout (pairfft.cuh); rows per block fill one transform
+// group of PF_POINTS points.
+void pair_shapes(PairPlan& pl, int ncomp) {
+  const PairFft& pf = pl.pf;
+  const int Px = 1 << pf.logP[0], Py = 1 << pf.logP[1], Pz = 1 << pf.logP[2], Hx = Px / 2 + 1;
+  auto cdiv = [](int a, int b) { return (a + b - 1) / b; };
+  const int f2 = (int)sizeof(float2);
+  pl.ry_f = std::max(1, std::min(pf.nin[1], PF_POINTS / Px));
+  pl.g_xf = ncomp * pf.nin[2] * cdiv(pf.nin[1], pl.ry_f);
+  pl.s_xf = (pl.ry_f * plen(Px) + Px) * f2;
+  pl.zc_f = std::max(1, std::min(pf.nin[2], PF_POINTS / Py));
+  pl.g_yf = Hx * ncomp * cdiv(pf.nin[2], pl.zc_f);
+  pl.s_yf = (pl.zc_f * plen(Py) + Py) * f2;
+  pl.tky = std::max(1, std::min(Py, PF_POINTS / (ncomp * Pz)));
+  pl.g_z = Hx * cdiv(Py, pl.tky);
+  pl.s_z = (ncomp * pl.tky * plen(Pz) + Pz) * f2;
+  pl.zc_i = std::max(1, std::min(pf.nout[2], PF_POINTS / Py));
+  pl.g_yi = Hx * ncomp * cdiv(pf.nout[2], pl.zc_i);
+  pl.s_yi = (pl.zc_i * plen(Py) + Py) * f2;
+  pl.ry_i = std::max(1, std::min(pf.nout[1], PF_POINTS / Px));
+  pl.g_xi = ncomp * pf.nout[2] * cdiv(pf.nout[1], pl.ry_i);
+  pl.s_xi = (pl.ry_i * plen(Px) + Px) * f2;
+  const int syz = (3 * Pz * plen(Py) + Py) * f2;
+  pl.s_yz = (ncomp == 3 && Pz <= 8 && syz <= SMEM_MAX - 8192) ? syz : 0;
+}
+
+void free_pair_plan(mpx_engine* e, PairPlan& pl) {
+  pfree(e, pl.t);
+  pfree(e, pl.ks);
+  pl.t = pl.ks = nullptr;
+}
+
+// The plan of source A on the destination grid (nB, oB): FFT lengths, the
+// buffers, and the kernel spectrum from the FP64-built table of the pair's
+// displacements (periodic images of `gimg`: mastergrid and repetitions).
+mpx_status build_pair_fft(mpx_engine* e, const Magnet* A, const int nB[3], const int oB[3], const KernelGeom& gimg,
+                          PairPlan& pl) {
+  PairFft& pf = pl.pf;
+  if (!pair_fft_lengths(A->dev.n, nB, pf.logP)) return fail(MPX_ERR_UNSUPPORTED, "stray-field FFT grid too large");
+  int K[3], O[3];
+  for (int a = 0; a < 3; ++a) {
+    K[a] = A->dev.n[a] + nB[a] - 1;
+    O[a] = oB[a] - A->dev.o[a] - (A->dev.n[a] - 1);
   }
-  auto m = std::make_unique<Magnet>();
-  std::memset(&m->dev, 0, sizeof(MagnetDev));
-  m->slot = slot;
-  m->group = A->group;
-  m->hull = true;
-  m->uid = e->next_uid++;
-  mpx_status st = setup_magnet(e, m.get(), &d, false);
-  if (st == MPX_OK) {
-    const cudaError_t ce = cudaMemsetAsync(m->dev.buf[0], 0, sizeof(float) * 3 * (size_t)m->dev.N, e->stream);
-    if (ce != cudaSuccess) st = fail(MPX_ERR_CUDA, cudaGetErrorString(ce));
-  }
+  const int Px = 1 << pf.logP[0], Py = 1 << pf.logP[1], Pz = 1 << pf.logP[2], Hx = Px / 2 + 1;
+  const size_t vol = (size_t)Hx * Pz * Py;
+  MPX_TRY(palloc(e, (void**)&pl.t, sizeof(float2) * 3 * vol));
+  mpx_status st = palloc(e, (void**)&pl.ks, sizeof(float2) * 6 * vol);
+  float* tab = nullptr;
+  if (st == MPX_OK) st = palloc(e, (void**)&tab, sizeof(float) * 6 * (size_t)K[0] * K[1] * K[2]);
   if (st != MPX_OK) {
-    std::string msg = g_last_error;
-    release_all(e, m.get());
-    g_last_error = msg;
+    free_pair_plan(e, pl);
     return st;
   }
-  e->mags[slot] = std::move(m);
-  *out = slot;
+  k_newell_reflayout<<<148 * 8, 128, 0, e->stream>>>(tab, gimg, K[0], K[1], K[2], O[0], O[1], O[2]);
+  // kernel spectrum: the forward passes over the six tabulated components
+  PairPlan kp;
+  kp.pf = pf;
+  kp.pf.t = pl.ks;
+  kp.pf.ks = nullptr;
+  for (int a = 0; a < 3; ++a) kp.pf.nin[a] = kp.pf.nout[a] = K[a];
+  kp.pf.win[0] = kp.pf.win[1] = kp.pf.win[2] = 0;
+  pair_shapes(kp, 6);
+  k_pair_xfwd<true><<<kp.g_xf, PF_THREADS, kp.s_xf, e->stream>>>(e->d_mags, e->d_groups, -1, 0, 0, tab, kp.pf, 6,
+                                                                  kp.ry_f, e->d_tw);
+  k_pair_yfft<-1><<<kp.g_yf, PF_THREADS, kp.s_yf, e->stream>>>(e->d_mags, e->d_groups, -1, 0, 0, kp.pf, 6, kp.zc_f,
+                                                                e->d_tw);
+  k_pair_zmul<false><<<kp.g_z, PF_THREADS, kp.s_z, e->stream>>>(e->d_mags, e->d_groups, -1, 0, 0, kp.pf, 6, kp.tky,
+                                                                 e->d_tw);
+  e->launches += 4;
+  pfree(e, tab);
+  pf.t = pl.t;
+  pf.ks = pl.ks;
+  for (int a = 0; a < 3; ++a) {
+    pf.nin[a] = A->dev.n[a];
+    pf.win[a] = A->dev.n[a] - 1;
+    pf.nout[a] = nB[a];
+  }
+  pf.scale = (float)(-1.25663706212e-6 / ((double)Px * Py * Pz));
+  pair_shapes(pl, 3);
+  const cudaError_t ce = cudaGetLastError();
+  if (ce != cudaSuccess) {
+    free_pair_plan(e, pl);
+    return fail(MPX_ERR_CUDA, std::string("stray-field FFT kernel: ") + cudaGetErrorString(ce));
+  }
   return MPX_OK;
+}
+
+// The five passes of one evaluation: the field of `src`'s state for `stage`
+// into out (3 x N of `dst`, added with `add`); `gate` as the stage kernels.
+void launch_pair_fft(mpx_engine* e, const PairPlan& pl, int src, int dst, int stage, int gate, int add, float* out) {
+  const PairFft& pf = pl.pf;
+  k_pair_xfwd<false><<<pl.g_xf, PF_THREADS, pl.s_xf, e->stream>>>(e->d_mags, e->d_groups, src, stage, gate, nullptr,
+                                                                   pf, 3, pl.ry_f, e->d_tw);
+  if (pl.s_yz > 0) {
+    const int Hx = (1 << pf.logP[0]) / 2 + 1;
+    switch (pf.logP[2]) {
+      case 0: k_pair_yz<1><<<Hx, PF_THREADS, pl.s_yz, e->stream>>>(e->d_mags, e->d_groups, src, stage, gate, pf, e->d_tw); break;
+      case 1: k_pair_yz<2><<<Hx, PF_THREADS, pl.s_yz, e->stream>>>(e->d_mags, e->d_groups, src, stage, gate, pf, e->d_tw); break;
+      case 2: k_pair_yz<4><<<Hx, PF_THREADS, pl.s_yz, e->stream>>>(e->d_mags, e->d_groups, src, stage, gate, pf, e->d_tw); break;
+      default: k_pair_yz<8><<<Hx, PF_THREADS, pl.s_yz, e->stream>>>(e->d_mags, e->d_groups, src, stage, gate, pf, e->d_tw); break;
+    }
+  } else {
+    k_pair_yfft<-1><<<pl.g_yf, PF_THREADS, pl.s_yf, e->stream>>>(e->d_mags, e->d_groups, src, stage, gate, pf, 3,
+                                                                  pl.zc_f, e->d_tw);
+    k_pair_zmul<true><<<pl.g_z, PF_THREADS, pl.s_z, e->stream>>>(e->d_mags, e->d_groups, src, stage, gate, pf, 3,
+                                                                  pl.tky, e->d_tw);
+    k_pair_yfft<1><<<pl.g_yi, PF_THREADS, pl.s_yi, e->stream>>>(e->d_mags, e->d_groups, src, stage, gate, pf, 3,
+                                                                 pl.zc_i, e->d_tw);
+  }
+  k_pair_xinv<<<pl.g_xi, PF_THREADS, pl.s_xi, e->stream>>>(e->d_mags, e->d_groups, dst, stage, gate, pf, pl.ry_i, add,
+                                                           out, e->d_tw);
+  e->launches += pl.launches();
 }
 
 mpx_status rebuild_pairs(mpx_engine* e) {
   NvtxRange nvtx_range("rebuild_pairs");
-  for (auto& p : e->pairs) pfree(e, p.k);
+  for (auto& p : e->pairs) {
+    pfree(e, p.k);
+    free_pair_plan(e, p.plan);
+  }
   e->pairs.clear();
-  for (auto& mp : e->mags)  // helpers of the previous pairs
-    if (mp && mp->hull) {
-      release_all(e, mp.get());
-      mp.reset();
-    }
   std::vector<bool> is_dst(e->mags.size(), false);
   for (auto& gp : e->groups) {
     if (!gp) continue;
@@ -931,16 +1018,6 @@ mpx_status rebuild_pairs(mpx_engine* e) {
         p.src = a;
         p.dst = b;
         p.k = nullptr;
-        bool periodic = false;
-        for (int ax = 0; ax < 3; ++ax) periodic = periodic || A->dev.mg[ax] > 0 || B->dev.mg[ax] > 0;
-        if (!periodic && (long long)A->dev.N * B->dev.N >= STRAY_FFT_MIN_INTERACTIONS) {
-          MPX_TRY(create_hull(e, A, B, &p.hull));
-          const Magnet* H = e->mags[p.hull].get();
-          p.launches = 4 + (H->split ? 3 : 1);
-          e->pairs.push_back(p);
-          is_dst[b] = true;
-          continue;
-        }
         KernelGeom g;
         for (int ax = 0; ax < 3; ++ax) {
           p.tab.K[ax] = A->dev.n[ax] + B->dev.n[ax] - 1;
@@ -949,6 +1026,15 @@ mpx_status rebuild_pairs(mpx_engine* e) {
           g.mg[ax] = B->dev.mg[ax];
           g.pbc[ax] = B->pbc_rep[ax];
           g.cs[ax] = B->cs_d[ax];
+        }
+        int logP[3];
+        if ((long long)A->dev.N * B->dev.N >= STRAY_FFT_MIN_INTERACTIONS && pair_fft_lengths(A->dev.n, B->dev.n, logP)) {
+          MPX_TRY(build_pair_fft(e, A, B->dev.n, B->dev.o, g, p.plan));
+          p.fft = true;
+          p.launches = p.plan.launches();
+          e->pairs.push_back(p);
+          is_dst[b] = true;
+          continue;
         }
         const size_t KK = (size_t)p.tab.K[0] * p.tab.K[1] * p.tab.K[2];
         MPX_TRY(palloc(e, (void**)&p.k, sizeof(float) * 6 * KK));
@@ -962,7 +1048,7 @@ mpx_status rebuild_pairs(mpx_engine* e) {
   }
   for (size_t i = 0; i < e->mags.size(); ++i) {
     Magnet* m = e->mags[i].get();
-    if (!m || m->hull) continue;
+    if (!m || m->probe) continue;
     unsigned terms = m->terms_base;
     if (i < is_dst.size() && is_dst[i]) {
       if (!m->hstray) MPX_TRY(palloc(e, (void**)&m->hstray, sizeof(float) * 3 * (size_t)m->dev.N));
@@ -992,31 +1078,8 @@ mpx_status launch_pairs(mpx_engine* e, int dst, int stage, int gate) {
     const bool add = std::find(seen.begin(), seen.end(), p.dst) != seen.end();
     if (!add) seen.push_back(p.dst);
     Magnet* B = get_mag(e, p.dst);
-    if (p.hull >= 0) {  // FFT form through the helper magnet
-      Magnet* A = get_mag(e, p.src);
-      Magnet* H = get_mag(e, p.hull);
-      k_hull_scatter<<<(A->dev.N + 255) / 256, 256, 0, e->stream>>>(e->d_mags, e->d_groups, p.src, p.hull, stage,
-                                                                     gate);
-      const int ntile = (int)H->tiles.size(), sx = x_smem(H), nt = x_threads(H);
-      k_xfwd<false><<<ntile, nt, sx, e->stream>>>(e->d_mags, e->d_groups, H->d_tiles, stage, gate, H->dev.buf[0],
-                                                  e->d_tw);
-      if (H->split)
-        MPX_TRY(launch_split(e, H->d_ycw, (int)H->ycw.size(), H->d_zmw, (int)H->zmw.size(), ycols_smem(H),
-                             zmul_smem(H), H->P[1], H->P[2], stage, gate));
-      else
-        MPX_TRY(launch_yz(e, yz_class(H), H->d_kxw, (int)H->kxw.size(), yz_smem(H), stage, gate));
-      EpiArgs ea;
-      ea.mode = EPI_EVAL;
-      ea.stage = stage;
-      ea.quantity = MPX_Q_DEMAG_FIELD;
-      ea.fsal_err = 0;
-      ea.gate = gate;
-      ea.out = H->dev.buf[1];
-      ea.msrc = H->dev.buf[0];
-      CUDA_TRY(launch_pdl(k_xinv, ntile, nt, sx, e->stream, e->d_mags, e->d_groups, H->d_tiles, ea, e->d_tw));
-      k_hull_gather<<<(B->dev.N + 255) / 256, 256, 0, e->stream>>>(e->d_mags, e->d_groups, p.hull, p.dst, stage, gate,
-                                                                    add ? 1 : 0, B->hstray);
-      e->launches += 4;
+    if (p.fft) {
+      launch_pair_fft(e, p.plan, p.src, p.dst, stage, gate, add ? 1 : 0, B->hstray);
       continue;
     }
     k_stray_pair<<<(B->dev.N + 255) / 256, 256, 0, e->stream>>>(e->d_mags, e->d_groups, p.src, p.dst, p.tab, stage,
@@ -1348,7 +1411,7 @@ mpx_status setup_magnet(mpx_engine* e, Magnet* m, const mpx_magnet_desc* d, bool
                                        "(grid side above 1024 along x or 2048 along y)");
     // thick magnets (nz > 8) and long y transforms of many columns take the split y/z path;
     // so do y lengths 1024 and 2048 when the engine runs the tensor-core y transforms
-    m->tc = e->dft_mode == MPX_DFT_TF32X3 && (m->P[1] == 1024 || m->P[1] == 2048) && !m->hull;
+    m->tc = e->dft_mode == MPX_DFT_TF32X3 && (m->P[1] == 1024 || m->P[1] == 2048) && !m->probe;
     m->split = m->tc || m->P[2] > 16 || yz_smem(m) > SMEM_DYN_MAX;
     if (m->split) {
       if (m->P[2] > MAX_FFT) return fail(MPX_ERR_UNSUPPORTED, "demag: padded FFT length above 4096 along z");
@@ -1793,7 +1856,12 @@ mpx_status mpx_engine_create(int device, mpx_engine** out) {
                                (const void*)k_yzw<1>, (const void*)k_yzw<2>, (const void*)k_yzw<4>,
                                (const void*)k_yzw<8>, (const void*)k_yzw<16>, (const void*)k_yzw32<1>,
                                (const void*)k_yzw32<2>, (const void*)k_yzw32<4>, (const void*)k_yzw32<8>,
-                               (const void*)k_yzw32<16>};
+                               (const void*)k_yzw32<16>, (const void*)k_pair_xfwd<true>,
+                               (const void*)k_pair_xfwd<false>, (const void*)k_pair_yfft<-1>,
+                               (const void*)k_pair_yfft<1>, (const void*)k_pair_zmul<true>,
+                               (const void*)k_pair_zmul<false>, (const void*)k_pair_xinv,
+                               (const void*)k_pair_yz<1>, (const void*)k_pair_yz<2>, (const void*)k_pair_yz<4>,
+                               (const void*)k_pair_yz<8>};
   // the DFT32 matrix of the tensor-core y transforms in its real 64 x 64 form
   // B[2 k + r][2 n + s] (output k, part r; input n, part s; forward, angle
   // 2 pi k n / 32): re <- cos re + sin im, im <- -sin re + cos im; split into
@@ -1874,7 +1942,7 @@ mpx_status mpx_engine_set_dft(mpx_engine* e, int mode) {
   if (!e) return fail(MPX_ERR_INVALID, "null engine");
   if (mode != MPX_DFT_FP32 && mode != MPX_DFT_TF32X3) return fail(MPX_ERR_INVALID, "unknown DFT mode");
   for (auto& m : e->mags)
-    if (m && !m->hull) return fail(MPX_ERR_INVALID, "set the DFT mode before adding magnets");
+    if (m && !m->probe) return fail(MPX_ERR_INVALID, "set the DFT mode before adding magnets");
   e->dft_mode = mode;
   return MPX_OK;
 }
@@ -2242,7 +2310,7 @@ mpx_status mpx_magnet_bytes(const mpx_magnet_desc* d, int64_t* resident, int64_t
 
 mpx_status mpx_magnet_remove(mpx_engine* e, int magnet) {
   Magnet* m = get_mag(e, magnet);
-  if (!m || m->hull) return fail(MPX_ERR_RANGE, "no such magnet");
+  if (!m || m->probe) return fail(MPX_ERR_RANGE, "no such magnet");
   DeviceGuard guard(e->device);
   // frees are stream-ordered: attempts queued before still see the buffers
   Group* g = get_group(e, m->group);
@@ -2360,21 +2428,21 @@ mpx_status mpx_energy(mpx_engine* e, int magnet, int quantity, double* out) {
 // the field of `src`'s current state on a destination grid, by direct sum over
 // the source cells (METHOD_BRUTE, physics/strayfieldbrute.cu:15-57: the FP64
 // Newell tensor of the displacements with the world's periodic images,
-// tabulated in FP32) or by FFT convolution (METHOD_FFT, the default of the
-// reference, physics/strayfieldfft.cu): the demag passes of a helper magnet
-// spanning both grids, holding Ms m of the source and zero elsewhere.
+// tabulated in FP32) or by FFT convolution of the same table on the pair's
+// kernel grid (METHOD_FFT, the default of the reference,
+// physics/strayfieldfft.cu; pairfft.cuh).
 mpx_status mpx_stray_field(mpx_engine* e, int src, int dst_magnet, const int size[3], const int origin[3], int method,
                            float* out, int on_device) {
   if (!e || !out) return fail(MPX_ERR_INVALID, "null engine / output");
   if (method != MPX_STRAY_FFT && method != MPX_STRAY_BRUTE)
     return fail(MPX_ERR_INVALID, "Method should be \"fft\" or \"brute\"");
   Magnet* A = get_mag(e, src);
-  if (!A || A->hull) return fail(MPX_ERR_RANGE, "no such source magnet");
+  if (!A || A->probe) return fail(MPX_ERR_RANGE, "no such source magnet");
   DeviceGuard guard(e->device);
   int dst = dst_magnet, tmp = -1;
   if (dst_magnet >= 0) {
     Magnet* B0 = get_mag(e, dst_magnet);
-    if (!B0 || B0->hull) return fail(MPX_ERR_RANGE, "no such destination magnet");
+    if (!B0 || B0->probe) return fail(MPX_ERR_RANGE, "no such destination magnet");
     if (B0->group != A->group) return fail(MPX_ERR_RUNTIME, "Can not compute the magnetic field of the magnet");
   } else {
     if (!size || !origin) return fail(MPX_ERR_INVALID, "null grid");
@@ -2401,7 +2469,7 @@ mpx_status mpx_stray_field(mpx_engine* e, int src, int dst_magnet, const int siz
     std::memset(&m->dev, 0, sizeof(MagnetDev));
     m->slot = tmp;
     m->group = A->group;
-    m->hull = true;  // a probe of the destination grid: in no group's tables
+    m->probe = true;  // a probe of the destination grid: in no group's tables
     m->uid = e->next_uid++;
     const mpx_status st = setup_magnet(e, m.get(), &d, false);
     if (st != MPX_OK) {
@@ -2432,60 +2500,37 @@ mpx_status mpx_stray_field(mpx_engine* e, int src, int dst_magnet, const int siz
   if (A->msat_zero) {  // physics/strayfield.cpp:77-80: assuredly zero
     const cudaError_t ce = cudaMemsetAsync(dout, 0, sizeof(float) * 3 * (size_t)NB, e->stream);
     if (ce != cudaSuccess) st = fail(MPX_ERR_CUDA, cudaGetErrorString(ce));
-  } else if (method == MPX_STRAY_BRUTE) {
-    StrayTable tab;
-    KernelGeom g;
+  } else {
+    KernelGeom g;  // the source world's periodic images
     for (int ax = 0; ax < 3; ++ax) {
-      tab.K[ax] = A->dev.n[ax] + B->dev.n[ax] - 1;
-      tab.O[ax] = B->dev.o[ax] - A->dev.o[ax] - (A->dev.n[ax] - 1);
       g.n[ax] = B->dev.n[ax];
       g.mg[ax] = A->dev.mg[ax];
       g.pbc[ax] = A->pbc_rep[ax];
       g.cs[ax] = A->cs_d[ax];
     }
-    const size_t KK = (size_t)tab.K[0] * tab.K[1] * tab.K[2];
-    float* k = nullptr;
-    st = palloc(e, (void**)&k, sizeof(float) * 6 * KK);
-    if (st == MPX_OK) {
-      k_newell_reflayout<<<148 * 8, 128, 0, e->stream>>>(k, g, tab.K[0], tab.K[1], tab.K[2], tab.O[0], tab.O[1],
-                                                         tab.O[2]);
-      tab.k = k;
-      k_stray_pair<<<(NB + 255) / 256, 256, 0, e->stream>>>(e->d_mags, e->d_groups, src, dst, tab, 0, 0, 0, dout);
-      e->launches += 2;
-      pfree(e, k);
-    }
-  } else {
-    bool periodic = false;
-    for (int ax = 0; ax < 3; ++ax) periodic = periodic || A->dev.mg[ax] > 0;
-    int hull = -1;
-    st = create_hull(e, A, B, &hull, periodic);
-    if (st == MPX_OK) {
-      Magnet* H = get_mag(e, hull);
-      k_hull_scatter<<<(A->dev.N + 255) / 256, 256, 0, e->stream>>>(e->d_mags, e->d_groups, src, hull, 0, 0);
-      const int ntile = (int)H->tiles.size(), sx = x_smem(H), nt = x_threads(H);
-      k_xfwd<false><<<ntile, nt, sx, e->stream>>>(e->d_mags, e->d_groups, H->d_tiles, 0, 0, H->dev.buf[0], e->d_tw);
-      if (H->split)
-        st = launch_split(e, H->d_ycw, (int)H->ycw.size(), H->d_zmw, (int)H->zmw.size(), ycols_smem(H), zmul_smem(H),
-                          H->P[1], H->P[2], 0, 0);
-      else
-        st = launch_yz(e, yz_class(H), H->d_kxw, (int)H->kxw.size(), yz_smem(H), 0, 0);
-      if (st == MPX_OK) {
-        EpiArgs ea;
-        ea.mode = EPI_EVAL;
-        ea.stage = 0;
-        ea.quantity = MPX_Q_DEMAG_FIELD;
-        ea.fsal_err = 0;
-        ea.gate = 0;
-        ea.out = H->dev.buf[1];
-        ea.msrc = H->dev.buf[0];
-        const cudaError_t ce =
-            launch_pdl(k_xinv, ntile, nt, sx, e->stream, e->d_mags, e->d_groups, H->d_tiles, ea, e->d_tw);
-        if (ce != cudaSuccess) st = fail(MPX_ERR_CUDA, cudaGetErrorString(ce));
-        k_hull_gather<<<(NB + 255) / 256, 256, 0, e->stream>>>(e->d_mags, e->d_groups, hull, dst, 0, 0, 0, dout);
-        e->launches += 4;
+    int logP[3];
+    if (method == MPX_STRAY_FFT && pair_fft_lengths(A->dev.n, B->dev.n, logP)) {
+      PairPlan pl;
+      st = build_pair_fft(e, A, B->dev.n, B->dev.o, g, pl);
+      if (st == MPX_OK) launch_pair_fft(e, pl, src, dst, 0, 0, 0, dout);
+      free_pair_plan(e, pl);
+    } else {  // the direct sum (also the FFT method's form for pair grids beyond the FFT lengths)
+      StrayTable tab;
+      for (int ax = 0; ax < 3; ++ax) {
+        tab.K[ax] = A->dev.n[ax] + B->dev.n[ax] - 1;
+        tab.O[ax] = B->dev.o[ax] - A->dev.o[ax] - (A->dev.n[ax] - 1);
       }
-      release_all(e, H);
-      e->mags[hull].reset();
+      const size_t KK = (size_t)tab.K[0] * tab.K[1] * tab.K[2];
+      float* k = nullptr;
+      st = palloc(e, (void**)&k, sizeof(float) * 6 * KK);
+      if (st == MPX_OK) {
+        k_newell_reflayout<<<148 * 8, 128, 0, e->stream>>>(k, g, tab.K[0], tab.K[1], tab.K[2], tab.O[0], tab.O[1],
+                                                           tab.O[2]);
+        tab.k = k;
+        k_stray_pair<<<(NB + 255) / 256, 256, 0, e->stream>>>(e->d_mags, e->d_groups, src, dst, tab, 0, 0, 0, dout);
+        e->launches += 2;
+        pfree(e, k);
+      }
     }
   }
   if (st == MPX_OK) {

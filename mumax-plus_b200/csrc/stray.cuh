@@ -88,47 +88,4 @@ __global__ void __launch_bounds__(256) k_stray_pair(const MagnetDev* __restrict_
   store3(out, NB, i, h);
 }
 
-// FFT form for large pairs (the reference's default executor, physics/strayfieldfft.cu):
-// a helper magnet spanning the bounding box of A and B (msat 1, demag only)
-// takes Ms_A m_A in A's cells and zero elsewhere; its demag field, evaluated by
-// the x / y-z / x passes, is at B's cells the stray field of A (the Newell
-// tensor depends on the displacement only).
-
-// Ms_A m_A of the stage state into the helper's magnetisation buffer (buf[0]) at A's cells.
-__global__ void __launch_bounds__(256) k_hull_scatter(const MagnetDev* __restrict__ mags,
-                                                      const GroupDev* __restrict__ groups, int src, int hull, int stage,
-                                                      int gate) {
-  __shared__ MagnetDev MA;
-  __shared__ GroupDev G;
-  if (!load_descs(MA, G, mags, groups, src, gate, stage)) return;
-  const MagnetDev& MH = mags[hull];
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= MA.N) return;
-  const int x = i % MA.n[0], y = (i / MA.n[0]) % MA.n[1], z = i / (MA.n[0] * MA.n[1]);
-  const int h = (MA.o[0] - MH.o[0] + x) + MH.n[0] * ((MA.o[1] - MH.o[1] + y) + MH.n[1] * (MA.o[2] - MH.o[2] + z));
-  const bool ing = !MA.geom || MA.geom[i];
-  const float ms = ing ? MA.msat.at(i) : 0.f;
-  const float3 m = load3(stage_m(MA, G, stage), MA.N, i);
-  store3(MH.buf[0], MH.N, h, ms * m);
-}
-
-// The helper's demag field (buf[1]) at B's cells into out (added with `add`),
-// zero outside B's geometry, as k_stray_pair.
-__global__ void __launch_bounds__(256) k_hull_gather(const MagnetDev* __restrict__ mags,
-                                                     const GroupDev* __restrict__ groups, int hull, int dst, int stage,
-                                                     int gate, int add, float* __restrict__ out) {
-  __shared__ MagnetDev MB;
-  __shared__ GroupDev G;
-  if (!load_descs(MB, G, mags, groups, dst, gate, stage)) return;
-  const MagnetDev& MH = mags[hull];
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= MB.N) return;
-  const int x = i % MB.n[0], y = (i / MB.n[0]) % MB.n[1], z = i / (MB.n[0] * MB.n[1]);
-  const int h = (MB.o[0] - MH.o[0] + x) + MH.n[0] * ((MB.o[1] - MH.o[1] + y) + MH.n[1] * (MB.o[2] - MH.o[2] + z));
-  float3 v = load3(MH.buf[1], MH.N, h);
-  if (MB.geom && !MB.geom[i]) v = f3(0.f, 0.f, 0.f);
-  if (add) v = v + load3(out, MB.N, i);
-  store3(out, MB.N, i, v);
-}
-
 }  // namespace mpx

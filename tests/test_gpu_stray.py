@@ -96,8 +96,8 @@ def _large_specs(dz=0):
 
 @pytest.mark.parametrize("dz", [0, 3])
 def test_large_pair_fft_form(mpx, dz):
-    """Pairs of at least 2^22 cell interactions take the FFT form (a helper magnet spanning both, its demag field
-    at the destination cells): fields of both magnets against the oracle's direct sum."""
+    """Pairs of at least 2^22 cell interactions take the FFT form on the pair's kernel grid (n_A + n_B - 1 per
+    axis): fields of both magnets against the oracle's direct sum."""
     specs = _large_specs(dz)
     assert specs[0].shape[0] * specs[0].shape[1] * specs[0].shape[2] * \
         specs[1].shape[0] * specs[1].shape[1] * specs[1].shape[2] >= 1 << 22
@@ -130,6 +130,63 @@ def test_large_pair_fft_form_trajectory(mpx):
             worst = max(worst, float(np.max(np.abs(np.array(mag.magnetization.average())
                                                     - np.array(ow.average(q, abi.Q_MAGNETIZATION))))))
     assert worst < 1e-5, worst
+
+
+def test_large_pair_fft_form_periodic(mpx):
+    """The FFT form in a world with periodic images (mastergrid 128 x 64, one repetition along x and y): the
+    tabulated tensor carries the images, so the pair keeps the FFT form; fields of both magnets against the
+    oracle's direct sum with the same images."""
+    mg, pbc = (128, 64, 0), (1, 1, 0)
+    specs = _large_specs(0)
+    for s in specs:
+        s.mastergrid_size, s.pbc = mg, pbc
+    ms = [random_m(s.shape, seed=60 + k, smooth=2) for k, s in enumerate(specs)]
+    ow, qs = _oracle(specs, ms)
+    world = mpx.World(CS, pbc_repetitions=pbc, mastergrid=mpx.Grid(mg))
+    mags = []
+    for s, m in zip(specs, ms):
+        mag = mpx.Ferromagnet(world, mpx.Grid(s.size, s.origin))
+        mag._suspend = True
+        mag.msat, mag.aex, mag.alpha = s.msat, s.aex, s.alpha
+        mag._suspend = False
+        mag._update()
+        mag.magnetization = m
+        mags.append(mag)
+    for q, mag, s in zip(qs, mags, specs):
+        for quantity in (abi.Q_EXTERNAL_FIELD, abi.Q_EFFECTIVE_FIELD):
+            want = ow.eval(q, quantity)
+            got = mag._engine.eval(mag._id, quantity, (3, *s.shape))
+            assert max_rel(got, want) < 1e-5, (quantity, max_rel(got, want))
+
+
+# Grids far apart: the pair's kernel grid depends on the two sizes only (a
+# single-layer source and a single-layer destination 40 layers above convolve
+# in 2-D; a destination 600 cells along x needs no longer x transforms than an
+# adjacent one).  z lengths 1 .. 8 take the fused y / z pass, 16 the three
+# separate passes.
+FAR_CASES = [
+    ((64, 48, 1), (0, 0, 0), (64, 48, 1), (0, 0, 40)),
+    ((64, 48, 1), (0, 0, 0), (40, 30, 2), (600, 10, 3)),
+    ((30, 20, 3), (0, 0, 0), (50, 70, 1), (-20, -90, -12)),
+    ((20, 16, 8), (0, 0, 0), (16, 12, 8), (30, 0, 4)),  # z length 16: the y / z passes unfused
+]
+
+
+@pytest.mark.parametrize("pbc", [None, (1, 1, 0)])
+@pytest.mark.parametrize("case", FAR_CASES)
+def test_stray_field_far_grids_fft_against_brute(mpx, case, pbc):
+    msize, morig, hsize, horig = case
+    world = mpx.World(STRAY_CS)
+    magnet = mpx.Ferromagnet(world, mpx.Grid(msize, morig))
+    magnet.msat = 800e3
+    magnet.magnetization = random_m((msize[2], msize[1], msize[0]), seed=7, smooth=1)
+    if pbc is not None:
+        world.set_pbc(pbc)
+    sf = mpx.StrayField(magnet, mpx.Grid(hsize, horig))
+    result = sf.eval()
+    sf.set_method("brute")
+    wanted = sf.eval()
+    assert max_rel(result, wanted) < 1e-5, max_rel(result, wanted)
 
 
 # ------------------------------------------------ StrayField on other grids

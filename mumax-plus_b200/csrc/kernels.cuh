@@ -948,11 +948,25 @@ __device__ __forceinline__ bool lean_ok(const MagnetDev& M) {
   return M.fast && !M.geom && (M.mg[0] == 0 || (off >= 0 && off + M.n[0] <= M.mg[0]));
 }
 
+// DMI tensor kinds of the lean path: DMI_IFACE when the only nonzero entries
+// are D_x^{xz} and D_y^{yz} (interfacial DMI: the x and y neighbours each add
+// two products, the z neighbours none), DMI_GENERAL otherwise.  Leaving out
+// the products with zero coefficients changes no sum: each of them added an
+// exact zero.
+constexpr int DMI_IFACE = 1, DMI_GENERAL = 2;
+__device__ __forceinline__ int dmi_kind(const MagnetDev& M) {
+  const float* f = M.fd;
+  return (f[0] == 0.f && f[2] == 0.f && f[3] == 0.f && f[4] == 0.f && f[6] == 0.f && f[7] == 0.f && f[8] == 0.f)
+             ? DMI_IFACE
+             : DMI_GENERAL;
+}
+
 // Contribution of neighbour r (0..5: x-, x+, y-, y+, z-, z+) of a cell with
 // state mc to its exchange (he) and DMI (hd) sums on the lean path; `present`:
 // the neighbour exists (its state mn), else the Neumann ghost or nothing.
-// INNER: every neighbour is present (the ghost-cell code is left out).
-template <bool INNER>
+// INNER: every neighbour is present (the ghost-cell code is left out).  DK:
+// the DMI tensor kind.
+template <bool INNER, int DK = DMI_GENERAL>
 __device__ __forceinline__ void neighbour_term(const MagnetDev& M, int r, bool present, float3 mn, float3 mc,
                                                bool neumann, bool dmi_open, bool do_exch, bool do_dmi, float3& he,
                                                float3& hd) {
@@ -966,17 +980,29 @@ __device__ __forceinline__ void neighbour_term(const MagnetDev& M, int r, bool p
   }
   if (do_exch && (nin || neumann)) he = he + M.fe[axis] * (m_ - mc);
   if (do_dmi && (nin || !dmi_open)) {
-    const float Dxy = M.fd[3 * axis], Dxz = M.fd[3 * axis + 1], Dyz = M.fd[3 * axis + 2];
     const float inv_delta = d * M.inv_cs[axis];
-    hd.x += (Dxy * m_.y + Dxz * m_.z) * inv_delta;
-    hd.y += (-Dxy * m_.x + Dyz * m_.z) * inv_delta;
-    hd.z += (-Dxz * m_.x - Dyz * m_.y) * inv_delta;
+    if constexpr (DK == DMI_IFACE) {
+      if (axis == 0) {
+        const float Dxz = M.fd[1];
+        hd.x += (Dxz * m_.z) * inv_delta;
+        hd.z += (-Dxz * m_.x) * inv_delta;
+      } else if (axis == 1) {
+        const float Dyz = M.fd[5];
+        hd.y += (Dyz * m_.z) * inv_delta;
+        hd.z += (-Dyz * m_.y) * inv_delta;
+      }
+    } else {
+      const float Dxy = M.fd[3 * axis], Dxz = M.fd[3 * axis + 1], Dyz = M.fd[3 * axis + 2];
+      hd.x += (Dxy * m_.y + Dxz * m_.z) * inv_delta;
+      hd.y += (-Dxy * m_.x + Dyz * m_.z) * inv_delta;
+      hd.z += (-Dxz * m_.x - Dyz * m_.y) * inv_delta;
+    }
   }
 }
 
 // Exchange and DMI sums over the six neighbours nb[] (-1: none) of the lean
 // path, in the order of local_terms_fast.
-template <bool INNER>
+template <bool INNER, int DK>
 __device__ __forceinline__ void neighbour_sums(const MagnetDev& M, const float* __restrict__ m, int N, const int (&nb)[6],
                                                float3 mc, bool neumann, bool dmi_open, bool do_exch, bool do_dmi,
                                                float3& he, float3& hd) {
@@ -985,7 +1011,7 @@ __device__ __forceinline__ void neighbour_sums(const MagnetDev& M, const float* 
   for (int r = 0; r < 6; ++r) mn[r] = (INNER || nb[r] >= 0) ? ldg3(m, N, nb[r]) : mc;
 #pragma unroll
   for (int r = 0; r < 6; ++r)
-    neighbour_term<INNER>(M, r, nb[r] >= 0, mn[r], mc, neumann, dmi_open, do_exch, do_dmi, he, hd);
+    neighbour_term<INNER, DK>(M, r, nb[r] >= 0, mn[r], mc, neumann, dmi_open, do_exch, do_dmi, he, hd);
 }
 
 // The rest of a lean-path cell once its exchange / DMI sums are known:
@@ -1041,10 +1067,13 @@ __device__ __forceinline__ float3 stage_cell_lean(const MagnetDev& M, const Grou
       nb[2 + q] = b >= 0 ? b + x : -1;
     }
     const bool inner = nb[0] >= 0 && nb[1] >= 0 && nb[2] >= 0 && nb[3] >= 0 && nb[4] >= 0 && nb[5] >= 0;
+    const bool ifc = do_dmi && dmi_kind(M) == DMI_IFACE;
     if (__all_sync(__activemask(), inner)) {  // every neighbour present: no ghost cells
-      neighbour_sums<true>(M, m, N, nb, mc, neumann, dmi_open, do_exch, do_dmi, he, hd);
+      if (ifc) neighbour_sums<true, DMI_IFACE>(M, m, N, nb, mc, neumann, dmi_open, do_exch, do_dmi, he, hd);
+      else neighbour_sums<true, DMI_GENERAL>(M, m, N, nb, mc, neumann, dmi_open, do_exch, do_dmi, he, hd);
     } else {
-      neighbour_sums<false>(M, m, N, nb, mc, neumann, dmi_open, do_exch, do_dmi, he, hd);
+      if (ifc) neighbour_sums<false, DMI_IFACE>(M, m, N, nb, mc, neumann, dmi_open, do_exch, do_dmi, he, hd);
+      else neighbour_sums<false, DMI_GENERAL>(M, m, N, nb, mc, neumann, dmi_open, do_exch, do_dmi, he, hd);
     }
   }
   float3 ext = f3(0, 0, 0);
@@ -1102,24 +1131,24 @@ __device__ __forceinline__ void st4x3(float* a, int N, int i0, const float3 (&v)
 // yl: the y and z neighbour rows with 16-byte loads, the x neighbours inside
 // the quad from its own values, per cell the terms in the order r = 0 .. 5
 // of neighbour_sums (so each cell gets the same arithmetic as there).
-template <bool INNER>
+template <bool INNER, int DK>
 __device__ __forceinline__ void quad_sums(const MagnetDev& M, const float* __restrict__ m, int N, int i0, int x0,
                                           int il, int ir, const int (&rb)[4], const float3 (&mc)[4], bool neumann,
                                           bool dmi_open, bool do_exch, bool do_dmi, float3 (&he)[4],
                                           float3 (&hd)[4]) {
   {  // x-
     const float3 xl = (INNER || il >= 0) ? ldg3(m, N, il) : mc[0];
-    neighbour_term<INNER>(M, 0, il >= 0, xl, mc[0], neumann, dmi_open, do_exch, do_dmi, he[0], hd[0]);
+    neighbour_term<INNER, DK>(M, 0, il >= 0, xl, mc[0], neumann, dmi_open, do_exch, do_dmi, he[0], hd[0]);
 #pragma unroll
     for (int q = 1; q < 4; ++q)
-      neighbour_term<INNER>(M, 0, true, mc[q - 1], mc[q], neumann, dmi_open, do_exch, do_dmi, he[q], hd[q]);
+      neighbour_term<INNER, DK>(M, 0, true, mc[q - 1], mc[q], neumann, dmi_open, do_exch, do_dmi, he[q], hd[q]);
   }
   {  // x+
 #pragma unroll
     for (int q = 0; q < 3; ++q)
-      neighbour_term<INNER>(M, 1, true, mc[q + 1], mc[q], neumann, dmi_open, do_exch, do_dmi, he[q], hd[q]);
+      neighbour_term<INNER, DK>(M, 1, true, mc[q + 1], mc[q], neumann, dmi_open, do_exch, do_dmi, he[q], hd[q]);
     const float3 xr = (INNER || ir >= 0) ? ldg3(m, N, ir) : mc[3];
-    neighbour_term<INNER>(M, 1, ir >= 0, xr, mc[3], neumann, dmi_open, do_exch, do_dmi, he[3], hd[3]);
+    neighbour_term<INNER, DK>(M, 1, ir >= 0, xr, mc[3], neumann, dmi_open, do_exch, do_dmi, he[3], hd[3]);
   }
 #pragma unroll
   for (int r = 2; r < 6; ++r) {  // y-, y+, z-, z+: whole neighbour rows
@@ -1129,11 +1158,11 @@ __device__ __forceinline__ void quad_sums(const MagnetDev& M, const float* __res
       ldg4x3(m, N, b + x0, nn);
 #pragma unroll
       for (int q = 0; q < 4; ++q)
-        neighbour_term<INNER>(M, r, true, nn[q], mc[q], neumann, dmi_open, do_exch, do_dmi, he[q], hd[q]);
+        neighbour_term<INNER, DK>(M, r, true, nn[q], mc[q], neumann, dmi_open, do_exch, do_dmi, he[q], hd[q]);
     } else {
 #pragma unroll
       for (int q = 0; q < 4; ++q)
-        neighbour_term<INNER>(M, r, false, mc[q], mc[q], neumann, dmi_open, do_exch, do_dmi, he[q], hd[q]);
+        neighbour_term<INNER, DK>(M, r, false, mc[q], mc[q], neumann, dmi_open, do_exch, do_dmi, he[q], hd[q]);
     }
   }
 }
@@ -1171,10 +1200,14 @@ __device__ __forceinline__ void stage_quad_lean(const MagnetDev& M, const GroupD
 #pragma unroll
     for (int q = 0; q < 4; ++q) rb[q] = T.r[yl][q];
     const bool inner = il >= 0 && ir >= 0 && rb[0] >= 0 && rb[1] >= 0 && rb[2] >= 0 && rb[3] >= 0;
-    if (__all_sync(__activemask(), inner))
-      quad_sums<true>(M, m, N, i0, x0, il, ir, rb, mc, neumann, dmi_open, do_exch, do_dmi, he, hd);
-    else
-      quad_sums<false>(M, m, N, i0, x0, il, ir, rb, mc, neumann, dmi_open, do_exch, do_dmi, he, hd);
+    const bool ifc = do_dmi && dmi_kind(M) == DMI_IFACE;
+    if (__all_sync(__activemask(), inner)) {
+      if (ifc) quad_sums<true, DMI_IFACE>(M, m, N, i0, x0, il, ir, rb, mc, neumann, dmi_open, do_exch, do_dmi, he, hd);
+      else quad_sums<true, DMI_GENERAL>(M, m, N, i0, x0, il, ir, rb, mc, neumann, dmi_open, do_exch, do_dmi, he, hd);
+    } else {
+      if (ifc) quad_sums<false, DMI_IFACE>(M, m, N, i0, x0, il, ir, rb, mc, neumann, dmi_open, do_exch, do_dmi, he, hd);
+      else quad_sums<false, DMI_GENERAL>(M, m, N, i0, x0, il, ir, rb, mc, neumann, dmi_open, do_exch, do_dmi, he, hd);
+    }
   }
   const float3 ext = (terms & TERM_EXT) ? f3(M.fb[0], M.fb[1], M.fb[2]) : f3(0.f, 0.f, 0.f);
 #pragma unroll

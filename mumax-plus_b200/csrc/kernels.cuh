@@ -339,56 +339,52 @@ __global__ void __launch_bounds__(X_THREADS_MAX, 2) k_xfwd(const MagnetDev* __re
   float2* S = M.spec;
   const int tyl = tile_log(ty);
   if ((ny & 1) == 0) {
-    // even ny: rows 2p, 2p + 1 of one (kx, c) with one 16-byte store (every
-    // offset is even); the z values of the pair come from one packed row
+    // even ny: rows 2p, 2p + 1 of one kx, all three components (one 16-byte
+    // store each, every offset is even); the x and y values come from the two
+    // complex rows, the z values of the pair from one packed row
     const int pl = tyl - 1;
-    for (int e = threadIdx.x; e < (Fh * 3) << pl; e += blockDim.x) {
+    const size_t cstr = (size_t)nz * ny, stot = (size_t)Fh * 3 * cstr;
+    for (int e = threadIdx.x; e < Fh << pl; e += blockDim.x) {
       const int yp = e & ((1 << pl) - 1);
       if (2 * yp >= ty) continue;
-      const int rest = e >> pl;
-      const int c = rest % 3, kx = rest / 3;
-      float2 v0, v1;
-      if (c < 2) {
-        const float2* Z0 = sm + (2 * yp) * cs;
-        const float2* Z1 = Z0 + cs;
-        const float2 zk0 = Z0[xidx(kx, sh)], zc0 = cconj(Z0[xidx((L - kx) & (L - 1), sh)]);
-        const float2 zk1 = Z1[xidx(kx, sh)], zc1 = cconj(Z1[xidx((L - kx) & (L - 1), sh)]);
-        if (c == 0) {
-          v0 = make_float2(0.5f * (zk0.x + zc0.x), 0.5f * (zk0.y + zc0.y));
-          v1 = make_float2(0.5f * (zk1.x + zc1.x), 0.5f * (zk1.y + zc1.y));
-        } else {  // -i/2 (zk - zc)
-          v0 = make_float2(0.5f * (zk0.y - zc0.y), -0.5f * (zk0.x - zc0.x));
-          v1 = make_float2(0.5f * (zk1.y - zc1.y), -0.5f * (zk1.x - zc1.x));
-        }
-      } else {
-        const float2* Z = sm + (ty + yp) * cs;
-        const float2 zk = Z[xidx(kx, sh)], zc = cconj(Z[xidx((L - kx) & (L - 1), sh)]);
-        v0 = make_float2(0.5f * (zk.x + zc.x), 0.5f * (zk.y + zc.y));
-        v1 = make_float2(0.5f * (zk.y - zc.y), -0.5f * (zk.x - zc.x));
+      const int kx = e >> pl;
+      const int xk = xidx(kx, sh), xc = xidx((L - kx) & (L - 1), sh);
+      const float2* Z0 = sm + (2 * yp) * cs;
+      const float2* Z1 = Z0 + cs;
+      const float2* Zz = sm + (ty + yp) * cs;
+      const float2 zk0 = Z0[xk], zc0 = cconj(Z0[xc]), zk1 = Z1[xk], zc1 = cconj(Z1[xc]);
+      const float2 zkz = Zz[xk], zcz = cconj(Zz[xc]);
+      const size_t si = ((size_t)kx * 3 * nz + z) * ny + y0 + 2 * yp;
+      if (span_ok(si + 2 * cstr + 1, stot)) {
+        // x: (zk + zc) / 2 ; y: -i/2 (zk - zc), of each row
+        *reinterpret_cast<float4*>(S + si) = make_float4(0.5f * (zk0.x + zc0.x), 0.5f * (zk0.y + zc0.y),
+                                                         0.5f * (zk1.x + zc1.x), 0.5f * (zk1.y + zc1.y));
+        *reinterpret_cast<float4*>(S + si + cstr) = make_float4(0.5f * (zk0.y - zc0.y), -0.5f * (zk0.x - zc0.x),
+                                                                0.5f * (zk1.y - zc1.y), -0.5f * (zk1.x - zc1.x));
+        *reinterpret_cast<float4*>(S + si + 2 * cstr) = make_float4(0.5f * (zkz.x + zcz.x), 0.5f * (zkz.y + zcz.y),
+                                                                    0.5f * (zkz.y - zcz.y), -0.5f * (zkz.x - zcz.x));
       }
-      const size_t si = ((size_t)(kx * 3 + c) * nz + z) * ny + y0 + 2 * yp;
-      if (span_ok(si + 1, (size_t)Fh * 3 * nz * ny))
-        *reinterpret_cast<float4*>(S + si) = make_float4(v0.x, v0.y, v1.x, v1.y);
     }
     return;
   }
-  for (int e = threadIdx.x; e < (Fh * 3) << tyl; e += blockDim.x) {
+  // odd ny: row yl of one kx, all three components (x, y from its complex row,
+  // z from the first or second half of the packed row of its pair)
+  const size_t cstr = (size_t)nz * ny, stot = (size_t)Fh * 3 * cstr;
+  for (int e = threadIdx.x; e < Fh << tyl; e += blockDim.x) {
     const int yl = e & ((1 << tyl) - 1);
     if (yl >= ty) continue;
-    const int rest = e >> tyl;
-    const int c = rest % 3, kx = rest / 3;
-    const float2* Z = (c < 2) ? (sm + yl * cs) : (sm + (ty + (yl >> 1)) * cs);
-    const float2 zk = Z[xidx(kx, sh)];
-    const float2 zc = cconj(Z[xidx((L - kx) & (L - 1), sh)]);
-    float2 val;
-    const bool second = (c == 1) || (c == 2 && (yl & 1));
-    if (!second) {
-      val = make_float2(0.5f * (zk.x + zc.x), 0.5f * (zk.y + zc.y));
-    } else {  // -i/2 (zk - zc)
-      val = make_float2(0.5f * (zk.y - zc.y), -0.5f * (zk.x - zc.x));
+    const int kx = e >> tyl;
+    const int xk = xidx(kx, sh), xc = xidx((L - kx) & (L - 1), sh);
+    const float2* Z = sm + yl * cs;
+    const float2* Zz = sm + (ty + (yl >> 1)) * cs;
+    const float2 zk = Z[xk], zc = cconj(Z[xc]), zkz = Zz[xk], zcz = cconj(Zz[xc]);
+    const size_t si = ((size_t)kx * 3 * nz + z) * ny + y0 + yl;
+    if (span_ok(si + 2 * cstr, stot)) {
+      S[si] = make_float2(0.5f * (zk.x + zc.x), 0.5f * (zk.y + zc.y));
+      S[si + cstr] = make_float2(0.5f * (zk.y - zc.y), -0.5f * (zk.x - zc.x));  // -i/2 (zk - zc)
+      S[si + 2 * cstr] = (yl & 1) ? make_float2(0.5f * (zkz.y - zcz.y), -0.5f * (zkz.x - zcz.x))
+                                  : make_float2(0.5f * (zkz.x + zcz.x), 0.5f * (zkz.y + zcz.y));
     }
-    const size_t si = ((size_t)(kx * 3 + c) * nz + z) * ny + y0 + yl;
-    if (span_ok(si, (size_t)Fh * 3 * nz * ny)) S[si] = val;
   }
 }
 

@@ -316,6 +316,16 @@ struct mpx_engine {
     int launches = 1;  // kernels per evaluation
   };
   std::vector<Pair> pairs;
+  // FFT plans of recent stray-field evaluations on other grids (mpx_stray_field),
+  // by geometry: source and destination grids, cell size, periodic images
+  struct PairCacheEntry {
+    int key[18];
+    double cs[3];
+    PairPlan plan;
+    uint64_t used;
+  };
+  std::vector<PairCacheEntry> pair_cache;
+  uint64_t pair_cache_tick = 0;
   bool pairs_dirty = true;
   bool any_thermal = false;  // some started group has thermal noise: stage 0 is evaluated every attempt
   int sampling_group = -1;   // group of the sampled run in progress (its magnets get sample kernels)
@@ -868,6 +878,42 @@ void release_all(mpx_engine* e, Magnet* m);
 // the FFT form on the pair's kernel grid (periodic images included).
 constexpr long long STRAY_FFT_MIN_INTERACTIONS = 1LL << 22;
 
+// The FP32 table of the Newell tensor, with the periodic images of g, at the
+// displacements O + j, j < K per axis (k_newell_reflayout's layout).  Where a
+// displacement range reaches both signs the tensor is evaluated over the
+// absolute displacements only and expanded by the components' parities
+// (k_newell_expand_abs): for two overlapping grids a quarter to an eighth of
+// the FP64 evaluations.
+mpx_status build_pair_table(mpx_engine* e, const KernelGeom& g, const int K[3], const int O[3], float* out) {
+  int A[3], L[3];
+  long long lt = 1, kt = 1;
+  for (int a = 0; a < 3; ++a) {
+    const int lo = O[a], hi = O[a] + K[a] - 1;
+    if (lo <= 0 && hi >= 0) {
+      A[a] = 0;
+      L[a] = std::max(-lo, hi) + 1;
+    } else {
+      A[a] = std::min(std::abs(lo), std::abs(hi));
+      L[a] = std::max(std::abs(lo), std::abs(hi)) - A[a] + 1;
+    }
+    lt *= L[a];
+    kt *= K[a];
+  }
+  if (2 * lt > kt) {
+    k_newell_reflayout<<<148 * 8, 128, 0, e->stream>>>(out, g, K[0], K[1], K[2], O[0], O[1], O[2]);
+    e->launches++;
+  } else {
+    float* abs_tab = nullptr;
+    MPX_TRY(palloc(e, (void**)&abs_tab, sizeof(float) * 6 * (size_t)lt));
+    k_newell_reflayout<<<148 * 8, 128, 0, e->stream>>>(abs_tab, g, L[0], L[1], L[2], A[0], A[1], A[2]);
+    k_newell_expand_abs<<<148 * 8, 256, 0, e->stream>>>(out, abs_tab, K[0], K[1], K[2], O[0], O[1], O[2], A[0], A[1],
+                                                        A[2], L[0], L[1], L[2]);
+    e->launches += 2;
+    pfree(e, abs_tab);
+  }
+  return MPX_OK;
+}
+
 // log2 of the FFT lengths of the pair grid n_A + n_B - 1 per axis; false when
 // a length exceeds what the pair passes transform (4096 along x and y, 2048
 // along z, where six kernel components share one block's shared memory).
@@ -937,7 +983,12 @@ mpx_status build_pair_fft(mpx_engine* e, const Magnet* A, const int nB[3], const
     free_pair_plan(e, pl);
     return st;
   }
-  k_newell_reflayout<<<148 * 8, 128, 0, e->stream>>>(tab, gimg, K[0], K[1], K[2], O[0], O[1], O[2]);
+  st = build_pair_table(e, gimg, K, O, tab);
+  if (st != MPX_OK) {
+    pfree(e, tab);
+    free_pair_plan(e, pl);
+    return st;
+  }
   // kernel spectrum: the forward passes over the six tabulated components
   PairPlan kp;
   kp.pf = pf;
@@ -952,7 +1003,7 @@ mpx_status build_pair_fft(mpx_engine* e, const Magnet* A, const int nB[3], const
                                                                 e->d_tw);
   k_pair_zmul<false><<<kp.g_z, PF_THREADS, kp.s_z, e->stream>>>(e->d_mags, e->d_groups, -1, 0, 0, kp.pf, 6, kp.tky,
                                                                  e->d_tw);
-  e->launches += 4;
+  e->launches += 3;
   pfree(e, tab);
   pf.t = pl.t;
   pf.ks = pl.ks;
@@ -968,6 +1019,45 @@ mpx_status build_pair_fft(mpx_engine* e, const Magnet* A, const int nB[3], const
     free_pair_plan(e, pl);
     return fail(MPX_ERR_CUDA, std::string("stray-field FFT kernel: ") + cudaGetErrorString(ce));
   }
+  return MPX_OK;
+}
+
+// The plan of source A on destination grid B with the images of g, from the
+// cache of recent evaluations or built (the least recently used of
+// PAIR_CACHE_MAX plans is released).  The kernel spectrum depends on the
+// geometry only, so repeated evaluations of one StrayField reuse it.
+constexpr int PAIR_CACHE_MAX = 2;
+mpx_status cached_pair_plan(mpx_engine* e, const Magnet* A, const Magnet* B, const KernelGeom& g, PairPlan** out) {
+  int key[18];
+  for (int a = 0; a < 3; ++a) {
+    key[a] = A->dev.n[a];
+    key[3 + a] = A->dev.o[a];
+    key[6 + a] = B->dev.n[a];
+    key[9 + a] = B->dev.o[a];
+    key[12 + a] = g.mg[a];
+    key[15 + a] = g.pbc[a];
+  }
+  for (auto& c : e->pair_cache)
+    if (std::memcmp(c.key, key, sizeof key) == 0 && c.cs[0] == g.cs[0] && c.cs[1] == g.cs[1] && c.cs[2] == g.cs[2]) {
+      c.used = ++e->pair_cache_tick;
+      *out = &c.plan;
+      return MPX_OK;
+    }
+  if ((int)e->pair_cache.size() >= PAIR_CACHE_MAX) {
+    auto lru = std::min_element(e->pair_cache.begin(), e->pair_cache.end(),
+                                [](const mpx_engine::PairCacheEntry& x, const mpx_engine::PairCacheEntry& y) {
+                                  return x.used < y.used;
+                                });
+    free_pair_plan(e, lru->plan);
+    e->pair_cache.erase(lru);
+  }
+  mpx_engine::PairCacheEntry c;
+  std::memcpy(c.key, key, sizeof key);
+  for (int a = 0; a < 3; ++a) c.cs[a] = g.cs[a];
+  MPX_TRY(build_pair_fft(e, A, B->dev.n, B->dev.o, g, c.plan));
+  c.used = ++e->pair_cache_tick;
+  e->pair_cache.push_back(c);
+  *out = &e->pair_cache.back().plan;
   return MPX_OK;
 }
 
@@ -1038,9 +1128,7 @@ mpx_status rebuild_pairs(mpx_engine* e) {
         }
         const size_t KK = (size_t)p.tab.K[0] * p.tab.K[1] * p.tab.K[2];
         MPX_TRY(palloc(e, (void**)&p.k, sizeof(float) * 6 * KK));
-        k_newell_reflayout<<<148 * 8, 128, 0, e->stream>>>(p.k, g, p.tab.K[0], p.tab.K[1], p.tab.K[2], p.tab.O[0],
-                                                           p.tab.O[1], p.tab.O[2]);
-        e->launches++;
+        MPX_TRY(build_pair_table(e, g, p.tab.K, p.tab.O, p.k));
         p.tab.k = p.k;
         e->pairs.push_back(p);
         is_dst[b] = true;
@@ -1914,6 +2002,8 @@ mpx_status mpx_engine_destroy(mpx_engine* e) {
   if (e->graph_nok0) cudaGraphExecDestroy(e->graph_nok0);
   for (auto& m : e->mags)
     if (m) release_all(e, m.get());
+  for (auto& c : e->pair_cache) free_pair_plan(e, c.plan);
+  e->pair_cache.clear();
   cudaFree(e->d_mags);
   cudaFree(e->d_groups);
   cudaFree(e->d_tw);
@@ -2510,10 +2600,9 @@ mpx_status mpx_stray_field(mpx_engine* e, int src, int dst_magnet, const int siz
     }
     int logP[3];
     if (method == MPX_STRAY_FFT && pair_fft_lengths(A->dev.n, B->dev.n, logP)) {
-      PairPlan pl;
-      st = build_pair_fft(e, A, B->dev.n, B->dev.o, g, pl);
-      if (st == MPX_OK) launch_pair_fft(e, pl, src, dst, 0, 0, 0, dout);
-      free_pair_plan(e, pl);
+      PairPlan* pl = nullptr;
+      st = cached_pair_plan(e, A, B, g, &pl);
+      if (st == MPX_OK) launch_pair_fft(e, *pl, src, dst, 0, 0, 0, dout);
     } else {  // the direct sum (also the FFT method's form for pair grids beyond the FFT lengths)
       StrayTable tab;
       for (int ax = 0; ax < 3; ++ax) {
@@ -2523,14 +2612,13 @@ mpx_status mpx_stray_field(mpx_engine* e, int src, int dst_magnet, const int siz
       const size_t KK = (size_t)tab.K[0] * tab.K[1] * tab.K[2];
       float* k = nullptr;
       st = palloc(e, (void**)&k, sizeof(float) * 6 * KK);
+      if (st == MPX_OK) st = build_pair_table(e, g, tab.K, tab.O, k);
       if (st == MPX_OK) {
-        k_newell_reflayout<<<148 * 8, 128, 0, e->stream>>>(k, g, tab.K[0], tab.K[1], tab.K[2], tab.O[0], tab.O[1],
-                                                           tab.O[2]);
         tab.k = k;
         k_stray_pair<<<(NB + 255) / 256, 256, 0, e->stream>>>(e->d_mags, e->d_groups, src, dst, tab, 0, 0, 0, dout);
-        e->launches += 2;
-        pfree(e, k);
+        e->launches++;
       }
+      pfree(e, k);
     }
   }
   if (st == MPX_OK) {

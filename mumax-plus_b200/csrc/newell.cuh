@@ -127,6 +127,31 @@ __global__ void k_newell_reflayout(float* __restrict__ out, KernelGeom g, int K0
   }
 }
 
+// The same table from one over absolute displacements: entry j of the output
+// is displacement O + j (K per axis); the input holds |d| = A + a (a < L per
+// axis), same layout.  Diagonal components are even in every displacement
+// component, xy odd in x and y, xz in x and z, yz in y and z, also after the sum
+// over periodic images (their repetitions run over -p .. p), so each output is
+// an input entry times the signs of its odd components.
+__global__ void k_newell_expand_abs(float* __restrict__ out, const float* __restrict__ abs_tab, int K0, int K1,
+                                    int K2, int O0, int O1, int O2, int A0, int A1, int A2, int L0, int L1, int L2) {
+  const long long total = (long long)K0 * K1 * K2, ltot = (long long)L0 * L1 * L2;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
+       t += (long long)gridDim.x * blockDim.x) {
+    const int x = O0 + (int)(t % K0);
+    const int y = O1 + (int)((t / K0) % K1);
+    const int z = O2 + (int)(t / ((long long)K0 * K1));
+    const long long p = ((long long)(abs(z) - A2) * L1 + (abs(y) - A1)) * L0 + (abs(x) - A0);
+    const float sx = x < 0 ? -1.f : 1.f, sy = y < 0 ? -1.f : 1.f, sz = z < 0 ? -1.f : 1.f;
+    out[t] = abs_tab[p];
+    out[total + t] = abs_tab[ltot + p];
+    out[2 * total + t] = abs_tab[2 * ltot + p];
+    out[3 * total + t] = (sx * sy) * abs_tab[3 * ltot + p];
+    out[4 * total + t] = (sx * sz) * abs_tab[4 * ltot + p];
+    out[5 * total + t] = (sy * sz) * abs_tab[5 * ltot + p];
+  }
+}
+
 // Expand component c of the octant table to the circular P-grid (imag = 0).
 // Parity: xy odd in x,y; xz odd in x,z; yz odd in y,z; diagonal even.
 __global__ void k_kernel_expand(double2* __restrict__ full, const double* __restrict__ oct, int c, KernelGeom g,

@@ -189,6 +189,34 @@ def test_stray_field_far_grids_fft_against_brute(mpx, case, pbc):
     assert max_rel(result, wanted) < 1e-5, max_rel(result, wanted)
 
 
+def test_stray_field_repeated_evaluations(mpx):
+    """The FFT form keeps the kernel spectra of recent evaluations by geometry:
+    a second evaluation gives the same field, a new magnetization the new field
+    (against the direct sum), and switching between three grids (more than the
+    cache holds) and back gives the same fields again."""
+    world = mpx.World(STRAY_CS)
+    magnet = mpx.Ferromagnet(world, mpx.Grid((24, 20, 2), (0, 0, 0)))
+    magnet.msat = 800e3
+    magnet.magnetization = random_m((2, 20, 24), seed=8, smooth=1)
+    grids = [mpx.Grid((30, 10, 1), (5, 25, 3)), mpx.Grid((16, 16, 2), (-20, 0, 0)), mpx.Grid((8, 40, 1), (0, 0, 9))]
+    first = []
+    for g in grids:
+        sf = mpx.StrayField(magnet, g)
+        a = sf.eval()
+        np.testing.assert_array_equal(sf.eval(), a)
+        sf.set_method("brute")
+        assert max_rel(a, sf.eval()) < 1e-5
+        first.append(a)
+    for g, a in zip(grids, first):
+        np.testing.assert_array_equal(mpx.StrayField(magnet, g).eval(), a)
+    magnet.magnetization = random_m((2, 20, 24), seed=9, smooth=1)
+    sf = mpx.StrayField(magnet, grids[0])
+    new = sf.eval()
+    assert max_rel(new, first[0]) > 1e-2
+    sf.set_method("brute")
+    assert max_rel(new, sf.eval()) < 1e-5
+
+
 # ------------------------------------------------ StrayField on other grids
 # test/test_strayfield.py:29-136: a magnet on mgrid, its field on hgrid, by the
 # FFT method against the brute-force method (with and without periodic

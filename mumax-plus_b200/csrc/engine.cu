@@ -73,7 +73,7 @@ constexpr int MAX_FFT = 4096;
 constexpr int SMEM_MAX = 227 * 1024;
 // dynamic shared memory left next to the static descriptor copies of a block
 constexpr int SMEM_DYN_MAX = SMEM_MAX - 2048;
-constexpr int YZ_CLASSES = 20;  // k_yz / k_yzw / k_yzw32 launch classes (yz_class)
+constexpr int YZ_CLASSES = 24;  // k_yz / k_yzw / k_yzw32 / k_yzw64 launch classes (yz_class)
 
 // ------------------------------------------------------------ tableaus
 // core/butchertableau.cpp: Heun, Bogacki-Shampine, Cash-Karp, Fehlberg, Dormand-Prince
@@ -511,17 +511,21 @@ int x_smem(const Magnet* m) {
 }
 // y lengths of the warp-column y/z pass (k_yzw)
 bool yz_warp(int Py) { return Py >= 64 && Py <= 1024; }
+// y length 2048 with z lengths up to 8: warp pairs (k_yzw64)
+bool yz_pair(int Py, int Pz) { return Py == 2048 && Pz <= 8; }
 int yzw_threads_of(int Pz) { return Pz == 16 ? 384 : 256; }
-int yz_smem_of(int nz, int nkx, int Py) {
-  return (nkx * 3 * nz * (yz_warp(Py) ? qlen(Py) : plen(Py)) + Py) * (int)sizeof(float2);
+int yz_smem_of(int nz, int nkx, int Py, int Pz) {
+  return (nkx * 3 * nz * (yz_warp(Py) || yz_pair(Py, Pz) ? qlen(Py) : plen(Py)) + Py) * (int)sizeof(float2);
 }
-int yz_smem(const Magnet* m) { return yz_smem_of(m->dev.n[2], m->nkx, m->P[1]); }
-// y/z class of a magnet: 15 + log2 Pz for the warp-column pass of y length
-// 1024, 10 + log2 Pz for y lengths 64 .. 512, else log2 Pz, plus 5 for y
-// transforms longer than 2048 (which
-// need the radix-16 form).  The FFT plan of a magnet depends on its own lengths
-// only, so it computes the same alone and in any batch.
+int yz_smem(const Magnet* m) { return yz_smem_of(m->dev.n[2], m->nkx, m->P[1], m->P[2]); }
+// y/z class of a magnet: 20 + log2 Pz for the warp-pair pass of y length 2048
+// (z lengths up to 8), 15 + log2 Pz for the warp-column pass of y length 1024,
+// 10 + log2 Pz for y lengths 64 .. 512, else log2 Pz, plus 5 for y transforms
+// longer than 2048 (which need the radix-16 form).  The FFT plan of a magnet
+// depends on its own lengths only, so it computes the same alone and in any
+// batch.
 int yz_class(const Magnet* m) {
+  if (yz_pair(m->P[1], m->P[2])) return 20 + ilog2(m->P[2]);
   if (m->P[1] == 1024) return 15 + ilog2(m->P[2]);
   if (yz_warp(m->P[1])) return 10 + ilog2(m->P[2]);
   return ilog2(m->P[2]) + (m->P[1] > 2048 ? 5 : 0);
@@ -544,6 +548,8 @@ int choose_ty(int ny, int len) {
   return even_rows(std::max(1, std::min(t, ny)), ny);
 }
 int choose_nkx(int nz, int Py, int Pz, int Fh) {
+  // warp pairs (y length 2048): up to 12 columns, two per pair of the 6 pairs
+  if (yz_pair(Py, Pz)) return std::max(1, std::min(Fh, 12 / (3 * nz)));
   // warp columns (y lengths 64 .. 1024): 32 values per thread, one 1024-value unit per warp
   const int pts = yz_warp(Py) ? 32 * yzw_threads_of(Pz) : YZ_VPT * YZ_THREADS;
   return std::max(1, std::min(Fh, pts / (3 * nz * Py)));
@@ -622,6 +628,8 @@ mpx_status launch_yz(mpx_engine* e, int cls, const Work* work, int n, int smem, 
 #define MPX_YZW32(PZ) \
   CUDA_TRY(launch_pdl(k_yzw32<PZ>, n, yzw_threads<PZ>(), smem, e->stream, e->d_mags, e->d_groups, work, stage, gate, \
                       e->d_tw))
+#define MPX_YZW64(PZ) \
+  CUDA_TRY(launch_pdl(k_yzw64<PZ>, n, YZP_THREADS, smem, e->stream, e->d_mags, e->d_groups, work, stage, gate, e->d_tw))
   switch (cls) {
     case 0: MPX_YZ(1, 3); break;
     case 1: MPX_YZ(2, 3); break;
@@ -641,11 +649,16 @@ mpx_status launch_yz(mpx_engine* e, int cls, const Work* work, int n, int smem, 
     case 17: MPX_YZW32(4); break;
     case 18: MPX_YZW32(8); break;
     case 19: MPX_YZW32(16); break;
+    case 20: MPX_YZW64(1); break;
+    case 21: MPX_YZW64(2); break;
+    case 22: MPX_YZW64(4); break;
+    case 23: MPX_YZW64(8); break;
     default: MPX_YZ(16, 4); break;  // 4 and 9 (z length 16)
   }
 #undef MPX_YZ
 #undef MPX_YZW
 #undef MPX_YZW32
+#undef MPX_YZW64
   e->launches++;
   return MPX_OK;
 }
@@ -1944,7 +1957,8 @@ mpx_status mpx_engine_create(int device, mpx_engine** out) {
                                (const void*)k_yzw<1>, (const void*)k_yzw<2>, (const void*)k_yzw<4>,
                                (const void*)k_yzw<8>, (const void*)k_yzw<16>, (const void*)k_yzw32<1>,
                                (const void*)k_yzw32<2>, (const void*)k_yzw32<4>, (const void*)k_yzw32<8>,
-                               (const void*)k_yzw32<16>, (const void*)k_pair_xfwd<true>,
+                               (const void*)k_yzw32<16>, (const void*)k_yzw64<1>, (const void*)k_yzw64<2>,
+                               (const void*)k_yzw64<4>, (const void*)k_yzw64<8>, (const void*)k_pair_xfwd<true>,
                                (const void*)k_pair_xfwd<false>, (const void*)k_pair_yfft<-1>,
                                (const void*)k_pair_yfft<1>, (const void*)k_pair_zmul<true>,
                                (const void*)k_pair_zmul<false>, (const void*)k_pair_xinv,
@@ -2384,7 +2398,7 @@ mpx_status mpx_magnet_bytes(const mpx_magnet_desc* d, int64_t* resident, int64_t
     res += 4 * Fh * (P[1] / 2 + 1) * (P[2] / 2 + 1) * kc;        // kernel spectrum
     const int nkx = choose_nkx(d->size[2], P[1], P[2], (int)Fh);
     res += (int64_t)sizeof(Work) * ((Fh + nkx - 1) / nkx);       // y/z work items
-    const int yzs = yz_smem_of(d->size[2], nkx, P[1]);
+    const int yzs = yz_smem_of(d->size[2], nkx, P[1], P[2]);
     if (P[2] > 16 || yzs > SMEM_DYN_MAX) {  // split y/z path: T and its work items
       res += 8 * Fh * 3 * d->size[2] * P[1];
       const int64_t ncy = std::max<int64_t>(1, std::min<int64_t>(Fh * 3 * d->size[2], (YZ_VPT * YZ_THREADS) / P[1]));

@@ -447,6 +447,48 @@ __device__ __forceinline__ void four_step_outer(float2 (&v)[32], float2* base, i
   DftZ<32, DIR, false, LO>::run(v);
 }
 
+// ------------------------------------------- warp pairs (four-step, L = 2048)
+// A 2048-point column as 64 x 32 taken by a pair of warps p = 0, 1 (64 lanes):
+// with n = j + 32 r and k = s + 64 t,
+//   X[s + 64 t] = sum_j W32^{j t} W2048^{j s} Y_j[s],  Y_j[s] = sum_r x[j + 32 r] W64^{r s}.
+// Warp p forms the inner outputs s = 2 s' + p of lane j's 32 values as a
+// 32-point DFT over r (s' its index) of x[j + 32 r] W64^{r p}: inputs r < 32
+// only, the rest being zero padding (forward) or folded in beforehand as
+// x[j + 32 r] + (-1)^p x[j + 32 (r + 32)] (inverse, all 64 inputs).  The pair
+// then transposes through the column in shared memory (qidx layout) and lane
+// c = lane + 32 p does the outer 32-point DFT of index s = c.  Registers stay at
+// 32 values per lane, as in the single-warp form of length 1024.
+
+// 64-thread barrier of warp pair `pair` (named barriers 1 .. 8; 0 is the block's).
+__device__ __forceinline__ void pair_sync(int pair) { asm volatile("bar.sync %0, 64;" ::"r"(1 + pair) : "memory"); }
+
+// Inner step of warp p for lane j: v[r] (r < 32) in, Y_j[2 s' + p] W2048^{j (2 s' + p)}
+// stored at element j + 32 (2 s' + p) of column C.  twq: W2048^{j s} at
+// [j * 63 + s - 1] (load_twq of length 2048).
+template <int DIR>
+__device__ __forceinline__ void pair_inner(float2 (&v)[32], const float2* twq, int lane, int p, float2* C) {
+  if (p) {
+#pragma unroll
+    for (int r = 1; r < 32; ++r) v[r] = cmul(v[r], twiddle_raw<DIR>(twq + r * 63 - 1, 32));  // W64^r = W2048^{32 r}
+  }
+  DftZ<32, DIR, false, false>::run(v);
+  const float2* t = twq + lane * 63 - 1;
+#pragma unroll
+  for (int q = 0; q < 32; ++q) {
+    const int s = 2 * q + p;
+    const float2 w = (s == 0) ? v[q] : cmul(v[q], twiddle_raw<DIR>(t, s));
+    C[qidx(lane + 32 * s)] = w;
+  }
+}
+
+// Outer step of lane c = lane + 32 p of the pair: v[t] = X[c + 64 t] (t < 16 only with LO).
+template <int DIR, bool LO>
+__device__ __forceinline__ void pair_outer(float2 (&v)[32], const float2* C, int c) {
+#pragma unroll
+  for (int j = 0; j < 32; ++j) v[j] = C[qidx(j + 32 * c)];
+  DftZ<32, DIR, false, LO>::run(v);
+}
+
 // Transforms of length 32 Q of `nrows` rows in shared memory (row r at
 // buf + r*cs, qidx layout), W = 32 / Q rows per warp at a time, in place.  ZIN:
 // the upper half of every input row is zero padding (not read).  LO: only the

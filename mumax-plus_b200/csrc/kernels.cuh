@@ -755,6 +755,85 @@ __global__ void __launch_bounds__(yzw_threads<PZ>(), PZ == 16 ? 1 : 2)
   yzw_body<PZ, 32>(M, wk.z, wk.y0, sm, tw);
 }
 
+// y length 2048 in warp pairs (pair_inner / pair_outer of fft.cuh): every pair
+// of warps transforms whole columns of length 2048, one at a time, with one
+// shared-memory transpose per direction; nkx consecutive kx per block
+// (3 nz nkx <= 12 columns, 6 pairs); the z stage as in k_yzw.  Columns in the
+// qidx layout, cs = qlen(2048).
+constexpr int YZP_THREADS = 384;
+template <int PZ>
+__global__ void __launch_bounds__(YZP_THREADS, 1)
+    k_yzw64(const MagnetDev* __restrict__ mags, const GroupDev* __restrict__ groups, const Work* __restrict__ work,
+            int stage, int gate, const float2* __restrict__ tw) {
+  extern __shared__ float2 sm[];
+  __shared__ MagnetDev M;
+  __shared__ GroupDev G;
+  pdl_trigger();  // the x-inverse pass may start its prologue during the last wave
+  const Work wk = work[blockIdx.x];
+  if (!load_descs(M, G, mags, groups, wk.mag, gate, stage)) return;
+  constexpr int Py = 2048, LOGPY = 11, cs = qlen(Py);
+  const int kx0 = wk.z, nkx = wk.y0;
+  const int ny = M.n[1], nz = M.n[2];
+  const int ncol = nkx * 3 * nz;
+  float2* D = sm;
+  float2* twq = sm + ncol * cs;
+  load_twq(twq, tw, LOGPY);
+  prefetch_kslab(M, kx0, nkx, PZ);
+  __syncthreads();
+  pdl_wait();  // the spectrum is written by the x pass
+  float2* S = M.spec + (size_t)kx0 * 3 * nz * ny;
+  const size_t sleft = (size_t)(M.Fh - kx0) * 3 * nz * ny;  // elements from S on (checked build)
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, pair = warp >> 1, p = warp & 1;
+  const int npairs = blockDim.x >> 6, c = lane + 32 * p;
+  for (int col = pair; col < ncol; col += npairs) {  // forward: y < ny in, zero above
+    float2* C = D + col * cs;
+    float2 v[32];
+#pragma unroll
+    for (int r = 0; r < 32; ++r) {
+      const int y = lane + 32 * r;
+      v[r] = (y < ny && span_ok((size_t)col * ny + y, sleft)) ? __ldg(S + (size_t)col * ny + y) : make_float2(0.f, 0.f);
+    }
+    pair_inner<-1>(v, twq, lane, p, C);
+    pair_sync(pair);
+    pair_outer<-1, false>(v, C, c);
+    pair_sync(pair);  // both warps have read the column before it takes the outputs
+#pragma unroll
+    for (int t = 0; t < 32; ++t) C[qidx(c + 64 * t)] = v[t];  // ky = c + 64 t
+  }
+  __syncthreads();
+  if constexpr (PZ == 1) {
+    for (int t = threadIdx.x; t < nkx << LOGPY; t += blockDim.x) {
+      const int j = t >> LOGPY;
+      zstage_single<true>(D + j * 3 * cs, cs, M, kx0 + j, t & (Py - 1), Py);
+    }
+  } else {
+    // lanes l and l + 16 of a warp share one (kx, ky): the even and odd kz halves
+    for (int t = threadIdx.x; t < (2 * nkx) << LOGPY; t += blockDim.x) {
+      const int u = ((t >> 5) << 4) | (t & 15), j = u >> LOGPY;
+      zstage_pair<PZ, true, 16>(D + j * 3 * nz * cs, cs, M, kx0 + j, u & (Py - 1), (t >> 4) & 1, nz, Py);
+    }
+  }
+  __syncthreads();
+  for (int col = pair; col < ncol; col += npairs) {  // inverse: the y < ny outputs go to S
+    float2* C = D + col * cs;
+    float2 v[32];
+#pragma unroll
+    for (int b = 0; b < 32; ++b) {  // fold k and k + 1024: x + (-1)^p x'
+      const float2 lo = C[qidx(lane + 32 * b)], hi = C[qidx(lane + 32 * b + 1024)];
+      v[b] = p ? csub(lo, hi) : cadd(lo, hi);
+    }
+    pair_sync(pair);  // both warps have read the column before the inner step overwrites it
+    pair_inner<1>(v, twq, lane, p, C);
+    pair_sync(pair);
+    pair_outer<1, true>(v, C, c);
+#pragma unroll
+    for (int t = 0; t < 16; ++t) {  // y = c + 64 t < 1024
+      const int y = c + 64 * t;
+      if (y < ny && span_ok((size_t)col * ny + y, sleft)) S[(size_t)col * ny + y] = v[t];
+    }
+  }
+}
+
 // ------------------------------------------------------------- epilogue
 __device__ __forceinline__ void block_max2(double a, double b, unsigned long long* pa, unsigned long long* pb) {
   // warp max then one atomic per warp (values are >= 0 or NaN; NaN bits order above +inf)

@@ -398,6 +398,37 @@ def test_demag_warp_transform_lengths(mpx, size):
     compare(MagnetSpec(size=size, cellsize=(1e-9, 2e-9, 1.5e-9), msat=8e5), mpx, [abi.Q_DEMAG_FIELD])
 
 
+@pytest.mark.parametrize("size", [(3, 600, 1), (2, 700, 2), (3, 1000, 3), (2, 513, 4), (1, 1024, 2)])
+def test_demag_warp_pair_length_2048(mpx, size):
+    """y length 2048 (k_yzw64: four-step 64 x 32 by pairs of warps, the inverse folding the upper half in) at z
+    lengths 1, 4, 8 and 8, several kx per block for thin magnets, ny from 513 to 1024."""
+    compare(MagnetSpec(size=size, cellsize=(1e-9, 2e-9, 1.5e-9), msat=8e5), mpx, [abi.Q_DEMAG_FIELD])
+
+
+def test_warp_pair_trajectory_vs_oracle(mpx):
+    """Dormand-Prince stages through the warp-pair y transforms (Py = 2048, Pz = 4): <m>(t) against the FP64
+    oracle."""
+    s = MagnetSpec(size=(12, 600, 2), cellsize=(3e-9, 3e-9, 3e-9), msat=8e5, aex=1.3e-11, alpha=0.1,
+                   world_bias=(0.0, 0.01, 0.0))
+    m0 = random_m(s.shape, seed=9, smooth=3)
+    ow, q = s.oracle_world(m0)
+    ow.set_method("DormandPrince")
+    world, magnet = s.product(mpx, m0)
+    world.timesolver.set_method("DormandPrince")
+    dt0 = ow.sensible_timestep()
+    ow.timestep = dt0
+    world.timesolver.timestep = dt0
+    worst = 0.0
+    for k in range(1, 4):
+        tp = k * 3e-12
+        ow.run(tp - ow.time)
+        world.timesolver._e.run(world._group, tp - world.timesolver.time)
+        a = np.array(magnet.magnetization.average())
+        b = np.array(ow.average(q, abi.Q_MAGNETIZATION))
+        worst = max(worst, float(np.max(np.abs(a - b))))
+    assert worst < 1e-4, worst
+
+
 def test_warp_transform_trajectory_vs_oracle(mpx):
     """Dormand-Prince stages through the warp transforms of both axes (Px = 512, Py = 128) and the lean stage
     epilogue (uniform parameters): <m>(t) and the field m(t) against the FP64 oracle."""

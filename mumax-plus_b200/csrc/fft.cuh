@@ -489,6 +489,41 @@ __device__ __forceinline__ void pair_outer(float2 (&v)[32], const float2* C, int
   DftZ<32, DIR, false, LO>::run(v);
 }
 
+// Transforms of length 2048 of `nrows` rows in shared memory (row r at
+// buf + r*cs, qidx layout) by warp pairs, one row per pair at a time, in
+// place.  ZIN: the upper half of every input row is zero padding (not read);
+// otherwise the inner step folds it in.  LO: only the lower half of every output
+// row is written.  A trailing warp without a partner takes no row.  No block
+// barrier: the caller synchronises before (rows and twiddles written) and after.
+template <int DIR, bool ZIN, bool LO>
+__device__ __forceinline__ void pair_rows(float2* buf, int nrows, int cs, const float2* twq) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, pair = warp >> 1, p = warp & 1;
+  const int npairs = blockDim.x >> 6;
+  if (pair >= npairs) return;
+  const int c = lane + 32 * p;
+  for (int r0 = pair; r0 < nrows; r0 += npairs) {
+    float2* R = buf + r0 * cs;
+    float2 v[32];
+#pragma unroll
+    for (int b = 0; b < 32; ++b) {
+      const float2 lo = R[qidx(lane + 32 * b)];
+      if constexpr (ZIN) {
+        v[b] = lo;
+      } else {  // x + (-1)^p x' of elements lane + 32 b and lane + 32 b + 1024
+        const float2 hi = R[qidx(lane + 32 * b + 1024)];
+        v[b] = p ? csub(lo, hi) : cadd(lo, hi);
+      }
+    }
+    pair_sync(pair);  // both warps have read the row before the inner step overwrites it
+    pair_inner<DIR>(v, twq, lane, p, R);
+    pair_sync(pair);
+    pair_outer<DIR, LO>(v, R, c);
+    pair_sync(pair);  // both warps have read the row before it takes the outputs
+#pragma unroll
+    for (int t = 0; t < (LO ? 16 : 32); ++t) R[qidx(c + 64 * t)] = v[t];
+  }
+}
+
 // Transforms of length 32 Q of `nrows` rows in shared memory (row r at
 // buf + r*cs, qidx layout), W = 32 / Q rows per warp at a time, in place.  ZIN:
 // the upper half of every input row is zero padding (not read).  LO: only the
@@ -525,13 +560,14 @@ __device__ __forceinline__ void warp_rows(float2* buf, int nrows, int cs, const 
 // else pidx.
 __device__ __forceinline__ int xidx(int i, int sh) { return i + (i >> sh); }
 
-// Row stride of the x passes for tiles of ty rows.  512- and 1024-point rows
-// (warp rows, qidx layout): qlen plus 16 / (row slots of the tile, ty rounded up
-// to a power of two) complex values, so that the gather and the unpack, whose
-// half-warps touch the same few x of every row slot, hit 16 different 8-byte
-// banks (the outer step of these lengths reads within one row per half-warp).
+// Row stride of the x passes for tiles of ty rows.  512-, 1024- and 2048-point
+// rows (warp rows and warp-pair rows, qidx layout): qlen plus 16 / (row slots of
+// the tile, ty rounded up to a power of two) complex values, so that the gather
+// and the unpack, whose half-warps touch the same few x of every row slot, hit
+// 16 different 8-byte banks (the outer step of these lengths reads within one
+// row per half-warp).
 __host__ __device__ inline int xrow_stride(int L, int ty) {
-  if (L != 1024 && L != 512) return xstride(L);
+  if (L != 1024 && L != 512 && L != 2048) return xstride(L);
   int slots = 1;
   while (slots < ty) slots <<= 1;
   return qlen(L) + (slots >= 16 ? 1 : 16 / slots);

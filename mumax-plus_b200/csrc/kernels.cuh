@@ -240,7 +240,7 @@ __global__ void __launch_bounds__(X_THREADS_MAX, 2) k_xfwd(const MagnetDev* __re
   const float* x0 = M.buf[G.map[0]];
   const int rowbase = nx * (y0 + ny * z);
   float2* tws = sm + (ty + nzrows) * cs;  // twiddles of length L
-  const bool wrow = logL == 10 || logL == 9;  // 1024- / 512-point rows: warp rows (four-step)
+  const bool wrow = logL == 11 || logL == 10 || logL == 9;  // 2048- / 1024- / 512-point rows: warp (pair) rows
   const int sh = wrow ? 5 : 4;
   if (wrow) load_twq(tws, tw, logL);
   else load_twiddles<3>(tws, tw, logL);
@@ -327,7 +327,8 @@ __global__ void __launch_bounds__(X_THREADS_MAX, 2) k_xfwd(const MagnetDev* __re
   }
   __syncthreads();
   if (wrow) {
-    if (logL == 10) warp_rows<32, -1, true, false>(sm, ty + nzrows, cs, tws);
+    if (logL == 11) pair_rows<-1, true, false>(sm, ty + nzrows, cs, tws);
+    else if (logL == 10) warp_rows<32, -1, true, false>(sm, ty + nzrows, cs, tws);
     else warp_rows<16, -1, true, false>(sm, ty + nzrows, cs, tws);
     __syncthreads();
   } else {
@@ -1311,7 +1312,7 @@ __global__ void __launch_bounds__(X_THREADS_MAX, 2) k_xinv(const MagnetDev* __re
   const int Fh = M.Fh;
   float2* rows_z = sm + ty * cs;
   float2* tws = sm + (ty + nzrows) * cs;  // twiddles of length L
-  const bool wrow = logL == 10 || logL == 9;  // 1024- / 512-point rows: warp rows (four-step)
+  const bool wrow = logL == 11 || logL == 10 || logL == 9;  // 2048- / 1024- / 512-point rows: warp (pair) rows
   const int sh = wrow ? 5 : 4;
   if (wrow) load_twq(tws, tw, logL);
   else load_twiddles<3>(tws, tw, logL);
@@ -1408,7 +1409,8 @@ __global__ void __launch_bounds__(X_THREADS_MAX, 2) k_xinv(const MagnetDev* __re
   }
   __syncthreads();
   if (wrow) {  // only x < nx <= L/2 is used
-    if (logL == 10) warp_rows<32, 1, false, true>(sm, ty + nzrows, cs, tws);
+    if (logL == 11) pair_rows<1, false, true>(sm, ty + nzrows, cs, tws);
+    else if (logL == 10) warp_rows<32, 1, false, true>(sm, ty + nzrows, cs, tws);
     else warp_rows<16, 1, false, true>(sm, ty + nzrows, cs, tws);
     __syncthreads();
   } else {

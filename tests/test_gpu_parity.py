@@ -398,17 +398,20 @@ def test_demag_warp_transform_lengths(mpx, size):
     compare(MagnetSpec(size=size, cellsize=(1e-9, 2e-9, 1.5e-9), msat=8e5), mpx, [abi.Q_DEMAG_FIELD])
 
 
-@pytest.mark.parametrize("size", [(3, 600, 1), (2, 700, 2), (3, 1000, 3), (2, 513, 4), (1, 1024, 2)])
+@pytest.mark.parametrize("size", [(3, 600, 1), (2, 700, 2), (3, 1000, 3), (2, 513, 4), (1, 1024, 2), (600, 3, 2),
+                                  (1000, 2, 1), (700, 4, 3), (520, 520, 1)])
 def test_demag_warp_pair_length_2048(mpx, size):
-    """y length 2048 (k_yzw64: four-step 64 x 32 by pairs of warps, the inverse folding the upper half in) at z
-    lengths 1, 4, 8 and 8, several kx per block for thin magnets, ny from 513 to 1024."""
+    """Length 2048 in warp pairs (four-step 64 x 32, the inverse folding the upper half in): y transforms
+    (k_yzw64) at z lengths 1, 4, 8 and 8, several kx per block for thin magnets, ny from 513 to 1024; x rows
+    (pair_rows in both x passes) for nx from 520 to 1000."""
     compare(MagnetSpec(size=size, cellsize=(1e-9, 2e-9, 1.5e-9), msat=8e5), mpx, [abi.Q_DEMAG_FIELD])
 
 
-def test_warp_pair_trajectory_vs_oracle(mpx):
-    """Dormand-Prince stages through the warp-pair y transforms (Py = 2048, Pz = 4): <m>(t) against the FP64
-    oracle."""
-    s = MagnetSpec(size=(12, 600, 2), cellsize=(3e-9, 3e-9, 3e-9), msat=8e5, aex=1.3e-11, alpha=0.1,
+@pytest.mark.parametrize("size", [(12, 600, 2), (600, 12, 2)])
+def test_warp_pair_trajectory_vs_oracle(mpx, size):
+    """Dormand-Prince stages through the warp-pair transforms of length 2048 (y transforms at Pz = 4, then the
+    x passes with the stage combination and the lean epilogue): <m>(t) against the FP64 oracle."""
+    s = MagnetSpec(size=size, cellsize=(3e-9, 3e-9, 3e-9), msat=8e5, aex=1.3e-11, alpha=0.1,
                    world_bias=(0.0, 0.01, 0.0))
     m0 = random_m(s.shape, seed=9, smooth=3)
     ow, q = s.oracle_world(m0)

@@ -80,10 +80,11 @@ __global__ void __launch_bounds__(PF_THREADS, 2) k_pair_xfwd(const MagnetDev* __
     float v = 0.f;
     if (x < nxi) {
       if (TABLE) {
-        v = __ldg(tab + (((size_t)c * nzi + z) * nyi + y0 + r) * nxi + x);
+        const size_t ti = (((size_t)c * nzi + z) * nyi + y0 + r) * nxi + x;
+        if (span_ok(ti, (size_t)ncomp * nzi * nyi * nxi)) v = __ldg(tab + ti);
       } else {
         const int j = x + nxi * (y0 + r + nyi * z);
-        if (!MA.geom || MA.geom[j]) v = MA.msat.at(j) * m[(size_t)c * MA.N + j];
+        if (cell_ok(MA.N, j) && (!MA.geom || MA.geom[j])) v = MA.msat.at(j) * m[(size_t)c * MA.N + j];
       }
     }
     D[r * cs + pidx(x)] = make_float2(v, 0.f);
@@ -92,9 +93,11 @@ __global__ void __launch_bounds__(PF_THREADS, 2) k_pair_xfwd(const MagnetDev* __
   fft_many<-1, PF_LR>(D, logPx, nr, cs, tws);
   __syncthreads();
   const int Hx = Px / 2 + 1, Py = 1 << pf.logP[1], Pz = 1 << pf.logP[2];
+  const size_t tsize = (size_t)Hx * ncomp * Pz * Py;  // elements of the spectrum (checked build)
   for (int e = threadIdx.x; e < Hx * nr; e += blockDim.x) {  // consecutive threads: consecutive y
     const int r = e % nr, kx = e / nr;
-    pf.t[(((size_t)kx * ncomp + c) * Pz + z) * Py + y0 + r] = D[r * cs + pidx(kx)];
+    const size_t ti = (((size_t)kx * ncomp + c) * Pz + z) * Py + y0 + r;
+    if (span_ok(ti, tsize)) pf.t[ti] = D[r * cs + pidx(kx)];
   }
 }
 
@@ -119,11 +122,14 @@ __global__ void __launch_bounds__(PF_THREADS, 2) k_pair_yfft(const MagnetDev* __
   float2* D = sm;
   float2* tws = sm + zc * cs;
   load_twiddles<PF_LR>(tws, tw, logPy);
-  float2* __restrict__ T = pf.t + (((size_t)kx * ncomp + c) * Pz + z0) * Py;
+  const size_t t0 = (((size_t)kx * ncomp + c) * Pz + z0) * Py;
+  const size_t tleft = (size_t)((1 << pf.logP[0]) / 2 + 1) * ncomp * Pz * Py - t0;  // elements from T on (checked build)
+  float2* __restrict__ T = pf.t + t0;
   const int nyin = DIR < 0 ? pf.nin[1] : Py;
   for (int e = threadIdx.x; e < (nc << logPy); e += blockDim.x) {
     const int col = e >> logPy, y = e & (Py - 1);
-    D[col * cs + pidx(y)] = y < nyin ? T[(size_t)col * Py + y] : make_float2(0.f, 0.f);
+    D[col * cs + pidx(y)] =
+        (y < nyin && span_ok((size_t)col * Py + y, tleft)) ? T[(size_t)col * Py + y] : make_float2(0.f, 0.f);
   }
   __syncthreads();
   fft_many<DIR, PF_LR>(D, logPy, nc, cs, tws);
@@ -131,13 +137,13 @@ __global__ void __launch_bounds__(PF_THREADS, 2) k_pair_yfft(const MagnetDev* __
   if (DIR < 0) {
     for (int e = threadIdx.x; e < (nc << logPy); e += blockDim.x) {
       const int col = e >> logPy, y = e & (Py - 1);
-      T[(size_t)col * Py + y] = D[col * cs + pidx(y)];
+      if (span_ok((size_t)col * Py + y, tleft)) T[(size_t)col * Py + y] = D[col * cs + pidx(y)];
     }
   } else {
     const int ylo = pf.win[1], ny = pf.nout[1];
     for (int e = threadIdx.x; e < nc * ny; e += blockDim.x) {
       const int col = e / ny, y = ylo + e % ny;
-      T[(size_t)col * Py + y] = D[col * cs + pidx(y)];
+      if (span_ok((size_t)col * Py + y, tleft)) T[(size_t)col * Py + y] = D[col * cs + pidx(y)];
     }
   }
 }
@@ -162,22 +168,31 @@ __global__ void __launch_bounds__(PF_THREADS, 2) k_pair_zmul(const MagnetDev* __
   float2* D = sm;
   float2* tws = sm + ncomp * tky * cs;
   load_twiddles<PF_LR>(tws, tw, logPz);
-  float2* __restrict__ Tk = pf.t + (size_t)kx * ncomp * Pz * Py + ky0;
+  const size_t tk0 = (size_t)kx * ncomp * Pz * Py + ky0;
+  const int Hx = (1 << pf.logP[0]) / 2 + 1;
+  const size_t tleft = (size_t)Hx * ncomp * Pz * Py - tk0;  // elements from Tk on (checked build)
+  float2* __restrict__ Tk = pf.t + tk0;
   const int nzin = pf.nin[2];
   for (int e = threadIdx.x; e < (ncol << logPz); e += blockDim.x) {  // consecutive threads: consecutive ky
     const int kyl = e % nky, rest = e / nky, c = rest % ncomp, z = rest / ncomp;
-    D[(c * nky + kyl) * cs + pidx(z)] = z < nzin ? Tk[((size_t)c * Pz + z) * Py + kyl] : make_float2(0.f, 0.f);
+    const size_t ti = ((size_t)c * Pz + z) * Py + kyl;
+    D[(c * nky + kyl) * cs + pidx(z)] = (z < nzin && span_ok(ti, tleft)) ? Tk[ti] : make_float2(0.f, 0.f);
   }
   __syncthreads();
   fft_many<-1, PF_LR>(D, logPz, ncol, cs, tws);
   __syncthreads();
   if (MUL) {
-    const float2* __restrict__ K = pf.ks + (size_t)kx * 6 * Pz * Py + ky0;
+    const size_t k0 = (size_t)kx * 6 * Pz * Py + ky0;
+    const size_t kleft = (size_t)Hx * 6 * Pz * Py - k0;  // elements of the kernel spectrum from K on (checked build)
+    const float2* __restrict__ K = pf.ks + k0;
     for (int t = threadIdx.x; t < (nky << logPz); t += blockDim.x) {
       const int kyl = t % nky, kz = t / nky;
       float2 k[6];
 #pragma unroll
-      for (int q = 0; q < 6; ++q) k[q] = __ldg(K + ((size_t)q * Pz + kz) * Py + kyl);
+      for (int q = 0; q < 6; ++q) {
+        const size_t ki = ((size_t)q * Pz + kz) * Py + kyl;
+        k[q] = span_ok(ki, kleft) ? __ldg(K + ki) : make_float2(0.f, 0.f);
+      }
       float2* p0 = &D[kyl * cs + pidx(kz)];
       float2* p1 = &D[(nky + kyl) * cs + pidx(kz)];
       float2* p2 = &D[(2 * nky + kyl) * cs + pidx(kz)];
@@ -192,12 +207,14 @@ __global__ void __launch_bounds__(PF_THREADS, 2) k_pair_zmul(const MagnetDev* __
     const int zlo = pf.win[2], nz = pf.nout[2];
     for (int e = threadIdx.x; e < ncol * nz; e += blockDim.x) {
       const int kyl = e % nky, rest = e / nky, c = rest % ncomp, z = zlo + rest / ncomp;
-      Tk[((size_t)c * Pz + z) * Py + kyl] = D[(c * nky + kyl) * cs + pidx(z)];
+      const size_t ti = ((size_t)c * Pz + z) * Py + kyl;
+      if (span_ok(ti, tleft)) Tk[ti] = D[(c * nky + kyl) * cs + pidx(z)];
     }
   } else {
     for (int e = threadIdx.x; e < (ncol << logPz); e += blockDim.x) {
       const int kyl = e % nky, rest = e / nky, c = rest % ncomp, z = rest / ncomp;
-      Tk[((size_t)c * Pz + z) * Py + kyl] = D[(c * nky + kyl) * cs + pidx(z)];
+      const size_t ti = ((size_t)c * Pz + z) * Py + kyl;
+      if (span_ok(ti, tleft)) Tk[ti] = D[(c * nky + kyl) * cs + pidx(z)];
     }
   }
 }
@@ -223,16 +240,19 @@ __global__ void __launch_bounds__(PF_THREADS, 2) k_pair_yz(const MagnetDev* __re
   float2* tws = sm + 3 * PZ * cs;
   load_twiddles<PF_LR>(tws, tw, logPy);
   float2* __restrict__ Tk = pf.t + (size_t)kx * 3 * PZ * Py;  // [c][z][y]
+  const size_t tleft = (size_t)((1 << pf.logP[0]) / 2 + 1 - kx) * 3 * PZ * Py;  // elements from Tk on (checked build)
   const int nzi = pf.nin[2], nyi = pf.nin[1];
   for (int e = threadIdx.x; e < ((3 * nzi) << logPy); e += blockDim.x) {
     const int col = e >> logPy, y = e & (Py - 1);
     const int z = col / 3, c = col - 3 * z;
-    D[col * cs + pidx(y)] = y < nyi ? Tk[((size_t)c * PZ + z) * Py + y] : make_float2(0.f, 0.f);
+    const size_t ti = ((size_t)c * PZ + z) * Py + y;
+    D[col * cs + pidx(y)] = (y < nyi && span_ok(ti, tleft)) ? Tk[ti] : make_float2(0.f, 0.f);
   }
   __syncthreads();
   fft_many<-1, PF_LR>(D, logPy, 3 * nzi, cs, tws);
   __syncthreads();
   const float2* __restrict__ K = pf.ks + (size_t)kx * 6 * PZ * Py;
+  const size_t kleft = 2 * tleft;  // the kernel spectrum has 6 components where T has 3
   const int zlo = pf.win[2], nzo = pf.nout[2];
   for (int ky = threadIdx.x; ky < Py; ky += blockDim.x) {
     float2 v[3][PZ];
@@ -246,7 +266,10 @@ __global__ void __launch_bounds__(PF_THREADS, 2) k_pair_yz(const MagnetDev* __re
     for (int kz = 0; kz < PZ; ++kz) {
       float2 k[6];
 #pragma unroll
-      for (int q = 0; q < 6; ++q) k[q] = __ldg(K + ((size_t)q * PZ + kz) * Py + ky);
+      for (int q = 0; q < 6; ++q) {
+        const size_t ki = ((size_t)q * PZ + kz) * Py + ky;
+        k[q] = span_ok(ki, kleft) ? __ldg(K + ki) : make_float2(0.f, 0.f);
+      }
       const float2 m0 = v[0][kz], m1 = v[1][kz], m2 = v[2][kz];
       v[0][kz] = cadd(cadd(cmul(k[0], m0), cmul(k[3], m1)), cmul(k[4], m2));
       v[1][kz] = cadd(cadd(cmul(k[3], m0), cmul(k[1], m1)), cmul(k[5], m2));
@@ -267,7 +290,8 @@ __global__ void __launch_bounds__(PF_THREADS, 2) k_pair_yz(const MagnetDev* __re
   for (int e = threadIdx.x; e < 3 * nzo * nyo; e += blockDim.x) {
     const int col = e / nyo, y = ylo + (e - col * nyo);
     const int z = zlo + col / 3, c = col % 3;
-    Tk[((size_t)c * PZ + z) * Py + y] = D[(3 * zlo + col) * cs + pidx(y)];
+    const size_t ti = ((size_t)c * PZ + z) * Py + y;
+    if (span_ok(ti, tleft)) Tk[ti] = D[(3 * zlo + col) * cs + pidx(y)];
   }
 }
 
@@ -293,10 +317,13 @@ __global__ void __launch_bounds__(PF_THREADS, 2) k_pair_xinv(const MagnetDev* __
   float2* D = sm;
   float2* tws = sm + ry * cs;
   load_twiddles<PF_LR>(tws, tw, logPx);
-  const float2* __restrict__ T = pf.t + ((size_t)c * Pz + pf.win[2] + zz) * Py + pf.win[1] + y0;
+  const size_t t0 = ((size_t)c * Pz + pf.win[2] + zz) * Py + pf.win[1] + y0;
+  const size_t tleft = (size_t)Hx * 3 * Pz * Py - t0;  // elements from T on (checked build)
+  const float2* __restrict__ T = pf.t + t0;
   for (int e = threadIdx.x; e < Hx * nr; e += blockDim.x) {  // consecutive threads: consecutive y
     const int r = e % nr, kx = e / nr;
-    const float2 v = T[(size_t)kx * 3 * Pz * Py + r];
+    const size_t ti = (size_t)kx * 3 * Pz * Py + r;
+    const float2 v = span_ok(ti, tleft) ? T[ti] : make_float2(0.f, 0.f);
     D[r * cs + pidx(kx)] = v;
     if (kx > 0 && kx < Px - kx) D[r * cs + pidx(Px - kx)] = cconj(v);
   }
@@ -307,6 +334,7 @@ __global__ void __launch_bounds__(PF_THREADS, 2) k_pair_xinv(const MagnetDev* __
   for (int e = threadIdx.x; e < nr * nxo; e += blockDim.x) {
     const int r = e / nxo, x = e - r * nxo;
     const int i = x + nxo * (y0 + r + nyo * zz);
+    if (!cell_ok(NB, i)) continue;
     float v = pf.scale * D[r * cs + pidx(pf.win[0] + x)].x;
     if (MB.geom && !MB.geom[i]) v = 0.f;
     if (add) v += out[(size_t)c * NB + i];

@@ -4,7 +4,9 @@ run again against libmpx_checked.so (the same sources compiled with
 neighbours under every boundary condition, stage states and derivatives,
 stray-field buffers -- and every spectrum access of the x passes and of the
 y/z passes (column gathers and scatters, kernel-spectrum reads, the split
-path's y-transformed spectrum) verifies its index.  A bad access is skipped and recorded, never trapped; the
+path's y-transformed spectrum) and of the stray-field FFT passes on the pair
+grid (its tables, work and kernel spectra, destination cells) verifies its
+index.  A bad access is skipped and recorded, never trapped; the
 session hook in conftest.py then requires mpx_bounds_check to report none.
 This stands in for compute-sanitizer's memcheck, which is not available on
 these GPUs.

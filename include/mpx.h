@@ -421,7 +421,9 @@ mpx_status mpx_reduce_noalloc(const float* field, int ncells, int ncomp, const u
  * the forward x pass, the spectrum stores / gathers of the x passes, and in
  * the y/z passes the spectrum column gathers and scatters, the kernel-spectrum
  * reads and the split path's y-transformed spectrum (FFT and tensor-core
- * forms) are checked the same way.  In libmpx.so the checks are compiled out
+ * forms), and the stray-field FFT passes on the pair grid (tables, work and
+ * kernel spectra, destination cells) are checked the same way.  In libmpx.so
+ * the checks are compiled out
  * and this returns MPX_ERR_UNSUPPORTED. */
 mpx_status mpx_bounds_check(unsigned long long* first_bad);
 

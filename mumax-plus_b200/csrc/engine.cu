@@ -301,6 +301,7 @@ struct mpx_engine {
   float* d_dftB = nullptr;
   int n_sm = 148;  // multiprocessors of the engine's device
   int smem_x = 0, nt_x = 256;
+  bool x_pair = false;  // a launched magnet has 2048-point x rows: the PAIR forms of the x passes
   bool any_nodemag = false;
   int64_t bytes = 0;
   int64_t launches = 0;
@@ -662,6 +663,18 @@ mpx_status launch_yz(mpx_engine* e, int cls, const Work* work, int n, int smem, 
   e->launches++;
   return MPX_OK;
 }
+// The x-pass kernels of a launch: the PAIR forms (2048-point warp-pair rows
+// compiled in) when one of its magnets has 2048-point x rows, else the forms
+// without them (the shorter lengths keep their registers and code).
+using XfwdFn = void (*)(const MagnetDev*, const GroupDev*, const Work*, int, int, const float*, const float2*);
+using XinvFn = void (*)(const MagnetDev*, GroupDev*, const Work*, EpiArgs, const float2*);
+XfwdFn xfwd_fn(bool combine, bool pair) {
+  if (combine) return pair ? k_xfwd<true, true> : k_xfwd<true, false>;
+  return pair ? k_xfwd<false, true> : k_xfwd<false, false>;
+}
+XinvFn xinv_fn(bool pair) { return pair ? k_xinv<true> : k_xinv<false>; }
+bool x_pair_of(const Magnet* m) { return m->P[0] == 2048; }
+
 int x_threads(const Magnet* m) {
   int rows = m->ty + (m->ty + 1) / 2;
   int t = (rows * m->P[0] + 7) / 8;  // 8 values per thread in the x FFTs
@@ -761,6 +774,7 @@ mpx_status rebuild_tables(mpx_engine* e) {
   e->smem_ycols = e->smem_zmul = e->maxpy_split = e->maxpz_split = 0;
   e->smem_x = 0;
   e->nt_x = 256;
+  e->x_pair = false;
   for (int c = 0; c < YZ_CLASSES; ++c) e->smem_yz[c] = 0;
   for (auto& mp : e->mags) {
     if (!mp || mp->probe) continue;  // probe grids of stray-field evaluations
@@ -784,6 +798,7 @@ mpx_status rebuild_tables(mpx_engine* e) {
         e->smem_yz[cls] = std::max(e->smem_yz[cls], yz_smem(m));
       }
       e->nt_x = std::max(e->nt_x, x_threads(m));
+      e->x_pair = e->x_pair || x_pair_of(m);
     } else {
       want[mpx_engine::TT_LOCAL].push_back({m, &m->tiles});
     }
@@ -871,7 +886,8 @@ mpx_status rebuild_tables(mpx_engine* e) {
   std::vector<long long> sig;
   for (int t = 0; t < NT; ++t) sig.insert(sig.end(), {(long long)(uintptr_t)e->tt[t].dev, (long long)e->tt[t].items.size()});
   for (int c = 0; c < YZ_CLASSES; ++c) sig.push_back(e->smem_yz[c]);
-  sig.insert(sig.end(), {e->smem_x, e->nt_x, e->smem_ycols, e->smem_zmul, e->maxpy_split, e->maxpz_split});
+  sig.insert(sig.end(), {e->smem_x, e->nt_x, e->x_pair ? 1 : 0, e->smem_ycols, e->smem_zmul, e->maxpy_split,
+                         e->maxpz_split});
   e->tables_dirty = false;
   if (e->tables_valid && sig == e->tables_sig) return MPX_OK;
   e->tables_sig = std::move(sig);
@@ -1641,14 +1657,16 @@ mpx_status eval_into(mpx_engine* e, Magnet* m, int q, float* out) {
   if (m->hstray) MPX_TRY(launch_pairs(e, m->slot, 0, 0));  // stray fields of the other magnets' states
   if (m->demag && needs_demag) {
     const int sx = x_smem(m), syz = yz_smem(m), nt = x_threads(m);
-    k_xfwd<false><<<ntile, nt, sx, e->stream>>>(e->d_mags, e->d_groups, m->d_tiles, 0, 0, nullptr, e->d_tw);
+    xfwd_fn(false, x_pair_of(m))<<<ntile, nt, sx, e->stream>>>(e->d_mags, e->d_groups, m->d_tiles, 0, 0, nullptr,
+                                                                e->d_tw);
     if (m->split)
       MPX_TRY(launch_split(e, m->d_ycw, (int)m->ycw.size(), m->d_zmw, (int)m->zmw.size(), ycols_smem(m),
                            zmul_smem(m), m->P[1], m->P[2], 0, 0, m->d_tcw,
                            (int)m->tcw.size()));
     else
       MPX_TRY(launch_yz(e, yz_class(m), m->d_kxw, (int)m->kxw.size(), syz, 0, 0));
-    CUDA_TRY(launch_pdl(k_xinv, ntile, nt, sx, e->stream, e->d_mags, e->d_groups, m->d_tiles, ea, e->d_tw));
+    CUDA_TRY(launch_pdl(xinv_fn(x_pair_of(m)), ntile, nt, sx, e->stream, e->d_mags, e->d_groups, m->d_tiles, ea,
+                        e->d_tw));
     e->launches += 2;
   } else {
     k_local<<<ntile, 256, 0, e->stream>>>(e->d_mags, e->d_groups, m->d_tiles, ea);
@@ -1672,14 +1690,16 @@ mpx_status launch_attempt(mpx_engine* e, const TableauDev& T, int first_stage) {
     // stage states: combination fused into the x-forward pass, or k_combine
     if (e->n_t_demag > 0) {
       if (s == 0)
-        k_xfwd<false><<<e->n_t_demag, e->nt_x, e->smem_x, e->stream>>>(e->d_mags, e->d_groups, e->d_t_demag, 0, 1,
-                                                                       nullptr, e->d_tw);
+        xfwd_fn(false, e->x_pair)<<<e->n_t_demag, e->nt_x, e->smem_x, e->stream>>>(e->d_mags, e->d_groups,
+                                                                                    e->d_t_demag, 0, 1, nullptr,
+                                                                                    e->d_tw);
       else if (s == first_stage)  // after the step controller: fully serialised
-        k_xfwd<true><<<e->n_t_demag, e->nt_x, e->smem_x, e->stream>>>(e->d_mags, e->d_groups, e->d_t_demag, s, 1,
-                                                                      nullptr, e->d_tw);
+        xfwd_fn(true, e->x_pair)<<<e->n_t_demag, e->nt_x, e->smem_x, e->stream>>>(e->d_mags, e->d_groups,
+                                                                                   e->d_t_demag, s, 1, nullptr,
+                                                                                   e->d_tw);
       else  // after the previous stage (the group state is constant within an attempt)
-        CUDA_TRY(launch_pdl(k_xfwd<true>, e->n_t_demag, e->nt_x, e->smem_x, e->stream, e->d_mags, e->d_groups,
-                            e->d_t_demag, s, 1, (const float*)nullptr, e->d_tw));
+        CUDA_TRY(launch_pdl(xfwd_fn(true, e->x_pair), e->n_t_demag, e->nt_x, e->smem_x, e->stream, e->d_mags,
+                            e->d_groups, e->d_t_demag, s, 1, (const float*)nullptr, e->d_tw));
       e->launches++;
     }
     if (e->n_t_local > 0 && s > 0) {
@@ -1693,8 +1713,8 @@ mpx_status launch_attempt(mpx_engine* e, const TableauDev& T, int first_stage) {
         MPX_TRY(launch_yz(e, c, e->d_kx_demag[c], e->n_kx_demag[c], e->smem_yz[c], s, 1));
       MPX_TRY(launch_split(e, e->d_t_ycols, e->n_t_ycols, e->d_t_zmul, e->n_t_zmul, e->smem_ycols, e->smem_zmul,
                            e->maxpy_split, e->maxpz_split, s, 1, e->d_t_tc, e->n_t_tc));
-      CUDA_TRY(launch_pdl(k_xinv, e->n_t_demag, e->nt_x, e->smem_x, e->stream, e->d_mags, e->d_groups, e->d_t_demag, ea,
-                          e->d_tw));
+      CUDA_TRY(launch_pdl(xinv_fn(e->x_pair), e->n_t_demag, e->nt_x, e->smem_x, e->stream, e->d_mags, e->d_groups,
+                          e->d_t_demag, ea, e->d_tw));
       e->launches++;
     }
     if (e->n_t_local > 0) {
@@ -1948,7 +1968,9 @@ mpx_status mpx_engine_create(int device, mpx_engine** out) {
   CUDA_TRY(cudaMalloc(&e->d_red, sizeof(double) * 3 * 1024));
   CUDA_TRY(cudaMalloc(&e->d_redout, sizeof(double) * 4));  // 3 reduction results, or the 4 of k_min_final
   // large dynamic shared memory and the max-shared carveout for the FFT kernels
-  const void* fft_kernels[] = {(const void*)k_xfwd<false>, (const void*)k_xfwd<true>, (const void*)k_xinv,
+  const void* fft_kernels[] = {(const void*)k_xfwd<false, false>, (const void*)k_xfwd<true, false>,
+                               (const void*)k_xinv<false>, (const void*)k_xfwd<false, true>,
+                               (const void*)k_xfwd<true, true>, (const void*)k_xinv<true>,
                                (const void*)k_yz<1, 4>, (const void*)k_yz<2, 4>, (const void*)k_yz<4, 4>,
                                (const void*)k_yz<8, 4>, (const void*)k_yz<16, 4>, (const void*)k_yz<1, 3>,
                                (const void*)k_yz<2, 3>, (const void*)k_yz<4, 3>, (const void*)k_yz<8, 3>,
@@ -2668,7 +2690,7 @@ mpx_status mpx_profile_attempt(mpx_engine* e, int method, int reps, double ms[4]
   for (int r = 0; r <= reps; ++r) {
     CUDA_TRY(cudaEventRecord(ev[0], e->stream));
     if (e->n_t_demag > 0)
-      k_xfwd<true><<<e->n_t_demag, e->nt_x, e->smem_x, e->stream>>>(e->d_mags, e->d_groups, e->d_t_demag, s, 1,
+      xfwd_fn(true, e->x_pair)<<<e->n_t_demag, e->nt_x, e->smem_x, e->stream>>>(e->d_mags, e->d_groups, e->d_t_demag, s, 1,
                                                                     nullptr, e->d_tw);
     if (e->n_t_local > 0)
       k_combine<<<e->n_t_local, 256, 0, e->stream>>>(e->d_mags, e->d_groups, e->d_t_local, s, 0);
@@ -2683,7 +2705,7 @@ mpx_status mpx_profile_attempt(mpx_engine* e, int method, int reps, double ms[4]
     }
     CUDA_TRY(cudaEventRecord(ev[3], e->stream));
     if (e->n_t_demag > 0)
-      CUDA_TRY(launch_pdl(k_xinv, e->n_t_demag, e->nt_x, e->smem_x, e->stream, e->d_mags, e->d_groups, e->d_t_demag, ea,
+      CUDA_TRY(launch_pdl(xinv_fn(e->x_pair), e->n_t_demag, e->nt_x, e->smem_x, e->stream, e->d_mags, e->d_groups, e->d_t_demag, ea,
                           e->d_tw));
     if (e->n_t_local > 0) k_local<<<e->n_t_local, 256, 0, e->stream>>>(e->d_mags, e->d_groups, e->d_t_local, ea);
     CUDA_TRY(cudaEventRecord(ev[4], e->stream));
@@ -2759,7 +2781,7 @@ mpx_status mpx_profile_eval(mpx_engine* e, int magnet, int reps, double ms[4]) {
     float t[4] = {0, 0, 0, 0};
     if (m->demag) {
       CUDA_TRY(cudaEventRecord(ev[0], e->stream));
-      k_xfwd<false><<<ntile, nt, sx, e->stream>>>(e->d_mags, e->d_groups, m->d_tiles, 0, 0, nullptr, e->d_tw);
+      xfwd_fn(false, x_pair_of(m))<<<ntile, nt, sx, e->stream>>>(e->d_mags, e->d_groups, m->d_tiles, 0, 0, nullptr, e->d_tw);
       CUDA_TRY(cudaEventRecord(ev[1], e->stream));
       if (m->split)
         MPX_TRY(launch_split(e, m->d_ycw, (int)m->ycw.size(), m->d_zmw, (int)m->zmw.size(), ycols_smem(m),
@@ -2768,7 +2790,7 @@ mpx_status mpx_profile_eval(mpx_engine* e, int magnet, int reps, double ms[4]) {
       else
         MPX_TRY(launch_yz(e, yz_class(m), m->d_kxw, (int)m->kxw.size(), syz, 0, 0));
       CUDA_TRY(cudaEventRecord(ev[2], e->stream));
-      CUDA_TRY(launch_pdl(k_xinv, ntile, nt, sx, e->stream, e->d_mags, e->d_groups, m->d_tiles, ea, e->d_tw));
+      CUDA_TRY(launch_pdl(xinv_fn(x_pair_of(m)), ntile, nt, sx, e->stream, e->d_mags, e->d_groups, m->d_tiles, ea, e->d_tw));
       CUDA_TRY(cudaEventRecord(ev[3], e->stream));
       e->launches += 2;
       CUDA_TRY(cudaEventSynchronize(ev[3]));

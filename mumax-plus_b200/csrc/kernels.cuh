@@ -220,7 +220,10 @@ __device__ __forceinline__ int tile_log(int ty) { return ty <= 1 ? 0 : 32 - __cl
 // ------------------------------------------------------------------ k_xfwd
 // smem: padded rows [ty] for (Mx + i My) of each row, then [(ty+1)/2] for
 // (Mz(y) + i Mz(y+1)).
-template <bool COMBINE>
+// PAIR: the 2048-point rows of the warp pairs are compiled in (the forms launched
+// when a magnet with such rows is in the launch; without them the others keep
+// the registers and code of the shorter lengths).
+template <bool COMBINE, bool PAIR = false>
 __global__ void __launch_bounds__(X_THREADS_MAX, 2) k_xfwd(const MagnetDev* __restrict__ mags, const GroupDev* __restrict__ groups,
                                               const Work* __restrict__ work, int stage, int gate,
                                               const float* __restrict__ msrc_override,
@@ -234,13 +237,14 @@ __global__ void __launch_bounds__(X_THREADS_MAX, 2) k_xfwd(const MagnetDev* __re
   const int z = wk.z, y0 = wk.y0, ty = wk.ty;
   const int nx = M.n[0], ny = M.n[1], nz = M.n[2], N = M.N;
   const int logL = M.logP[0], L = 1 << logL, cs = xrow_stride(L, ty);
+  if (!PAIR && logL == 11) return;  // 2048-point rows only in the PAIR form (the host never launches them here)
   const int nzrows = (ty + 1) >> 1;
   const float* src = msrc_override ? msrc_override : stage_m(M, G, stage);
   float* xs = M.buf[G.map[1]];
   const float* x0 = M.buf[G.map[0]];
   const int rowbase = nx * (y0 + ny * z);
   float2* tws = sm + (ty + nzrows) * cs;  // twiddles of length L
-  const bool wrow = logL == 11 || logL == 10 || logL == 9;  // 2048- / 1024- / 512-point rows: warp (pair) rows
+  const bool wrow = (PAIR && logL == 11) || logL == 10 || logL == 9;  // 2048- / 1024- / 512-point rows: warp (pair) rows
   const int sh = wrow ? 5 : 4;
   if (wrow) load_twq(tws, tw, logL);
   else load_twiddles<3>(tws, tw, logL);
@@ -327,7 +331,7 @@ __global__ void __launch_bounds__(X_THREADS_MAX, 2) k_xfwd(const MagnetDev* __re
   }
   __syncthreads();
   if (wrow) {
-    if (logL == 11) pair_rows<-1, true, false>(sm, ty + nzrows, cs, tws);
+    if (PAIR && logL == 11) pair_rows<-1, true, false>(sm, ty + nzrows, cs, tws);
     else if (logL == 10) warp_rows<32, -1, true, false>(sm, ty + nzrows, cs, tws);
     else warp_rows<16, -1, true, false>(sm, ty + nzrows, cs, tws);
     __syncthreads();
@@ -1296,6 +1300,8 @@ __device__ __forceinline__ void stage_quad_lean(const MagnetDev& M, const GroupD
 }
 
 // ------------------------------------------------------------------ k_xinv
+// PAIR as for k_xfwd.
+template <bool PAIR = false>
 __global__ void __launch_bounds__(X_THREADS_MAX, 2) k_xinv(const MagnetDev* __restrict__ mags, GroupDev* __restrict__ groups,
                                               const Work* __restrict__ work, EpiArgs ea,
                                               const float2* __restrict__ tw) {
@@ -1308,11 +1314,12 @@ __global__ void __launch_bounds__(X_THREADS_MAX, 2) k_xinv(const MagnetDev* __re
   const int z = wk.z, y0 = wk.y0, ty = wk.ty;
   const int nx = M.n[0], ny = M.n[1], nz = M.n[2];
   const int logL = M.logP[0], L = 1 << logL, cs = xrow_stride(L, ty);
+  if (!PAIR && logL == 11) return;  // 2048-point rows only in the PAIR form (the host never launches them here)
   const int nzrows = (ty + 1) >> 1;
   const int Fh = M.Fh;
   float2* rows_z = sm + ty * cs;
   float2* tws = sm + (ty + nzrows) * cs;  // twiddles of length L
-  const bool wrow = logL == 11 || logL == 10 || logL == 9;  // 2048- / 1024- / 512-point rows: warp (pair) rows
+  const bool wrow = (PAIR && logL == 11) || logL == 10 || logL == 9;  // 2048- / 1024- / 512-point rows: warp (pair) rows
   const int sh = wrow ? 5 : 4;
   if (wrow) load_twq(tws, tw, logL);
   else load_twiddles<3>(tws, tw, logL);
@@ -1409,7 +1416,7 @@ __global__ void __launch_bounds__(X_THREADS_MAX, 2) k_xinv(const MagnetDev* __re
   }
   __syncthreads();
   if (wrow) {  // only x < nx <= L/2 is used
-    if (logL == 11) pair_rows<1, false, true>(sm, ty + nzrows, cs, tws);
+    if (PAIR && logL == 11) pair_rows<1, false, true>(sm, ty + nzrows, cs, tws);
     else if (logL == 10) warp_rows<32, 1, false, true>(sm, ty + nzrows, cs, tws);
     else warp_rows<16, 1, false, true>(sm, ty + nzrows, cs, tws);
     __syncthreads();

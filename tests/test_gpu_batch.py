@@ -49,6 +49,22 @@ def test_batch_results_match_plain(mpx):
         assert diff <= MIX_TOL, f"solve {p.key}: |dm| {diff:.3e}"
 
 
+def test_batch_with_2048_point_rows_matches_plain(mpx):
+    """A batch holding a solve with 2048-point x rows launches the x passes in
+    their warp-pair forms for every solve; each solve still gives the result it
+    gives alone (where only that one takes those forms)."""
+    from mumaxplus_b200 import batch as B
+
+    sols = _mix() + [_solve(4, (600, 16, 1), 2e-9, 8e5, 1.3e-11, 0.1, (0.0, 0.02, 0.05))]
+    plain, _, _ = B.run_plain(B.Batch(), sols, duration=10e-12, torque_stop=0.0)
+    mixed, _, _ = B.relax_batch(B.Batch(), sols, duration=10e-12, torque_stop=0.0)
+    for p, q in zip(plain, mixed):
+        assert p.steps == q.steps and p.steps > 0
+        assert not p.failed and not q.failed
+        diff = float(np.max(np.abs(p.m - q.m)))
+        assert diff <= MIX_TOL, f"solve {p.key}: |dm| {diff:.3e}"
+
+
 def test_relaxation_stops_on_torque(mpx):
     from mumaxplus_b200 import batch as B
 

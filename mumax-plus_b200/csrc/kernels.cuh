@@ -1058,18 +1058,22 @@ __device__ __forceinline__ void neighbour_term(const MagnetDev& M, int r, bool p
     const float3 Gm = gamma_uniform(M.fd, axis, mc);
     m_ = mc + (d * M.cs[axis]) * (M.finv_2a * Gm);
   }
-  if (do_exch && (nin || neumann)) he = he + M.fe[axis] * (m_ - mc);
+  if (do_exch && (nin || neumann)) {  // he += fe (m_ - mc), one rounding per operation as written
+    const float fe = M.fe[axis];
+    he = f3(__fmaf_rn(fe, __fsub_rn(m_.x, mc.x), he.x), __fmaf_rn(fe, __fsub_rn(m_.y, mc.y), he.y),
+            __fmaf_rn(fe, __fsub_rn(m_.z, mc.z), he.z));
+  }
   if (do_dmi && (nin || !dmi_open)) {
     const float inv_delta = d * M.inv_cs[axis];
-    if constexpr (DK == DMI_IFACE) {
+    if constexpr (DK == DMI_IFACE) {  // hd += (D m_) / delta, roundings as written
       if (axis == 0) {
         const float Dxz = M.fd[1];
-        hd.x += (Dxz * m_.z) * inv_delta;
-        hd.z += (-Dxz * m_.x) * inv_delta;
+        hd.x = __fmaf_rn(__fmul_rn(Dxz, m_.z), inv_delta, hd.x);
+        hd.z = __fmaf_rn(__fmul_rn(-Dxz, m_.x), inv_delta, hd.z);
       } else if (axis == 1) {
         const float Dyz = M.fd[5];
-        hd.y += (Dyz * m_.z) * inv_delta;
-        hd.z += (-Dyz * m_.y) * inv_delta;
+        hd.y = __fmaf_rn(__fmul_rn(Dyz, m_.z), inv_delta, hd.y);
+        hd.z = __fmaf_rn(__fmul_rn(-Dyz, m_.y), inv_delta, hd.z);
       }
     } else {
       const float Dxy = M.fd[3 * axis], Dxz = M.fd[3 * axis + 1], Dyz = M.fd[3 * axis + 2];
@@ -1097,26 +1101,41 @@ __device__ __forceinline__ void neighbour_sums(const MagnetDev& M, const float* 
 // The rest of a lean-path cell once its exchange / DMI sums are known:
 // anisotropy, applied field, demag, the sum in local_terms_fast's order and the
 // torque of epilogue_cell.  `ext` is the applied field of the cell.
+// LLG torque of the lean path with every rounding spelled out (the packed
+// four-cell form below repeats the same operations per component).
+__device__ __forceinline__ float llg_coef(float a) { return -GAMMA_LL / __fmaf_rn(a, a, 1.0f); }
+__device__ __forceinline__ float3 cross_rn(float3 a, float3 b) {
+  return f3(__fsub_rn(__fmul_rn(a.y, b.z), __fmul_rn(a.z, b.y)), __fsub_rn(__fmul_rn(a.z, b.x), __fmul_rn(a.x, b.z)),
+            __fsub_rn(__fmul_rn(a.x, b.y), __fmul_rn(a.y, b.x)));
+}
+__device__ __forceinline__ float3 llg_torque_rn(float3 m, float3 h, float a) {
+  const float g = llg_coef(a);
+  const float3 mxh = cross_rn(m, h), mxmxh = cross_rn(m, mxh);
+  return f3(__fmul_rn(g, __fmaf_rn(a, mxmxh.x, mxh.x)), __fmul_rn(g, __fmaf_rn(a, mxmxh.y, mxh.y)),
+            __fmul_rn(g, __fmaf_rn(a, mxmxh.z, mxh.z)));
+}
+
 __device__ __forceinline__ float3 finish_cell_lean(const MagnetDev& M, const GroupDev& G, float3 mc, float3 he,
                                                    float3 hd, float3 ext, float3 bdemag) {
   const unsigned terms = M.terms;
+  const float s = M.finv_ms;
   float3 exch = f3(0, 0, 0), dmi = f3(0, 0, 0), anis = f3(0, 0, 0);
-  if (terms & TERM_EXCH) exch = M.finv_ms * he;
-  if (terms & TERM_DMI) dmi = M.finv_ms * hd;
+  if (terms & TERM_EXCH) exch = f3(__fmul_rn(s, he.x), __fmul_rn(s, he.y), __fmul_rn(s, he.z));
+  if (terms & TERM_DMI) dmi = f3(__fmul_rn(s, hd.x), __fmul_rn(s, hd.y), __fmul_rn(s, hd.z));
   if ((terms & TERM_ANIS) && (terms & FLAG_CUBIC)) {
     anis = cubic_field(mc, f3(M.fc[0][0], M.fc[0][1], M.fc[0][2]), f3(M.fc[1][0], M.fc[1][1], M.fc[1][2]),
                        f3(M.fc[2][0], M.fc[2][1], M.fc[2][2]), M.fkc[0], M.fkc[1], M.fkc[2], M.finv_ms);
-  } else if (terms & TERM_ANIS) {
+  } else if (terms & TERM_ANIS) {  // (2 K1 mu + 4 K2 mu^3) u / Ms, roundings as written
     const float3 u = f3(M.fu[0], M.fu[1], M.fu[2]);
-    const float mu = dot3(mc, u);
-    anis = M.finv_ms * ((2 * M.fk1 * mu + 4 * M.fk2 * mu * mu * mu) * u);
+    const float mu = __fmaf_rn(mc.z, u.z, __fmaf_rn(mc.y, u.y, __fmul_rn(mc.x, u.x)));
+    const float c = __fadd_rn(__fmul_rn(2 * M.fk1, mu), __fmul_rn(__fmul_rn(__fmul_rn(4 * M.fk2, mu), mu), mu));
+    anis = f3(__fmul_rn(s, __fmul_rn(c, u.x)), __fmul_rn(s, __fmul_rn(c, u.y)), __fmul_rn(s, __fmul_rn(c, u.z)));
   }
-  float3 h = exch;
-  h = h + anis;
-  h = h + ext;
-  h = h + dmi;
-  h = h + bdemag;
-  return G.torque_kind ? damping_torque(mc, h) : llg_torque(mc, h, M.alpha.u);
+  // h = exch + anis + ext + dmi + bdemag, left to right
+  const float3 h = f3(__fadd_rn(__fadd_rn(__fadd_rn(__fadd_rn(exch.x, anis.x), ext.x), dmi.x), bdemag.x),
+                      __fadd_rn(__fadd_rn(__fadd_rn(__fadd_rn(exch.y, anis.y), ext.y), dmi.y), bdemag.y),
+                      __fadd_rn(__fadd_rn(__fadd_rn(__fadd_rn(exch.z, anis.z), ext.z), dmi.z), bdemag.z));
+  return G.torque_kind ? damping_torque(mc, h) : llg_torque_rn(mc, h, M.alpha.u);
 }
 
 // Right-hand side of one cell of a stage on the lean path: the arithmetic of
@@ -1247,6 +1266,104 @@ __device__ __forceinline__ void quad_sums(const MagnetDev& M, const float* __res
   }
 }
 
+// ------------------------------------------------ packed pairs of cells
+// The four cells of a quad as the pairs (0, 1) and (2, 3), every component a
+// float2 for the packed FP32 pair instructions (pmul, pfma, padd, psub of
+// fft.cuh, each rounded as its scalar counterpart).
+struct P3 {
+  float2 x, y, z;
+};
+__device__ __forceinline__ float2 bc(float v) { return make_float2(v, v); }
+__device__ __forceinline__ P3 pcross(const P3& a, const P3& b) {  // cross_rn per component pair
+  return P3{psub(pmul(a.y, b.z), pmul(a.z, b.y)), psub(pmul(a.z, b.x), pmul(a.x, b.z)),
+            psub(pmul(a.x, b.y), pmul(a.y, b.x))};
+}
+__device__ __forceinline__ P3 pick(const float3 (&v)[4], int p) {
+  return P3{make_float2(v[2 * p].x, v[2 * p + 1].x), make_float2(v[2 * p].y, v[2 * p + 1].y),
+            make_float2(v[2 * p].z, v[2 * p + 1].z)};
+}
+
+// stage_quad_lean for a quad whose neighbours are all present, with
+// interfacial DMI or none, uniaxial anisotropy or none and the LLG torque: the x
+// neighbours per cell (as quad_sums), then the y / z neighbour terms, the field
+// and the torque on the two cell pairs with packed instructions.  Every
+// operation is the one neighbour_term<true, DK> and finish_cell_lean perform,
+// with the same rounding, so a cell gets the same bits whichever path its warp
+// takes.
+template <int DK, typename BD>
+__device__ __forceinline__ void stage_quad_packed(const MagnetDev& M, const float* __restrict__ m, int N, int i0,
+                                                  int x0, int il, int ir, const int (&rb)[4], const float3 (&mc)[4],
+                                                  bool do_exch, bool do_dmi, float3 ext, BD bdemag, float4& kx,
+                                                  float4& ky, float4& kz) {
+  float3 he[4], hd[4];
+#pragma unroll
+  for (int q = 0; q < 4; ++q) he[q] = hd[q] = f3(0.f, 0.f, 0.f);
+  {  // x-, x+ (the x neighbours inside the quad are its own cells)
+    const float3 xl = ldg3(m, N, il);
+    neighbour_term<true, DK>(M, 0, true, xl, mc[0], false, false, do_exch, do_dmi, he[0], hd[0]);
+#pragma unroll
+    for (int q = 1; q < 4; ++q)
+      neighbour_term<true, DK>(M, 0, true, mc[q - 1], mc[q], false, false, do_exch, do_dmi, he[q], hd[q]);
+#pragma unroll
+    for (int q = 0; q < 3; ++q)
+      neighbour_term<true, DK>(M, 1, true, mc[q + 1], mc[q], false, false, do_exch, do_dmi, he[q], hd[q]);
+    const float3 xr = ldg3(m, N, ir);
+    neighbour_term<true, DK>(M, 1, true, xr, mc[3], false, false, do_exch, do_dmi, he[3], hd[3]);
+  }
+  P3 MC[2] = {pick(mc, 0), pick(mc, 1)}, HE[2] = {pick(he, 0), pick(he, 1)}, HD[2] = {pick(hd, 0), pick(hd, 1)};
+#pragma unroll
+  for (int r = 2; r < 6; ++r) {  // y-, y+, z-, z+: whole neighbour rows
+    const int axis = r >> 1;
+    float3 nn[4];
+    ldg4x3(m, N, rb[r - 2] + x0, nn);
+    const float2 fe = bc(M.fe[axis]);
+    const float inv_delta = ((r & 1) ? 1.f : -1.f) * M.inv_cs[axis];
+#pragma unroll
+    for (int p = 0; p < 2; ++p) {
+      const P3 nb = pick(nn, p);
+      if (do_exch) {
+        HE[p].x = pfma(fe, psub(nb.x, MC[p].x), HE[p].x);
+        HE[p].y = pfma(fe, psub(nb.y, MC[p].y), HE[p].y);
+        HE[p].z = pfma(fe, psub(nb.z, MC[p].z), HE[p].z);
+      }
+      if (DK == DMI_IFACE && do_dmi && axis == 1) {
+        const float Dyz = M.fd[5];
+        HD[p].y = pfma(pmul(bc(Dyz), nb.z), bc(inv_delta), HD[p].y);
+        HD[p].z = pfma(pmul(bc(-Dyz), nb.y), bc(inv_delta), HD[p].z);
+      }
+    }
+  }
+  const unsigned terms = M.terms;
+  const float2 s = bc(M.finv_ms), zero = make_float2(0.f, 0.f);
+  const float a = M.alpha.u;
+  const float2 g = bc(llg_coef(a)), a2 = bc(a);
+#pragma unroll
+  for (int p = 0; p < 2; ++p) {
+    P3 ex = {zero, zero, zero}, dm = ex, an = ex;
+    if (terms & TERM_EXCH) ex = P3{pmul(s, HE[p].x), pmul(s, HE[p].y), pmul(s, HE[p].z)};
+    if (terms & TERM_DMI) dm = P3{pmul(s, HD[p].x), pmul(s, HD[p].y), pmul(s, HD[p].z)};
+    if (terms & TERM_ANIS) {
+      const float2 ux = bc(M.fu[0]), uy = bc(M.fu[1]), uz = bc(M.fu[2]);
+      const float2 mu = pfma(MC[p].z, uz, pfma(MC[p].y, uy, pmul(MC[p].x, ux)));
+      const float2 c = padd(pmul(bc(2 * M.fk1), mu), pmul(pmul(pmul(bc(4 * M.fk2), mu), mu), mu));
+      an = P3{pmul(s, pmul(c, ux)), pmul(s, pmul(c, uy)), pmul(s, pmul(c, uz))};
+    }
+    const float3 b0 = bdemag(2 * p), b1 = bdemag(2 * p + 1);
+    const P3 h{padd(padd(padd(padd(ex.x, an.x), bc(ext.x)), dm.x), make_float2(b0.x, b1.x)),
+               padd(padd(padd(padd(ex.y, an.y), bc(ext.y)), dm.y), make_float2(b0.y, b1.y)),
+               padd(padd(padd(padd(ex.z, an.z), bc(ext.z)), dm.z), make_float2(b0.z, b1.z))};
+    const P3 mxh = pcross(MC[p], h), mxmxh = pcross(MC[p], mxh);
+    const float2 tx = pmul(g, pfma(a2, mxmxh.x, mxh.x));
+    const float2 ty = pmul(g, pfma(a2, mxmxh.y, mxh.y));
+    const float2 tz = pmul(g, pfma(a2, mxmxh.z, mxh.z));
+    if (p == 0) {
+      kx.x = tx.x; kx.y = tx.y; ky.x = ty.x; ky.y = ty.y; kz.x = tz.x; kz.y = tz.y;
+    } else {
+      kx.z = tx.x; kx.w = tx.y; ky.z = ty.x; ky.w = ty.y; kz.z = tz.x; kz.w = tz.y;
+    }
+  }
+}
+
 // stage_cell_lean for four consecutive cells (no stray field, spin-transfer
 // torque or thermal noise on the magnet): the same arithmetic per cell.  The
 // demag field of cell q comes from bdemag(q); the torques go to kx / ky / kz
@@ -1281,6 +1398,11 @@ __device__ __forceinline__ void stage_quad_lean(const MagnetDev& M, const GroupD
     for (int q = 0; q < 4; ++q) rb[q] = T.r[yl][q];
     const bool inner = il >= 0 && ir >= 0 && rb[0] >= 0 && rb[1] >= 0 && rb[2] >= 0 && rb[3] >= 0;
     const bool ifc = do_dmi && dmi_kind(M) == DMI_IFACE;
+    if (__all_sync(__activemask(), inner) && !(terms & FLAG_CUBIC) && !G.torque_kind && (!do_dmi || ifc)) {
+      const float3 ext = (terms & TERM_EXT) ? f3(M.fb[0], M.fb[1], M.fb[2]) : f3(0.f, 0.f, 0.f);
+      stage_quad_packed<DMI_IFACE>(M, m, N, i0, x0, il, ir, rb, mc, do_exch, do_dmi, ext, bdemag, kx, ky, kz);
+      return;
+    }
     if (__all_sync(__activemask(), inner)) {
       if (ifc) quad_sums<true, DMI_IFACE>(M, m, N, i0, x0, il, ir, rb, mc, neumann, dmi_open, do_exch, do_dmi, he, hd);
       else quad_sums<true, DMI_GENERAL>(M, m, N, i0, x0, il, ir, rb, mc, neumann, dmi_open, do_exch, do_dmi, he, hd);

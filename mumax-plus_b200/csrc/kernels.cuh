@@ -1283,37 +1283,39 @@ __device__ __forceinline__ P3 pick(const float3 (&v)[4], int p) {
             make_float2(v[2 * p].z, v[2 * p + 1].z)};
 }
 
-// stage_quad_lean for a quad whose neighbours are all present, with
-// interfacial DMI or none, uniaxial anisotropy or none and the LLG torque: the x
-// neighbours per cell (as quad_sums), then the y / z neighbour terms, the field
-// and the torque on the two cell pairs with packed instructions.  Every
-// operation is the one neighbour_term<true, DK> and finish_cell_lean perform,
-// with the same rounding, so a cell gets the same bits whichever path its warp
-// takes.
+// stage_quad_lean with interfacial DMI or none, uniaxial anisotropy or none and
+// the LLG torque: the x neighbours per cell (as quad_sums, ghost cells
+// included), then the y / z neighbour terms, the field and the torque on the two
+// cell pairs with packed instructions.  Every operation is the one
+// neighbour_term and finish_cell_lean perform, with the same rounding, so a cell
+// gets the same bits whichever path its warp takes.  A y / z neighbour row may
+// be missing (rb < 0) only where the caller has found that its ghost adds
+// nothing (no DMI entries along that axis): it is left out.
 template <int DK, typename BD>
 __device__ __forceinline__ void stage_quad_packed(const MagnetDev& M, const float* __restrict__ m, int N, int i0,
                                                   int x0, int il, int ir, const int (&rb)[4], const float3 (&mc)[4],
-                                                  bool do_exch, bool do_dmi, float3 ext, BD bdemag, float4& kx,
-                                                  float4& ky, float4& kz) {
+                                                  bool neumann, bool dmi_open, bool do_exch, bool do_dmi, float3 ext,
+                                                  BD bdemag, float4& kx, float4& ky, float4& kz) {
   float3 he[4], hd[4];
 #pragma unroll
   for (int q = 0; q < 4; ++q) he[q] = hd[q] = f3(0.f, 0.f, 0.f);
   {  // x-, x+ (the x neighbours inside the quad are its own cells)
-    const float3 xl = ldg3(m, N, il);
-    neighbour_term<true, DK>(M, 0, true, xl, mc[0], false, false, do_exch, do_dmi, he[0], hd[0]);
+    const float3 xl = il >= 0 ? ldg3(m, N, il) : mc[0];
+    neighbour_term<false, DK>(M, 0, il >= 0, xl, mc[0], neumann, dmi_open, do_exch, do_dmi, he[0], hd[0]);
 #pragma unroll
     for (int q = 1; q < 4; ++q)
-      neighbour_term<true, DK>(M, 0, true, mc[q - 1], mc[q], false, false, do_exch, do_dmi, he[q], hd[q]);
+      neighbour_term<false, DK>(M, 0, true, mc[q - 1], mc[q], neumann, dmi_open, do_exch, do_dmi, he[q], hd[q]);
 #pragma unroll
     for (int q = 0; q < 3; ++q)
-      neighbour_term<true, DK>(M, 1, true, mc[q + 1], mc[q], false, false, do_exch, do_dmi, he[q], hd[q]);
-    const float3 xr = ldg3(m, N, ir);
-    neighbour_term<true, DK>(M, 1, true, xr, mc[3], false, false, do_exch, do_dmi, he[3], hd[3]);
+      neighbour_term<false, DK>(M, 1, true, mc[q + 1], mc[q], neumann, dmi_open, do_exch, do_dmi, he[q], hd[q]);
+    const float3 xr = ir >= 0 ? ldg3(m, N, ir) : mc[3];
+    neighbour_term<false, DK>(M, 1, ir >= 0, xr, mc[3], neumann, dmi_open, do_exch, do_dmi, he[3], hd[3]);
   }
   P3 MC[2] = {pick(mc, 0), pick(mc, 1)}, HE[2] = {pick(he, 0), pick(he, 1)}, HD[2] = {pick(hd, 0), pick(hd, 1)};
 #pragma unroll
   for (int r = 2; r < 6; ++r) {  // y-, y+, z-, z+: whole neighbour rows
     const int axis = r >> 1;
+    if (rb[r - 2] < 0) continue;  // missing, and its ghost adds nothing (see the caller)
     float3 nn[4];
     ldg4x3(m, N, rb[r - 2] + x0, nn);
     const float2 fe = bc(M.fe[axis]);
@@ -1398,10 +1400,20 @@ __device__ __forceinline__ void stage_quad_lean(const MagnetDev& M, const GroupD
     for (int q = 0; q < 4; ++q) rb[q] = T.r[yl][q];
     const bool inner = il >= 0 && ir >= 0 && rb[0] >= 0 && rb[1] >= 0 && rb[2] >= 0 && rb[3] >= 0;
     const bool ifc = do_dmi && dmi_kind(M) == DMI_IFACE;
-    if (__all_sync(__activemask(), inner) && !(terms & FLAG_CUBIC) && !G.torque_kind && (!do_dmi || ifc)) {
-      const float3 ext = (terms & TERM_EXT) ? f3(M.fb[0], M.fb[1], M.fb[2]) : f3(0.f, 0.f, 0.f);
-      stage_quad_packed<DMI_IFACE>(M, m, N, i0, x0, il, ir, rb, mc, do_exch, do_dmi, ext, bdemag, kx, ky, kz);
-      return;
+    if (!(terms & FLAG_CUBIC) && !G.torque_kind && (!do_dmi || ifc)) {
+      // a missing y / z neighbour adds exactly nothing when the DMI tensor has no
+      // entries along its axis: with open boundaries it is skipped, and the
+      // Neumann ghost m + Gamma/(2A) delta is m itself (Gamma = 0)
+      const float* f = M.fd;
+      const bool y0 = f[3] == 0.f && f[4] == 0.f && f[5] == 0.f;
+      const bool z0 = f[6] == 0.f && f[7] == 0.f && f[8] == 0.f;
+      const bool qok = (y0 || (rb[0] >= 0 && rb[1] >= 0)) && (z0 || (rb[2] >= 0 && rb[3] >= 0));
+      if (__all_sync(__activemask(), qok)) {
+        const float3 ext = (terms & TERM_EXT) ? f3(M.fb[0], M.fb[1], M.fb[2]) : f3(0.f, 0.f, 0.f);
+        stage_quad_packed<DMI_IFACE>(M, m, N, i0, x0, il, ir, rb, mc, neumann, dmi_open, do_exch, do_dmi, ext,
+                                     bdemag, kx, ky, kz);
+        return;
+      }
     }
     if (__all_sync(__activemask(), inner)) {
       if (ifc) quad_sums<true, DMI_IFACE>(M, m, N, i0, x0, il, ir, rb, mc, neumann, dmi_open, do_exch, do_dmi, he, hd);

@@ -14,7 +14,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 SRC = os.path.join(HERE, "csrc", "engine.cu")
-HEADERS = [os.path.join(HERE, "csrc", f) for f in ("fft.cuh", "physics.cuh", "kernels.cuh", "newell.cuh", "stray.cuh", "yzsplit.cuh")]
+HEADERS = sorted(os.path.join(HERE, "csrc", f) for f in os.listdir(os.path.join(HERE, "csrc")) if f.endswith(".cuh"))
 OUT = os.path.join(HERE, "libmpx.so")
 OUT_CHECKED = os.path.join(HERE, "libmpx_checked.so")
 

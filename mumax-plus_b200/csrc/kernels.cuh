@@ -517,6 +517,98 @@ __device__ __forceinline__ void zstage_pair(float2* D, int cs, const MagnetDev& 
     }
 }
 
+// exp(DIR 2 pi i m / 16) v for m = 0 .. 7 known at compile time after unrolling
+template <int DIR>
+__device__ __forceinline__ float2 rot16_m(float2 v, int m) {
+  switch (m) {
+    case 1: return rot16<DIR, 1>(v);
+    case 2: return rot16<DIR, 2>(v);
+    case 3: return rot16<DIR, 3>(v);
+    case 4: return rot16<DIR, 4>(v);
+    case 5: return rot16<DIR, 5>(v);
+    case 6: return rot16<DIR, 6>(v);
+    case 7: return rot16<DIR, 7>(v);
+    default: return v;
+  }
+}
+
+// z stage of one ky in one lane (PZ = 2 .. 16): both halves of zstage_pair<PZ>
+// (the even kz = 2q from the PZ/2-point transform of x, the odd kz = 2q + 1
+// from that of x[n] W_PZ^n), the 3x3 multiply per kz, and the output as the
+// sum of the two PZ/2-point inverses: the same operations on the same values,
+// without the lane exchange, the per-lane branch of the odd half's twiddles or
+// the selects of the reduce-scatter.  kz and PZ - kz share their kernel entries
+// up to the sign of the xz and yz components (odd in z), so each lane loads the
+// PZ/2 + 1 kz' once.  The even half's inverse is parked in the lane's own input
+// entries while the odd half runs, so that one set of 3 PZ/2 values is live.
+template <int PZ, bool Q5>
+__device__ __forceinline__ void zstage_full(float2* D, int cs, const MagnetDev& M, int kx, int ky, int nz, int Py) {
+  constexpr int H = PZ / 2, R = 16 / PZ;  // kz per half; W_PZ = W16^R
+  const int pky = Q5 ? qidx(ky) : pidx(ky);
+  const int hy = Py / 2 + 1;
+  const int kyp = min(ky, Py - ky);
+  const float sy = (ky > Py / 2) ? -1.f : 1.f;
+  const int kc = M.kcomp;
+  const float* __restrict__ Kx = M.kspec + (size_t)kx * (H + 1) * kc * hy;
+  const size_t kleft = (size_t)(M.Fh - kx) * (H + 1) * kc * hy;
+  float kk[H + 1][6];  // kz' = 0 .. H: the even ones now, the odd ones before the odd kz
+#pragma unroll
+  for (int p = 0; p <= H; p += 2)
+    kernel_at<PZ>(Kx, kc, hy, kyp, sy, p, kk[p][0], kk[p][1], kk[p][2], kk[p][3], kk[p][4], kk[p][5], kleft);
+  float2 e[3][H];
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+#pragma unroll
+    for (int n = 0; n < H; ++n) e[c][n] = (n < nz) ? D[(c * nz + n) * cs + pky] : make_float2(0.f, 0.f);
+    dft_reg<H, -1>(e[c]);
+  }
+#pragma unroll
+  for (int q = 0; q < H; ++q) {  // kz = 2q, kz' = min(kz, PZ - kz), mirrored above PZ/2
+    const int p = 2 * q <= H ? 2 * q : PZ - 2 * q;
+    const float sg = 2 * q > H ? -1.f : 1.f;
+    apply3(&e[0][q], &e[1][q], &e[2][q], kk[p][0], kk[p][1], kk[p][2], kk[p][3], sg * kk[p][4], sg * kk[p][5]);
+  }
+#pragma unroll
+  for (int p = 1; p <= H; p += 2)
+    kernel_at<PZ>(Kx, kc, hy, kyp, sy, p, kk[p][0], kk[p][1], kk[p][2], kk[p][3], kk[p][4], kk[p][5], kleft);
+#pragma unroll
+  for (int c = 0; c < 3; ++c) dft_reg<H, 1>(e[c]);
+  float2 o[3][H];
+#pragma unroll
+  for (int c = 0; c < 3; ++c)
+#pragma unroll
+    for (int n = 0; n < H; ++n) o[c][n] = (n < nz) ? D[(c * nz + n) * cs + pky] : make_float2(0.f, 0.f);
+#pragma unroll
+  for (int c = 0; c < 3; ++c)
+#pragma unroll
+    for (int n = 0; n < H; ++n)
+      if (n < nz) D[(c * nz + n) * cs + pky] = e[c][n];
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+#pragma unroll
+    for (int n = 1; n < H; ++n) o[c][n] = rot16_m<-1>(o[c][n], R * n);
+    dft_reg<H, -1>(o[c]);
+  }
+#pragma unroll
+  for (int q = 0; q < H; ++q) {  // kz = 2q + 1
+    const int p = 2 * q + 1 <= H ? 2 * q + 1 : PZ - 2 * q - 1;
+    const float sg = 2 * q + 1 > H ? -1.f : 1.f;
+    apply3(&o[0][q], &o[1][q], &o[2][q], kk[p][0], kk[p][1], kk[p][2], kk[p][3], sg * kk[p][4], sg * kk[p][5]);
+  }
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    dft_reg<H, 1>(o[c]);
+#pragma unroll
+    for (int n = 1; n < H; ++n) o[c][n] = rot16_m<1>(o[c][n], R * n);
+#pragma unroll
+    for (int n = 0; n < H; ++n)
+      if (n < nz) {
+        const float2 ev = D[(c * nz + n) * cs + pky];
+        D[(c * nz + n) * cs + pky] = make_float2(ev.x + o[c][n].x, ev.y + o[c][n].y);
+      }
+  }
+}
+
 template <bool Q5 = false>
 __device__ __forceinline__ void zstage_single(float2* D, int cs, const MagnetDev& M, int kx, int ky, int Py) {
   const int pky = Q5 ? qidx(ky) : pidx(ky);
@@ -712,6 +804,11 @@ __device__ __forceinline__ void yzw_body(const MagnetDev& M, int kx0, int nkx, f
       const int j = t >> LOGPY;
       zstage_single<true>(D + j * 3 * cs, cs, M, kx0 + j, t & (Py - 1), Py);
     }
+  } else if constexpr (PZ >= 4) {  // one lane per (kx, ky)
+    for (int t = threadIdx.x; t < nkx << LOGPY; t += blockDim.x) {
+      const int j = t >> LOGPY;
+      zstage_full<PZ, true>(D + j * 3 * nz * cs, cs, M, kx0 + j, t & (Py - 1), nz, Py);
+    }
   } else {
     // lanes l and l + 16 of a warp share one (kx, ky): the even and odd kz
     // halves (the item count is a multiple of 32 and so is the block)
@@ -810,6 +907,11 @@ __global__ void __launch_bounds__(YZP_THREADS, 1)
     for (int t = threadIdx.x; t < nkx << LOGPY; t += blockDim.x) {
       const int j = t >> LOGPY;
       zstage_single<true>(D + j * 3 * cs, cs, M, kx0 + j, t & (Py - 1), Py);
+    }
+  } else if constexpr (PZ >= 4) {  // one lane per (kx, ky)
+    for (int t = threadIdx.x; t < nkx << LOGPY; t += blockDim.x) {
+      const int j = t >> LOGPY;
+      zstage_full<PZ, true>(D + j * 3 * nz * cs, cs, M, kx0 + j, t & (Py - 1), nz, Py);
     }
   } else {
     // lanes l and l + 16 of a warp share one (kx, ky): the even and odd kz halves

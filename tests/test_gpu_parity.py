@@ -391,10 +391,10 @@ def test_thick_magnet_pbc_and_trajectory(mpx):
 
 
 @pytest.mark.parametrize("size", [(6, 40, 3), (5, 70, 1), (4, 200, 2), (3, 300, 6), (3, 400, 2), (200, 6, 2),
-                                  (300, 5, 1), (130, 70, 4)])
+                                  (300, 5, 1), (130, 70, 4), (4, 200, 7), (3, 500, 8), (5, 100, 5)])
 def test_demag_warp_transform_lengths(mpx, size):
-    """y lengths 128 .. 1024 (k_yzw, k_yzw32: four-step Q x 32 with 32/Q columns per warp) at z lengths 1 .. 16,
-    and x rows of 512 and 1024 points (warp rows)."""
+    """y lengths 128 .. 1024 (k_yzw, k_yzw32: four-step Q x 32 with 32/Q columns per warp) at z lengths 1 .. 16
+    (z length 16, nz 5 .. 8, in one lane per ky), and x rows of 512 and 1024 points (warp rows)."""
     compare(MagnetSpec(size=size, cellsize=(1e-9, 2e-9, 1.5e-9), msat=8e5), mpx, [abi.Q_DEMAG_FIELD])
 
 

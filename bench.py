@@ -81,15 +81,31 @@ PROFILE_SOURCES = {
 }
 
 
+_CODE_TOKENS = None
+
+
+def code_only(text):
+    """C++ / CUDA source text without its comments and blank lines (string
+    literals kept), so that a change of comments leaves the hash of the code."""
+    import re
+
+    global _CODE_TOKENS
+    if _CODE_TOKENS is None:
+        _CODE_TOKENS = re.compile(r'//[^\n]*|/\*.*?\*/|"(?:\\.|[^"\\\n])*"|\'(?:\\.|[^\'\\\n])*\'', re.S)
+    text = _CODE_TOKENS.sub(lambda m: m.group(0) if m.group(0)[0] in "\"'" else "", text)
+    return "\n".join(line.rstrip() for line in text.splitlines() if line.strip())
+
+
 def kernel_sources_sha(files):
-    """Hash of the given CUDA sources of the product library (csrc/)."""
+    """Hash of the code (comments left out) of the given CUDA sources of the
+    product library (csrc/)."""
     import hashlib
 
     d = os.path.join(ROOT, "mumax-plus_b200", "csrc")
     h = hashlib.sha256()
     for name in sorted(files):
-        with open(os.path.join(d, name), "rb") as f:
-            h.update(name.encode() + b"\0" + f.read())
+        with open(os.path.join(d, name), encoding="utf-8") as f:
+            h.update(name.encode() + b"\0" + code_only(f.read()).encode())
     return h.hexdigest()[:16]
 
 

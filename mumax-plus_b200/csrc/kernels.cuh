@@ -8,7 +8,8 @@
 //            real-to-complex FFT along x (two real rows per complex FFT) ->
 //            S[kx][c][z][y]
 //   k_yz     per kx: FFT along y of the 3*nz columns, then per ky an in-register
-//            FFT along z split over two lanes (even / odd kz), the 3x3 multiply
+//            FFT along z (in one lane in the warp-column kernels, split over
+//            two lanes, even / odd kz, in the block-wide one), the 3x3 multiply
 //            by the real Newell spectrum (its -mu0/P prefactor folded in) and
 //            the inverse z FFT, then the inverse FFT along y; writes back S
 //   k_xinv   per tile: complex-to-real FFT along x -> B_demag in shared memory ->

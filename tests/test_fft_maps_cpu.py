@@ -1,5 +1,7 @@
-"""numpy restatements of two transform plans of the CUDA kernels, no GPU.
+"""numpy restatements of three transform plans of the CUDA kernels, no GPU.
 
+- Warp columns for lengths 64 .. 1024 (32 x q four-step, one warp per column):
+  against np.fft, the forward with the upper half zero, the inverse's first half.
 - Warp pairs for length 2048 (fft.cuh `pair_inner` / `pair_outer`): a column is
   64 x 32; warp p of the pair forms the inner outputs s = 2s' + p of lane j as
   one 32-point DFT over r of x[j + 32r] W64^(rp) (the forward's inputs r >= 32
@@ -61,6 +63,38 @@ def test_warp_pair_2048_maps_match_numpy(ny):
     y = _pair_transform(Y, +1, True)
     ref = np.fft.ifft(Y) * 2048
     assert np.max(np.abs(y[:1024] - ref[:1024])) < 1e-12 * np.max(np.abs(ref))
+
+
+def _four_step(x, q, d):
+    """Warp columns (fft.cuh `four_step_inner` / `four_step_outer`) of length
+    L = 32 q: lane j takes x[j + 32 r] (r < q), a q-point DFT over r gives
+    Y_j[s], times W_L^(j s); after the transpose lane (s) does the 32-point DFT
+    over j and holds X[s + q t] in t."""
+    L = 32 * q
+    Y = np.zeros((32, q), complex)
+    for j in range(32):
+        u = np.array([x[j + 32 * r] for r in range(q)])
+        u = np.fft.fft(u) if d < 0 else np.fft.ifft(u) * q
+        Y[j] = u * _w(L, j * np.arange(q), d)
+    X = np.zeros(L, complex)
+    for s in range(q):
+        X[s + q * np.arange(32)] = _dft32(Y[:, s], d)
+    return X
+
+
+@pytest.mark.parametrize("q", [2, 4, 8, 16, 32])
+def test_warp_column_maps_match_numpy(q):
+    L = 32 * q
+    rng = np.random.default_rng(q)
+    x = np.zeros(L, complex)  # forward: the upper half is zero padding (r >= q/2 not read)
+    x[:L // 2] = rng.standard_normal(L // 2) + 1j * rng.standard_normal(L // 2)
+    X = _four_step(x, q, -1)
+    ref = np.fft.fft(x)
+    assert np.max(np.abs(X - ref)) < 1e-12 * np.max(np.abs(ref))
+    Y = rng.standard_normal(L) + 1j * rng.standard_normal(L)
+    y = _four_step(Y, q, +1)  # inverse: outputs t < 16 (y < L/2) kept
+    ref = np.fft.ifft(Y) * L
+    assert np.max(np.abs(y[:L // 2] - ref[:L // 2])) < 1e-12 * np.max(np.abs(ref))
 
 
 def _p2(k):

@@ -1,5 +1,6 @@
-"""numpy restatements of three transform plans of the CUDA kernels, no GPU.
+"""numpy restatements of transform plans of the CUDA kernels, no GPU.
 
+- Two real rows per complex x transform (the x passes' pack and unpack).
 - Warp columns for lengths 64 .. 1024 (32 x q four-step, one warp per column):
   against np.fft, the forward with the upper half zero, the inverse's first half.
 - Warp pairs for length 2048 (fft.cuh `pair_inner` / `pair_outer`): a column is
@@ -95,6 +96,39 @@ def test_warp_column_maps_match_numpy(q):
     y = _four_step(Y, q, +1)  # inverse: outputs t < 16 (y < L/2) kept
     ref = np.fft.ifft(Y) * L
     assert np.max(np.abs(y[:L // 2] - ref[:L // 2])) < 1e-12 * np.max(np.abs(ref))
+
+
+@pytest.mark.parametrize("L,n", [(16, 9), (512, 300), (1024, 512)])
+def test_two_real_rows_per_complex_transform(L, n):
+    """The x passes (k_xfwd / k_xinv) transform two real rows a, b (zero-padded
+    from n to L) as one complex row z = a + i b.  Forward unpack: A[k] = (Z[k] +
+    conj Z[L-k]) / 2, B[k] = -i/2 (Z[k] - conj Z[L-k]) for k <= L/2.  Inverse
+    gather: Z[k] = A[k] + i B[k] and Z[L-k] = conj A[k] + i conj B[k], with the
+    imaginary parts of A, B dropped at k = 0 and L/2."""
+    rng = np.random.default_rng(L + n)
+    a = np.zeros(L)
+    b = np.zeros(L)
+    a[:n] = rng.standard_normal(n)
+    b[:n] = rng.standard_normal(n)
+    Z = np.fft.fft(a + 1j * b)
+    k = np.arange(L // 2 + 1)
+    zc = np.conj(Z[(L - k) % L])
+    A = 0.5 * (Z[k] + zc)
+    B = -0.5j * (Z[k] - zc)
+    assert np.max(np.abs(A - np.fft.rfft(a))) < 1e-12 * L and np.max(np.abs(B - np.fft.rfft(b))) < 1e-12 * L
+    # inverse from the half spectra (here those of two other real rows)
+    c = rng.standard_normal(L)
+    e = rng.standard_normal(L)
+    Ac, Ae = np.fft.rfft(c), np.fft.rfft(e)
+    Ac[[0, L // 2]] = Ac[[0, L // 2]].real
+    Ae[[0, L // 2]] = Ae[[0, L // 2]].real
+    Zi = np.zeros(L, complex)
+    for kx in range(L // 2 + 1):
+        Zi[kx] = Ac[kx] + 1j * Ae[kx]
+        if 0 < kx < L - kx:
+            Zi[L - kx] = np.conj(Ac[kx]) + 1j * np.conj(Ae[kx])
+    z = np.fft.ifft(Zi) * L
+    assert np.max(np.abs(z.real - L * c)) < 1e-9 * L and np.max(np.abs(z.imag - L * e)) < 1e-9 * L
 
 
 def _p2(k):
